@@ -1,0 +1,533 @@
+"""SpMV throughput benchmark of libsparse_b200 on B200.
+
+Workload (default, `format_sweep_fp64`): the FP64 format sweep -- a banded
+matrix with 4,000,000 rows and 11 diagonals at offsets -5..5 (values N(0,1),
+43,999,970 nonzeros) in COO, CSR, DIA and ELL, and a power-law matrix with
+2,000,000 rows (row lengths min(2000, Zipf(2)+15), ~41M nonzeros, uniform
+distinct columns, values U[-1,1]) in COO and CSR (its DIA/ELL forms are
+refused by the admission test).  One step = one y <- y + A x per (matrix,
+format) pair.  The metric is algorithmic HBM GB/s (bytes that must move per
+call, x counted once) at <= 1e-5 relative error against an FP64 check.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload format_sweep_fp64|laplacian_fp32] [--small]
+
+With N > 1 (torchrun, one rank per GPU) every rank processes its own copy
+of the workload (independent objects, no collective on the data path):
+weak scaling, value = bytes of all ranks / max-over-ranks time.
+`--impl reference` times the CPU restatement of the reference's parallel
+worker kernels (static_nnz CSR split, private-y COO, row-split DIA/ELL) on all
+host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SpMV HBM GB/s at <=1e-5 rel err"
+UNIT = "GB/s"
+
+
+# ------------------------------------------------------------------ workload
+
+def algo_bytes(fmt: str, N: int, nnz: int, s_v: int, width: int = 0) -> int:
+    """Compulsory bytes of one y <- y + A x call (x read once, y read+written)."""
+    vec = N * s_v + 2 * N * s_v
+    if fmt == "csr":
+        return nnz * (s_v + 4) + 4 * (N + 1) + vec
+    if fmt == "coo":
+        return nnz * (8 + s_v) + vec
+    if fmt == "dia":
+        return width * N * s_v + 4 * width + vec
+    if fmt == "ell":
+        return width * N * (s_v + 4) + vec
+    raise ValueError(fmt)
+
+
+def make_workload(name: str, small: bool):
+    """Host arrays of every (label, format, arrays...) job."""
+    from sciwasm.sparse_b200 import synth
+    jobs = []
+    if name == "format_sweep_fp64":
+        nb = 1_000_000 if small else 4_000_000
+        npl = 500_000 if small else 2_000_000
+        rp, col, val = synth.banded(nb, half=5, seed=1, dtype=np.float64)
+        jobs.append(dict(label="banded", N=nb, rp=rp, col=col, val=val,
+                         formats=["coo", "csr", "dia", "ell"]))
+        rp, col, val = synth.power_law(npl, seed=2, dtype=np.float64)
+        jobs.append(dict(label="powerlaw", N=npl, rp=rp, col=col, val=val,
+                         formats=["coo", "csr"]))
+    elif name == "laplacian_fp32":
+        n = 1024 if small else 256
+        rp, col, val = synth.laplacian_2d(n, dtype=np.float32)
+        jobs.append(dict(label=f"laplacian{n}", N=n * n, rp=rp, col=col, val=val,
+                         formats=["coo", "csr", "dia", "ell"]))
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    for j in jobs:
+        j["x"] = synth.uniform_vec(j["N"], 0, dtype=j["val"].dtype)
+    return jobs
+
+
+def truth_f64(rp, col, val, x):
+    prod = val.astype(np.float64) * x.astype(np.float64)[col]
+    out = np.zeros(rp.size - 1)
+    nz = np.diff(rp) > 0
+    out[nz] = np.add.reduceat(prod, rp[:-1][nz])
+    return out
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during timing."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ------------------------------------------------------------------ CPU arm
+
+def cpu_pass(jobs, nthreads, fmt_data):
+    """One pass of every (matrix, format) SpMV on the CPU restatement."""
+    from oracle import binding as orc
+    for j in jobs:
+        for fmt in j["formats"]:
+            d = fmt_data[(j["label"], fmt)]
+            y = d["y"]
+            y[:] = 0
+            if fmt == "csr":
+                orc.par_spmv_csr(nthreads, j["rp"], j["col"], j["val"], j["x"], y)
+            elif fmt == "coo":
+                orc.par_spmv_coo(d["nt_coo"], d["row"], j["col"], j["val"], j["x"], y, j["N"],
+                                 d["wy"])
+            elif fmt == "dia":
+                orc.par_spmv_dia(nthreads, d["off"], d["data"], j["N"], j["x"], y)
+            elif fmt == "ell":
+                orc.par_spmv_ell(nthreads, d["ind"], d["data"], j["N"], d["nc"], j["x"], y)
+
+
+def prepare_cpu(jobs):
+    from sciwasm.sparse_b200 import synth
+    nthreads = os.cpu_count() or 1
+    fmt_data = {}
+    for j in jobs:
+        for fmt in j["formats"]:
+            d = {"y": np.zeros(j["N"], j["val"].dtype)}
+            if fmt == "coo":
+                d["row"] = synth.csr_to_coo_rows(j["rp"])
+                budget = 2 << 30
+                d["nt_coo"] = max(1, min(nthreads, budget // max(1, j["N"] * j["val"].itemsize)))
+                d["wy"] = np.zeros(d["nt_coo"] * j["N"], j["val"].dtype)
+            elif fmt == "dia":
+                d["off"], d["data"] = synth.csr_to_dia_host(j["rp"], j["col"], j["val"])
+            elif fmt == "ell":
+                d["ind"], d["data"], d["nc"] = synth.csr_to_ell_host(j["rp"], j["col"], j["val"])
+            fmt_data[(j["label"], fmt)] = d
+    return nthreads, fmt_data
+
+
+def step_bytes(jobs, fmt_data=None):
+    tot = 0
+    for j in jobs:
+        s_v = j["val"].itemsize
+        nnz = j["col"].size
+        for fmt in j["formats"]:
+            w = 0
+            if fmt == "dia":
+                w = int(np.unique(j["col"].astype(np.int64) -
+                                  np.repeat(np.arange(j["N"]), np.diff(j["rp"]))).size) \
+                    if fmt_data is None else fmt_data[(j["label"], fmt)]["off"].size
+            if fmt == "ell":
+                w = int(np.diff(j["rp"]).max())
+            tot += algo_bytes(fmt, j["N"], nnz, s_v, w)
+    return tot
+
+
+def run_reference(args, jobs, config):
+    nthreads, fmt_data = prepare_cpu(jobs)
+    bytes_step = step_bytes(jobs, fmt_data)
+    for _ in range(args.warmup):
+        cpu_pass(jobs, nthreads, fmt_data)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_pass(jobs, nthreads, fmt_data)
+    dt = time.perf_counter() - t0
+    value = bytes_step * args.steps / dt / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": config["dtype"], "data": "synthetic",
+        "config": config,
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": nthreads,
+                         "kind": "port",
+                         "sample": f"full workload, {args.steps} passes of every "
+                                   "(matrix, format) SpMV, pthreads over all host cores "
+                                   "(reference algorithm restated in C, not V8/wasm)"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(jobs, budget_s=12.0):
+    nthreads, fmt_data = prepare_cpu(jobs)
+    bytes_step = step_bytes(jobs, fmt_data)
+    cpu_pass(jobs, nthreads, fmt_data)  # warm
+    t0 = time.perf_counter()
+    cpu_pass(jobs, nthreads, fmt_data)
+    one = time.perf_counter() - t0
+    reps = max(1, min(50, int(budget_s / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        cpu_pass(jobs, nthreads, fmt_data)
+    dt = time.perf_counter() - t0
+    return {"value": round(bytes_step * reps / dt / 1e9, 3), "unit": UNIT, "cores": nthreads,
+            "kind": "port",
+            "sample": f"{reps} full passes of the workload's SpMVs on {nthreads} threads "
+                      "(C restatement of the reference's worker kernels, pthreads)"}
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def run_ours(args, jobs, config, rank, world, local_rank):
+    import torch
+    import sciwasm.sparse_b200 as sb
+    from sciwasm.sparse_b200 import _lib, synth
+
+    sb.load_library()
+    torch.cuda.set_device(local_rank)
+    _lib.call("sb_set_device", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        dist = dist_
+
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+
+    # upload every (matrix, format) object
+    objs = []
+    for j in jobs:
+        N, rp, col, val = j["N"], j["rp"], j["col"], j["val"]
+        s_v = val.itemsize
+        x = sb.vec_from_host(j["x"])
+        for fmt in j["formats"]:
+            if fmt == "csr":
+                A = sb.csr_from_host(rp, col, val)
+                w = 0
+            elif fmt == "coo":
+                A = sb.coo_from_host(synth.csr_to_coo_rows(rp), col, val, N)
+                w = 0
+            elif fmt == "dia":
+                off, dat = synth.csr_to_dia_host(rp, col, val)
+                A = sb.dia_from_host(off, dat, N, nnz=col.size)
+                w = off.size
+            else:
+                ind, dat, nc = synth.csr_to_ell_host(rp, col, val)
+                A = sb.ell_from_host(ind, dat, nc, N, nnz=col.size)
+                w = nc
+            y = sb.create_vec(N, 0, val.dtype)
+            objs.append(dict(label=f"{j['label']}/{fmt}", fmt=fmt, A=A, x=x, y=y, job=j,
+                             bytes=algo_bytes(fmt, N, col.size, s_v, w)))
+    bytes_step = sum(o["bytes"] for o in objs)
+
+    # correctness gate: one call from y = 0 against an FP64 check
+    max_err = 0.0
+    truths = {}
+    for o in objs:
+        j = o["job"]
+        if j["label"] not in truths:
+            truths[j["label"]] = truth_f64(j["rp"], j["col"], j["val"], j["x"])
+        o["y"].vec_index.fill_zero(sptr)
+        sb.spmv(o["A"], o["x"], o["y"], stream=sptr)
+        stream.synchronize()
+        t = truths[j["label"]]
+        err = float(np.max(np.abs(o["y"].array() - t)) / max(np.max(np.abs(t)), 1e-300))
+        o["rel_err"] = err
+        max_err = max(max_err, err)
+    if max_err > 1e-5:
+        raise SystemExit(f"correctness gate failed: max rel err {max_err:.3e}")
+
+    def step(ev=None):
+        for k, o in enumerate(objs):
+            if ev is not None:
+                ev[k][0].record(stream)
+            sb.spmv(o["A"], o["x"], o["y"], stream=sptr)
+            if ev is not None:
+                ev[k][1].record(stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    # pad the sampled window so the clock record has samples under load
+    pad_until = time.perf_counter() + 0.5
+    with torch.cuda.stream(stream):
+        while time.perf_counter() < pad_until:
+            step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in objs] for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        t_start.record(stream)
+        for s in range(args.steps):
+            step(evs[s])
+        t_end.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    pad_until = time.perf_counter() + 0.3
+    with torch.cuda.stream(stream):
+        while time.perf_counter() < pad_until:
+            step()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    elapsed_ms = t_start.elapsed_time(t_end)
+    per_obj_ms = [float(np.mean([evs[s][k][0].elapsed_time(evs[s][k][1])
+                                 for s in range(args.steps)])) for k in range(len(objs))]
+    if dist:
+        t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = bytes_step * args.steps * world / (elapsed_ms / 1e3) / 1e9
+
+    # ---------------- e2e through the public API with host buffers
+    h2d = 0
+    d2h = 0
+    host = []
+    for o in objs:
+        N = o["job"]["N"]
+        dt = o["job"]["val"].dtype
+        nb = N * dt.itemsize
+        xp, yp, yo = _pinned(nb), _pinned(nb), _pinned(nb)
+        _host_view(xp, N, dt)[:] = o["job"]["x"]
+        _host_view(yp, N, dt)[:] = 0
+        host.append((xp, yp, yo, nb))
+        h2d += 2 * nb
+        d2h += nb
+
+    def e2e_step():
+        for o, (xp, yp, yo, nb) in zip(objs, host):
+            _lib.call("sb_memcpy_htod", o["x"].vec_index.ptr, xp, nb, sptr)
+            _lib.call("sb_memcpy_htod", o["y"].vec_index.ptr, yp, nb, sptr)
+            sb.spmv(o["A"], o["x"], o["y"], stream=sptr)
+            _lib.call("sb_memcpy_dtoh", yo, o["y"].vec_index.ptr, nb, sptr)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = bytes_step * args.steps * world / (e2e_ms / 1e3) / 1e9
+    for xp, yp, yo, _ in host:
+        for p in (xp, yp, yo):
+            _lib.call("sb_host_free", p)
+
+    # ---------------- roofline of the dominant kernel
+    peak, peak_kind = measured_peak()
+    tot = [per_obj_ms[k] for k in range(len(objs))]
+    dom = int(np.argmax(tot))
+    achieved = objs[dom]["bytes"] / (per_obj_ms[dom] / 1e3) / 1e9
+    traffic = profiled_traffic().get(objs[dom]["label"] + ("/small" if args.small else ""))
+    detail = {o["label"]: {"ms": round(per_obj_ms[k], 4),
+                           "GB_s": round(o["bytes"] / (per_obj_ms[k] / 1e3) / 1e9, 1),
+                           "frac": round(o["bytes"] / (per_obj_ms[k] / 1e3) / 1e9 / peak, 3),
+                           "rel_err": o["rel_err"]}
+              for k, o in enumerate(objs)}
+    config["per_call"] = detail
+    config["max_rel_err"] = max_err
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(elapsed_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": config["dtype"], "data": "synthetic",
+        "config": config,
+        "roofline": {"bound": "hbm", "kernel": objs[dom]["label"],
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "traffic": traffic,
+                     "algorithmic_bytes": objs[dom]["bytes"]},
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "path": "sciwasm.sparse_b200.spmv via the C ABI; per call x and y uploaded "
+                        "from pinned host memory and y read back; matrices resident"},
+        "gpu_launches": len(objs) * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(jobs)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _pinned(nbytes):
+    import ctypes
+    from sciwasm.sparse_b200 import _lib
+    p = ctypes.c_void_p()
+    _lib.call("sb_host_alloc", ctypes.byref(p), nbytes)
+    return p.value
+
+
+def _host_view(ptr, n, dtype):
+    import ctypes
+    raw = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_uint8)),
+                                shape=(n * np.dtype(dtype).itemsize,))
+    return raw.view(dtype)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="format_sweep_fp64")
+    ap.add_argument("--small", action="store_true",
+                    help="quarter-size matrices (profiling captures)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    config = {"workload": args.workload + ("_small" if args.small else ""),
+              "dtype": "f64" if "fp64" in args.workload else "f32",
+              "l2": "inputs larger than L2 (126 MB); no flush between steps",
+              "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+    if args.workload == "laplacian_fp32":
+        config["l2"] = "3.7 MB working set stays L2-resident (reported, not a roofline claim)"
+    dtype = config["dtype"]
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        jobs = make_workload(args.workload, args.small)
+        run_reference(args, jobs, {**config, "dtype": dtype})
+        return
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        jobs = make_workload(args.workload, args.small)
+        run_ours(args, jobs, config, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

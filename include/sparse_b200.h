@@ -1,0 +1,107 @@
+/*
+ * sparse_b200.h -- C ABI of libsparse_b200.so, the B200 (sm_100a) sparse
+ * hot path of SciWasm.Sparse.
+ *
+ * The reference's JavaScript module (src/sequential/src/sparse32.js and its
+ * f64 twin sparse64.js) keeps every matrix as typed arrays in one wasm linear
+ * memory and calls wasm exports with i32 byte offsets plus sizes, e.g.
+ * `spmv_csr(rowptr, col, val, x, y, N)`
+ * (src/sequential/src/sparse_opt_32.wat:227).  This ABI keeps that shape:
+ * every array argument is a DEVICE pointer (allocate it with sb_malloc or any
+ * CUDA allocator of the same process), every size is an integer, and each
+ * call is ordered on the CUDA stream passed as `stream` (NULL = the legacy
+ * default stream).  The f32 and f64 wasm modules become one entry point with
+ * a dtype argument.  No torch type appears anywhere in this ABI.
+ *
+ * Status codes: every function returns SB_OK (0) or a negative SB_E* code;
+ * sb_last_error() returns a message for the calling host thread.  Calls never
+ * fall back to the CPU: without a usable CUDA device they return SB_ENODEV.
+ *
+ * Each declaration cites the reference interface it replaces (file:line,
+ * relative to the SciWasm.Sparse project root).
+ */
+#ifndef SPARSE_B200_H
+#define SPARSE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SB_OK 0
+#define SB_EINVAL (-1)    /* bad argument (null pointer, negative size, bad dtype) */
+#define SB_ENOMEM (-2)    /* device allocation failed */
+#define SB_EREFUSED (-3)  /* conversion refused by the reference's admission test */
+#define SB_ETIMEOUT (-4)  /* a bounded device wait ran out (dependency never ready) */
+#define SB_ECUDA (-5)     /* CUDA runtime error (message in sb_last_error) */
+#define SB_ENODEV (-6)    /* no CUDA device usable by this library */
+#define SB_EALIGN (-7)    /* pointer misaligned for the requested path */
+
+/* Value types.  SB_F32 / SB_F64 are the reference's *32 / *64 modules;
+ * SB_BF16 is a storage-only type for SpMV values (FP32 accumulation). */
+#define SB_F32 0
+#define SB_F64 1
+#define SB_BF16 2
+
+/* ---------------------------------------------------------------------- */
+/* Runtime: the stand-in for MatMachJS's _malloc/_free on wasm memory     */
+/* (src/sequential/libs/matmachjs.wat:46-48) and for typed-array views.    */
+/* ---------------------------------------------------------------------- */
+int sb_version(void);
+const char* sb_last_error(void);
+const char* sb_status_string(int status);
+int sb_device_count(int* count);
+int sb_set_device(int device);
+int sb_malloc(void** ptr, size_t bytes);
+int sb_free(void* ptr);
+int sb_host_alloc(void** ptr, size_t bytes); /* pinned host memory */
+int sb_host_free(void* ptr);
+int sb_memcpy_htod(void* dst, const void* src, size_t bytes, void* stream);
+int sb_memcpy_dtoh(void* dst, const void* src, size_t bytes, void* stream);
+int sb_memcpy_dtod(void* dst, const void* src, size_t bytes, void* stream);
+int sb_memset(void* dst, int value, size_t bytes, void* stream);
+int sb_stream_create(void** stream);
+int sb_stream_destroy(void* stream);
+int sb_stream_synchronize(void* stream);
+int sb_mem_info(size_t* free_bytes, size_t* total_bytes);
+
+/* ---------------------------------------------------------------------- */
+/* SpMV: y <- y + A x, repeated inner_max times (the *_wrapper exports).   */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces spmv_coo / spmv_coo_wrapper
+ * (src/sequential/src/sparse_opt_32.wat:175-225; dispatch
+ * src/sequential/src/sparse32.js:1256-1262).  Any entry order is accepted. */
+int sb_spmv_coo(int dtype, const int32_t* row, const int32_t* col, const void* val,
+                const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
+                void* stream);
+
+/* Replaces spmv_csr / spmv_csr_wrapper
+ * (src/sequential/src/sparse_opt_32.wat:227-288; dispatch
+ * src/sequential/src/sparse32.js:1264-1270).  nnz = row_ptr[N] is passed
+ * explicitly so that no device read is needed to plan the launch.  Rows
+ * without entries leave y untouched, as in the reference. */
+int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
+                void* stream);
+
+/* Replaces spmv_dia / spmv_dia_wrapper
+ * (src/sequential/src/sparse_opt_32.wat:290-425; dispatch
+ * src/sequential/src/sparse32.js:1272-1278).  offset[nd] diagonal offsets
+ * (device), data[nd*stride] diagonal-major. */
+int sb_spmv_dia(int dtype, const int32_t* offset, const void* data, int32_t N, int32_t nd,
+                int32_t stride, const void* x, void* y, int32_t inner_max, void* stream);
+
+/* Replaces spmv_ell / spmv_ell_wrapper
+ * (src/sequential/src/sparse_opt_32.wat:427-498; dispatch
+ * src/sequential/src/sparse32.js:1280-1286).  Column-major indices/data of
+ * nc*N slots; padding slots (data 0, index 0) are applied like the reference. */
+int sb_spmv_ell(int dtype, const int32_t* indices, const void* data, int32_t N, int32_t nc,
+                const void* x, void* y, int32_t inner_max, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPARSE_B200_H */

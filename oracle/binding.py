@@ -1,0 +1,307 @@
+"""ctypes binding of the CPU oracle (liboracle_sparse.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, as the checker and the timed CPU baseline.  The
+product package never imports this module.  Parity status of the oracle:
+unpinned by reference artefacts (see sparse_oracle.h).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_sparse.so")
+
+_P = C.c_void_p
+_I32 = C.c_int32
+_I64 = C.c_int64
+
+_SIG = {
+    "or_spmv_coo_f32": ([_P, _P, _P, _P, _P, _I64], None),
+    "or_spmv_coo_f64": ([_P, _P, _P, _P, _P, _I64], None),
+    "or_spmv_csr_f32": ([_P, _P, _P, _P, _P, _I32], None),
+    "or_spmv_csr_f64": ([_P, _P, _P, _P, _P, _I32], None),
+    "or_spmv_dia_f32": ([_P, _P, _I32, _I32, _I32, _P, _P], None),
+    "or_spmv_dia_f64": ([_P, _P, _I32, _I32, _I32, _P, _P], None),
+    "or_spmv_ell_f32": ([_P, _P, _I32, _I32, _P, _P], None),
+    "or_spmv_ell_f64": ([_P, _P, _I32, _I32, _P, _P], None),
+    "or_truth_csr_f32": ([_P, _P, _P, _P, _P, _P, _I32], None),
+    "or_truth_csr_f64": ([_P, _P, _P, _P, _P, _P, _I32], None),
+    "or_static_nnz": ([_P, _I32, _I32, _P, _P], None),
+    "or_par_spmv_csr_f32": ([C.c_int, _P, _P, _P, _P, _P, _I32], None),
+    "or_par_spmv_csr_f64": ([C.c_int, _P, _P, _P, _P, _P, _I32], None),
+    "or_par_spmv_coo_f32": ([C.c_int, _P, _P, _P, _P, _P, _I32, _I64, _P], None),
+    "or_par_spmv_coo_f64": ([C.c_int, _P, _P, _P, _P, _P, _I32, _I64, _P], None),
+    "or_par_spmv_dia_f32": ([C.c_int, _P, _P, _I32, _I32, _I32, _P, _P], None),
+    "or_par_spmv_dia_f64": ([C.c_int, _P, _P, _I32, _I32, _I32, _P, _P], None),
+    "or_par_spmv_ell_f32": ([C.c_int, _P, _P, _I32, _I32, _P, _P], None),
+    "or_par_spmv_ell_f64": ([C.c_int, _P, _P, _I32, _I32, _P, _P], None),
+    "or_coo_csr": ([C.c_int, _P, _P, _P, _I32, _I64, _P, _P, _P], None),
+    "or_coo_csc": ([C.c_int, _P, _P, _P, _I32, _I64, _P, _P, _P], None),
+    "or_num_cols": ([_P, _I32], _I32),
+    "or_format_admitted": ([_I64, _I64, _I64], C.c_int),
+    "or_csr_ell": ([C.c_int, _P, _P, _P, _I32, _I32, _P, _P], None),
+    "or_num_diags": ([_P, _P, _I32, _P], _I32),
+    "or_csr_dia": ([C.c_int, _P, _P, _P, _I32, _I32, _I32, _P, _P], None),
+    "or_quick_sort_coo": ([C.c_int, _P, _P, _P, _I64, _I64], None),
+    "or_level_sets": ([C.c_int, _P, _P, _P, _I32, _P, _P, _P, _P, _P, _P, _P], _I32),
+    "or_spts_csr_f32": ([_P, _P, _P, _P, _P, _I32], None),
+    "or_spts_csr_f64": ([_P, _P, _P, _P, _P, _I32], None),
+    "or_spts_syncfree_f32": ([_P, _P, _P, _P, _P, _I32], None),
+    "or_spts_syncfree_f64": ([_P, _P, _P, _P, _P, _I32], None),
+    "or_truth_spts": ([C.c_int, _P, _P, _P, _P, _P, _I32], None),
+    "or_par_spts_level_f32": ([C.c_int, _P, _I32, _P, _P, _P, _P, _P, _I32], None),
+    "or_par_spts_level_f64": ([C.c_int, _P, _I32, _P, _P, _P, _P, _P, _I32], None),
+    "or_fletcher_f32": ([_P, _I64], _I64),
+    "or_fletcher_f64": ([_P, _I64], _I64),
+}
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIG.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data if a is not None else None
+
+
+def _sfx(dtype) -> str:
+    dt = np.dtype(dtype)
+    if dt == np.float32:
+        return "f32"
+    if dt == np.float64:
+        return "f64"
+    raise TypeError(dt)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+# ------------------------------------------------------------------ SpMV
+
+def spmv_csr(row_ptr, col, val, x, y):
+    """y + A x in the reference's serial order; returns a new array."""
+    y = np.array(y, dtype=val.dtype, copy=True)
+    row_ptr, col = _i32(row_ptr), _i32(col)
+    getattr(lib(), "or_spmv_csr_" + _sfx(val.dtype))(
+        _p(row_ptr), _p(col), _p(val), _p(np.ascontiguousarray(x, val.dtype)), _p(y),
+        row_ptr.size - 1)
+    return y
+
+
+def spmv_coo(row, col, val, x, y):
+    y = np.array(y, dtype=val.dtype, copy=True)
+    row, col = _i32(row), _i32(col)
+    getattr(lib(), "or_spmv_coo_" + _sfx(val.dtype))(
+        _p(row), _p(col), _p(val), _p(np.ascontiguousarray(x, val.dtype)), _p(y), row.size)
+    return y
+
+
+def spmv_dia(offset, data, N, x, y, stride=None):
+    y = np.array(y, dtype=data.dtype, copy=True)
+    offset = _i32(offset)
+    stride = N if stride is None else stride
+    getattr(lib(), "or_spmv_dia_" + _sfx(data.dtype))(
+        _p(offset), _p(data), N, offset.size, stride, _p(np.ascontiguousarray(x, data.dtype)),
+        _p(y))
+    return y
+
+
+def spmv_ell(indices, data, N, nc, x, y):
+    y = np.array(y, dtype=data.dtype, copy=True)
+    indices = _i32(indices)
+    getattr(lib(), "or_spmv_ell_" + _sfx(data.dtype))(
+        _p(indices), _p(data), N, nc, _p(np.ascontiguousarray(x, data.dtype)), _p(y))
+    return y
+
+
+def truth_csr(row_ptr, col, val, x, y0=None):
+    """Extended-precision y0 + A x (float64 result)."""
+    row_ptr, col = _i32(row_ptr), _i32(col)
+    out = np.empty(row_ptr.size - 1, dtype=np.float64)
+    x = np.ascontiguousarray(x, val.dtype)
+    y0c = None if y0 is None else np.ascontiguousarray(y0, val.dtype)
+    getattr(lib(), "or_truth_csr_" + _sfx(val.dtype))(
+        _p(row_ptr), _p(col), _p(val), _p(x), _p(y0c), _p(out), row_ptr.size - 1)
+    return out
+
+
+def static_nnz(row_ptr, nw):
+    row_ptr = _i32(row_ptr)
+    rs = np.zeros(nw, np.int32)
+    re = np.zeros(nw, np.int32)
+    lib().or_static_nnz(_p(row_ptr), row_ptr.size - 1, nw, _p(rs), _p(re))
+    return rs, re
+
+
+def par_spmv_csr(nthreads, row_ptr, col, val, x, y):
+    """Parallel CPU baseline; updates y in place."""
+    getattr(lib(), "or_par_spmv_csr_" + _sfx(val.dtype))(
+        nthreads, _p(row_ptr), _p(col), _p(val), _p(x), _p(y), row_ptr.size - 1)
+
+
+def par_spmv_coo(nthreads, row, col, val, x, y, N, wy):
+    getattr(lib(), "or_par_spmv_coo_" + _sfx(val.dtype))(
+        nthreads, _p(row), _p(col), _p(val), _p(x), _p(y), N, row.size, _p(wy))
+
+
+def par_spmv_dia(nthreads, offset, data, N, x, y):
+    getattr(lib(), "or_par_spmv_dia_" + _sfx(data.dtype))(
+        nthreads, _p(offset), _p(data), N, offset.size, N, _p(x), _p(y))
+
+
+def par_spmv_ell(nthreads, indices, data, N, nc, x, y):
+    getattr(lib(), "or_par_spmv_ell_" + _sfx(data.dtype))(
+        nthreads, _p(indices), _p(data), N, nc, _p(x), _p(y))
+
+
+# ------------------------------------------------------------------ conversions
+
+def coo_csr(row, col, val, N):
+    row, col = _i32(row), _i32(col)
+    val = np.ascontiguousarray(val)
+    nnz = row.size
+    rp = np.zeros(N + 1, np.int32)
+    c = np.zeros(nnz, np.int32)
+    v = np.zeros(nnz, val.dtype)
+    lib().or_coo_csr(val.dtype.itemsize, _p(row), _p(col), _p(val), N, nnz, _p(rp), _p(c), _p(v))
+    return rp, c, v
+
+
+def coo_csc(row, col, val, ncols):
+    row, col = _i32(row), _i32(col)
+    val = np.ascontiguousarray(val)
+    nnz = row.size
+    cp = np.zeros(ncols + 1, np.int32)
+    r = np.zeros(nnz, np.int32)
+    v = np.zeros(nnz, val.dtype)
+    lib().or_coo_csc(val.dtype.itemsize, _p(row), _p(col), _p(val), ncols, nnz, _p(cp), _p(r),
+                     _p(v))
+    return cp, r, v
+
+
+def num_cols(row_ptr):
+    row_ptr = _i32(row_ptr)
+    return int(lib().or_num_cols(_p(row_ptr), row_ptr.size - 1))
+
+
+def format_admitted(width, N, nnz) -> bool:
+    return bool(lib().or_format_admitted(int(width), int(N), int(nnz)))
+
+
+def csr_ell(row_ptr, col, val):
+    """Returns (indices, data, nc) or None when the admission test refuses."""
+    row_ptr, col = _i32(row_ptr), _i32(col)
+    N = row_ptr.size - 1
+    nc = num_cols(row_ptr)
+    if not format_admitted(nc, N, col.size):
+        return None
+    ind = np.zeros(nc * N, np.int32)
+    dat = np.zeros(nc * N, val.dtype)
+    lib().or_csr_ell(val.dtype.itemsize, _p(row_ptr), _p(col), _p(val), N, nc, _p(ind), _p(dat))
+    return ind, dat, nc
+
+
+def num_diags(row_ptr, col):
+    row_ptr, col = _i32(row_ptr), _i32(col)
+    stride = np.zeros(1, np.int32)
+    nd = lib().or_num_diags(_p(row_ptr), _p(col), row_ptr.size - 1, _p(stride))
+    return int(nd), int(stride[0])
+
+
+def csr_dia(row_ptr, col, val):
+    """Returns (offset, data, nd, stride) or None when refused."""
+    row_ptr, col = _i32(row_ptr), _i32(col)
+    N = row_ptr.size - 1
+    nd, stride = num_diags(row_ptr, col)
+    if not format_admitted(nd, stride, col.size):
+        return None
+    off = np.zeros(nd, np.int32)
+    dat = np.zeros(nd * stride, val.dtype)
+    lib().or_csr_dia(val.dtype.itemsize, _p(row_ptr), _p(col), _p(val), N, nd, stride, _p(off),
+                     _p(dat))
+    return off, dat, nd, stride
+
+
+def quick_sort_coo(row, col, val):
+    row, col = _i32(row).copy(), _i32(col).copy()
+    val = np.array(val, copy=True)
+    if row.size:
+        lib().or_quick_sort_coo(val.dtype.itemsize, _p(row), _p(col), _p(val), 0, row.size - 1)
+    return row, col, val
+
+
+# ------------------------------------------------------------------ SpTS
+
+def level_sets(row_ptr, col, val):
+    """Returns dict(level, level_ptr, permutation, order, row_ptr, col, val, nlevels)."""
+    row_ptr, col = _i32(row_ptr), _i32(col)
+    val = np.ascontiguousarray(val)
+    N = row_ptr.size - 1
+    level = np.zeros(N, np.int32)
+    level_ptr = np.zeros(N + 2, np.int32)
+    perm = np.zeros(N, np.int32)
+    order = np.zeros(N, np.int32)
+    nr = np.zeros(N + 1, np.int32)
+    nc = np.zeros(col.size, np.int32)
+    nv = np.zeros(col.size, val.dtype)
+    nl = lib().or_level_sets(val.dtype.itemsize, _p(row_ptr), _p(col), _p(val), N, _p(level),
+                             _p(level_ptr), _p(perm), _p(order), _p(nr), _p(nc), _p(nv))
+    return dict(level=level, level_ptr=level_ptr[:nl + 1].copy(), permutation=perm, order=order,
+                row_ptr=nr, col=nc, val=nv, nlevels=int(nl))
+
+
+def spts_csr(row_ptr, col, val, b):
+    y = np.zeros(row_ptr.size - 1, val.dtype)
+    getattr(lib(), "or_spts_csr_" + _sfx(val.dtype))(
+        _p(_i32(row_ptr)), _p(_i32(col)), _p(val), _p(np.ascontiguousarray(b, val.dtype)), _p(y),
+        row_ptr.size - 1)
+    return y
+
+
+def spts_syncfree(row_ptr, col, val, b):
+    y = np.zeros(row_ptr.size - 1, val.dtype)
+    getattr(lib(), "or_spts_syncfree_" + _sfx(val.dtype))(
+        _p(_i32(row_ptr)), _p(_i32(col)), _p(val), _p(np.ascontiguousarray(b, val.dtype)), _p(y),
+        row_ptr.size - 1)
+    return y
+
+
+def truth_spts(row_ptr, col, val, b):
+    y = np.zeros(row_ptr.size - 1, np.float64)
+    lib().or_truth_spts(val.dtype.itemsize, _p(_i32(row_ptr)), _p(_i32(col)), _p(val),
+                        _p(np.ascontiguousarray(b, val.dtype)), _p(y), row_ptr.size - 1)
+    return y
+
+
+def par_spts_level(nthreads, level_ptr, row_ptr, col, val, b, y):
+    getattr(lib(), "or_par_spts_level_" + _sfx(val.dtype))(
+        nthreads, _p(level_ptr), level_ptr.size - 1, _p(row_ptr), _p(col), _p(val), _p(b), _p(y),
+        row_ptr.size - 1)
+
+
+def fletcher(y):
+    y = np.ascontiguousarray(y)
+    return int(getattr(lib(), "or_fletcher_" + _sfx(y.dtype))(_p(y), y.size))

@@ -1,0 +1,690 @@
+/*
+ * sparse_oracle.c -- CPU restatement of SciWasm.Sparse's sparse kernels.
+ *
+ * TEST INFRASTRUCTURE ONLY (correctness oracle + timed CPU baseline); the
+ * product never links it.  Parity status: UNPINNED by reference artefacts
+ * (the reference ships no golden vectors or fixtures for this path and cannot
+ * run here).  Each function cites the reference lines it restates; paths are
+ * relative to the SciWasm.Sparse project root.  Build with
+ * -O2 -ffp-contract=off -fno-fast-math so that separate mul and add are kept
+ * (wasm has no fused multiply-add).
+ */
+#include "sparse_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+
+/* ======================= SpMV, serial storage order ======================= */
+
+/* spmv_coo: src/sequential/src/sparse_opt_32.wat:175-202.  For k in storage
+ * order: y[row[k]] = (val[k]*x[col[k]]) + y[row[k]]. */
+#define DEF_SPMV_COO(T, SFX)                                                        \
+  void or_spmv_coo_##SFX(const int32_t* row, const int32_t* col, const T* val,       \
+                         const T* x, T* y, int64_t nnz) {                           \
+    for (int64_t k = 0; k < nnz; ++k) {                                             \
+      T p = val[k] * x[col[k]];                                                     \
+      y[row[k]] = p + y[row[k]];                                                    \
+    }                                                                               \
+  }
+DEF_SPMV_COO(float, f32)
+DEF_SPMV_COO(double, f64)
+
+/* spmv_csr: src/sequential/src/sparse_opt_32.wat:227-271.  Rows without
+ * entries are not written (:243 `if j < rowptr[i+1]`); otherwise
+ * temp = y[i]; temp = (val*x[col]) + temp in storage order; y[i] = temp. */
+#define DEF_SPMV_CSR(T, SFX)                                                        \
+  void or_spmv_csr_##SFX(const int32_t* row_ptr, const int32_t* col, const T* val,   \
+                         const T* x, T* y, int32_t N) {                             \
+    for (int32_t i = 0; i < N; ++i) {                                               \
+      int32_t j = row_ptr[i], e = row_ptr[i + 1];                                   \
+      if (j < e) {                                                                  \
+        T t = y[i];                                                                 \
+        for (; j != e; ++j) {                                                       \
+          T p = val[j] * x[col[j]];                                                 \
+          t = p + t;                                                                \
+        }                                                                           \
+        y[i] = t;                                                                   \
+      }                                                                             \
+    }                                                                               \
+  }
+DEF_SPMV_CSR(float, f32)
+DEF_SPMV_CSR(double, f64)
+
+/* spmv_dia: src/sequential/src/sparse_opt_32.wat:290-407.  For each stored
+ * diagonal d (offset k) and i in [max(0,-k), min(N, N-k)):
+ * y[i] = (data[d*stride + i - move]*x[i+k]) + y[i], move = N - stride for
+ * k < 0 (0 with stride = N).  The SIMD body is element-wise, so the scalar
+ * loop below gives identical bits. */
+#define DEF_SPMV_DIA(T, SFX)                                                        \
+  void or_spmv_dia_##SFX(const int32_t* offset, const T* data, int32_t N,           \
+                         int32_t nd, int32_t stride, const T* x, T* y) {            \
+    for (int32_t d = 0; d < nd; ++d) {                                              \
+      int32_t k = offset[d];                                                        \
+      int64_t move = (k < 0) ? (int64_t)(N - stride) : 0;                           \
+      int32_t n = (k < 0) ? -k : 0;                                                 \
+      int32_t iend = (N < N - k) ? N : N - k;                                       \
+      const T* dd = data + (int64_t)d * stride - move;                              \
+      for (int32_t i = n; i < iend; ++i) {                                          \
+        T p = dd[i] * x[i + k];                                                     \
+        y[i] = p + y[i];                                                            \
+      }                                                                             \
+    }                                                                               \
+  }
+DEF_SPMV_DIA(float, f32)
+DEF_SPMV_DIA(double, f64)
+
+/* spmv_ell: src/sequential/src/sparse_opt_32.wat:427-479.  Column-major; all
+ * nc*N slots are visited, padding (data 0, index 0) included. */
+#define DEF_SPMV_ELL(T, SFX)                                                        \
+  void or_spmv_ell_##SFX(const int32_t* indices, const T* data, int32_t N,          \
+                         int32_t nc, const T* x, T* y) {                            \
+    if (!(nc > 0 && N > 0)) return;                                                 \
+    for (int32_t j = 0; j < nc; ++j) {                                              \
+      const int64_t base = (int64_t)j * N;                                          \
+      for (int32_t i = 0; i < N; ++i) {                                             \
+        T p = data[base + i] * x[indices[base + i]];                                \
+        y[i] = p + y[i];                                                            \
+      }                                                                             \
+    }                                                                               \
+  }
+DEF_SPMV_ELL(float, f32)
+DEF_SPMV_ELL(double, f64)
+
+#define DEF_TRUTH_CSR(T, SFX)                                                       \
+  void or_truth_csr_##SFX(const int32_t* row_ptr, const int32_t* col, const T* val,  \
+                          const T* x, const T* y0, double* y, int32_t N) {          \
+    for (int32_t i = 0; i < N; ++i) {                                               \
+      long double t = y0 ? (long double)y0[i] : 0.0L;                               \
+      for (int32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j)                         \
+        t += (long double)val[j] * (long double)x[col[j]];                          \
+      y[i] = (double)t;                                                             \
+    }                                                                               \
+  }
+DEF_TRUTH_CSR(float, f32)
+DEF_TRUTH_CSR(double, f64)
+
+/* ======================= parallel CPU baseline ======================= */
+
+/* static_nnz: src/parallel/src/sparse32.js:2769-2821.  Greedy contiguous
+ * row ranges: each worker takes rows while its running sum is below
+ * floor(rem_nnz/rem_nw).  row_end entries that the reference never assigns
+ * keep the zero of a fresh Int32Array. */
+void or_static_nnz(const int32_t* row_ptr, int32_t N, int32_t nw, int32_t* row_start,
+                   int32_t* row_end) {
+  int64_t rem_nnz = (int64_t)row_ptr[N] - row_ptr[0];
+  int32_t rem_nw = nw;
+  int32_t index = 0;
+  int32_t i;
+  for (i = 0; i < nw; ++i) { row_start[i] = 0; row_end[i] = 0; }
+  for (i = 0; i < nw; ++i) {
+    if (index == N) {
+      row_start[i] = row_end[i] = N;
+      continue;
+    }
+    int64_t ideal = (int64_t)floor((double)rem_nnz / (double)rem_nw);
+    row_start[i] = index;
+    int64_t sum = 0;
+    for (int32_t j = index; j < N; ++j) {
+      if (sum < ideal) {
+        sum += row_ptr[j + 1] - row_ptr[j];
+        index++;
+      } else {
+        row_end[i] = index;
+        break;
+      }
+    }
+    rem_nnz -= sum;
+    rem_nw--;
+  }
+  row_end[i - 1] = N;
+}
+
+static int clamp_threads(int nt) { return nt < 1 ? 1 : (nt > 256 ? 256 : nt); }
+
+/* Worker pool stand-in: nt POSIX threads, each with its id, sharing one
+ * barrier, as the reference's Web Workers share one wasm memory. */
+typedef struct par_job {
+  int nt;
+  pthread_barrier_t bar;
+  void (*fn)(struct par_job*, int);
+  const void* a[8];
+  void* m[4];
+  int64_t n[6];
+} par_job;
+
+typedef struct { par_job* job; int id; } par_arg;
+
+static void* par_entry(void* p) {
+  par_arg* a = (par_arg*)p;
+  a->job->fn(a->job, a->id);
+  return NULL;
+}
+
+static void par_run(par_job* job) {
+  int nt = job->nt;
+  pthread_t th[256];
+  par_arg args[256];
+  pthread_barrier_init(&job->bar, NULL, (unsigned)nt);
+  for (int i = 1; i < nt; ++i) {
+    args[i].job = job;
+    args[i].id = i;
+    pthread_create(&th[i], NULL, par_entry, &args[i]);
+  }
+  job->fn(job, 0);
+  for (int i = 1; i < nt; ++i) pthread_join(th[i], NULL);
+  pthread_barrier_destroy(&job->bar);
+}
+
+#define DEF_PAR_CSR(T, SFX)                                                         \
+  static void par_csr_##SFX(par_job* j, int id) {                                   \
+    const int32_t* rs = (const int32_t*)j->a[5];                                    \
+    const int32_t* re = (const int32_t*)j->a[6];                                    \
+    if (re[id] > rs[id])                                                            \
+      or_spmv_csr_##SFX((const int32_t*)j->a[0] + rs[id], (const int32_t*)j->a[1],   \
+                        (const T*)j->a[2], (const T*)j->a[3], (T*)j->m[0] + rs[id],  \
+                        re[id] - rs[id]);                                           \
+  }                                                                                 \
+  void or_par_spmv_csr_##SFX(int nthreads, const int32_t* row_ptr,                   \
+                             const int32_t* col, const T* val, const T* x, T* y,     \
+                             int32_t N) {                                           \
+    par_job job;                                                                    \
+    job.nt = clamp_threads(nthreads);                                               \
+    int32_t* rs = (int32_t*)malloc(sizeof(int32_t) * job.nt);                       \
+    int32_t* re = (int32_t*)malloc(sizeof(int32_t) * job.nt);                       \
+    or_static_nnz(row_ptr, N, job.nt, rs, re);                                      \
+    job.fn = par_csr_##SFX;                                                         \
+    job.a[0] = row_ptr; job.a[1] = col; job.a[2] = val; job.a[3] = x;               \
+    job.a[5] = rs; job.a[6] = re; job.m[0] = y;                                     \
+    par_run(&job);                                                                  \
+    free(rs);                                                                       \
+    free(re);                                                                       \
+  }
+DEF_PAR_CSR(float, f32)
+DEF_PAR_CSR(double, f64)
+
+/* sparse_spmv_coo: src/parallel/src/sparse32.js:2637-2693.  Worker i takes
+ * nnz [i*q, (i+1)*q) (last worker + remainder) into its private w_y[i]; then
+ * nw rounds of `sum` (src/parallel/src/sparse_opt_32.wat:1420-1481) add
+ * w_y[0], w_y[1], ... into y, each round row-split across the workers. */
+#define DEF_PAR_COO(T, SFX)                                                         \
+  static void par_coo_##SFX(par_job* j, int id) {                                   \
+    int nt = j->nt;                                                                 \
+    int64_t nnz = j->n[0];                                                          \
+    int32_t N = (int32_t)j->n[1];                                                   \
+    T* y = (T*)j->m[0];                                                             \
+    T* wy = (T*)j->m[1];                                                            \
+    int64_t q = nnz / nt, remq = nnz - q * nt;                                      \
+    int32_t npw = N / nt, remN = N - npw * nt;                                      \
+    T* w = wy + (int64_t)id * N;                                                    \
+    memset(w, 0, sizeof(T) * (size_t)N);                                            \
+    int64_t s = id * q, e = (id + 1) * q + (id == nt - 1 ? remq : 0);               \
+    or_spmv_coo_##SFX((const int32_t*)j->a[0] + s, (const int32_t*)j->a[1] + s,      \
+                      (const T*)j->a[2] + s, (const T*)j->a[3], w, e - s);          \
+    pthread_barrier_wait(&j->bar);                                                  \
+    for (int k = 0; k < nt; ++k) {                                                  \
+      const T* wk = wy + (int64_t)k * N;                                            \
+      int32_t rs = id * npw, re = (id + 1) * npw + (id == nt - 1 ? remN : 0);       \
+      for (int32_t r = rs; r < re; ++r) y[r] = y[r] + wk[r];                        \
+      pthread_barrier_wait(&j->bar);                                                \
+    }                                                                               \
+  }                                                                                 \
+  void or_par_spmv_coo_##SFX(int nthreads, const int32_t* row, const int32_t* col,  \
+                             const T* val, const T* x, T* y, int32_t N, int64_t nnz, \
+                             T* wy) {                                               \
+    par_job job;                                                                    \
+    job.nt = clamp_threads(nthreads);                                               \
+    job.fn = par_coo_##SFX;                                                         \
+    job.a[0] = row; job.a[1] = col; job.a[2] = val; job.a[3] = x;                   \
+    job.m[0] = y; job.m[1] = wy; job.n[0] = nnz; job.n[1] = N;                      \
+    par_run(&job);                                                                  \
+  }
+DEF_PAR_COO(float, f32)
+DEF_PAR_COO(double, f64)
+
+/* Row-split DIA (src/parallel/tests/main32.js:749-790, row-major kernel
+ * src/parallel/src/sparse_opt_32.wat:8213-8269): each worker applies every
+ * diagonal to its own row range, so the per-row order equals the serial one. */
+#define DEF_PAR_DIA(T, SFX)                                                         \
+  static void par_dia_##SFX(par_job* j, int id) {                                   \
+    int nt = j->nt;                                                                 \
+    const int32_t* offset = (const int32_t*)j->a[0];                                \
+    const T* data = (const T*)j->a[1];                                              \
+    const T* x = (const T*)j->a[3];                                                 \
+    T* y = (T*)j->m[0];                                                             \
+    int32_t N = (int32_t)j->n[0], nd = (int32_t)j->n[1], stride = (int32_t)j->n[2];  \
+    int32_t npw = N / nt, remN = N - npw * nt;                                      \
+    int32_t s = id * npw, e = (id + 1) * npw + (id == nt - 1 ? remN : 0);           \
+    for (int32_t d = 0; d < nd; ++d) {                                              \
+      int32_t k = offset[d];                                                        \
+      int64_t move = (k < 0) ? (int64_t)(N - stride) : 0;                           \
+      int32_t lo = (k < 0) ? -k : 0;                                                \
+      int32_t hi = (N < N - k) ? N : N - k;                                         \
+      if (lo < s) lo = s;                                                           \
+      if (hi > e) hi = e;                                                           \
+      const T* dd = data + (int64_t)d * stride - move;                              \
+      for (int32_t i = lo; i < hi; ++i) {                                           \
+        T p = dd[i] * x[i + k];                                                     \
+        y[i] = p + y[i];                                                            \
+      }                                                                             \
+    }                                                                               \
+  }                                                                                 \
+  void or_par_spmv_dia_##SFX(int nthreads, const int32_t* offset, const T* data,    \
+                             int32_t N, int32_t nd, int32_t stride, const T* x,     \
+                             T* y) {                                                \
+    par_job job;                                                                    \
+    job.nt = clamp_threads(nthreads);                                               \
+    job.fn = par_dia_##SFX;                                                         \
+    job.a[0] = offset; job.a[1] = data; job.a[3] = x; job.m[0] = y;                 \
+    job.n[0] = N; job.n[1] = nd; job.n[2] = stride;                                 \
+    par_run(&job);                                                                  \
+  }
+DEF_PAR_DIA(float, f32)
+DEF_PAR_DIA(double, f64)
+
+/* Row-split column-major ELL (src/parallel/src/sparse_opt_32.wat:11055-11106). */
+#define DEF_PAR_ELL(T, SFX)                                                         \
+  static void par_ell_##SFX(par_job* j, int id) {                                   \
+    int nt = j->nt;                                                                 \
+    const int32_t* indices = (const int32_t*)j->a[0];                               \
+    const T* data = (const T*)j->a[1];                                              \
+    const T* x = (const T*)j->a[3];                                                 \
+    T* y = (T*)j->m[0];                                                             \
+    int32_t N = (int32_t)j->n[0], nc = (int32_t)j->n[1];                            \
+    int32_t npw = N / nt, remN = N - npw * nt;                                      \
+    int32_t s = id * npw, e = (id + 1) * npw + (id == nt - 1 ? remN : 0);           \
+    for (int32_t c = 0; c < nc; ++c) {                                              \
+      const int64_t base = (int64_t)c * N;                                          \
+      for (int32_t i = s; i < e; ++i) {                                             \
+        T p = data[base + i] * x[indices[base + i]];                                \
+        y[i] = p + y[i];                                                            \
+      }                                                                             \
+    }                                                                               \
+  }                                                                                 \
+  void or_par_spmv_ell_##SFX(int nthreads, const int32_t* indices, const T* data,   \
+                             int32_t N, int32_t nc, const T* x, T* y) {             \
+    par_job job;                                                                    \
+    job.nt = clamp_threads(nthreads);                                               \
+    job.fn = par_ell_##SFX;                                                         \
+    job.a[0] = indices; job.a[1] = data; job.a[3] = x; job.m[0] = y;                \
+    job.n[0] = N; job.n[1] = nc;                                                    \
+    par_run(&job);                                                                  \
+  }
+DEF_PAR_ELL(float, f32)
+DEF_PAR_ELL(double, f64)
+
+/* ======================= conversions ======================= */
+
+static void swap_bytes(void* a, int64_t i, int64_t j, int w) {
+  if (w == 4) {
+    uint32_t* p = (uint32_t*)a;
+    uint32_t t = p[i]; p[i] = p[j]; p[j] = t;
+  } else {
+    uint64_t* p = (uint64_t*)a;
+    uint64_t t = p[i]; p[i] = p[j]; p[j] = t;
+  }
+}
+
+static void copy_elem(void* dst, int64_t i, const void* src, int64_t j, int w) {
+  if (w == 4) ((uint32_t*)dst)[i] = ((const uint32_t*)src)[j];
+  else ((uint64_t*)dst)[i] = ((const uint64_t*)src)[j];
+}
+
+/* sort: src/sequential/src/sparse32.js:1612-1627.  Bubble sort of
+ * array1[start, end) with array2 carried along; strict '>' keeps it stable. */
+static void bubble_sort(int64_t start, int64_t end, int32_t* a1, void* a2, int w) {
+  int64_t n = end - start;
+  for (int64_t i = 0; i < n - 1; ++i) {
+    for (int64_t j = start; j < end - i - 1; ++j) {
+      if (a1[j] > a1[j + 1]) {
+        int32_t t = a1[j]; a1[j] = a1[j + 1]; a1[j + 1] = t;
+        swap_bytes(a2, j, j + 1, w);
+      }
+    }
+  }
+}
+
+/* coo_csr: src/sequential/src/sparse32.js:1674-1720. */
+void or_coo_csr(int w, const int32_t* row, const int32_t* col, const void* val, int32_t N,
+                int64_t nnz, int32_t* csr_row, int32_t* csr_col, void* csr_val) {
+  memset(csr_row, 0, sizeof(int32_t) * ((size_t)N + 1));
+  for (int64_t i = 0; i < nnz; ++i) csr_row[row[i]]++;
+  int32_t j = 0, j0;
+  for (int32_t i = 0; i < N; ++i) {
+    j0 = csr_row[i];
+    csr_row[i] = j;
+    j += j0;
+  }
+  for (int64_t i = 0; i < nnz; ++i) {
+    int32_t p = csr_row[row[i]];
+    csr_col[p] = col[i];
+    copy_elem(csr_val, p, val, i, w);
+    csr_row[row[i]]++;
+  }
+  for (int32_t i = N - 1; i > 0; --i) csr_row[i] = csr_row[i - 1];
+  csr_row[0] = 0;
+  csr_row[N] = (int32_t)nnz;
+  for (int32_t i = 0; i < N; ++i) bubble_sort(csr_row[i], csr_row[i + 1], csr_col, csr_val, w);
+}
+
+/* coo_csc: src/sequential/src/sparse32.js:1629-1671 (same shape with the
+ * roles of row and col exchanged). */
+void or_coo_csc(int w, const int32_t* row, const int32_t* col, const void* val,
+                int32_t ncols, int64_t nnz, int32_t* csc_col, int32_t* csc_row,
+                void* csc_val) {
+  or_coo_csr(w, col, row, val, ncols, nnz, csc_col, csc_row, csc_val);
+}
+
+/* num_cols: src/sequential/src/sparse32.js:1436-1447. */
+int32_t or_num_cols(const int32_t* row_ptr, int32_t N) {
+  int32_t mx = 0;
+  for (int32_t i = 0; i < N; ++i) {
+    int32_t t = row_ptr[i + 1] - row_ptr[i];
+    if (mx < t) mx = t;
+  }
+  return mx;
+}
+
+/* The admission test of csr_ell (:1457) and csr_dia (:1525), in doubles.
+ * nnz == 0 gives 0/0 = NaN, and NaN <= 5 is false: refused. */
+int or_format_admitted(int64_t width, int64_t N, int64_t nnz) {
+  double wn = (double)width * (double)N;
+  double ratio = wn / (double)nnz;
+  return (wn < 134217728.0) && (ratio <= 5.0);
+}
+
+/* csr_ell: src/sequential/src/sparse32.js:1464-1484. */
+void or_csr_ell(int w, const int32_t* row_ptr, const int32_t* col, const void* val,
+                int32_t N, int32_t nc, int32_t* indices, void* data) {
+  size_t slots = (size_t)nc * (size_t)N;
+  memset(indices, 0, sizeof(int32_t) * slots);
+  memset(data, 0, (size_t)w * slots);
+  for (int32_t i = 0; i < N; ++i) {
+    int64_t k = 0;
+    for (int32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j) {
+      copy_elem(data, k * N + i, val, j, w);
+      indices[k * N + i] = col[j];
+      k++;
+    }
+  }
+}
+
+/* num_diags: src/sequential/src/sparse32.js:1486-1512.  Diagonal c - i maps
+ * to ind[N + c - i - 1]; stride is N. */
+int32_t or_num_diags(const int32_t* row_ptr, const int32_t* col, int32_t N, int32_t* stride) {
+  int32_t nd = 0;
+  if (N <= 0) { *stride = N; return 0; }
+  int32_t* ind = (int32_t*)calloc((size_t)2 * N - 1, sizeof(int32_t));
+  for (int32_t i = 0; i < N; ++i)
+    for (int32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j)
+      if (!ind[(int64_t)N + col[j] - i - 1]++) nd++;
+  free(ind);
+  *stride = N;
+  return nd;
+}
+
+/* csr_dia: src/sequential/src/sparse32.js:1516-1574.  Offsets are the present
+ * diagonals in ascending order; each entry is placed by a linear search over
+ * the offsets, so a later duplicate (i, c) overwrites an earlier one. */
+void or_csr_dia(int w, const int32_t* row_ptr, const int32_t* col, const void* val,
+                int32_t N, int32_t nd, int32_t stride, int32_t* offset, void* data) {
+  memset(data, 0, (size_t)w * (size_t)nd * (size_t)stride);
+  if (N <= 0) return;
+  int32_t* ind = (int32_t*)calloc((size_t)2 * N - 1, sizeof(int32_t));
+  for (int32_t i = 0; i < N; ++i)
+    for (int32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j) ind[(int64_t)N + col[j] - i - 1]++;
+  int32_t diag_no = -((2 * N - 1) / 2);
+  int32_t index = 0;
+  for (int64_t i = 0; i < 2 * (int64_t)N - 1; ++i) {
+    if (ind[i]) offset[index++] = diag_no;
+    diag_no++;
+  }
+  free(ind);
+  for (int32_t i = 0; i < N; ++i) {
+    for (int32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j) {
+      int32_t c = col[j];
+      for (int32_t k = 0; k < nd; ++k) {
+        int64_t move = 0;
+        if (c - i == offset[k]) {
+          if (offset[k] < 0) move = (int64_t)N - stride;
+          copy_elem(data, (int64_t)k * stride + i - move, val, j, w);
+          break;
+        }
+      }
+    }
+  }
+}
+
+/* quick_sort_COO: src/sequential/src/sparse32.js:1577-1608 (Hoare partition
+ * on the middle element, keyed by (row, col); not stable). */
+void or_quick_sort_coo(int w, int32_t* row, int32_t* col, void* val, int64_t left,
+                       int64_t right) {
+  while (left < right) {
+    int64_t i = left, j = right;
+    int64_t mid = (left + right) / 2;
+    int32_t pivot = row[mid], pivot_col = col[mid];
+    while (i <= j) {
+      while (row[i] < pivot || (row[i] == pivot && col[i] < pivot_col)) i++;
+      while (row[j] > pivot || (row[j] == pivot && col[j] > pivot_col)) j--;
+      if (i <= j) {
+        int32_t t = row[i]; row[i] = row[j]; row[j] = t;
+        t = col[i]; col[i] = col[j]; col[j] = t;
+        swap_bytes(val, i, j, w);
+        i++;
+        j--;
+      }
+    }
+    /* recurse into the smaller side, loop on the larger (same result as the
+     * reference's two recursive calls, bounded stack) */
+    if (j - left < right - i) {
+      if (left < j) or_quick_sort_coo(w, row, col, val, left, j);
+      left = i;
+    } else {
+      if (i < right) or_quick_sort_coo(w, row, col, val, i, right);
+      right = j;
+    }
+  }
+}
+
+/* ======================= level sets and SpTS ======================= */
+
+/* CSR_create_level_sets_with_reorder: src/parallel/src/sparse32.js:3010-3181.
+ * level[i] = 0 when row i holds exactly one entry; otherwise 1 + the maximum
+ * (initialised at 0) of level[col] over all entries but the last, where rows
+ * not yet visited (col >= i) still read 0.  An empty row therefore gets
+ * level 1.  Rows are stably counting-sorted by level. */
+int32_t or_level_sets(int w, const int32_t* row_ptr, const int32_t* col, const void* val,
+                      int32_t N, int32_t* level, int32_t* level_ptr, int32_t* permutation,
+                      int32_t* order, int32_t* new_row, int32_t* new_col, void* new_val) {
+  int32_t max_level = 0;
+  memset(level, 0, sizeof(int32_t) * (size_t)N);
+  for (int32_t i = 0; i < N; ++i) {
+    int32_t len = row_ptr[i + 1] - row_ptr[i];
+    if (len == 1) {
+      level[i] = 0;
+    } else {
+      int32_t m = 0;
+      for (int32_t j = row_ptr[i]; j < row_ptr[i + 1] - 1; ++j)
+        if (level[col[j]] > m) m = level[col[j]];
+      level[i] = 1 + m;
+      if (level[i] > max_level) max_level = level[i];
+    }
+  }
+  int32_t nlev = max_level + 1;
+  int32_t* freq = (int32_t*)calloc((size_t)nlev, sizeof(int32_t));
+  int32_t* start = (int32_t*)calloc((size_t)nlev, sizeof(int32_t));
+  for (int32_t i = 0; i < N; ++i) freq[level[i]]++;
+  level_ptr[0] = 0;
+  start[0] = 0;
+  for (int32_t l = 1; l < nlev; ++l) start[l] = level_ptr[l] = level_ptr[l - 1] + freq[l - 1];
+  level_ptr[nlev] = level_ptr[nlev - 1] + freq[nlev - 1];
+  for (int32_t i = 0; i < N; ++i) {
+    permutation[start[level[i]]] = i;
+    order[i] = start[level[i]];
+    start[level[i]]++;
+  }
+  free(freq);
+  free(start);
+  if (new_row) {
+    int64_t j = 0;
+    new_row[0] = 0;
+    for (int32_t i = 0; i < N; ++i) {
+      int32_t p = permutation[i];
+      int32_t k = row_ptr[p];
+      int32_t t = row_ptr[p + 1] - row_ptr[p];
+      new_row[i + 1] = new_row[i] + t;
+      while (t != 0) {
+        new_col[j] = order[col[k]];
+        copy_elem(new_val, j, val, k, w);
+        j++;
+        k++;
+        t--;
+      }
+    }
+  }
+  return nlev;
+}
+
+/* spts_csr row kernel: src/parallel/src/sparse_opt_32.wat:11679-11757. */
+#define DEF_SPTS_CSR(T, SFX)                                                        \
+  void or_spts_csr_##SFX(const int32_t* row_ptr, const int32_t* col, const T* val,   \
+                         const T* b, T* y, int32_t N) {                             \
+    for (int32_t i = 0; i < N; ++i) {                                               \
+      int32_t j = row_ptr[i], end = row_ptr[i + 1] - 1;                             \
+      if (end > j) {                                                                \
+        T t = (T)0;                                                                 \
+        for (; j != end; ++j) {                                                     \
+          T p = val[j] * y[col[j]];                                                 \
+          t = t + p;                                                                \
+        }                                                                           \
+        y[i] = (b[i] - t) / val[end];                                               \
+      } else {                                                                      \
+        y[i] = b[i] / val[end];                                                     \
+      }                                                                             \
+    }                                                                               \
+  }
+DEF_SPTS_CSR(float, f32)
+DEF_SPTS_CSR(double, f64)
+
+/* spts_csr_sync_free: src/parallel/src/spts_opt_32.wat:8-117 (x aliases y,
+ * pre-copied from b). */
+#define DEF_SPTS_SF(T, SFX)                                                         \
+  void or_spts_syncfree_##SFX(const int32_t* row_ptr, const int32_t* col,            \
+                              const T* val, const T* b, T* y, int32_t N) {          \
+    for (int32_t i = 0; i < N; ++i) y[i] = b[i];                                    \
+    for (int32_t i = 0; i < N; ++i) {                                               \
+      int32_t j = row_ptr[i] + 1, end = row_ptr[i + 1];                             \
+      if (end > j) {                                                                \
+        T t = y[i];                                                                 \
+        int32_t k = row_ptr[i];                                                     \
+        for (; k != end - 1; ++k) {                                                 \
+          T p = val[k] * y[col[k]];                                                 \
+          t = t - p;                                                                \
+        }                                                                           \
+        y[i] = t / val[end - 1];                                                    \
+      } else {                                                                      \
+        y[i] = y[i] / val[row_ptr[i]];                                              \
+      }                                                                             \
+    }                                                                               \
+  }
+DEF_SPTS_SF(float, f32)
+DEF_SPTS_SF(double, f64)
+
+void or_truth_spts(int w, const int32_t* row_ptr, const int32_t* col, const void* val,
+                   const void* b, double* y, int32_t N) {
+  long double* t = (long double*)malloc(sizeof(long double) * (size_t)(N > 0 ? N : 1));
+  for (int32_t i = 0; i < N; ++i) {
+    int32_t s = row_ptr[i], e = row_ptr[i + 1] - 1;
+    long double acc = 0.0L;
+    for (int32_t j = s; j < e; ++j) {
+      long double v = (w == 4) ? (long double)((const float*)val)[j]
+                               : (long double)((const double*)val)[j];
+      acc += v * t[col[j]];
+    }
+    long double bi = (w == 4) ? (long double)((const float*)b)[i]
+                              : (long double)((const double*)b)[i];
+    long double d = (w == 4) ? (long double)((const float*)val)[e]
+                             : (long double)((const double*)val)[e];
+    t[i] = (bi - acc) / d;
+    y[i] = (double)t[i];
+  }
+  free(t);
+}
+
+/* spts_level_csr: src/parallel/src/spts_opt_32.wat:339-546 and
+ * src/parallel/src/sparse_opt_32.wat:11759-11980.  Per level, rows
+ * [level_ptr[l], level_ptr[l+1]) are split len = nrows/nt with the first
+ * nrows%nt workers taking one more; a barrier follows every level. */
+#define DEF_PAR_SPTS(T, SFX)                                                        \
+  static void par_spts_##SFX(par_job* jb, int id) {                                 \
+    int nt = jb->nt;                                                                \
+    const int32_t* level_ptr = (const int32_t*)jb->a[0];                            \
+    const int32_t* row_ptr = (const int32_t*)jb->a[1];                              \
+    const int32_t* col = (const int32_t*)jb->a[2];                                  \
+    const T* val = (const T*)jb->a[3];                                              \
+    const T* b = (const T*)jb->a[4];                                                \
+    T* y = (T*)jb->m[0];                                                            \
+    int32_t nlevels = (int32_t)jb->n[0];                                            \
+    for (int32_t l = 0; l < nlevels; ++l) {                                         \
+      int32_t nrows = level_ptr[l + 1] - level_ptr[l];                              \
+      int32_t len = nrows / nt, rem = nrows % nt, s;                                \
+      if (len != 0) {                                                               \
+        if (rem > id) { s = level_ptr[l] + id * len + id; len++; }                  \
+        else s = level_ptr[l] + id * len + rem;                                     \
+      } else {                                                                      \
+        len = (nrows > id) ? 1 : 0;                                                 \
+        s = level_ptr[l] + id;                                                      \
+      }                                                                             \
+      for (int32_t i = s; i < s + len; ++i) {                                       \
+        int32_t j = row_ptr[i], end = row_ptr[i + 1] - 1;                           \
+        if (end > j) {                                                              \
+          T t = (T)0;                                                               \
+          for (; j != end; ++j) {                                                   \
+            T p = val[j] * y[col[j]];                                               \
+            t = t + p;                                                              \
+          }                                                                         \
+          y[i] = (b[i] - t) / val[end];                                             \
+        } else {                                                                    \
+          y[i] = b[i] / val[end];                                                   \
+        }                                                                           \
+      }                                                                             \
+      pthread_barrier_wait(&jb->bar);                                               \
+    }                                                                               \
+  }                                                                                 \
+  void or_par_spts_level_##SFX(int nthreads, const int32_t* level_ptr,              \
+                               int32_t nlevels, const int32_t* row_ptr,             \
+                               const int32_t* col, const T* val, const T* b, T* y,  \
+                               int32_t N) {                                         \
+    par_job job;                                                                    \
+    (void)N;                                                                        \
+    job.nt = clamp_threads(nthreads);                                               \
+    job.fn = par_spts_##SFX;                                                        \
+    job.a[0] = level_ptr; job.a[1] = row_ptr; job.a[2] = col; job.a[3] = val;       \
+    job.a[4] = b; job.m[0] = y; job.n[0] = nlevels;                                 \
+    par_run(&job);                                                                  \
+  }
+DEF_PAR_SPTS(float, f32)
+DEF_PAR_SPTS(double, f64)
+
+/* ======================= checksum ======================= */
+
+/* matlab_modulo / fletcher_sum / fletcher_sum_y:
+ * src/sequential/src/sparse32.js:1286-1311. */
+static double matlab_modulo(double x, double y) {
+  double n = floor(x / y);
+  return x - n * y;
+}
+
+#define DEF_FLETCHER(T, SFX)                                                        \
+  int64_t or_fletcher_##SFX(const T* y, int64_t n) {                                \
+    double s1 = 0.0, s2 = 0.0;                                                      \
+    for (int64_t i = 0; i < n; ++i) {                                               \
+      s1 = matlab_modulo(s1 + (double)y[i], 255.0);                                 \
+      s2 = matlab_modulo(s2 + s1, 255.0);                                           \
+    }                                                                               \
+    double r = s2 * 256.0 + s1;                                                     \
+    return (int64_t)r; /* parseInt truncates toward zero */                         \
+  }
+DEF_FLETCHER(float, f32)
+DEF_FLETCHER(double, f64)

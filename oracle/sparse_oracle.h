@@ -1,0 +1,160 @@
+/*
+ * sparse_oracle.h -- CPU restatement of SciWasm.Sparse's sparse kernels.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the correctness oracle and the
+ * timed CPU baseline.  Only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline / --impl reference leg may load it; the product path
+ * (libsparse_b200.so and the sciwasm.sparse_b200 package) never does.
+ *
+ * Parity status: UNPINNED by reference artefacts.  The reference ships no
+ * golden vectors, fixtures or known-answer tests for this path, its JS/wasm
+ * code cannot run in this environment (no JS or wasm runtime), and the only
+ * published pins are Fletcher checksums of real-world matrices whose files
+ * are not distributed with it.  Every function below restates one reference
+ * function line by line (cited as file:line, paths relative to the
+ * SciWasm.Sparse project root) and is compiled with -ffp-contract=off so that
+ * wasm's separate mul/add (wasm has no FMA) is reproduced bit for bit.
+ *
+ * Index arrays are int32 as in the reference (i32 in wasm linear memory).
+ * Counts that can exceed 2^31 in this build's workloads are int64.
+ */
+#ifndef SPARSE_ORACLE_H
+#define SPARSE_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- SpMV (y += A x), serial storage order ---------------- */
+/* src/sequential/src/sparse_opt_32.wat:175-202 (spmv_coo), :227-271
+ * (spmv_csr), :290-407 (spmv_dia), :427-479 (spmv_ell); the f64 module
+ * src/sequential/src/sparse_opt_64.wat:187/239/302/439 is the same loop. */
+void or_spmv_coo_f32(const int32_t* row, const int32_t* col, const float* val,
+                     const float* x, float* y, int64_t nnz);
+void or_spmv_coo_f64(const int32_t* row, const int32_t* col, const double* val,
+                     const double* x, double* y, int64_t nnz);
+void or_spmv_csr_f32(const int32_t* row_ptr, const int32_t* col, const float* val,
+                     const float* x, float* y, int32_t N);
+void or_spmv_csr_f64(const int32_t* row_ptr, const int32_t* col, const double* val,
+                     const double* x, double* y, int32_t N);
+void or_spmv_dia_f32(const int32_t* offset, const float* data, int32_t N, int32_t nd,
+                     int32_t stride, const float* x, float* y);
+void or_spmv_dia_f64(const int32_t* offset, const double* data, int32_t N, int32_t nd,
+                     int32_t stride, const double* x, double* y);
+void or_spmv_ell_f32(const int32_t* indices, const float* data, int32_t N, int32_t nc,
+                     const float* x, float* y);
+void or_spmv_ell_f64(const int32_t* indices, const double* data, int32_t N, int32_t nc,
+                     const double* x, double* y);
+
+/* Extended-precision "truth" y += A x for relative-error measurement (long
+ * double accumulation of the stored operands).  Not a reference function. */
+void or_truth_csr_f32(const int32_t* row_ptr, const int32_t* col, const float* val,
+                      const float* x, const float* y0, double* y, int32_t N);
+void or_truth_csr_f64(const int32_t* row_ptr, const int32_t* col, const double* val,
+                      const double* x, const double* y0, double* y, int32_t N);
+
+/* ---------------- parallel CPU baseline (reference worker partitioning) -- */
+/* static_nnz: src/parallel/src/sparse32.js:2769-2821.  Fills row_start /
+ * row_end (nw entries each). */
+void or_static_nnz(const int32_t* row_ptr, int32_t N, int32_t nw,
+                   int32_t* row_start, int32_t* row_end);
+/* Parallel CSR over static_nnz ranges (src/parallel/tests/main32.js:150-313,
+ * src/parallel/src/sparse_opt_32.wat:1712-1771). */
+void or_par_spmv_csr_f32(int nthreads, const int32_t* row_ptr, const int32_t* col,
+                         const float* val, const float* x, float* y, int32_t N);
+void or_par_spmv_csr_f64(int nthreads, const int32_t* row_ptr, const int32_t* col,
+                         const double* val, const double* x, double* y, int32_t N);
+/* Parallel COO: nnz split, private y per worker, then nw row-split
+ * reductions (src/parallel/src/sparse32.js:2637-2693,
+ * src/parallel/src/sparse_opt_32.wat:1389-1481).  wy: nthreads*N scratch. */
+void or_par_spmv_coo_f32(int nthreads, const int32_t* row, const int32_t* col,
+                         const float* val, const float* x, float* y, int32_t N,
+                         int64_t nnz, float* wy);
+void or_par_spmv_coo_f64(int nthreads, const int32_t* row, const int32_t* col,
+                         const double* val, const double* x, double* y, int32_t N,
+                         int64_t nnz, double* wy);
+/* Parallel DIA / ELL: even row split (src/parallel/tests/main32.js:749-790,
+ * :1048-1080). */
+void or_par_spmv_dia_f64(int nthreads, const int32_t* offset, const double* data,
+                         int32_t N, int32_t nd, int32_t stride, const double* x, double* y);
+void or_par_spmv_dia_f32(int nthreads, const int32_t* offset, const float* data,
+                         int32_t N, int32_t nd, int32_t stride, const float* x, float* y);
+void or_par_spmv_ell_f64(int nthreads, const int32_t* indices, const double* data,
+                         int32_t N, int32_t nc, const double* x, double* y);
+void or_par_spmv_ell_f32(int nthreads, const int32_t* indices, const float* data,
+                         int32_t N, int32_t nc, const float* x, float* y);
+
+/* ---------------- conversions ---------------- */
+/* coo_csr: src/sequential/src/sparse32.js:1674-1720 with the per-row stable
+ * bubble sort `sort` :1612-1627.  val_bytes = 4 or 8. */
+void or_coo_csr(int val_bytes, const int32_t* row, const int32_t* col, const void* val,
+                int32_t N, int64_t nnz, int32_t* csr_row, int32_t* csr_col, void* csr_val);
+/* coo_csc: src/sequential/src/sparse32.js:1629-1671. */
+void or_coo_csc(int val_bytes, const int32_t* row, const int32_t* col, const void* val,
+                int32_t ncols, int64_t nnz, int32_t* csc_col, int32_t* csc_row, void* csc_val);
+/* num_cols: :1436-1447.  Returns max row length. */
+int32_t or_num_cols(const int32_t* row_ptr, int32_t N);
+/* Refusal predicate of csr_ell (:1457) and csr_dia (:1525), evaluated in
+ * double precision as JS does: admit iff w*N < 2^27 and (w*N)/nnz <= 5.
+ * Returns 1 when admitted. */
+int or_format_admitted(int64_t width, int64_t N, int64_t nnz);
+/* csr_ell fill: :1464-1484 (indices/data zero-filled, column-major). */
+void or_csr_ell(int val_bytes, const int32_t* row_ptr, const int32_t* col, const void* val,
+                int32_t N, int32_t nc, int32_t* indices, void* data);
+/* num_diags: :1486-1512.  Returns nd; *stride = N. */
+int32_t or_num_diags(const int32_t* row_ptr, const int32_t* col, int32_t N, int32_t* stride);
+/* csr_dia fill: :1516-1574 (offsets ascending, last write wins). */
+void or_csr_dia(int val_bytes, const int32_t* row_ptr, const int32_t* col, const void* val,
+                int32_t N, int32_t nd, int32_t stride, int32_t* offset, void* data);
+/* quick_sort_COO: :1577-1608 (unstable, as in the reference). */
+void or_quick_sort_coo(int val_bytes, int32_t* row, int32_t* col, void* val, int64_t left,
+                       int64_t right);
+
+/* ---------------- level sets and SpTS ---------------- */
+/* CSR_create_level_sets_with_reorder: src/parallel/src/sparse32.js:3010-3181
+ * (level rule :3035-3055; level_ptr :3094-3108; permutation/order
+ * :3110-3119; reordered CSR :3127-3138).  Returns nlevels.  level (N),
+ * level_ptr (N+1 capacity), permutation (N), order (N); the reordered CSR is
+ * written when new_row != NULL. */
+int32_t or_level_sets(int val_bytes, const int32_t* row_ptr, const int32_t* col,
+                      const void* val, int32_t N, int32_t* level, int32_t* level_ptr,
+                      int32_t* permutation, int32_t* order, int32_t* new_row,
+                      int32_t* new_col, void* new_val);
+/* Row kernel used by the level-set and hybrid solves:
+ * src/parallel/src/sparse_opt_32.wat:11679-11757.  t = 0; t += L_ij*y_j over
+ * the off-diagonals in order; y_i = (b_i - t)/L_ii (diagonal stored last).
+ * Rows are solved in index order, which for a level-ordered matrix gives the
+ * same values as the level-by-level parallel solve (:11759-11980). */
+void or_spts_csr_f32(const int32_t* row_ptr, const int32_t* col, const float* val,
+                     const float* b, float* y, int32_t N);
+void or_spts_csr_f64(const int32_t* row_ptr, const int32_t* col, const double* val,
+                     const double* b, double* y, int32_t N);
+/* Sync-free order: src/parallel/src/spts_opt_32.wat:8-117.  t = b_i;
+ * t -= L_ij*y_j in order; y_i = t/L_ii. */
+void or_spts_syncfree_f32(const int32_t* row_ptr, const int32_t* col, const float* val,
+                          const float* b, float* y, int32_t N);
+void or_spts_syncfree_f64(const int32_t* row_ptr, const int32_t* col, const double* val,
+                          const double* b, double* y, int32_t N);
+/* Extended-precision truth solve (not a reference function). */
+void or_truth_spts(int val_bytes, const int32_t* row_ptr, const int32_t* col,
+                   const void* val, const void* b, double* y, int32_t N);
+/* Parallel level-set CPU baseline: level barrier + even row split per level
+ * (src/parallel/src/spts_opt_32.wat:339-546), on the level-reordered matrix. */
+void or_par_spts_level_f64(int nthreads, const int32_t* level_ptr, int32_t nlevels,
+                           const int32_t* row_ptr, const int32_t* col, const double* val,
+                           const double* b, double* y, int32_t N);
+void or_par_spts_level_f32(int nthreads, const int32_t* level_ptr, int32_t nlevels,
+                           const int32_t* row_ptr, const int32_t* col, const float* val,
+                           const float* b, float* y, int32_t N);
+
+/* ---------------- checksum ---------------- */
+/* fletcher_sum: src/sequential/src/sparse32.js:1286-1311 (matlab_modulo on
+ * doubles, 255 modulus, sum2*256 + sum1, parseInt). */
+int64_t or_fletcher_f32(const float* y, int64_t n);
+int64_t or_fletcher_f64(const double* y, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,116 @@
+"""ctypes binding of libsparse_b200.so (the C ABI declared in include/sparse_b200.h).
+
+The library is loaded from this package directory.  There is no fallback: if
+the shared object is missing, or a call returns an error status, the call
+raises.  Every array argument is a device pointer passed as an integer.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsparse_b200.so")
+
+P = C.c_void_p
+I32 = C.c_int32
+I64 = C.c_int64
+SZ = C.c_size_t
+
+SB_OK = 0
+SB_EINVAL = -1
+SB_ENOMEM = -2
+SB_EREFUSED = -3
+SB_ETIMEOUT = -4
+SB_ECUDA = -5
+SB_ENODEV = -6
+SB_EALIGN = -7
+
+SB_F32 = 0
+SB_F64 = 1
+SB_BF16 = 2
+
+# name -> argtypes (all functions return int status unless listed in _RESTYPE)
+SIGNATURES: dict[str, list] = {
+    "sb_version": [],
+    "sb_last_error": [],
+    "sb_status_string": [C.c_int],
+    "sb_device_count": [C.POINTER(C.c_int)],
+    "sb_set_device": [C.c_int],
+    "sb_malloc": [C.POINTER(P), SZ],
+    "sb_free": [P],
+    "sb_host_alloc": [C.POINTER(P), SZ],
+    "sb_host_free": [P],
+    "sb_memcpy_htod": [P, P, SZ, P],
+    "sb_memcpy_dtoh": [P, P, SZ, P],
+    "sb_memcpy_dtod": [P, P, SZ, P],
+    "sb_memset": [P, C.c_int, SZ, P],
+    "sb_stream_create": [C.POINTER(P)],
+    "sb_stream_destroy": [P],
+    "sb_stream_synchronize": [P],
+    "sb_mem_info": [C.POINTER(SZ), C.POINTER(SZ)],
+    "sb_spmv_coo": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
+    "sb_spmv_csr": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
+    "sb_spmv_dia": [C.c_int, P, P, I32, I32, I32, P, P, I32, P],
+    "sb_spmv_ell": [C.c_int, P, P, I32, I32, P, P, I32, P],
+}
+_RESTYPE = {"sb_last_error": C.c_char_p, "sb_status_string": C.c_char_p}
+
+
+class SparseError(RuntimeError):
+    """A libsparse_b200 call returned a negative status."""
+
+    def __init__(self, fn: str, status: int, message: str):
+        super().__init__(f"{fn} failed with status {status}: {message}")
+        self.fn = fn
+        self.status = status
+
+
+class RefusedError(SparseError):
+    """The format admission test of csr_ell / csr_dia refused the matrix."""
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load() -> C.CDLL:
+    """Load the shared object (once) and attach signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m sciwasm.sparse_b200.build` "
+                "(the CUDA path has no CPU fallback)")
+        lib = C.CDLL(LIB_PATH)
+        for name, argtypes in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = argtypes
+            fn.restype = _RESTYPE.get(name, C.c_int)
+        _lib = lib
+        return lib
+
+
+def declared_symbols() -> list[str]:
+    return list(SIGNATURES)
+
+
+def call(name: str, *args) -> int:
+    """Call `name`; raise SparseError on a negative status, return the status."""
+    lib = load()
+    st = getattr(lib, name)(*args)
+    if st < 0:
+        msg = (lib.sb_last_error() or b"").decode(errors="replace")
+        if st == SB_EREFUSED:
+            raise RefusedError(name, st, msg)
+        raise SparseError(name, st, msg)
+    return st
+
+
+def last_error() -> str:
+    return (load().sb_last_error() or b"").decode(errors="replace")

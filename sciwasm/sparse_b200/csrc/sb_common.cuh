@@ -1,0 +1,129 @@
+// sb_common.cuh -- shared helpers of libsparse_b200.so: status handling,
+// dtype dispatch, streaming-load intrinsics and launch sizing for sm_100a.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdarg.h>
+
+#include "sparse_b200.h"
+
+namespace sb {
+
+// ---------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+int cuda_status(cudaError_t e, const char* what);
+int ensure_device();  // SB_OK when a CUDA device is usable, else SB_ENODEV
+
+#define SB_CHECK_CUDA(call)                                   \
+  do {                                                        \
+    cudaError_t e__ = (call);                                 \
+    if (e__ != cudaSuccess) return ::sb::cuda_status(e__, #call); \
+  } while (0)
+
+#define SB_REQUIRE(cond, ...)                                 \
+  do {                                                        \
+    if (!(cond)) {                                            \
+      ::sb::set_error(__VA_ARGS__);                           \
+      return SB_EINVAL;                                       \
+    }                                                         \
+  } while (0)
+
+// Launch check: a failed launch reports SB_ECUDA with the kernel name.
+#define SB_CHECK_LAUNCH(name) SB_CHECK_CUDA(cudaGetLastError())
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Number of SMs of the current device (148 on B200), cached per device.
+int sm_count();
+
+// Scratch allocation ordered on a stream (stream-ordered pool).
+int scratch_alloc(void** p, size_t bytes, cudaStream_t s);
+void scratch_free(void* p, cudaStream_t s);
+
+// ---------------------------------------------------------------- loads
+// Streaming loads for matrix arrays that are read exactly once per call: do
+// not allocate in L1 (keep L1 for the gathered x) and tag the L2 lines
+// evict-first through an L2 cache policy.
+__device__ __forceinline__ uint64_t evict_first_policy() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ int4 ld_stream_v4(const int* p) {
+  int4 r;
+  const uint64_t pol = evict_first_policy();
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(p), "l"(pol));
+  return r;
+}
+__device__ __forceinline__ int ld_stream(const int* p) {
+  int r;
+  const uint64_t pol = evict_first_policy();
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
+               : "=r"(r) : "l"(p), "l"(pol));
+  return r;
+}
+__device__ __forceinline__ float4 ld_stream_v4(const float* p) {
+  float4 r;
+  const uint64_t pol = evict_first_policy();
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+               : "l"(p), "l"(pol));
+  return r;
+}
+__device__ __forceinline__ float ld_stream(const float* p) {
+  float r;
+  const uint64_t pol = evict_first_policy();
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;"
+               : "=f"(r) : "l"(p), "l"(pol));
+  return r;
+}
+__device__ __forceinline__ double2 ld_stream_v2(const double* p) {
+  double2 r;
+  const uint64_t pol = evict_first_policy();
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;"
+               : "=d"(r.x), "=d"(r.y)
+               : "l"(p), "l"(pol));
+  return r;
+}
+__device__ __forceinline__ double ld_stream(const double* p) {
+  double r;
+  const uint64_t pol = evict_first_policy();
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;"
+               : "=d"(r) : "l"(p), "l"(pol));
+  return r;
+}
+__device__ __forceinline__ unsigned short ld_stream(const unsigned short* p) {
+  unsigned short r;
+  const uint64_t pol = evict_first_policy();
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;"
+               : "=h"(r) : "l"(p), "l"(pol));
+  return r;
+}
+__device__ __forceinline__ uint2 ld_stream_v4(const unsigned short* p) {
+  uint2 r;
+  const uint64_t pol = evict_first_policy();
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
+               : "=r"(r.x), "=r"(r.y)
+               : "l"(p), "l"(pol));
+  return r;
+}
+
+// Read-only cached load (x vectors: reused across rows).
+template <typename T>
+__device__ __forceinline__ T ld_ro(const T* p) {
+  return __ldg(p);
+}
+
+// Value-type traits: storage type S, accumulation type A.
+template <int DT> struct vt;
+template <> struct vt<SB_F32> { using S = float; using A = float; };
+template <> struct vt<SB_F64> { using S = double; using A = double; };
+
+inline size_t dtype_size(int dt) { return dt == SB_F64 ? 8 : (dt == SB_F32 ? 4 : 2); }
+
+}  // namespace sb

@@ -1,0 +1,194 @@
+// sb_runtime.cu -- device memory, streams and error reporting of the C ABI.
+// Stands in for MatMachJS's _malloc/_free over wasm linear memory
+// (src/sequential/libs/matmachjs.wat:46-48) with device memory.
+#include <mutex>
+#include <string.h>
+
+#include "sb_common.cuh"
+
+namespace sb {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+  set_error("%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+  if (e == cudaErrorMemoryAllocation) return SB_ENOMEM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return SB_ENODEV;
+  return SB_ECUDA;
+}
+
+int ensure_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device available (%s)", e == cudaSuccess ? "count 0" : cudaGetErrorString(e));
+    return SB_ENODEV;
+  }
+  return SB_OK;
+}
+
+int sm_count() {
+  static int cache[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 148;
+  if (cache[dev] == 0) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cache[dev] = n > 0 ? n : 148;
+  }
+  return cache[dev];
+}
+
+int scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMallocAsync(p, bytes, s);
+  if (e != cudaSuccess) return cuda_status(e, "cudaMallocAsync(scratch)");
+  return SB_OK;
+}
+
+void scratch_free(void* p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
+}  // namespace sb
+
+using namespace sb;
+
+extern "C" {
+
+int sb_version(void) { return 10000; }
+
+const char* sb_last_error(void) { return g_err; }
+
+const char* sb_status_string(int s) {
+  switch (s) {
+    case SB_OK: return "ok";
+    case SB_EINVAL: return "invalid argument";
+    case SB_ENOMEM: return "out of device memory";
+    case SB_EREFUSED: return "refused by the format admission test";
+    case SB_ETIMEOUT: return "bounded device wait timed out";
+    case SB_ECUDA: return "CUDA error";
+    case SB_ENODEV: return "no CUDA device";
+    case SB_EALIGN: return "misaligned pointer";
+    default: return "unknown status";
+  }
+}
+
+int sb_device_count(int* count) {
+  SB_REQUIRE(count, "sb_device_count: null output");
+  *count = 0;
+  cudaError_t e = cudaGetDeviceCount(count);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *count = 0;
+  }
+  return SB_OK;
+}
+
+int sb_set_device(int device) {
+  int r = ensure_device();
+  if (r) return r;
+  SB_CHECK_CUDA(cudaSetDevice(device));
+  return SB_OK;
+}
+
+int sb_malloc(void** ptr, size_t bytes) {
+  SB_REQUIRE(ptr, "sb_malloc: null output");
+  *ptr = nullptr;
+  int r = ensure_device();
+  if (r) return r;
+  if (bytes == 0) bytes = 16;
+  SB_CHECK_CUDA(cudaMalloc(ptr, bytes));
+  return SB_OK;
+}
+
+int sb_free(void* ptr) {
+  if (!ptr) return SB_OK;
+  SB_CHECK_CUDA(cudaFree(ptr));
+  return SB_OK;
+}
+
+int sb_host_alloc(void** ptr, size_t bytes) {
+  SB_REQUIRE(ptr, "sb_host_alloc: null output");
+  *ptr = nullptr;
+  int r = ensure_device();
+  if (r) return r;
+  if (bytes == 0) bytes = 16;
+  SB_CHECK_CUDA(cudaMallocHost(ptr, bytes));
+  return SB_OK;
+}
+
+int sb_host_free(void* ptr) {
+  if (!ptr) return SB_OK;
+  SB_CHECK_CUDA(cudaFreeHost(ptr));
+  return SB_OK;
+}
+
+int sb_memcpy_htod(void* dst, const void* src, size_t bytes, void* stream) {
+  if (bytes == 0) return SB_OK;
+  SB_REQUIRE(dst && src, "sb_memcpy_htod: null pointer");
+  SB_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, as_stream(stream)));
+  return SB_OK;
+}
+
+int sb_memcpy_dtoh(void* dst, const void* src, size_t bytes, void* stream) {
+  if (bytes == 0) return SB_OK;
+  SB_REQUIRE(dst && src, "sb_memcpy_dtoh: null pointer");
+  SB_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, as_stream(stream)));
+  return SB_OK;
+}
+
+int sb_memcpy_dtod(void* dst, const void* src, size_t bytes, void* stream) {
+  if (bytes == 0) return SB_OK;
+  SB_REQUIRE(dst && src, "sb_memcpy_dtod: null pointer");
+  SB_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, as_stream(stream)));
+  return SB_OK;
+}
+
+int sb_memset(void* dst, int value, size_t bytes, void* stream) {
+  if (bytes == 0) return SB_OK;
+  SB_REQUIRE(dst, "sb_memset: null pointer");
+  SB_CHECK_CUDA(cudaMemsetAsync(dst, value, bytes, as_stream(stream)));
+  return SB_OK;
+}
+
+int sb_stream_create(void** stream) {
+  SB_REQUIRE(stream, "sb_stream_create: null output");
+  int r = ensure_device();
+  if (r) return r;
+  cudaStream_t s;
+  SB_CHECK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  *stream = reinterpret_cast<void*>(s);
+  return SB_OK;
+}
+
+int sb_stream_destroy(void* stream) {
+  if (!stream) return SB_OK;
+  SB_CHECK_CUDA(cudaStreamDestroy(as_stream(stream)));
+  return SB_OK;
+}
+
+int sb_stream_synchronize(void* stream) {
+  SB_CHECK_CUDA(cudaStreamSynchronize(as_stream(stream)));
+  return SB_OK;
+}
+
+int sb_mem_info(size_t* free_bytes, size_t* total_bytes) {
+  SB_REQUIRE(free_bytes && total_bytes, "sb_mem_info: null output");
+  int r = ensure_device();
+  if (r) return r;
+  SB_CHECK_CUDA(cudaMemGetInfo(free_bytes, total_bytes));
+  return SB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,358 @@
+"""Host mirror of SciWasm.Sparse's JavaScript API over libsparse_b200.so.
+
+The reference module (src/sequential/src/sparse32.js, f64 twin sparse64.js)
+keeps matrices as typed arrays in wasm linear memory and exposes
+`spmv(A, x, y, inner_max)`, `coo_csr`, `csr_dia`, `csr_ell`, `transpose`,
+`eliminate_zeros`, the element-wise maps, `create_vec`, `free`, ...  This
+module keeps those names and object shapes (`sparse_COO_t`, `sparse_CSR_t`,
+`sparse_DIA_t`, `sparse_ELL_t`, `sparse_vec_t`), but the arrays live in
+device memory (HBM) and every operation is a CUDA kernel of
+libsparse_b200.so.  There is no CPU compute path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import call
+
+_DT_CODE = {np.dtype(np.float32): _lib.SB_F32, np.dtype(np.float64): _lib.SB_F64}
+
+
+def _dtcode(dtype) -> int:
+    dt = np.dtype(dtype)
+    if dt not in _DT_CODE:
+        raise TypeError(f"value dtype must be float32 or float64, got {dt}")
+    return _DT_CODE[dt]
+
+
+def _sp(stream) -> Optional[int]:
+    return None if stream is None else int(stream)
+
+
+class DeviceArray:
+    """A 1-D array in device memory (the stand-in for a wasm-heap block)."""
+
+    __slots__ = ("n", "dtype", "nbytes", "ptr", "_owned")
+
+    def __init__(self, n: int, dtype, ptr: Optional[int] = None):
+        self.n = int(n)
+        self.dtype = np.dtype(dtype)
+        self.nbytes = self.n * self.dtype.itemsize
+        if ptr is None:
+            p = C.c_void_p()
+            call("sb_malloc", C.byref(p), max(self.nbytes, 16))
+            self.ptr = int(p.value)
+            self._owned = True
+        else:
+            self.ptr = int(ptr)
+            self._owned = False
+
+    @classmethod
+    def from_host(cls, arr, dtype=None, stream=None) -> "DeviceArray":
+        a = np.ascontiguousarray(arr, dtype=dtype)
+        d = cls(a.size, a.dtype)
+        d.upload(a, stream)
+        return d
+
+    def upload(self, arr, stream=None) -> None:
+        a = np.ascontiguousarray(arr, dtype=self.dtype)
+        if a.size != self.n:
+            raise ValueError(f"upload of {a.size} elements into an array of {self.n}")
+        if self.nbytes:
+            call("sb_memcpy_htod", self.ptr, a.ctypes.data, self.nbytes, _sp(stream))
+            call("sb_stream_synchronize", _sp(stream))
+
+    def to_host(self, stream=None) -> np.ndarray:
+        out = np.empty(self.n, dtype=self.dtype)
+        if self.nbytes:
+            call("sb_memcpy_dtoh", out.ctypes.data, self.ptr, self.nbytes, _sp(stream))
+            call("sb_stream_synchronize", _sp(stream))
+        return out
+
+    def fill_zero(self, stream=None) -> None:
+        if self.nbytes:
+            call("sb_memset", self.ptr, 0, self.nbytes, _sp(stream))
+
+    def free(self) -> None:
+        if self._owned and self.ptr:
+            try:
+                _lib.load().sb_free(self.ptr)
+            except Exception:
+                pass
+        self.ptr = 0
+        self._owned = False
+
+    def __del__(self):
+        self.free()
+
+
+# --------------------------------------------------------------- objects
+# Shapes follow src/sequential/src/sparse32.js:29-198.
+
+
+class sparse_COO_t:
+    """COO matrix: row_index / col_index / val_index arrays of nnz entries."""
+
+    def __init__(self, row_index, col_index, val_index, N, nnz):
+        self.row_index, self.col_index, self.val_index = row_index, col_index, val_index
+        self.N, self.nnz = int(N), int(nnz)
+
+    @property
+    def dtype(self):
+        return self.val_index.dtype
+
+    def row_array(self):
+        return self.row_index.to_host()
+
+    def col_array(self):
+        return self.col_index.to_host()
+
+    def val_array(self):
+        return self.val_index.to_host()
+
+
+class sparse_CSR_t:
+    """CSR matrix: row_index (N+1), col_index / val_index (nnz)."""
+
+    def __init__(self, row_index, col_index, val_index, N, nnz):
+        self.row_index, self.col_index, self.val_index = row_index, col_index, val_index
+        self.N, self.nnz = int(N), int(nnz)
+
+    @property
+    def dtype(self):
+        return self.val_index.dtype
+
+    def row_array(self):
+        return self.row_index.to_host()
+
+    def col_array(self):
+        return self.col_index.to_host()
+
+    def val_array(self):
+        return self.val_index.to_host()
+
+
+class sparse_DIA_t:
+    """DIA matrix: offset_index (ndiags), data_index (ndiags*stride), stride N."""
+
+    def __init__(self, offset_index, data_index, ndiags, stride, N, nnz):
+        self.offset_index, self.data_index = offset_index, data_index
+        self.ndiags, self.stride, self.N, self.nnz = int(ndiags), int(stride), int(N), int(nnz)
+
+    @property
+    def dtype(self):
+        return self.data_index.dtype
+
+    def offset_array(self):
+        return self.offset_index.to_host()
+
+    def data_array(self):
+        return self.data_index.to_host()
+
+
+class sparse_ELL_t:
+    """ELL matrix: column-major indices_index / data_index of ncols*N slots."""
+
+    def __init__(self, indices_index, data_index, ncols, N, nnz):
+        self.indices_index, self.data_index = indices_index, data_index
+        self.ncols, self.N, self.nnz = int(ncols), int(N), int(nnz)
+
+    @property
+    def dtype(self):
+        return self.data_index.dtype
+
+    def indices_array(self):
+        return self.indices_index.to_host()
+
+    def data_array(self):
+        return self.data_index.to_host()
+
+
+class sparse_vec_t:
+    """Dense vector of vec_nelem values."""
+
+    def __init__(self, vec_index, vec_nelem):
+        self.vec_index = vec_index
+        self.vec_nelem = int(vec_nelem)
+
+    @property
+    def dtype(self):
+        return self.vec_index.dtype
+
+    def array(self):
+        return self.vec_index.to_host()
+
+    def size(self):
+        return self.vec_nelem
+
+
+# --------------------------------------------------------------- allocation
+# allocate_*: src/sequential/src/sparse32.js:2174-2395.
+
+
+def allocate_COO(N, nnz, dtype=np.float32):
+    return sparse_COO_t(DeviceArray(nnz, np.int32), DeviceArray(nnz, np.int32),
+                        DeviceArray(nnz, dtype), N, nnz)
+
+
+def allocate_CSR(N, nnz, dtype=np.float32):
+    return sparse_CSR_t(DeviceArray(N + 1, np.int32), DeviceArray(nnz, np.int32),
+                        DeviceArray(nnz, dtype), N, nnz)
+
+
+def allocate_DIA(N, nnz, ndiags, stride, dtype=np.float32):
+    return sparse_DIA_t(DeviceArray(ndiags, np.int32), DeviceArray(ndiags * stride, dtype),
+                        ndiags, stride, N, nnz)
+
+
+def allocate_ELL(N, nnz, ncols, dtype=np.float32):
+    return sparse_ELL_t(DeviceArray(ncols * N, np.int32), DeviceArray(ncols * N, dtype),
+                        ncols, N, nnz)
+
+
+def create_vec(nelem, val=0, dtype=np.float32):
+    """create_vec (src/sequential/src/sparse32.js:2371-2379)."""
+    v = sparse_vec_t(DeviceArray(nelem, dtype), nelem)
+    if val == 0:
+        v.vec_index.fill_zero()
+    else:
+        v.vec_index.upload(np.full(nelem, val, dtype=dtype))
+    return v
+
+
+def vec_from_host(arr, dtype=None):
+    a = np.ascontiguousarray(arr, dtype=dtype)
+    return sparse_vec_t(DeviceArray.from_host(a), a.size)
+
+
+def _check_indices(name, idx, N):
+    if idx.size and (idx.min() < 0 or idx.max() >= N):
+        raise ValueError(f"{name} index outside [0, {N})")
+
+
+def coo_from_host(row, col, val, N, dtype=None):
+    """Upload a COO matrix; indices are validated on the host first."""
+    row = np.ascontiguousarray(row, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=dtype if dtype is not None else None)
+    _dtcode(val.dtype)
+    if not (row.size == col.size == val.size):
+        raise ValueError("row, col and val must have the same length")
+    _check_indices("row", row, N)
+    _check_indices("col", col, N)
+    return sparse_COO_t(DeviceArray.from_host(row), DeviceArray.from_host(col),
+                        DeviceArray.from_host(val), N, row.size)
+
+
+def csr_from_host(row_ptr, col, val, dtype=None):
+    """Upload a CSR matrix after checking row_ptr monotonicity and col range."""
+    row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=dtype if dtype is not None else None)
+    _dtcode(val.dtype)
+    N = row_ptr.size - 1
+    if N < 0 or row_ptr[0] != 0 or row_ptr[-1] != col.size or col.size != val.size:
+        raise ValueError("inconsistent CSR arrays")
+    if N and np.any(np.diff(row_ptr) < 0):
+        raise ValueError("row_ptr must be non-decreasing")
+    _check_indices("col", col, N)
+    return sparse_CSR_t(DeviceArray.from_host(row_ptr), DeviceArray.from_host(col),
+                        DeviceArray.from_host(val), N, col.size)
+
+
+def dia_from_host(offset, data, N, nnz=None):
+    offset = np.ascontiguousarray(offset, dtype=np.int32)
+    data = np.ascontiguousarray(data)
+    _dtcode(data.dtype)
+    nd = offset.size
+    if data.size != nd * N:
+        raise ValueError("DIA data must hold ndiags*N values (stride N)")
+    if nd and (offset.min() <= -N or offset.max() >= N):
+        raise ValueError("DIA offset outside (-N, N)")
+    return sparse_DIA_t(DeviceArray.from_host(offset), DeviceArray.from_host(data), nd, N, N,
+                        nnz if nnz is not None else int(np.count_nonzero(data)))
+
+
+def ell_from_host(indices, data, ncols, N, nnz=None):
+    indices = np.ascontiguousarray(indices, dtype=np.int32)
+    data = np.ascontiguousarray(data)
+    _dtcode(data.dtype)
+    if indices.size != ncols * N or data.size != ncols * N:
+        raise ValueError("ELL arrays must hold ncols*N slots")
+    _check_indices("ELL", indices, N)
+    return sparse_ELL_t(DeviceArray.from_host(indices), DeviceArray.from_host(data), ncols, N,
+                        nnz if nnz is not None else int(np.count_nonzero(data)))
+
+
+def free(obj) -> None:
+    """free (src/sequential/src/sparse32.js:2204-2231)."""
+    if obj is None:
+        return
+    for name in ("row_index", "col_index", "val_index", "offset_index", "data_index",
+                 "indices_index", "vec_index"):
+        arr = getattr(obj, name, None)
+        if isinstance(arr, DeviceArray):
+            arr.free()
+
+
+# --------------------------------------------------------------- SpMV
+
+
+def spmv(A, x_view, y_view, inner_max=1, stream=None):
+    """y <- y + A x, inner_max times (src/sequential/src/sparse32.js:1232-1286).
+
+    Returns None like the reference; raises for an undefined matrix instead of
+    logging (the reference prints "spmv input : undefined" and returns)."""
+    if A is None:
+        raise ValueError("spmv input : undefined")
+    if x_view.dtype != A.dtype or y_view.dtype != A.dtype:
+        raise TypeError("x, y and A must share one value dtype")
+    if x_view.vec_nelem < A.N or y_view.vec_nelem < A.N:
+        raise ValueError("x and y must hold N values")
+    dt = _dtcode(A.dtype)
+    s = _sp(stream)
+    x, y = x_view.vec_index.ptr, y_view.vec_index.ptr
+    if isinstance(A, sparse_COO_t):
+        call("sb_spmv_coo", dt, A.row_index.ptr, A.col_index.ptr, A.val_index.ptr, x, y, A.N,
+             A.nnz, inner_max, s)
+    elif isinstance(A, sparse_CSR_t):
+        call("sb_spmv_csr", dt, A.row_index.ptr, A.col_index.ptr, A.val_index.ptr, x, y, A.N,
+             A.nnz, inner_max, s)
+    elif isinstance(A, sparse_DIA_t):
+        call("sb_spmv_dia", dt, A.offset_index.ptr, A.data_index.ptr, A.N, A.ndiags, A.stride, x,
+             y, inner_max, s)
+    elif isinstance(A, sparse_ELL_t):
+        call("sb_spmv_ell", dt, A.indices_index.ptr, A.data_index.ptr, A.N, A.ncols, x, y,
+             inner_max, s)
+    else:
+        raise TypeError(f"spmv: unsupported matrix object {type(A).__name__}")
+
+
+def synchronize(stream=None) -> None:
+    call("sb_stream_synchronize", _sp(stream))
+
+
+# --------------------------------------------------------------- checksum
+
+
+def fletcher_sum(a) -> int:
+    """fletcher_sum (src/sequential/src/sparse32.js:1291-1304) on host values:
+    sum1 = (sum1 + a_i) mod 255, sum2 = (sum2 + sum1) mod 255 with a floored
+    modulo on doubles; result parseInt(sum2*256 + sum1)."""
+    s1 = 0.0
+    s2 = 0.0
+    for v in np.asarray(a, dtype=np.float64).tolist():
+        t = s1 + v
+        s1 = t - np.floor(t / 255.0) * 255.0
+        t = s2 + s1
+        s2 = t - np.floor(t / 255.0) * 255.0
+    return int(s2 * 256.0 + s1)
+
+
+def fletcher_sum_y(y_view) -> int:
+    """fletcher_sum_y (src/sequential/src/sparse32.js:1306-1311)."""
+    return fletcher_sum(y_view.array())
