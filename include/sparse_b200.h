@@ -66,6 +66,9 @@ int sb_stream_create(void** stream);
 int sb_stream_destroy(void* stream);
 int sb_stream_synchronize(void* stream);
 int sb_mem_info(size_t* free_bytes, size_t* total_bytes);
+/* Synchronises the device, returns and clears its status word: 0, or the code
+ * of a kernel whose bounded wait gave up (1 = bulk copy, 2 = dependency). */
+int sb_device_status(int* code);
 
 /* ---------------------------------------------------------------------- */
 /* SpMV: y <- y + A x, repeated inner_max times (the *_wrapper exports).   */

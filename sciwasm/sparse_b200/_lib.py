@@ -50,6 +50,7 @@ SIGNATURES: dict[str, list] = {
     "sb_stream_destroy": [P],
     "sb_stream_synchronize": [P],
     "sb_mem_info": [C.POINTER(SZ), C.POINTER(SZ)],
+    "sb_device_status": [C.POINTER(C.c_int)],
     "sb_spmv_coo": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
     "sb_spmv_csr": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
     "sb_spmv_dia": [C.c_int, P, P, I32, I32, I32, P, P, I32, P],

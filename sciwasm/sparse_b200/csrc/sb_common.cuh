@@ -39,6 +39,10 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // Number of SMs of the current device (148 on B200), cached per device.
 int sm_count();
 
+// Per-device status word (device pointer) that kernels set on a bounded-wait
+// timeout; read and cleared by sb_device_status().
+int* device_status_word();
+
 // Scratch allocation ordered on a stream (stream-ordered pool).
 int scratch_alloc(void** p, size_t bytes, cudaStream_t s);
 void scratch_free(void* p, cudaStream_t s);
@@ -118,6 +122,60 @@ template <typename T>
 __device__ __forceinline__ T ld_ro(const T* p) {
   return __ldg(p);
 }
+
+// ---------------------------------------------------------------- async copy
+// Bulk (non-tensor) async copies global -> shared completed on an mbarrier.
+// Only this GPU's own memory is read and no multicast form is used.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after ~2^31 SM cycles (about a second) and returns
+// false so that the caller can record an error status and leave.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > (1LL << 31)) return false;
+  }
+  return true;
+}
+
+// Device status codes written by kernels whose bounded waits ran out.
+#define SB_DEV_OK 0
+#define SB_DEV_TIMEOUT_BULK 1
+#define SB_DEV_TIMEOUT_DEP 2
 
 // Value-type traits: storage type S, accumulation type A.
 template <int DT> struct vt;

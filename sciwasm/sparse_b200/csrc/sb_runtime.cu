@@ -48,6 +48,25 @@ int sm_count() {
   return cache[dev];
 }
 
+int* device_status_word() {
+  static std::mutex mu;
+  static int* words[64] = {nullptr};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!words[dev]) {
+    int* p = nullptr;
+    if (cudaMalloc(&p, 64) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    cudaMemset(p, 0, 64);
+    words[dev] = p;
+  }
+  return words[dev];
+}
+
 int scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
   *p = nullptr;
   if (bytes == 0) bytes = 16;
@@ -180,6 +199,19 @@ int sb_stream_destroy(void* stream) {
 
 int sb_stream_synchronize(void* stream) {
   SB_CHECK_CUDA(cudaStreamSynchronize(as_stream(stream)));
+  return SB_OK;
+}
+
+int sb_device_status(int* code) {
+  SB_REQUIRE(code, "sb_device_status: null output");
+  *code = 0;
+  int r = ensure_device();
+  if (r) return r;
+  int* w = device_status_word();
+  if (!w) return SB_OK;
+  SB_CHECK_CUDA(cudaDeviceSynchronize());
+  SB_CHECK_CUDA(cudaMemcpy(code, w, sizeof(int), cudaMemcpyDeviceToHost));
+  SB_CHECK_CUDA(cudaMemset(w, 0, sizeof(int)));
   return SB_OK;
 }
 

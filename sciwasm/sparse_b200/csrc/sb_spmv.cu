@@ -4,43 +4,53 @@
 // src/sequential/src/sparse_opt_64.wat:187-515 (f64).  The reference walks
 // storage order on one core (or splits rows / nnz over Web Workers,
 // src/parallel/src/sparse32.js:2637-2821).  Here:
-//   * CSR is a merge-path kernel: every warp consumes a fixed number of
-//     (row-end + nonzero) merge items, so rows of any length distribution
-//     give equal work per warp; col/val are streamed with 128-bit loads into
-//     shared memory and reduced with a per-lane walk plus a warp segmented
-//     scan (rows per warp adapt to the row lengths by construction).
+//   * CSR (default) is a row-block kernel: a warp owns 32 consecutive rows,
+//     reduces the short ones V lanes per row (V from the mean row length:
+//     adaptive rows per warp) with unrolled independent loads and shuffle
+//     reductions, and the long ones with the whole warp.  An alternative
+//     streams fixed-size nonzero tiles into a shared-memory ring with bulk
+//     async copies (SB_CSR_KERNEL=s).
 //   * COO is the same tile scheme keyed on the row array; every row segment
 //     is added with one atomic, so unsorted input is accepted.
 //   * DIA and ELL assign one row per thread and keep the reference's per-row
 //     addition order (separately rounded mul and add), so their results are
 //     bit-identical to the reference's serial loops.
 #include <algorithm>
+#include <stdlib.h>
 
 #include "sb_common.cuh"
 
 namespace sb {
 
 constexpr int kWarp = 32;
-constexpr int kItems = 8;                  // merge items per lane per tile
-constexpr int kTile = kWarp * kItems;      // 256 merge items per warp tile
-constexpr int kPadTile = kTile + kTile / 8;
-constexpr int kReCap = kTile + kWarp;      // row-end staging capacity
+constexpr int kItems = 8;                  // COO items per lane per tile
+constexpr int kTile = kWarp * kItems;      // 256 COO items per warp tile
 constexpr int kWarpsPerCta = 8;
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ int pad8(int i) { return i + (i >> 3); }
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+template <typename K>
+static int resident_ctas(K kernel, int threads) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  if (per_sm < 1) per_sm = 1;
+  return per_sm * sm_count();
+}
 
 // ------------------------------------------------------------ CSR (merge)
 
-// Smallest a in [0, N] with a == N or a + row_ptr[a+1] >= D: the number of
-// row-end markers among the first D merge items.  32-ary search by a warp.
-__device__ __forceinline__ int merge_search(const int* __restrict__ row_ptr, int N, long long D,
-                                            int lane) {
+// ------------------------------------------------------------ CSR (stream)
+
+// Smallest a in [0, N] with a == N or row_ptr[a+1] > b: the row holding
+// nonzero b (rows ending at or before b are skipped).  32-ary warp search.
+__device__ __forceinline__ int row_of_item(const int* __restrict__ row_ptr, int N, long long b,
+                                           int lane) {
   int lo = 0, hi = N;
   while (hi - lo > kWarp) {
     int step = (hi - lo) / kWarp;
     int p = lo + lane * step;
-    bool pred = ((long long)p + __ldg(row_ptr + p + 1)) >= D;
+    bool pred = (long long)__ldg(row_ptr + p + 1) > b;
     unsigned m = __ballot_sync(kFull, pred);
     if (m == 0) {
       lo = lo + (kWarp - 1) * step + 1;
@@ -51,161 +61,330 @@ __device__ __forceinline__ int merge_search(const int* __restrict__ row_ptr, int
     }
   }
   int p = lo + lane;
-  bool pred = (p >= hi) || (((long long)p + __ldg(row_ptr + p + 1)) >= D);
+  bool pred = (p >= hi) || ((long long)__ldg(row_ptr + p + 1) > b);
   unsigned m = __ballot_sync(kFull, pred);
   return lo + __ffs(m) - 1;
 }
 
-template <typename S, typename A>
-__device__ __forceinline__ void emit_row(S* __restrict__ y, int r, int rs, int re, long long b0,
-                                         A p) {
-  if (re <= rs) return;                 // empty row: y untouched (reference :243)
-  if ((long long)re <= b0) return;      // no items of this row in this tile
-  if ((long long)rs >= b0) {
-    y[r] = (S)((A)y[r] + p);            // whole row inside this tile: exclusive
+constexpr int kStreamThreads = 256;
+template <typename S, int T, int STAGES>
+struct CsrStreamSmem {
+  int col[STAGES][T];
+  S val[STAGES][T];  // values, overwritten in place by the products
+  int re[2][kStreamThreads];
+  S ys[2][kStreamThreads];  // y of the chunk's rows, prefetched
+  // (row, lo, hi, atomic) of rows left to whole warps: a deferred row holds
+  // more than 16 items, so at most T/17 of them fit in one tile
+  int4 lrow[2][T / 16 + 2];
+  uint64_t bar[STAGES];
+  int lcount[2];
+  int rfirst;
+};
+
+// Products of 4 consecutive staged items (col int4, values as 16-byte words).
+template <typename S>
+__device__ __forceinline__ void prod4(int* pc, S* pv, const S* __restrict__ x) {
+  const int4 c = *reinterpret_cast<const int4*>(pc);
+  if constexpr (sizeof(S) == 8) {
+    double2 v0 = reinterpret_cast<const double2*>(pv)[0];
+    double2 v1 = reinterpret_cast<const double2*>(pv)[1];
+    v0.x *= ld_ro(x + c.x);
+    v0.y *= ld_ro(x + c.y);
+    v1.x *= ld_ro(x + c.z);
+    v1.y *= ld_ro(x + c.w);
+    reinterpret_cast<double2*>(pv)[0] = v0;
+    reinterpret_cast<double2*>(pv)[1] = v1;
   } else {
-    atomicAdd(y + r, (S)p);             // row continues from an earlier tile
+    float4 v = *reinterpret_cast<const float4*>(pv);
+    v.x *= ld_ro(x + c.x);
+    v.y *= ld_ro(x + c.y);
+    v.z *= ld_ro(x + c.z);
+    v.w *= ld_ro(x + c.w);
+    *reinterpret_cast<float4*>(pv) = v;
   }
 }
 
-template <typename S, typename A, bool VEC>
-__global__ void __launch_bounds__(kWarpsPerCta * kWarp)
-    csr_merge_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
-                     const S* __restrict__ val, const S* __restrict__ x, S* __restrict__ y,
-                     int N, long long total, long long ntiles, long long tiles_per_warp) {
-  __shared__ A s_prod[kWarpsPerCta][kPadTile];
-  __shared__ int s_re[kWarpsPerCta][kReCap];
-  const int lane = threadIdx.x & (kWarp - 1);
-  const int wib = threadIdx.x >> 5;
-  A* prod = s_prod[wib];
-  int* re = s_re[wib];
-  const long long gw = (long long)blockIdx.x * kWarpsPerCta + wib;
-  long long tile = gw * tiles_per_warp;
-  const long long tile_end = min(tile + tiles_per_warp, ntiles);
-  if (tile >= tile_end) return;
+// Streaming CSR: a persistent CTA walks a contiguous range of T-nonzero
+// tiles through a STAGES-deep shared-memory ring.  One elected thread keeps
+// STAGES-1 tiles of col/val in flight with bulk async copies completed on
+// per-stage mbarriers, while the CTA multiplies the current tile (x gathers,
+// 4 items per thread per pass) and reduces its rows with groups of V lanes,
+// V = 256 / next_pow2(rows in the tile) capped at a warp (adaptive rows per
+// CTA), warp-shuffle reductions inside each group.  A row much longer than
+// its group's share is deferred to a whole warp.  Rows wholly inside a tile
+// are written with a plain y += sum (y prefetched with the row ends); rows cut
+// by a tile boundary are added atomically.
+template <typename S, int T, int STAGES>
+__global__ void __launch_bounds__(kStreamThreads)
+    csr_stream_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
+                      const S* __restrict__ val, const S* __restrict__ x, S* __restrict__ y,
+                      int N, long long nnz, long long ntiles, long long tpc, int* status) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  CsrStreamSmem<S, T, STAGES>& sm = *reinterpret_cast<CsrStreamSmem<S, T, STAGES>*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int lane = tid & (kWarp - 1);
+  const int warp = tid >> 5;
+  const long long t0 = (long long)blockIdx.x * tpc;
+  const long long t_end = min(t0 + tpc, ntiles);
+  if (t0 >= t_end) return;
+  const int ntile = (int)(t_end - t0);
 
-  long long D0 = tile * kTile;
-  int a0 = merge_search(row_ptr, N, D0, lane);
-  long long b0 = D0 - a0;
-
-  for (; tile < tile_end; ++tile) {
-    const long long D1 = min(D0 + kTile, total);
-    // ---- rows whose end marker falls inside this tile
-    int nr = 0;
-    while (true) {
-      int r = a0 + nr + lane;
-      int e = (r < N) ? __ldg(row_ptr + r + 1) : 0x7fffffff;
-      bool f = (r < N) && ((long long)r + e < D1);
-      if (nr + lane < kReCap) re[nr + lane] = e;
-      unsigned m = __ballot_sync(kFull, f);
-      int c = __popc(m);
-      nr += c;
-      if (c < kWarp) break;
+  auto issue = [&](long long tt, int st) {
+    const long long b0 = tt * T;
+    const int n = (int)min((long long)T, nnz - b0);
+    const int nal = n & ~3;
+    mbar_expect_tx(&sm.bar[st], (uint32_t)nal * (uint32_t)(sizeof(int) + sizeof(S)));
+    if (nal > 0) {
+      bulk_g2s(sm.col[st], col + b0, (uint32_t)nal * sizeof(int), &sm.bar[st]);
+      bulk_g2s(sm.val[st], val + b0, (uint32_t)nal * sizeof(S), &sm.bar[st]);
     }
-    const int a1 = a0 + nr;
-    const long long b1 = D1 - a1;
-    const int ni = (int)(b1 - b0);
-    const int M = nr + ni;
-    const int rs0 = (a0 < N) ? __ldg(row_ptr + a0) : 0;
+  };
 
-    // ---- stream col/val of items [b0, b1) and stage the products
-    {
-      const long long g0 = b0 & ~3LL;
-      const int nvec = (int)((b1 - g0 + 3) >> 2);
-#pragma unroll 2
-      for (int v = lane; v < nvec; v += kWarp) {
-        const long long g = g0 + 4LL * v;
-        if (VEC && g >= b0 && g + 4 <= b1) {
-          int4 c = ld_stream_v4(col + g);
-          const int o = (int)(g - b0);
-          if constexpr (sizeof(S) == 4) {
-            float4 w = ld_stream_v4(reinterpret_cast<const float*>(val) + g);
-            prod[pad8(o + 0)] = (A)w.x * (A)ld_ro(x + c.x);
-            prod[pad8(o + 1)] = (A)w.y * (A)ld_ro(x + c.y);
-            prod[pad8(o + 2)] = (A)w.z * (A)ld_ro(x + c.z);
-            prod[pad8(o + 3)] = (A)w.w * (A)ld_ro(x + c.w);
-          } else {
-            double2 w0 = ld_stream_v2(reinterpret_cast<const double*>(val) + g);
-            double2 w1 = ld_stream_v2(reinterpret_cast<const double*>(val) + g + 2);
-            prod[pad8(o + 0)] = (A)w0.x * (A)ld_ro(x + c.x);
-            prod[pad8(o + 1)] = (A)w0.y * (A)ld_ro(x + c.y);
-            prod[pad8(o + 2)] = (A)w1.x * (A)ld_ro(x + c.z);
-            prod[pad8(o + 3)] = (A)w1.y * (A)ld_ro(x + c.w);
-          }
-        } else {
+  if (tid == 0) {
+    for (int st = 0; st < STAGES; ++st) mbar_init(&sm.bar[st], 1);
+    mbar_fence_init();
+    sm.lcount[0] = sm.lcount[1] = 0;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int st = 0; st < STAGES && st < ntile; ++st) issue(t0 + st, st);
+  }
+  if (warp == 0) {
+    int r = row_of_item(row_ptr, N, t0 * (long long)T, lane);
+    if (lane == 0) sm.rfirst = r;
+  }
+  __syncthreads();
+  int r = sm.rfirst;
+  int cp = 0;  // chunk parity (double-buffered row ends / y / long-row lists)
+
+  for (int k = 0; k < ntile; ++k) {
+    const long long t = t0 + k;
+    const int st = k % STAGES;
+    const uint32_t par = (uint32_t)((k / STAGES) & 1);
+    const long long b0 = t * T;
+    const int n = (int)min((long long)T, nnz - b0);
+    const int nal = n & ~3;
+    // first chunk of row ends and y, issued before the wait
+    int e = (r + tid < N) ? (int)(__ldg(row_ptr + r + tid + 1) - b0) : 0x7fffffff;
+    S yp = (r + tid < N) ? y[r + tid] : (S)0;
+    int prev_end = (r < N) ? (int)max((long long)__ldg(row_ptr + r) - b0, -1LL) : n;
+
+    const bool ok = mbar_wait_bounded(&sm.bar[st], par);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(status, SB_DEV_TIMEOUT_BULK);
+        for (int j = k + 1; j < ntile && j < k + STAGES; ++j)
+          mbar_wait_bounded(&sm.bar[j % STAGES], (uint32_t)((j / STAGES) & 1));
+      }
+      return;
+    }
+
+    S* pv = sm.val[st];
+    int* pc = sm.col[st];
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const long long k = g + e;
-            if (k >= b0 && k < b1) {
-              int c = ld_stream(col + k);
-              prod[pad8((int)(k - b0))] = (A)ld_stream(val + k) * (A)ld_ro(x + c);
+    for (int base = 0; base < T; base += 4 * kStreamThreads) {
+      const int i = base + 4 * tid;
+      if (i + 4 <= nal) {
+        prod4<S>(pc + i, pv + i, x);
+      } else if (i < n) {
+        for (int q = i; q < n && q < i + 4; ++q) {
+          int c;
+          S v;
+          if (q < nal) {
+            c = pc[q];
+            v = pv[q];
+          } else {
+            c = ld_stream(col + b0 + q);
+            v = ld_stream(val + b0 + q);
+          }
+          pv[q] = v * ld_ro(x + c);
+        }
+      }
+    }
+
+    bool first_chunk = true;
+    while (true) {
+      sm.re[cp][tid] = e;
+      sm.ys[cp][tid] = yp;
+      const int c = __syncthreads_count(e <= n);
+      if (first_chunk) {
+        // every thread is past tile k-1: refill its stage with tile k-1+STAGES
+        if (tid == 0 && k >= 1 && k - 1 + STAGES < ntile) {
+          fence_proxy_async_smem();
+          issue(t0 + k - 1 + STAGES, (k - 1) % STAGES);
+        }
+        first_chunk = false;
+      }
+      const bool last_chunk = c < kStreamThreads;
+      // rows of this pass: c rows ending in the tile, plus the cut row
+      const bool has_cut = last_chunk && (r + c < N);
+      const int nrows = c + (has_cut ? 1 : 0);
+      if (nrows > 0) {
+        const int p2 = nrows <= 1 ? 1 : (1 << (32 - __clz(nrows - 1)));
+        const int V = min(kWarp, max(1, kStreamThreads / p2));
+        const int G = kStreamThreads / V;
+        const int g = tid / V;
+        const int q = tid - g * V;
+        for (int j0 = 0; j0 < nrows; j0 += G) {
+          const int j = j0 + g;
+          int lo = 0, hi = 0;
+          bool atom = false;
+          if (j < nrows) {
+            const int s0 = (j == 0) ? prev_end : sm.re[cp][j - 1];
+            hi = (j < c) ? sm.re[cp][j] : n;
+            lo = max(s0, 0);
+            atom = (s0 < 0) || (j >= c);
+          }
+          const bool longrow = (V < kWarp) && (hi - lo > 16 * V);
+          S sum = 0;
+          if (!longrow) {
+            for (int qq = lo + q; qq < hi; qq += V) sum += pv[qq];
+          }
+          for (int off = V >> 1; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
+          if (q == 0 && j < nrows && hi > lo) {
+            const int row = r + j;
+            if (longrow) {
+              const int slot = atomicAdd(&sm.lcount[cp], 1);
+              sm.lrow[cp][slot] = make_int4(row, lo, hi, atom ? 1 : 0);
+            } else if (atom) {
+              atomicAdd(y + row, sum);
+            } else {
+              y[row] = sm.ys[cp][j] + sum;
             }
           }
         }
       }
-    }
-    __syncwarp();
-
-    // ---- per-lane merge walk over ITEMS merge steps
-    const int dl = min(lane * kItems, M);
-    const int dh = min(dl + kItems, M);
-    int lo = 0, hi = nr;
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if ((long long)mid + (re[mid] - b0) < dl) lo = mid + 1; else hi = mid;
-    }
-    int ra = lo;
-    int rb = dl - ra;
-    A acc = 0;
-    bool head = false;
-    int first_ra = 0;
-    A first_val = 0;
-    for (int s = dl; s < dh; ++s) {
-      const bool take_end = (ra < nr) && (rb >= ni || (long long)re[ra] <= b0 + rb);
-      if (take_end) {
-        if (!head) {
-          head = true;
-          first_ra = ra;
-          first_val = acc;
-        } else {
-          emit_row<S, A>(y, a0 + ra, ra ? re[ra - 1] : rs0, re[ra], b0, acc);
+      __syncthreads();
+      const int L = sm.lcount[cp];
+      for (int j = warp; j < L; j += kStreamThreads / kWarp) {
+        const int4 w = sm.lrow[cp][j];
+        S sum = 0;
+        for (int qq = w.y + lane; qq < w.z; qq += kWarp) sum += pv[qq];
+        for (int off = kWarp / 2; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
+        if (lane == 0) {
+          if (w.w) atomicAdd(y + w.x, sum);
+          else y[w.x] = sm.ys[cp][w.x - r] + sum;
         }
-        acc = 0;
-        ++ra;
-      } else {
-        acc += prod[pad8(rb)];
-        ++rb;
       }
+      if (c > 0) prev_end = sm.re[cp][c - 1];
+      if (tid == 0) sm.lcount[cp ^ 1] = 0;
+      r += c;
+      cp ^= 1;
+      if (last_chunk) break;
+      e = (r + tid < N) ? (int)(__ldg(row_ptr + r + tid + 1) - b0) : 0x7fffffff;
+      yp = (r + tid < N) ? y[r + tid] : (S)0;
     }
-    // ---- warp segmented inclusive scan of the lanes' trailing partials
-    A S_ = acc;
-    bool hf = head;
-#pragma unroll
-    for (int off = 1; off < kWarp; off <<= 1) {
-      A v = __shfl_up_sync(kFull, S_, off);
-      bool f = __shfl_up_sync(kFull, hf, off);
-      if (lane >= off) {
-        if (!hf) S_ += v;
-        hf = hf || f;
-      }
-    }
-    A carry = __shfl_up_sync(kFull, S_, 1);
-    if (lane == 0) carry = 0;
-    if (head) {
-      emit_row<S, A>(y, a0 + first_ra, first_ra ? re[first_ra - 1] : rs0, re[first_ra], b0,
-                     first_val + carry);
-    }
-    // ---- row a1 continues past this tile: add its partial atomically
-    if (lane == kWarp - 1 && a1 < N) {
-      const int rs1 = nr ? re[nr - 1] : rs0;
-      const long long lo_item = max((long long)rs1, b0);
-      if (b1 > lo_item) atomicAdd(y + a1, (S)S_);
-    }
-    __syncwarp();
-    a0 = a1;
-    b0 = b1;
-    D0 = D1;
   }
+}
+
+// ------------------------------------------------------------ CSR (rows)
+
+// Row-block CSR: each warp owns 32 consecutive rows.  It reads their row_ptr
+// entries once (one per lane), then reduces the short rows in batches of
+// 32/V rows, V lanes per row, each lane issuing UNROLL independent col/val
+// loads before the dependent x gathers and one shuffle reduction per batch;
+// rows longer than the short limit are reduced afterwards by the whole warp.
+// V is picked per matrix from its mean row length.  No shared memory and no
+// block barrier: occupancy and unrolled loads keep the loads in flight.
+template <typename S, int V, int UNROLL>
+__global__ void __launch_bounds__(256)
+    csr_rows_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
+                    const S* __restrict__ val, const S* __restrict__ x, S* __restrict__ y,
+                    int N) {
+  constexpr int RPB = kWarp / V;           // rows per batch
+  constexpr int SHORT = V * UNROLL;        // a short row needs one unrolled pass
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int g = lane / V;
+  const int q = lane - g * V;
+  const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+       w * kWarp < N; w += warps) {
+    const int r0 = (int)(w * kWarp);
+    const int rr = r0 + lane;
+    const int s_l = rr < N ? __ldg(row_ptr + rr) : 0;
+    const int e_l = rr < N ? __ldg(row_ptr + rr + 1) : 0;
+    const int len_l = e_l - s_l;
+    const S y_l = (rr < N && len_l > 0) ? y[rr] : (S)0;
+#pragma unroll
+    for (int b = 0; b < V; ++b) {
+      const int j = b * RPB + g;  // row of this group within the block
+      const int s = __shfl_sync(kFull, s_l, j);
+      const int e = __shfl_sync(kFull, e_l, j);
+      const int len = e - s;
+      S sum = 0;
+      if (len <= SHORT) {
+        int cc[UNROLL];
+        S vv[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          const int k = s + q + u * V;
+          cc[u] = k < e ? ld_stream(col + k) : 0;
+          vv[u] = k < e ? ld_stream(val + k) : (S)0;
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          const int k = s + q + u * V;
+          if (k < e) sum += vv[u] * ld_ro(x + cc[u]);
+        }
+      }
+#pragma unroll
+      for (int off = V >> 1; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
+      const S yj = __shfl_sync(kFull, y_l, j);
+      if (q == 0 && len > 0 && len <= SHORT && r0 + j < N) y[r0 + j] = yj + sum;
+    }
+    // long rows of the block: whole warp each
+    unsigned longm = __ballot_sync(kFull, rr < N && len_l > SHORT);
+    while (longm) {
+      const int j = __ffs(longm) - 1;
+      longm &= longm - 1;
+      const int s = __shfl_sync(kFull, s_l, j);
+      const int e = __shfl_sync(kFull, e_l, j);
+      S sum = 0;
+      for (int k0 = s; k0 < e; k0 += kWarp * 4) {
+        int cc[4];
+        S vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = k0 + lane + u * kWarp;
+          cc[u] = k < e ? ld_stream(col + k) : 0;
+          vv[u] = k < e ? ld_stream(val + k) : (S)0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = k0 + lane + u * kWarp;
+          if (k < e) sum += vv[u] * ld_ro(x + cc[u]);
+        }
+      }
+#pragma unroll
+      for (int off = kWarp / 2; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
+      const S yj = __shfl_sync(kFull, y_l, j);
+      if (lane == 0) y[r0 + j] = yj + sum;
+    }
+  }
+}
+
+template <typename S, int V, int UNROLL>
+static int launch_csr_rows_v(const int* row_ptr, const int* col, const S* val, const S* x, S* y,
+                             int N, cudaStream_t st) {
+  auto kern = csr_rows_kernel<S, V, UNROLL>;
+  const long long warps_needed = ((long long)N + kWarp - 1) / kWarp;
+  const long long max_warps = (long long)resident_ctas(kern, 256) * 8;
+  const long long warps = std::min(warps_needed, max_warps);
+  const unsigned ctas = (unsigned)((warps + 7) / 8);
+  kern<<<ctas, 256, 0, st>>>(row_ptr, col, val, x, y, N);
+  SB_CHECK_LAUNCH("csr_rows_kernel");
+  return SB_OK;
+}
+
+// V from the mean row length: about three items per lane per row.
+template <typename S>
+static int launch_csr_rows(const int* row_ptr, const int* col, const S* val, const S* x, S* y,
+                           int N, long long nnz, cudaStream_t st) {
+  const double avg = N ? (double)nnz / N : 0.0;
+  if (avg <= 6) return launch_csr_rows_v<S, 2, 4>(row_ptr, col, val, x, y, N, st);
+  if (avg <= 14) return launch_csr_rows_v<S, 4, 4>(row_ptr, col, val, x, y, N, st);
+  if (avg <= 28) return launch_csr_rows_v<S, 8, 4>(row_ptr, col, val, x, y, N, st);
+  return launch_csr_rows_v<S, 16, 4>(row_ptr, col, val, x, y, N, st);
 }
 
 // ------------------------------------------------------------ COO
@@ -317,6 +496,8 @@ template <> __device__ __forceinline__ double add_rn(double a, double b) { retur
 
 // One row per thread; diagonals in stored order, each added with a
 // separately rounded product (src/sequential/src/sparse_opt_32.wat:290-407).
+// The in-band test is a predicate so that the unrolled loop issues the data
+// and x loads of several diagonals before their dependent additions.
 template <typename T>
 __global__ void __launch_bounds__(256)
     dia_row_kernel(const int* __restrict__ offset, const T* __restrict__ data, int N, int nd,
@@ -325,14 +506,15 @@ __global__ void __launch_bounds__(256)
   if (i >= N) return;
   T t = y[i];
   const long long move = (long long)N - stride;
+#pragma unroll 4
   for (int d = 0; d < nd; ++d) {
     const int k = __ldg(offset + d);
-    const int lo = k < 0 ? -k : 0;
-    const int hi = (N < N - k) ? N : N - k;
-    if (i >= lo && i < hi) {
-      const long long idx = (long long)d * stride + i - (k < 0 ? move : 0);
-      t = add_rn(mul_rn(ld_stream(data + idx), ld_ro(x + i + k)), t);
-    }
+    const bool in = (unsigned)(i + k) < (unsigned)N;
+    const long long idx = (long long)d * stride + i - (k < 0 ? move : 0);
+    T a = in ? ld_stream(data + idx) : (T)0;
+    T b = in ? ld_ro(x + i + k) : (T)0;
+    T p = mul_rn(a, b);
+    t = in ? add_rn(p, t) : t;
   }
   y[i] = t;
 }
@@ -357,32 +539,70 @@ __global__ void __launch_bounds__(256)
 
 // ------------------------------------------------------------ launchers
 
-static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-template <typename K>
-static int resident_ctas(K kernel, int threads) {
+template <typename S, int T, int STAGES>
+static int launch_csr_stream(const int* row_ptr, const int* col, const S* val, const S* x, S* y,
+                             int N, long long nnz, cudaStream_t st) {
+  const long long ntiles = (nnz + T - 1) / T;
+  auto kern = csr_stream_kernel<S, T, STAGES>;
+  const size_t smem = sizeof(CsrStreamSmem<S, T, STAGES>);
+  static int configured[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    SB_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    configured[dev] = 1;
+  }
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  SB_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads,
+                                                              smem));
   if (per_sm < 1) per_sm = 1;
-  return per_sm * sm_count();
+  const long long max_ctas = (long long)per_sm * sm_count();
+  const long long ctas = std::min(ntiles, max_ctas);
+  const long long tpc = (ntiles + ctas - 1) / ctas;
+  const long long used = (ntiles + tpc - 1) / tpc;
+  int* status = device_status_word();
+  if (!status) {
+    set_error("sb_spmv_csr: device status word unavailable");
+    return SB_ENOMEM;
+  }
+  kern<<<(unsigned)used, kStreamThreads, smem, st>>>(row_ptr, col, val, x, y, N, nnz, ntiles,
+                                                     tpc, status);
+  SB_CHECK_LAUNCH("csr_stream_kernel");
+  return SB_OK;
 }
 
+// CSR dispatch: the streaming kernel when col/val are 16-byte aligned (bulk
+// copies need it), the warp-tile kernel otherwise.  SB_CSR_KERNEL=tile forces
+// the warp-tile kernel (tuning runs).
+static int csr_kernel_choice() {
+  static int v = [] {
+    const char* e = getenv("SB_CSR_KERNEL");
+    return (e && e[0] == 's') ? 2 : 0;  // 's': streamed tiles
+  }();
+  return v;
+}
+
+static int csr_stream_tile() {
+  static int v = [] {
+    const char* e = getenv("SB_CSR_T");
+    return (e && atoi(e) == 2048) ? 2048 : 1024;
+  }();
+  return v;
+}
+
+// CSR dispatch: the row-block kernel by default; SB_CSR_KERNEL=s selects the
+// bulk-copy streamed-tile kernel (needs 16-byte aligned col/val).
 template <typename S, typename A>
 static int launch_csr(const int* row_ptr, const int* col, const S* val, const S* x, S* y, int N,
                       long long nnz, cudaStream_t st) {
-  const long long total = (long long)N + nnz;
-  const long long ntiles = (total + kTile - 1) / kTile;
-  const bool vec = aligned16(col) && aligned16(val);
-  auto kern = vec ? csr_merge_kernel<S, A, true> : csr_merge_kernel<S, A, false>;
-  const int threads = kWarpsPerCta * kWarp;
-  const long long max_warps = (long long)resident_ctas(kern, threads) * kWarpsPerCta;
-  const long long warps = std::min(ntiles, max_warps);
-  const long long tpw = (ntiles + warps - 1) / warps;
-  const long long used_warps = (ntiles + tpw - 1) / tpw;
-  const long long ctas = (used_warps + kWarpsPerCta - 1) / kWarpsPerCta;
-  kern<<<(unsigned)ctas, threads, 0, st>>>(row_ptr, col, val, x, y, N, total, ntiles, tpw);
-  SB_CHECK_LAUNCH("csr_merge_kernel");
-  return SB_OK;
+  if (csr_kernel_choice() == 2 && aligned16(col) && aligned16(val)) {
+    if (csr_stream_tile() == 2048)
+      return launch_csr_stream<S, 2048, 3>(row_ptr, col, val, x, y, N, nnz, st);
+    return launch_csr_stream<S, 1024, 4>(row_ptr, col, val, x, y, N, nnz, st);
+  }
+  return launch_csr_rows<S>(row_ptr, col, val, x, y, N, nnz, st);
 }
 
 template <typename S, typename A>

@@ -143,3 +143,39 @@ def test_zero_sized_calls_are_noops(gpu):
     xv, yv = gpu.create_vec(3, 1.0), gpu.create_vec(3, 2.0)
     gpu.spmv(A, xv, yv)
     assert yv.array().tolist() == [2.0, 2.0, 2.0]
+
+
+def _csr_check_all(sb, orc):
+    """Parity of every CSR case; run in a child process by the test below."""
+    for dt in DTYPES:
+        for name, (rp, col, val) in _mats(dt).items():
+            N = rp.size - 1
+            x, y0 = _x_y(N, dt)
+            A = sb.csr_from_host(rp, col, val)
+            xv, yv = sb.vec_from_host(x), sb.vec_from_host(y0)
+            sb.spmv(A, xv, yv)
+            err = rel_err(yv.array(), orc.truth_csr(rp, col, val, x, y0))
+            assert err <= TOL[np.dtype(dt)], (name, dt, err)
+
+
+@pytest.mark.parametrize("tile", ["1024", "2048"])
+def test_csr_streamed_tile_kernel(gpu, tile):
+    """The alternative bulk-copy streamed-tile CSR kernel (SB_CSR_KERNEL=s)."""
+    import os
+    import subprocess
+    import sys
+    env = dict(os.environ, SB_CSR_KERNEL="s", SB_CSR_T=tile)
+    r = subprocess.run([sys.executable, __file__, "--csr-check"], env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
+if __name__ == "__main__":
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    if "--csr-check" in sys.argv:
+        import sciwasm.sparse_b200 as _sb
+        from oracle import binding as _orc
+        _csr_check_all(_sb, _orc)
+        print("ok")
