@@ -104,6 +104,50 @@ int sb_spmv_dia(int dtype, const int32_t* offset, const void* data, int32_t N, i
 int sb_spmv_ell(int dtype, const int32_t* indices, const void* data, int32_t N, int32_t nc,
                 const void* x, void* y, int32_t inner_max, void* stream);
 
+/* ---------------------------------------------------------------------- */
+/* Format conversions (bit-exact with the reference).  These calls return */
+/* after the device work is complete (they may read results to the host). */
+/* CSR inputs must have monotone row_ptr with row_ptr[0] = 0 and columns  */
+/* in [0, N); COO indices are checked on the device (SB_EINVAL).          */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces coo_csr (src/sequential/src/sparse32.js:1674-1720 with the
+ * per-row stable sort :1612-1627; FP64 src/sequential/src/sparse64.js:1255).
+ * Outputs: csr_row_ptr[N+1], csr_col[nnz], csr_val[nnz] (caller-allocated,
+ * as allocate_CSR :2252 does); entries are stably ordered by (row, col). */
+int sb_coo_csr(int dtype, const int32_t* row, const int32_t* col, const void* val, int32_t N,
+               int64_t nnz, int32_t* csr_row_ptr, int32_t* csr_col, void* csr_val, void* stream);
+
+/* Replaces num_cols (src/sequential/src/sparse32.js:1436-1447): the maximum
+ * row length, returned to the host in *nc. */
+int sb_num_cols(const int32_t* row_ptr, int32_t N, int32_t* nc, void* stream);
+
+/* The admission test of csr_ell (src/sequential/src/sparse32.js:1457):
+ * returns 1 when nc*N < 2^27 and nc*N/nnz <= 5 (in doubles), else 0. */
+int sb_ell_admitted(int64_t ncols, int32_t N, int64_t nnz);
+
+/* Replaces the fill of csr_ell (src/sequential/src/sparse32.js:1449-1484).
+ * Returns SB_EREFUSED (writing nothing) where the reference returns
+ * undefined.  indices/data hold nc*N column-major slots, zero padded. */
+int sb_csr_ell(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val, int32_t N,
+               int64_t nnz, int32_t nc, int32_t* indices, void* data, void* stream);
+
+/* Replaces num_diags (src/sequential/src/sparse32.js:1486-1512): number of
+ * occupied diagonals in *nd, *stride = N. */
+int sb_num_diags(const int32_t* row_ptr, const int32_t* col, int32_t N, int32_t* nd,
+                 int32_t* stride, void* stream);
+
+/* The admission test of csr_dia (src/sequential/src/sparse32.js:1525). */
+int sb_dia_admitted(int64_t ndiags, int32_t stride, int64_t nnz);
+
+/* Replaces the fill of csr_dia (src/sequential/src/sparse32.js:1515-1574):
+ * offset[nd] ascending, data[nd*stride] diagonal-major (zero where no entry),
+ * a later duplicate (i, c) in row order overwriting an earlier one.  Returns
+ * SB_EREFUSED where the reference returns undefined. */
+int sb_csr_dia(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val, int32_t N,
+               int64_t nnz, int32_t nd, int32_t stride, int32_t* offset, void* data,
+               void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,13 @@ SIGNATURES: dict[str, list] = {
     "sb_spmv_csr": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
     "sb_spmv_dia": [C.c_int, P, P, I32, I32, I32, P, P, I32, P],
     "sb_spmv_ell": [C.c_int, P, P, I32, I32, P, P, I32, P],
+    "sb_coo_csr": [C.c_int, P, P, P, I32, I64, P, P, P, P],
+    "sb_num_cols": [P, I32, C.POINTER(I32), P],
+    "sb_ell_admitted": [I64, I32, I64],
+    "sb_csr_ell": [C.c_int, P, P, P, I32, I64, I32, P, P, P],
+    "sb_num_diags": [P, P, I32, C.POINTER(I32), C.POINTER(I32), P],
+    "sb_dia_admitted": [I64, I32, I64],
+    "sb_csr_dia": [C.c_int, P, P, P, I32, I64, I32, I32, P, P, P],
 }
 _RESTYPE = {"sb_last_error": C.c_char_p, "sb_status_string": C.c_char_p}
 

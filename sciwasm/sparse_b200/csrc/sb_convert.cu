@@ -1,0 +1,396 @@
+// sb_convert.cu -- format conversions on the device, bit-exact with the
+// reference's JavaScript loops:
+//   coo_csr   src/sequential/src/sparse32.js:1674-1720 (+ sort :1612-1627)
+//   num_cols  :1436-1447 and csr_ell :1449-1484
+//   num_diags :1486-1512 and csr_dia :1515-1574
+// coo_csr's per-row stable bubble sort makes the result a stable sort of the
+// COO entries by (row, col).  Sorted input (the reference's mmread always
+// quick-sorts by (row, col)) is detected and takes a copy-speed path; other
+// input is ordered by a stable LSD radix sort of packed (row, col) keys whose
+// payload is the original position, so equal keys keep their COO order.
+#include <algorithm>
+
+#include "sb_common.cuh"
+#include "sb_prims.cuh"
+
+namespace sb {
+
+constexpr int kThreads = 256;
+
+static unsigned grid_for(long long n, int per = kThreads) {
+  long long g = (n + per - 1) / per;
+  if (g < 1) g = 1;
+  if (g > 0x7fffffffLL) g = 0x7fffffffLL;
+  return (unsigned)g;
+}
+
+// flags[0] |= 1: index out of range; flags[1] |= 1: not sorted by (row, col)
+__global__ void coo_check(const int* __restrict__ row, const int* __restrict__ col, long long nnz,
+                          int N, int* __restrict__ flags) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnz) return;
+  const int r = row[i], c = col[i];
+  if (r < 0 || r >= N || c < 0 || c >= N) flags[0] = 1;
+  if (i + 1 < nnz) {
+    const int r1 = row[i + 1], c1 = col[i + 1];
+    if (r1 < r || (r1 == r && c1 < c)) flags[1] = 1;
+  }
+}
+
+// row_ptr from a row array sorted ascending: row_ptr[r] = first position of
+// a row >= r.  Every row_ptr entry is written exactly once.
+__global__ void row_ptr_from_sorted(const int* __restrict__ row, long long nnz, int N,
+                                    int* __restrict__ row_ptr) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > nnz) return;
+  const int prev = (i == 0) ? -1 : row[i - 1];
+  const int cur = (i == nnz) ? N : row[i];
+  for (int r = prev + 1; r <= cur; ++r) row_ptr[r] = (int)i;
+}
+
+__global__ void pack_keys(const int* __restrict__ row, const int* __restrict__ col,
+                          long long nnz, unsigned long long* __restrict__ keys,
+                          unsigned* __restrict__ idx) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnz) return;
+  keys[i] = ((unsigned long long)(unsigned)row[i] << 32) | (unsigned)col[i];
+  idx[i] = (unsigned)i;
+}
+
+template <typename T>
+__global__ void unpack_sorted(const unsigned long long* __restrict__ keys,
+                              const unsigned* __restrict__ idx, const T* __restrict__ val,
+                              long long nnz, int* __restrict__ row_out, int* __restrict__ col_out,
+                              T* __restrict__ val_out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnz) return;
+  const unsigned long long k = keys[i];
+  row_out[i] = (int)(k >> 32);
+  col_out[i] = (int)(k & 0xffffffffu);
+  val_out[i] = val[idx[i]];
+}
+
+// max row length (num_cols)
+__global__ void max_row_len(const int* __restrict__ row_ptr, int N, int* __restrict__ out) {
+  __shared__ int sm[32];
+  int m = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x)
+    m = max(m, row_ptr[i + 1] - row_ptr[i]);
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0;
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) atomicMax(out, m);
+  }
+}
+
+// csr_ell: thread per row writes all nc slots of its row (entries in storage
+// order, then zero padding with index 0), column-major slot k*N + i.
+template <typename T>
+__global__ void csr_to_ell(const int* __restrict__ row_ptr, const int* __restrict__ col,
+                           const T* __restrict__ val, int N, int nc, int* __restrict__ indices,
+                           T* __restrict__ data) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int s = row_ptr[i], e = row_ptr[i + 1];
+  for (int k = 0; k < nc; ++k) {
+    const long long o = (long long)k * N + i;
+    const int j = s + k;
+    if (j < e) {
+      indices[o] = col[j];
+      data[o] = val[j];
+    } else {
+      indices[o] = 0;
+      data[o] = (T)0;
+    }
+  }
+}
+
+// Presence of diagonal c - i, stored at index N + c - i - 1 as in the
+// reference (:1498); stores of 1 from several threads are benign.
+__global__ void mark_diagonals(const int* __restrict__ row_ptr, const int* __restrict__ col, int N,
+                               int* __restrict__ ind) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (int j = row_ptr[i]; j < row_ptr[i + 1]; ++j) {
+    const int c = col[j];
+    if (c >= 0 && c < N) ind[(long long)N + c - i - 1] = 1;
+  }
+}
+
+// Compact the present diagonals: slot[d] = rank of d among present ones
+// (from the exclusive scan), offset[slot] = d - (N - 1) ascending.
+__global__ void compact_diagonals(const int* __restrict__ present, const int* __restrict__ rank,
+                                  long long nd_all, int N, int* __restrict__ offset) {
+  const long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= nd_all) return;
+  if (present[d]) offset[rank[d]] = (int)(d - (N - 1));
+}
+
+// csr_dia fill: thread per row, entries in storage order so a later
+// duplicate (i, c) overwrites an earlier one exactly as the reference's
+// row-major loop does (:1559-1571).  data is zero-filled beforehand.
+template <typename T>
+__global__ void csr_to_dia(const int* __restrict__ row_ptr, const int* __restrict__ col,
+                           const T* __restrict__ val, int N, int stride,
+                           const int* __restrict__ rank, T* __restrict__ data) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const long long move = (long long)N - stride;
+  for (int j = row_ptr[i]; j < row_ptr[i + 1]; ++j) {
+    const int c = col[j];
+    if (c < 0 || c >= N) continue;
+    const int k = rank[(long long)N + c - i - 1];
+    const long long o = (long long)k * stride + i - ((c - i) < 0 ? move : 0);
+    data[o] = val[j];
+  }
+}
+
+static int check_dt(int dtype, const char* fn) {
+  if (dtype != SB_F32 && dtype != SB_F64) {
+    set_error("%s: dtype %d not supported", fn, dtype);
+    return SB_EINVAL;
+  }
+  return SB_OK;
+}
+
+// Host-side admission test of csr_ell / csr_dia, evaluated in doubles as in
+// JavaScript: admit iff w*N < 2^27 and (w*N)/nnz <= 5 (0/0 is NaN: refused).
+static bool admitted(long long w, long long N, long long nnz) {
+  const double wn = (double)w * (double)N;
+  const double ratio = wn / (double)nnz;
+  return (wn < 134217728.0) && (ratio <= 5.0);
+}
+
+template <typename T>
+static int coo_csr_impl(const int* row, const int* col, const T* val, int N, long long nnz,
+                        int* csr_row, int* csr_col, T* csr_val, cudaStream_t st) {
+  int* flags = nullptr;
+  int r = scratch_alloc((void**)&flags, 2 * sizeof(int), st);
+  if (r) return r;
+  SB_CHECK_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(int), st));
+  coo_check<<<grid_for(nnz), kThreads, 0, st>>>(row, col, nnz, N, flags);
+  SB_CHECK_LAUNCH("coo_check");
+  int hf[2] = {0, 0};
+  SB_CHECK_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+  SB_CHECK_CUDA(cudaStreamSynchronize(st));
+  scratch_free(flags, st);
+  if (hf[0]) {
+    set_error("coo_csr: row or column index outside [0, N)");
+    return SB_EINVAL;
+  }
+  if (!hf[1]) {
+    // already in (row, col) order: the stable sort is the identity
+    SB_CHECK_CUDA(cudaMemcpyAsync(csr_col, col, sizeof(int) * nnz, cudaMemcpyDeviceToDevice, st));
+    SB_CHECK_CUDA(cudaMemcpyAsync(csr_val, val, sizeof(T) * nnz, cudaMemcpyDeviceToDevice, st));
+    row_ptr_from_sorted<<<grid_for(nnz + 1), kThreads, 0, st>>>(row, nnz, N, csr_row);
+    SB_CHECK_LAUNCH("row_ptr_from_sorted");
+    return SB_OK;
+  }
+  // general order: stable radix sort of (row << 32 | col) with positions
+  prim::RadixBuffers b;
+  void* mem = nullptr;
+  const size_t kb = sizeof(unsigned long long) * (size_t)nnz, vb = sizeof(unsigned) * (size_t)nnz;
+  r = scratch_alloc(&mem, 2 * kb + 2 * vb + sizeof(int) * (size_t)nnz, st);
+  if (r) return r;
+  char* p = (char*)mem;
+  b.k[0] = (unsigned long long*)p;
+  b.k[1] = (unsigned long long*)(p + kb);
+  b.v[0] = (unsigned*)(p + 2 * kb);
+  b.v[1] = (unsigned*)(p + 2 * kb + vb);
+  int* rows_sorted = (int*)(p + 2 * kb + 2 * vb);
+  pack_keys<<<grid_for(nnz), kThreads, 0, st>>>(row, col, nnz, b.k[0], b.v[0]);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) r = cuda_status(e, "pack_keys");
+  const int nb = prim::bits_for(N > 0 ? N - 1 : 0);
+  const int ranges[4] = {0, nb, 32, 32 + nb};
+  int which = 0;
+  if (!r) r = prim::radix_sort_ranges(b, nnz, ranges, 2, &which, st);
+  if (!r) {
+    unpack_sorted<T><<<grid_for(nnz), kThreads, 0, st>>>(b.k[which], b.v[which], val, nnz,
+                                                         rows_sorted, csr_col, csr_val);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) r = cuda_status(e, "unpack_sorted");
+  }
+  if (!r) {
+    row_ptr_from_sorted<<<grid_for(nnz + 1), kThreads, 0, st>>>(rows_sorted, nnz, N, csr_row);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) r = cuda_status(e, "row_ptr_from_sorted");
+  }
+  if (!r) {
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) r = cuda_status(e, "coo_csr");
+  }
+  scratch_free(mem, st);
+  return r;
+}
+
+static int num_diags_impl(const int* row_ptr, const int* col, int N, int** present_out,
+                          int** rank_out, int* nd, cudaStream_t st) {
+  const long long nall = 2LL * N - 1;
+  int* present = nullptr;
+  int r = scratch_alloc((void**)&present, sizeof(int) * (size_t)(2 * nall + 1), st);
+  if (r) return r;
+  int* rank = present + nall;
+  SB_CHECK_CUDA(cudaMemsetAsync(present, 0, sizeof(int) * (size_t)nall, st));
+  mark_diagonals<<<grid_for(N), kThreads, 0, st>>>(row_ptr, col, N, present);
+  SB_CHECK_LAUNCH("mark_diagonals");
+  r = prim::exclusive_scan(present, rank, nall, st);
+  if (r) {
+    scratch_free(present, st);
+    return r;
+  }
+  int last[2] = {0, 0};
+  SB_CHECK_CUDA(cudaMemcpyAsync(&last[0], present + nall - 1, sizeof(int),
+                                cudaMemcpyDeviceToHost, st));
+  SB_CHECK_CUDA(cudaMemcpyAsync(&last[1], rank + nall - 1, sizeof(int), cudaMemcpyDeviceToHost,
+                                st));
+  SB_CHECK_CUDA(cudaStreamSynchronize(st));
+  *nd = last[0] + last[1];
+  *present_out = present;
+  *rank_out = rank;
+  return SB_OK;
+}
+
+}  // namespace sb
+
+using namespace sb;
+
+extern "C" {
+
+int sb_coo_csr(int dtype, const int32_t* row, const int32_t* col, const void* val, int32_t N,
+               int64_t nnz, int32_t* csr_row_ptr, int32_t* csr_col, void* csr_val,
+               void* stream) {
+  int r = check_dt(dtype, "sb_coo_csr");
+  if (r) return r;
+  SB_REQUIRE(N >= 0 && nnz >= 0, "sb_coo_csr: negative size");
+  SB_REQUIRE(nnz <= 0x7fffffffLL, "sb_coo_csr: nnz exceeds int32 row_ptr range");
+  SB_REQUIRE(csr_row_ptr, "sb_coo_csr: null row_ptr");
+  if ((r = ensure_device())) return r;
+  cudaStream_t st = as_stream(stream);
+  if (nnz == 0) {
+    SB_CHECK_CUDA(cudaMemsetAsync(csr_row_ptr, 0, sizeof(int) * ((size_t)N + 1), st));
+    SB_CHECK_CUDA(cudaStreamSynchronize(st));
+    return SB_OK;
+  }
+  SB_REQUIRE(row && col && val && csr_col && csr_val, "sb_coo_csr: null pointer");
+  if (dtype == SB_F32)
+    return coo_csr_impl<float>(row, col, (const float*)val, N, nnz, csr_row_ptr, csr_col,
+                               (float*)csr_val, st);
+  return coo_csr_impl<double>(row, col, (const double*)val, N, nnz, csr_row_ptr, csr_col,
+                              (double*)csr_val, st);
+}
+
+int sb_num_cols(const int32_t* row_ptr, int32_t N, int32_t* nc, void* stream) {
+  SB_REQUIRE(nc && N >= 0, "sb_num_cols: bad argument");
+  *nc = 0;
+  if (N == 0) return SB_OK;
+  SB_REQUIRE(row_ptr, "sb_num_cols: null row_ptr");
+  int r = ensure_device();
+  if (r) return r;
+  cudaStream_t st = as_stream(stream);
+  int* out = nullptr;
+  if ((r = scratch_alloc((void**)&out, sizeof(int), st))) return r;
+  SB_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(int), st));
+  const unsigned g = std::min<unsigned>(grid_for(N), (unsigned)sm_count() * 8);
+  max_row_len<<<g, kThreads, 0, st>>>(row_ptr, N, out);
+  SB_CHECK_LAUNCH("max_row_len");
+  SB_CHECK_CUDA(cudaMemcpyAsync(nc, out, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SB_CHECK_CUDA(cudaStreamSynchronize(st));
+  scratch_free(out, st);
+  return SB_OK;
+}
+
+int sb_ell_admitted(int64_t ncols, int32_t N, int64_t nnz) {
+  return admitted(ncols, N, nnz) ? 1 : 0;
+}
+
+int sb_csr_ell(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val, int32_t N,
+               int64_t nnz, int32_t nc, int32_t* indices, void* data, void* stream) {
+  int r = check_dt(dtype, "sb_csr_ell");
+  if (r) return r;
+  SB_REQUIRE(N >= 0 && nnz >= 0 && nc >= 0, "sb_csr_ell: negative size");
+  if (!admitted(nc, N, nnz)) {
+    set_error("csr_ell: not efficient to store this matrix in ELL (nc*N=%lld, nnz=%lld)",
+              (long long)nc * N, (long long)nnz);
+    return SB_EREFUSED;
+  }
+  SB_REQUIRE(row_ptr && indices && data && (nnz == 0 || (col && val)), "sb_csr_ell: null pointer");
+  if ((r = ensure_device())) return r;
+  cudaStream_t st = as_stream(stream);
+  if (dtype == SB_F32)
+    csr_to_ell<float><<<grid_for(N), kThreads, 0, st>>>(row_ptr, col, (const float*)val, N, nc,
+                                                        indices, (float*)data);
+  else
+    csr_to_ell<double><<<grid_for(N), kThreads, 0, st>>>(row_ptr, col, (const double*)val, N, nc,
+                                                         indices, (double*)data);
+  SB_CHECK_LAUNCH("csr_to_ell");
+  return SB_OK;
+}
+
+int sb_num_diags(const int32_t* row_ptr, const int32_t* col, int32_t N, int32_t* nd,
+                 int32_t* stride, void* stream) {
+  SB_REQUIRE(nd && stride && N >= 0, "sb_num_diags: bad argument");
+  *nd = 0;
+  *stride = N;
+  if (N == 0) return SB_OK;
+  SB_REQUIRE(row_ptr && col, "sb_num_diags: null pointer");
+  int r = ensure_device();
+  if (r) return r;
+  cudaStream_t st = as_stream(stream);
+  int *present = nullptr, *rank = nullptr;
+  if ((r = num_diags_impl(row_ptr, col, N, &present, &rank, nd, st))) return r;
+  scratch_free(present, st);
+  return SB_OK;
+}
+
+int sb_dia_admitted(int64_t ndiags, int32_t stride, int64_t nnz) {
+  return admitted(ndiags, stride, nnz) ? 1 : 0;
+}
+
+int sb_csr_dia(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val, int32_t N,
+               int64_t nnz, int32_t nd, int32_t stride, int32_t* offset, void* data,
+               void* stream) {
+  int r = check_dt(dtype, "sb_csr_dia");
+  if (r) return r;
+  SB_REQUIRE(N >= 0 && nnz >= 0 && nd >= 0, "sb_csr_dia: negative size");
+  SB_REQUIRE(stride == N, "sb_csr_dia: stride must equal N (reference :1510)");
+  if (!admitted(nd, stride, nnz)) {
+    set_error("csr_dia: not efficient to store this matrix in DIA (nd*stride=%lld, nnz=%lld)",
+              (long long)nd * stride, (long long)nnz);
+    return SB_EREFUSED;
+  }
+  SB_REQUIRE(row_ptr && col && val && offset && data, "sb_csr_dia: null pointer");
+  if ((r = ensure_device())) return r;
+  cudaStream_t st = as_stream(stream);
+  int *present = nullptr, *rank = nullptr;
+  int nd_found = 0;
+  if ((r = num_diags_impl(row_ptr, col, N, &present, &rank, &nd_found, st))) return r;
+  if (nd_found != nd) {
+    scratch_free(present, st);
+    set_error("sb_csr_dia: nd=%d does not match the matrix (%d diagonals)", nd, nd_found);
+    return SB_EINVAL;
+  }
+  const long long nall = 2LL * N - 1;
+  compact_diagonals<<<grid_for(nall), kThreads, 0, st>>>(present, rank, nall, N, offset);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(data, 0, dtype_size(dtype) * (size_t)nd * (size_t)stride, st);
+  if (e == cudaSuccess) {
+    if (dtype == SB_F32)
+      csr_to_dia<float><<<grid_for(N), kThreads, 0, st>>>(row_ptr, col, (const float*)val, N,
+                                                          stride, rank, (float*)data);
+    else
+      csr_to_dia<double><<<grid_for(N), kThreads, 0, st>>>(row_ptr, col, (const double*)val, N,
+                                                           stride, rank, (double*)data);
+    e = cudaGetLastError();
+  }
+  scratch_free(present, st);
+  if (e != cudaSuccess) return cuda_status(e, "sb_csr_dia");
+  return SB_OK;
+}
+
+}  // extern "C"

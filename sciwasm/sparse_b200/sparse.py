@@ -332,6 +332,64 @@ def spmv(A, x_view, y_view, inner_max=1, stream=None):
         raise TypeError(f"spmv: unsupported matrix object {type(A).__name__}")
 
 
+# --------------------------------------------------------------- conversions
+
+
+def coo_csr(A_coo, stream=None):
+    """coo_csr (src/sequential/src/sparse32.js:1674-1720): a new CSR object,
+    entries stably ordered by (row, col) exactly as the reference's count /
+    scan / scatter / per-row stable sort produces them."""
+    A = allocate_CSR(A_coo.N, A_coo.nnz, A_coo.dtype)
+    call("sb_coo_csr", _dtcode(A_coo.dtype), A_coo.row_index.ptr, A_coo.col_index.ptr,
+         A_coo.val_index.ptr, A_coo.N, A_coo.nnz, A.row_index.ptr, A.col_index.ptr,
+         A.val_index.ptr, _sp(stream))
+    return A
+
+
+def num_cols(A_csr, stream=None) -> int:
+    """num_cols (src/sequential/src/sparse32.js:1436-1447)."""
+    nc = C.c_int32(0)
+    call("sb_num_cols", A_csr.row_index.ptr, A_csr.N, C.byref(nc), _sp(stream))
+    return int(nc.value)
+
+
+def csr_ell(A_csr, stream=None):
+    """csr_ell (src/sequential/src/sparse32.js:1449-1484).  Returns None when
+    the reference's admission test refuses (it logs and returns undefined)."""
+    nc = num_cols(A_csr, stream)
+    lib = _lib.load()
+    if not lib.sb_ell_admitted(nc, A_csr.N, A_csr.nnz):
+        return None
+    E = allocate_ELL(A_csr.N, A_csr.nnz, nc, A_csr.dtype)
+    call("sb_csr_ell", _dtcode(A_csr.dtype), A_csr.row_index.ptr, A_csr.col_index.ptr,
+         A_csr.val_index.ptr, A_csr.N, A_csr.nnz, nc, E.indices_index.ptr, E.data_index.ptr,
+         _sp(stream))
+    return E
+
+
+def num_diags(A_csr, stream=None):
+    """num_diags (src/sequential/src/sparse32.js:1486-1512): [nd, stride]."""
+    nd = C.c_int32(0)
+    stride = C.c_int32(0)
+    call("sb_num_diags", A_csr.row_index.ptr, A_csr.col_index.ptr, A_csr.N, C.byref(nd),
+         C.byref(stride), _sp(stream))
+    return [int(nd.value), int(stride.value)]
+
+
+def csr_dia(A_csr, stream=None):
+    """csr_dia (src/sequential/src/sparse32.js:1515-1574).  Returns None when
+    the admission test refuses."""
+    nd, stride = num_diags(A_csr, stream)
+    lib = _lib.load()
+    if not lib.sb_dia_admitted(nd, stride, A_csr.nnz):
+        return None
+    D = allocate_DIA(A_csr.N, A_csr.nnz, nd, stride, A_csr.dtype)
+    call("sb_csr_dia", _dtcode(A_csr.dtype), A_csr.row_index.ptr, A_csr.col_index.ptr,
+         A_csr.val_index.ptr, A_csr.N, A_csr.nnz, nd, stride, D.offset_index.ptr,
+         D.data_index.ptr, _sp(stream))
+    return D
+
+
 def synchronize(stream=None) -> None:
     call("sb_stream_synchronize", _sp(stream))
 

@@ -73,3 +73,17 @@ def test_no_cpu_fallback_without_device(sb):
     assert st == -6, lib.sb_last_error()
     p = ctypes.c_void_p()
     assert lib.sb_malloc(ctypes.byref(p), 64) == -6
+
+
+def test_admission_predicates_match_oracle(sb, oracle):
+    """sb_ell_admitted / sb_dia_admitted are host-only: same answers as the
+    oracle's restatement of the reference's test on the known-answer cases."""
+    import json
+    k = json.load(open(os.path.join(ROOT, "tests", "golden", "kat_reference_semantics.json")))
+    lib = sb.load_library()
+    for c in k["admission"]["cases"]:
+        if c["N"] > 2**31 - 1:
+            continue
+        assert bool(lib.sb_ell_admitted(c["w"], c["N"], c["nnz"])) == c["admitted"], c
+        assert bool(lib.sb_dia_admitted(c["w"], c["N"], c["nnz"])) == c["admitted"], c
+        assert oracle.format_admitted(c["w"], c["N"], c["nnz"]) == c["admitted"]
