@@ -148,6 +148,58 @@ int sb_csr_dia(int dtype, const int32_t* row_ptr, const int32_t* col, const void
                int64_t nnz, int32_t nd, int32_t stride, int32_t* offset, void* data,
                void* stream);
 
+/* ---------------------------------------------------------------------- */
+/* Level sets and sparse triangular solves                                */
+/* ---------------------------------------------------------------------- */
+typedef struct sb_spts_plan sb_spts_plan;
+
+#define SB_SPTS_LEVEL 0    /* level by level (row kernel arithmetic)        */
+#define SB_SPTS_SYNCFREE 1 /* natural order, ready flags (sync-free order)  */
+#define SB_SPTS_HYBRID 2   /* level order, ready flags (row kernel order)   */
+
+#define SB_SPTS_ACC_NATIVE 0 /* accumulate and divide in the value type      */
+#define SB_SPTS_ACC_F64 1    /* f32 values: accumulate and divide in f64     */
+
+/* Replaces CSR_create_level_sets / CSR_create_level_sets_with_reorder
+ * (src/parallel/src/sparse32.js:2942-3181; older copy
+ * src/parallel/src/spts32.js:158-357).  Computes, bit-exactly, the level of
+ * every row, level_ptr, the stable permutation by level, its inverse
+ * (`order`) and the level-reordered CSR with relabelled columns.  The
+ * caller's row_ptr/col/val must outlive the plan (the sync-free solve reads
+ * them).  Returns after the analysis is complete. */
+int sb_spts_analyze(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                    int32_t N, int64_t nnz, void* stream, sb_spts_plan** plan);
+int sb_spts_plan_destroy(sb_spts_plan* plan);
+/* nlevels; solvable = 1 when every row ends with its diagonal and all other
+ * columns are below it (the solves' precondition). */
+int sb_spts_plan_info(const sb_spts_plan* plan, int32_t* nlevels, int32_t* solvable);
+/* Device-to-device copies of the analysis results (any pointer may be NULL):
+ * level[N], level_ptr[nlevels+1], permutation[N], order[N]. */
+int sb_spts_plan_levels(const sb_spts_plan* plan, int32_t* level, int32_t* level_ptr,
+                        int32_t* permutation, int32_t* order, void* stream);
+/* The level-reordered CSR (row_ptr[N+1], col[nnz], val[nnz]). */
+int sb_spts_plan_reordered(const sb_spts_plan* plan, int32_t* row_ptr, int32_t* col, void* val,
+                           void* stream);
+
+/* Solve L y = b (b, y in natural row order).  SB_SPTS_LEVEL replaces
+ * spts_level_csr (src/parallel/src/sparse_opt_32.wat:11759;
+ * src/parallel/src/spts_opt_32.wat:339-546), SB_SPTS_SYNCFREE replaces
+ * spts_csr_sync_free (src/parallel/src/spts_opt_32.wat:8-260) and
+ * SB_SPTS_HYBRID replaces spts_csr_opt_level_sync_free
+ * (src/parallel/src/sparse_opt_32.wat:12846-13445).  Stream-ordered; a
+ * dependency wait that runs out is reported by sb_device_status (code 2). */
+int sb_spts_solve(const sb_spts_plan* plan, int algo, int policy, const void* b, void* y,
+                  void* stream);
+
+/* Replaces the raw spts_csr_sync_free export on caller arrays without any
+ * structural check: every dependency wait is bounded by spin_limit_cycles
+ * (SM clock cycles, <= 0 for the default of about a second) and a wait that
+ * runs out makes the call return SB_ETIMEOUT instead of hanging.  Returns
+ * after the solve. */
+int sb_spts_syncfree_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                         int32_t N, const void* b, void* y, int64_t spin_limit_cycles,
+                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

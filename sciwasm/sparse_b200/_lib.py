@@ -31,6 +31,12 @@ SB_F32 = 0
 SB_F64 = 1
 SB_BF16 = 2
 
+SB_SPTS_LEVEL = 0
+SB_SPTS_SYNCFREE = 1
+SB_SPTS_HYBRID = 2
+SB_SPTS_ACC_NATIVE = 0
+SB_SPTS_ACC_F64 = 1
+
 # name -> argtypes (all functions return int status unless listed in _RESTYPE)
 SIGNATURES: dict[str, list] = {
     "sb_version": [],
@@ -62,6 +68,13 @@ SIGNATURES: dict[str, list] = {
     "sb_num_diags": [P, P, I32, C.POINTER(I32), C.POINTER(I32), P],
     "sb_dia_admitted": [I64, I32, I64],
     "sb_csr_dia": [C.c_int, P, P, P, I32, I64, I32, I32, P, P, P],
+    "sb_spts_analyze": [C.c_int, P, P, P, I32, I64, P, C.POINTER(P)],
+    "sb_spts_plan_destroy": [P],
+    "sb_spts_plan_info": [P, C.POINTER(I32), C.POINTER(I32)],
+    "sb_spts_plan_levels": [P, P, P, P, P, P],
+    "sb_spts_plan_reordered": [P, P, P, P, P],
+    "sb_spts_solve": [P, C.c_int, C.c_int, P, P, P],
+    "sb_spts_syncfree_csr": [C.c_int, P, P, P, I32, P, P, I64, P],
 }
 _RESTYPE = {"sb_last_error": C.c_char_p, "sb_status_string": C.c_char_p}
 

@@ -7,6 +7,9 @@
 
 namespace sb {
 namespace prim {
+// Internal linkage: each translation unit that includes this header gets its
+// own copy of these kernels and helpers.
+namespace {
 
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
@@ -216,5 +219,6 @@ inline int bits_for(long long maxval) {
   return b;
 }
 
+}  // namespace
 }  // namespace prim
 }  // namespace sb

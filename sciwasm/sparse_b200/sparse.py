@@ -390,6 +390,110 @@ def csr_dia(A_csr, stream=None):
     return D
 
 
+# --------------------------------------------------------------- level sets / SpTS
+
+_SPTS_ALGO = {"level": _lib.SB_SPTS_LEVEL, "syncfree": _lib.SB_SPTS_SYNCFREE,
+              "hybrid": _lib.SB_SPTS_HYBRID}
+_SPTS_POLICY = {"native": _lib.SB_SPTS_ACC_NATIVE, "f64": _lib.SB_SPTS_ACC_F64}
+
+
+class SptsPlan:
+    """Level-set analysis of a CSR matrix (owns the device plan; keeps the
+    analysed matrix alive because the sync-free solve reads it)."""
+
+    def __init__(self, A_csr, stream=None):
+        self.A = A_csr
+        p = C.c_void_p()
+        call("sb_spts_analyze", _dtcode(A_csr.dtype), A_csr.row_index.ptr, A_csr.col_index.ptr,
+             A_csr.val_index.ptr, A_csr.N, A_csr.nnz, _sp(stream), C.byref(p))
+        self.ptr = p.value
+        nl = C.c_int32(0)
+        ok = C.c_int32(0)
+        call("sb_spts_plan_info", self.ptr, C.byref(nl), C.byref(ok))
+        self.nlevels = int(nl.value)
+        self.solvable = bool(ok.value)
+
+    def levels(self, stream=None):
+        """(level, level_ptr, permutation, order) as device arrays."""
+        N = self.A.N
+        lv, perm, order = (DeviceArray(N, np.int32) for _ in range(3))
+        lp = DeviceArray(self.nlevels + 1, np.int32)
+        call("sb_spts_plan_levels", self.ptr, lv.ptr, lp.ptr, perm.ptr, order.ptr, _sp(stream))
+        call("sb_stream_synchronize", _sp(stream))
+        return lv, lp, perm, order
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            try:
+                _lib.load().sb_spts_plan_destroy(self.ptr)
+            except Exception:
+                pass
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
+
+
+def CSR_create_level_sets(A_csr, stream=None):
+    """CSR_create_level_sets (src/parallel/src/sparse32.js:2942-3008): attaches
+    nlevels, level_index (level_ptr) and permutation_index to A_csr."""
+    plan = SptsPlan(A_csr, stream)
+    lv, lp, perm, order = plan.levels(stream)
+    A_csr.nlevels, A_csr.level_index, A_csr.permutation_index = plan.nlevels, lp, perm
+    A_csr.level_per_row, A_csr.order_index, A_csr._plan = lv, order, plan
+    return A_csr
+
+
+def CSR_create_level_sets_with_reorder(A_csr, stream=None):
+    """CSR_create_level_sets_with_reorder (src/parallel/src/sparse32.js:3010-3181):
+    a new CSR whose rows are ordered by level and whose columns are relabelled
+    by order[], carrying nlevels, level_index, permutation_index."""
+    plan = SptsPlan(A_csr, stream)
+    lv, lp, perm, order = plan.levels(stream)
+    R = allocate_CSR(A_csr.N, A_csr.nnz, A_csr.dtype)
+    call("sb_spts_plan_reordered", plan.ptr, R.row_index.ptr, R.col_index.ptr, R.val_index.ptr,
+         _sp(stream))
+    call("sb_stream_synchronize", _sp(stream))
+    R.nlevels, R.level_index, R.permutation_index = plan.nlevels, lp, perm
+    R.level_per_row, R.order_index, R._plan = lv, order, plan
+    return R
+
+
+def _device_status() -> int:
+    code = C.c_int(0)
+    call("sb_device_status", C.byref(code))
+    return int(code.value)
+
+
+def spts(L, b_view, y_view, algo="level", policy="native", stream=None, check=True):
+    """Solve L y = b for a lower-triangular CSR L with its diagonal stored last
+    in every row (b, y in natural row order).  algo: "level" (level by level),
+    "syncfree" (ready flags, natural order) or "hybrid" (ready flags, level
+    order).  policy "f64" accumulates and divides in f64 for f32 values."""
+    plan = getattr(L, "_plan", None)
+    if plan is None or plan.ptr is None:
+        plan = SptsPlan(L, stream)
+        L._plan = plan
+    if b_view.dtype != L.dtype or y_view.dtype != L.dtype:
+        raise TypeError("b, y and L must share one value dtype")
+    call("sb_spts_solve", plan.ptr, _SPTS_ALGO[algo], _SPTS_POLICY[policy], b_view.vec_index.ptr,
+         y_view.vec_index.ptr, _sp(stream))
+    if check:
+        call("sb_stream_synchronize", _sp(stream))
+        st = _device_status()
+        if st:
+            raise _lib.SparseError("sb_spts_solve", _lib.SB_ETIMEOUT,
+                                   f"device status {st}: a dependency wait ran out")
+
+
+def spts_csr_sync_free(L, b_view, y_view, spin_limit_cycles=0, stream=None):
+    """The raw sync-free kernel (src/parallel/src/spts_opt_32.wat:8-260) on the
+    caller's arrays, without structural checks; waits are bounded."""
+    call("sb_spts_syncfree_csr", _dtcode(L.dtype), L.row_index.ptr, L.col_index.ptr,
+         L.val_index.ptr, L.N, b_view.vec_index.ptr, y_view.vec_index.ptr,
+         int(spin_limit_cycles), _sp(stream))
+
+
 def synchronize(stream=None) -> None:
     call("sb_stream_synchronize", _sp(stream))
 
