@@ -200,6 +200,93 @@ int sb_spts_syncfree_csr(int dtype, const int32_t* row_ptr, const int32_t* col, 
                          int32_t N, const void* b, void* y, int64_t spin_limit_cycles,
                          void* stream);
 
+/* ---------------------------------------------------------------------- */
+/* eliminate_zeros and transpose (bit-exact with the reference's kernels). */
+/* The nonzero test is v > 0 || v < 0 (+0, -0 and NaN count as zeros).    */
+/* Calls that return a count return after the device work is complete.    */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces count_nonzeros_coo (src/sequential/src/sparse_opt_32.wat:500),
+ * used for COO and CSR values (src/sequential/src/sparse32.js:1140-1175). */
+int sb_count_nonzeros(int dtype, const void* val, int64_t n, int64_t* count, void* stream);
+/* Replaces copy_nonzeros_coo (src/sequential/src/sparse_opt_32.wat:523-546). */
+int sb_copy_nonzeros_coo(int dtype, const int32_t* row, const int32_t* col, const void* val,
+                         int64_t nnz, int32_t* orow, int32_t* ocol, void* oval, void* stream);
+/* Replaces copy_nonzeros_csr (src/sequential/src/sparse_opt_32.wat:548-595)
+ * over the N rows (out_row_ptr[N+1] rebuilt). */
+int sb_copy_nonzeros_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                         int32_t N, int64_t nnz, int32_t* orow_ptr, int32_t* ocol, void* oval,
+                         void* stream);
+/* Replaces count_nonzeros_dia (src/sequential/src/sparse_opt_32.wat:1948-2039). */
+int sb_count_nonzeros_dia(int dtype, const int32_t* offset, const void* data, int32_t nd,
+                          int32_t stride, int32_t N, int32_t* count_diags, int64_t* count,
+                          void* stream);
+/* Replaces copy_nonzeros_dia (src/sequential/src/sparse_opt_32.wat:2041-2134):
+ * diagonals without nonzeros are dropped and each kept diagonal's nonzeros
+ * are packed contiguously from its first in-band row, as the reference does;
+ * odata (count_diags*stride) is zero-filled by the call. */
+int sb_copy_nonzeros_dia(int dtype, const int32_t* offset, const void* data, int32_t nd,
+                         int32_t stride, int32_t N, int32_t* ooffset, void* odata, void* stream);
+/* Replaces count_nonzeros_ell (src/sequential/src/sparse_opt_32.wat:5821-5893). */
+int sb_count_nonzeros_ell(int dtype, const void* data, int32_t nc, int32_t N, int32_t* count_cols,
+                          int64_t* count, void* stream);
+/* Replaces copy_nonzeros_ell (src/sequential/src/sparse_opt_32.wat:5895-5947):
+ * each row's nonzeros packed in slot order into out_nc column-major slots. */
+int sb_copy_nonzeros_ell(int dtype, const void* data, const int32_t* indices, int32_t nc,
+                         int32_t N, int32_t out_nc, void* odata, int32_t* oindices, void* stream);
+/* Replaces the COO branch of transpose (src/sequential/src/sparse32.js:1106-1115):
+ * row and column arrays exchanged, no re-sort. */
+int sb_transpose_coo(int dtype, const int32_t* row, const int32_t* col, const void* val,
+                     int64_t nnz, int32_t* orow, int32_t* ocol, void* oval, void* stream);
+/* Replaces transpose_csr (src/sequential/src/sparse_opt_32.wat:6348-6477). */
+int sb_transpose_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                     int32_t N, int64_t nnz, int32_t* orow_ptr, int32_t* ocol, void* oval,
+                     void* stream);
+/* Replaces transpose_dia (src/sequential/src/sparse_opt_32.wat:6479-6572):
+ * offsets negated in their stored order; out-of-band slots are zeroed. */
+int sb_transpose_dia(int dtype, const int32_t* offset, const void* data, int32_t nd,
+                     int32_t stride, int32_t N, int32_t* ooffset, void* odata, void* stream);
+/* Replaces count_transpose_cols_ell (src/sequential/src/sparse_opt_32.wat:6574-6632). */
+int sb_count_transpose_cols_ell(int dtype, const void* data, const int32_t* indices, int32_t nc,
+                                int32_t N, int32_t* count_cols, void* stream);
+/* Replaces transpose_ell (src/sequential/src/sparse_opt_32.wat:6634-6701);
+ * padding slots of the output are zeroed. */
+int sb_transpose_ell(int dtype, const void* data, const int32_t* indices, int32_t nc, int32_t N,
+                     int32_t out_nc, void* odata, int32_t* oindices, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* Element-wise maps                                                      */
+/* ---------------------------------------------------------------------- */
+#define SB_MAP_EXPM1 0
+#define SB_MAP_LOG1P 1
+#define SB_MAP_SIN 2
+#define SB_MAP_TAN 3
+#define SB_MAP_POW 4      /* p = exponent */
+#define SB_MAP_DEG2RAD 5  /* p = pi (the reference passes Math.PI) */
+#define SB_MAP_RAD2DEG 6  /* p = pi */
+#define SB_MAP_SIGN 7
+#define SB_MAP_ABS 8
+#define SB_MAP_NEG 9
+#define SB_MAP_SQRT 10
+#define SB_MAP_CEIL 11
+#define SB_MAP_FLOOR 12
+#define SB_MAP_TRUNC 13
+#define SB_MAP_NEAREST 14 /* round half to even */
+#define SB_MAP_MULTIPLY 15 /* p = scalar */
+
+/* Replaces the *_coo maps (src/sequential/src/sparse_opt_32.wat:597-1699),
+ * applied to COO and CSR value arrays (src/sequential/src/sparse32.js:671-1104);
+ * in == out is the in-place form. */
+int sb_map_coo(int dtype, int op, double p, const void* in, void* out, int64_t n, void* stream);
+/* Replaces the *_ell maps (src/sequential/src/sparse_opt_32.wat:4977-6346):
+ * every one of the ncols*N slots, padding included. */
+int sb_map_ell(int dtype, int op, double p, const void* in, void* out, int32_t ncols, int32_t N,
+               void* stream);
+/* Replaces the *_dia maps (src/sequential/src/sparse_opt_32.wat:2137-4976):
+ * in-band slots only. */
+int sb_map_dia(int dtype, int op, double p, const int32_t* offset, const void* in, void* out,
+               int32_t ndiags, int32_t stride, int32_t N, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

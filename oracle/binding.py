@@ -56,6 +56,19 @@ _SIG = {
     "or_truth_spts": ([C.c_int, _P, _P, _P, _P, _P, _I32], None),
     "or_par_spts_level_f32": ([C.c_int, _P, _I32, _P, _P, _P, _P, _P, _I32], None),
     "or_par_spts_level_f64": ([C.c_int, _P, _I32, _P, _P, _P, _P, _P, _I32], None),
+    "or_count_nonzeros": ([C.c_int, _P, _I64], _I64),
+    "or_copy_nonzeros_coo": ([C.c_int, _P, _P, _P, _I64, _P, _P, _P], _I64),
+    "or_copy_nonzeros_csr": ([C.c_int, _P, _P, _P, _I32, _P, _P, _P], None),
+    "or_count_nonzeros_dia": ([C.c_int, _P, _P, _I32, _I32, _I32, _P, _P], None),
+    "or_copy_nonzeros_dia": ([C.c_int, _P, _P, _I32, _I32, _I32, _P, _P], None),
+    "or_count_nonzeros_ell": ([C.c_int, _P, _I32, _I32, _P, _P], None),
+    "or_copy_nonzeros_ell": ([C.c_int, _P, _P, _I32, _I32, _P, _P], None),
+    "or_transpose_csr": ([C.c_int, _P, _P, _P, _I32, _I64, _P, _P, _P], None),
+    "or_transpose_dia": ([C.c_int, _P, _P, _I32, _I32, _I32, _P, _P], None),
+    "or_count_transpose_cols_ell": ([C.c_int, _P, _P, _I32, _I32], _I32),
+    "or_transpose_ell": ([C.c_int, _P, _P, _I32, _I32, _P, _P], None),
+    "or_map": ([C.c_int, C.c_int, C.c_int, C.c_double, _P, _P, _I64], None),
+    "or_map_dia": ([C.c_int, C.c_int, C.c_double, _P, _P, _P, _I32, _I32, _I32], None),
     "or_fletcher_f32": ([_P, _I64], _I64),
     "or_fletcher_f64": ([_P, _I64], _I64),
 }
@@ -305,3 +318,94 @@ def par_spts_level(nthreads, level_ptr, row_ptr, col, val, b, y):
 def fletcher(y):
     y = np.ascontiguousarray(y)
     return int(getattr(lib(), "or_fletcher_" + _sfx(y.dtype))(_p(y), y.size))
+
+
+# ------------------------------------------------------------------ structure ops
+
+def count_nonzeros(val):
+    val = np.ascontiguousarray(val)
+    return int(lib().or_count_nonzeros(val.dtype.itemsize, _p(val), val.size))
+
+
+def copy_nonzeros_coo(row, col, val):
+    row, col, val = _i32(row), _i32(col), np.ascontiguousarray(val)
+    n = count_nonzeros(val)
+    orow, ocol, oval = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, val.dtype)
+    lib().or_copy_nonzeros_coo(val.dtype.itemsize, _p(row), _p(col), _p(val), row.size, _p(orow),
+                               _p(ocol), _p(oval))
+    return orow, ocol, oval
+
+
+def copy_nonzeros_csr(row_ptr, col, val):
+    row_ptr, col, val = _i32(row_ptr), _i32(col), np.ascontiguousarray(val)
+    n = count_nonzeros(val)
+    orp, ocol, oval = np.zeros(row_ptr.size, np.int32), np.zeros(n, np.int32), np.zeros(n, val.dtype)
+    lib().or_copy_nonzeros_csr(val.dtype.itemsize, _p(row_ptr), _p(col), _p(val), row_ptr.size - 1,
+                               _p(orp), _p(ocol), _p(oval))
+    return orp, ocol, oval
+
+
+def nonzeros_dia(offset, data, N, stride=None):
+    offset, data = _i32(offset), np.ascontiguousarray(data)
+    stride = N if stride is None else stride
+    cd, cnt = np.zeros(1, np.int32), np.zeros(1, np.int64)
+    lib().or_count_nonzeros_dia(data.dtype.itemsize, _p(offset), _p(data), offset.size, stride, N,
+                                _p(cd), _p(cnt))
+    ooff = np.zeros(int(cd[0]), np.int32)
+    odat = np.zeros(int(cd[0]) * stride, data.dtype)
+    lib().or_copy_nonzeros_dia(data.dtype.itemsize, _p(offset), _p(data), offset.size, stride, N,
+                               _p(ooff), _p(odat))
+    return int(cd[0]), int(cnt[0]), ooff, odat
+
+
+def nonzeros_ell(data, indices, nc, N):
+    data, indices = np.ascontiguousarray(data), _i32(indices)
+    cc, cnt = np.zeros(1, np.int32), np.zeros(1, np.int64)
+    lib().or_count_nonzeros_ell(data.dtype.itemsize, _p(data), nc, N, _p(cc), _p(cnt))
+    onc = int(cc[0])
+    od, oi = np.zeros(onc * N, data.dtype), np.zeros(onc * N, np.int32)
+    lib().or_copy_nonzeros_ell(data.dtype.itemsize, _p(data), _p(indices), nc, N, _p(od), _p(oi))
+    return onc, int(cnt[0]), od, oi
+
+
+def transpose_csr(row_ptr, col, val):
+    row_ptr, col, val = _i32(row_ptr), _i32(col), np.ascontiguousarray(val)
+    N = row_ptr.size - 1
+    orp, ocol, oval = np.zeros(N + 1, np.int32), np.zeros(col.size, np.int32), np.zeros(col.size, val.dtype)
+    lib().or_transpose_csr(val.dtype.itemsize, _p(row_ptr), _p(col), _p(val), N, col.size, _p(orp),
+                           _p(ocol), _p(oval))
+    return orp, ocol, oval
+
+
+def transpose_dia(offset, data, N, stride=None):
+    offset, data = _i32(offset), np.ascontiguousarray(data)
+    stride = N if stride is None else stride
+    ooff, odat = np.zeros(offset.size, np.int32), np.zeros(data.size, data.dtype)
+    lib().or_transpose_dia(data.dtype.itemsize, _p(offset), _p(data), offset.size, stride, N,
+                           _p(ooff), _p(odat))
+    return ooff, odat
+
+
+def transpose_ell(data, indices, nc, N):
+    data, indices = np.ascontiguousarray(data), _i32(indices)
+    onc = int(lib().or_count_transpose_cols_ell(data.dtype.itemsize, _p(data), _p(indices), nc, N))
+    od, oi = np.zeros(onc * N, data.dtype), np.zeros(onc * N, np.int32)
+    lib().or_transpose_ell(data.dtype.itemsize, _p(data), _p(indices), nc, N, _p(od), _p(oi))
+    return onc, od, oi
+
+
+def map_values(values, kind, op, p=0.0):
+    """kind 0: COO/CSR kernels, 1: DIA/ELL kernels."""
+    a = np.ascontiguousarray(values)
+    out = np.empty_like(a)
+    lib().or_map(a.dtype.itemsize, kind, op, float(p), _p(a), _p(out), a.size)
+    return out
+
+
+def map_dia(offset, data, N, op, p=0.0, out=None, stride=None):
+    offset, data = _i32(offset), np.ascontiguousarray(data)
+    stride = N if stride is None else stride
+    out = np.zeros_like(data) if out is None else np.array(out, copy=True)
+    lib().or_map_dia(data.dtype.itemsize, op, float(p), _p(offset), _p(data), _p(out), offset.size,
+                     stride, N)
+    return out

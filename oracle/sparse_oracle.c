@@ -688,3 +688,267 @@ static double matlab_modulo(double x, double y) {
   }
 DEF_FLETCHER(float, f32)
 DEF_FLETCHER(double, f64)
+
+/* ======================= structure operations ======================= */
+
+static int is_nz(const void* a, int64_t i, int w) {
+  if (w == 4) { float v = ((const float*)a)[i]; return v > 0.0f || v < 0.0f; }
+  double v = ((const double*)a)[i];
+  return v > 0.0 || v < 0.0;
+}
+
+int64_t or_count_nonzeros(int w, const void* val, int64_t n) {
+  int64_t c = 0;
+  for (int64_t i = 0; i < n; ++i) c += is_nz(val, i, w);
+  return c;
+}
+
+int64_t or_copy_nonzeros_coo(int w, const int32_t* row, const int32_t* col, const void* val,
+                             int64_t nnz, int32_t* orow, int32_t* ocol, void* oval) {
+  int64_t o = 0;
+  for (int64_t i = 0; i < nnz; ++i) {
+    if (is_nz(val, i, w)) {
+      orow[o] = row[i];
+      ocol[o] = col[i];
+      copy_elem(oval, o, val, i, w);
+      o++;
+    }
+  }
+  return o;
+}
+
+void or_copy_nonzeros_csr(int w, const int32_t* row_ptr, const int32_t* col, const void* val,
+                          int32_t N, int32_t* orow_ptr, int32_t* ocol, void* oval) {
+  int64_t o = 0;
+  orow_ptr[0] = 0;
+  for (int32_t i = 0; i < N; ++i) {
+    for (int32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j) {
+      if (is_nz(val, j, w)) {
+        ocol[o] = col[j];
+        copy_elem(oval, o, val, j, w);
+        o++;
+      }
+    }
+    orow_ptr[i + 1] = (int32_t)o;
+  }
+}
+
+static void dia_range(int32_t k, int32_t N, int32_t* lo, int32_t* hi) {
+  *lo = k < 0 ? -k : 0;
+  *hi = (N < N - k) ? N : N - k;
+}
+
+void or_count_nonzeros_dia(int w, const int32_t* offset, const void* data, int32_t nd,
+                           int32_t stride, int32_t N, int32_t* count_diags, int64_t* count) {
+  int32_t cd = 0;
+  int64_t nz = 0;
+  for (int32_t d = 0; d < nd; ++d) {
+    int32_t lo, hi;
+    dia_range(offset[d], N, &lo, &hi);
+    int64_t base = (int64_t)d * stride - (offset[d] < 0 ? (int64_t)(N - stride) : 0);
+    int64_t c = 0;
+    for (int32_t n = lo; n < hi; ++n) c += is_nz(data, base + n, w);
+    if (c) { cd++; nz += c; }
+  }
+  *count_diags = cd;
+  *count = nz;
+}
+
+void or_copy_nonzeros_dia(int w, const int32_t* offset, const void* data, int32_t nd,
+                          int32_t stride, int32_t N, int32_t* ooffset, void* odata) {
+  int64_t j = 0; /* kept diagonals * stride */
+  int32_t od = 0;
+  for (int32_t d = 0; d < nd; ++d) {
+    int32_t lo, hi;
+    dia_range(offset[d], N, &lo, &hi);
+    int64_t base = (int64_t)d * stride - (offset[d] < 0 ? (int64_t)(N - stride) : 0);
+    int64_t out = j + lo, c = 0;
+    for (int32_t n = lo; n < hi; ++n) {
+      if (is_nz(data, base + n, w)) {
+        copy_elem(odata, out++, data, base + n, w);
+        c++;
+      }
+    }
+    if (c) {
+      ooffset[od++] = offset[d];
+      j += stride;
+    }
+  }
+}
+
+void or_count_nonzeros_ell(int w, const void* data, int32_t nc, int32_t N, int32_t* count_cols,
+                           int64_t* count) {
+  int32_t* per = (int32_t*)calloc((size_t)(N > 0 ? N : 1), sizeof(int32_t));
+  int32_t cc = 0;
+  int64_t nz = 0;
+  for (int32_t k = 0; k < nc; ++k)
+    for (int32_t i = 0; i < N; ++i)
+      if (is_nz(data, (int64_t)k * N + i, w)) {
+        per[i]++;
+        if (per[i] > cc) cc = per[i];
+        nz++;
+      }
+  free(per);
+  *count_cols = cc;
+  *count = nz;
+}
+
+void or_copy_nonzeros_ell(int w, const void* data, const int32_t* indices, int32_t nc, int32_t N,
+                          void* odata, int32_t* oindices) {
+  int64_t* pos = (int64_t*)calloc((size_t)(N > 0 ? N : 1), sizeof(int64_t));
+  for (int32_t k = 0; k < nc; ++k)
+    for (int32_t i = 0; i < N; ++i) {
+      int64_t s = (int64_t)k * N + i;
+      if (is_nz(data, s, w)) {
+        copy_elem(odata, pos[i] + i, data, s, w);
+        oindices[pos[i] + i] = indices[s];
+        pos[i] += N;
+      }
+    }
+  free(pos);
+}
+
+void or_transpose_csr(int w, const int32_t* row_ptr, const int32_t* col, const void* val,
+                      int32_t N, int64_t nnz, int32_t* orow_ptr, int32_t* ocol, void* oval) {
+  memset(orow_ptr, 0, sizeof(int32_t) * ((size_t)N + 1));
+  for (int64_t j = 0; j < nnz; ++j) orow_ptr[col[j]]++;
+  int32_t sum = 0;
+  for (int32_t i = 0; i < N; ++i) {
+    int32_t c = orow_ptr[i];
+    orow_ptr[i] = sum;
+    sum += c;
+  }
+  orow_ptr[N] = (int32_t)nnz;
+  for (int32_t i = 0; i < N; ++i)
+    for (int32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j) {
+      int32_t a = orow_ptr[col[j]]++;
+      ocol[a] = i;
+      copy_elem(oval, a, val, j, w);
+    }
+  sum = 0;
+  for (int32_t i = 0; i <= N; ++i) {
+    int32_t t = orow_ptr[i];
+    orow_ptr[i] = sum;
+    sum = t;
+  }
+}
+
+void or_transpose_dia(int w, const int32_t* offset, const void* data, int32_t nd, int32_t stride,
+                      int32_t N, int32_t* ooffset, void* odata) {
+  for (int32_t d = 0; d < nd; ++d) {
+    int32_t k = offset[d];
+    int32_t lo, hi;
+    dia_range(k, N, &lo, &hi);
+    ooffset[d] = -k;
+    int32_t olo, ohi;
+    dia_range(-k, N, &olo, &ohi);
+    int64_t ib = (int64_t)d * stride - (k < 0 ? (int64_t)(N - stride) : 0);
+    int64_t ob = (int64_t)d * stride - (-k < 0 ? (int64_t)(N - stride) : 0);
+    for (int32_t t = 0; t < hi - lo; ++t) copy_elem(odata, ob + olo + t, data, ib + lo + t, w);
+  }
+}
+
+int32_t or_count_transpose_cols_ell(int w, const void* data, const int32_t* indices, int32_t nc,
+                                    int32_t N) {
+  int32_t* cnt = (int32_t*)calloc((size_t)(N > 0 ? N : 1), sizeof(int32_t));
+  int32_t cc = 0;
+  for (int32_t k = 0; k < nc; ++k)
+    for (int32_t i = 0; i < N; ++i) {
+      int64_t s = (int64_t)k * N + i;
+      if (is_nz(data, s, w)) {
+        int32_t c = ++cnt[indices[s]];
+        if (c > cc) cc = c;
+      }
+    }
+  free(cnt);
+  return cc;
+}
+
+void or_transpose_ell(int w, const void* data, const int32_t* indices, int32_t nc, int32_t N,
+                      void* odata, int32_t* oindices) {
+  int64_t* pos = (int64_t*)calloc((size_t)(N > 0 ? N : 1), sizeof(int64_t));
+  for (int32_t j = 0; j < N; ++j)
+    for (int32_t k = 0; k < nc; ++k) {
+      int64_t s = (int64_t)k * N + j;
+      if (is_nz(data, s, w)) {
+        int32_t c = indices[s];
+        copy_elem(odata, pos[c] + c, data, s, w);
+        oindices[pos[c] + c] = j;
+        pos[c] += N;
+      }
+    }
+  free(pos);
+}
+
+/* ======================= element-wise maps ======================= */
+
+static double map_f64(int kind, int op, double p, double v) {
+  switch (op) {
+    case 0: return expm1(v);
+    case 1: return log1p(v);
+    case 2: return sin(v);
+    case 3: return tan(v);
+    case 4: return pow(v, p);
+    case 5: return v * (p / 180.0);
+    case 6: return v / (p / 180.0);
+    case 7:
+      if (kind == 1 && v == 0.0) return 0.0;
+      return v > 0.0 ? 1.0 : -1.0;
+    case 8: return fabs(v);
+    case 9: return -v;
+    case 10: return sqrt(v);
+    case 11: return ceil(v);
+    case 12: return floor(v);
+    case 13: return trunc(v);
+    case 14: return nearbyint(v); /* default rounding mode: ties to even */
+    case 15: return v * p;
+  }
+  return v;
+}
+
+static float map_f32(int kind, int op, float p, float v) {
+  switch (op) {
+    case 0: return (float)expm1((double)v);
+    case 1: return (float)log1p((double)v);
+    case 2: return (float)sin((double)v);
+    case 3: return (float)tan((double)v);
+    case 4: return (float)pow((double)v, (double)p);
+    case 5: { float k = p / 180.0f; return v * k; }
+    case 6: { float k = p / 180.0f; return v / k; }
+    case 7:
+      if (kind == 1 && v == 0.0f) return 0.0f;
+      return v > 0.0f ? 1.0f : -1.0f;
+    case 8: return fabsf(v);
+    case 9: return -v;
+    case 10: return sqrtf(v);
+    case 11: return ceilf(v);
+    case 12: return floorf(v);
+    case 13: return truncf(v);
+    case 14: return nearbyintf(v);
+    case 15: return v * p;
+  }
+  return v;
+}
+
+void or_map(int w, int kind, int op, double p, const void* in, void* out, int64_t n) {
+  if (w == 4) {
+    const float* a = (const float*)in;
+    float* b = (float*)out;
+    for (int64_t i = 0; i < n; ++i) b[i] = map_f32(kind, op, (float)p, a[i]);
+  } else {
+    const double* a = (const double*)in;
+    double* b = (double*)out;
+    for (int64_t i = 0; i < n; ++i) b[i] = map_f64(kind, op, p, a[i]);
+  }
+}
+
+void or_map_dia(int w, int op, double p, const int32_t* offset, const void* in, void* out,
+                int32_t nd, int32_t stride, int32_t N) {
+  for (int32_t d = 0; d < nd; ++d) {
+    int32_t lo, hi;
+    dia_range(offset[d], N, &lo, &hi);
+    int64_t base = (int64_t)d * stride - (offset[d] < 0 ? (int64_t)(N - stride) : 0);
+    if (hi > lo) or_map(w, 1, op, p, (const char*)in + (size_t)w * (base + lo),
+                        (char*)out + (size_t)w * (base + lo), hi - lo);
+  }
+}

@@ -154,6 +154,59 @@ void or_par_spts_level_f32(int nthreads, const int32_t* level_ptr, int32_t nleve
 int64_t or_fletcher_f32(const float* y, int64_t n);
 int64_t or_fletcher_f64(const double* y, int64_t n);
 
+/* ---------------- structure operations (FP32 and FP64 values) ---------------- */
+/* Nonzero test of every eliminate_zeros kernel: v > 0 || v < 0 (drops +0, -0
+ * and NaN): src/sequential/src/sparse_opt_32.wat:500-521. */
+int64_t or_count_nonzeros(int val_bytes, const void* val, int64_t n);
+/* copy_nonzeros_coo: :523-546 (stable compaction). Returns the count. */
+int64_t or_copy_nonzeros_coo(int val_bytes, const int32_t* row, const int32_t* col,
+                             const void* val, int64_t nnz, int32_t* orow, int32_t* ocol,
+                             void* oval);
+/* copy_nonzeros_csr: :548-595 over the N rows (out_row_ptr rebuilt). */
+void or_copy_nonzeros_csr(int val_bytes, const int32_t* row_ptr, const int32_t* col,
+                          const void* val, int32_t N, int32_t* orow_ptr, int32_t* ocol,
+                          void* oval);
+/* count_nonzeros_dia :1948-2039 -> (count_diags, nnz); copy_nonzeros_dia
+ * :2041-2134 packs each kept diagonal's nonzeros contiguously from the
+ * diagonal's first in-band row (odata must be zero-filled, ndiags_out*stride). */
+void or_count_nonzeros_dia(int val_bytes, const int32_t* offset, const void* data,
+                           int32_t nd, int32_t stride, int32_t N, int32_t* count_diags,
+                           int64_t* count);
+void or_copy_nonzeros_dia(int val_bytes, const int32_t* offset, const void* data, int32_t nd,
+                          int32_t stride, int32_t N, int32_t* ooffset, void* odata);
+/* count_nonzeros_ell :5821-5893 -> (count_cols, nnz); copy_nonzeros_ell
+ * :5895-5947 packs each row's nonzeros in slot order (outputs zero-filled). */
+void or_count_nonzeros_ell(int val_bytes, const void* data, int32_t nc, int32_t N,
+                           int32_t* count_cols, int64_t* count);
+void or_copy_nonzeros_ell(int val_bytes, const void* data, const int32_t* indices, int32_t nc,
+                          int32_t N, void* odata, int32_t* oindices);
+/* transpose_csr :6348-6477 (counting sort by column, stable in row order). */
+void or_transpose_csr(int val_bytes, const int32_t* row_ptr, const int32_t* col, const void* val,
+                      int32_t N, int64_t nnz, int32_t* orow_ptr, int32_t* ocol, void* oval);
+/* transpose_dia :6479-6572: offsets negated in the same order, each in-band
+ * run moved to the negated diagonal's in-band rows.  Slots outside the band
+ * are left as they are in odata (callers zero-fill). */
+void or_transpose_dia(int val_bytes, const int32_t* offset, const void* data, int32_t nd,
+                      int32_t stride, int32_t N, int32_t* ooffset, void* odata);
+/* count_transpose_cols_ell :6574-6632 and transpose_ell :6634-6701 (source
+ * rows outer, slots inner; odata/oindices zero-filled by the caller). */
+int32_t or_count_transpose_cols_ell(int val_bytes, const void* data, const int32_t* indices,
+                                    int32_t nc, int32_t N);
+void or_transpose_ell(int val_bytes, const void* data, const int32_t* indices, int32_t nc,
+                      int32_t N, void* odata, int32_t* oindices);
+
+/* ---------------- element-wise maps ---------------- */
+/* op codes (shared with libsparse_b200): 0 expm1, 1 log1p, 2 sin, 3 tan,
+ * 4 pow(p), 5 deg2rad, 6 rad2deg, 7 sign, 8 abs, 9 neg, 10 sqrt, 11 ceil,
+ * 12 floor, 13 trunc, 14 nearest, 15 multiply(p).  `kind` 0 = the COO/CSR
+ * kernels (sign: v > 0 ? 1 : -1), 1 = the DIA/ELL kernels (sign: 0 -> 0).
+ * f32 transcendentals are computed in double and rounded, as the imported
+ * JavaScript Math functions are (src/sequential/src/sparse_opt_32.wat:5-9). */
+void or_map(int val_bytes, int kind, int op, double p, const void* in, void* out, int64_t n);
+/* DIA maps touch only in-band slots (src/sequential/src/sparse_opt_32.wat:2137-4976). */
+void or_map_dia(int val_bytes, int op, double p, const int32_t* offset, const void* in,
+                void* out, int32_t nd, int32_t stride, int32_t N);
+
 #ifdef __cplusplus
 }
 #endif

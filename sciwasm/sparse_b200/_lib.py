@@ -75,6 +75,21 @@ SIGNATURES: dict[str, list] = {
     "sb_spts_plan_reordered": [P, P, P, P, P],
     "sb_spts_solve": [P, C.c_int, C.c_int, P, P, P],
     "sb_spts_syncfree_csr": [C.c_int, P, P, P, I32, P, P, I64, P],
+    "sb_count_nonzeros": [C.c_int, P, I64, C.POINTER(I64), P],
+    "sb_copy_nonzeros_coo": [C.c_int, P, P, P, I64, P, P, P, P],
+    "sb_copy_nonzeros_csr": [C.c_int, P, P, P, I32, I64, P, P, P, P],
+    "sb_count_nonzeros_dia": [C.c_int, P, P, I32, I32, I32, C.POINTER(I32), C.POINTER(I64), P],
+    "sb_copy_nonzeros_dia": [C.c_int, P, P, I32, I32, I32, P, P, P],
+    "sb_count_nonzeros_ell": [C.c_int, P, I32, I32, C.POINTER(I32), C.POINTER(I64), P],
+    "sb_copy_nonzeros_ell": [C.c_int, P, P, I32, I32, I32, P, P, P],
+    "sb_transpose_coo": [C.c_int, P, P, P, I64, P, P, P, P],
+    "sb_transpose_csr": [C.c_int, P, P, P, I32, I64, P, P, P, P],
+    "sb_transpose_dia": [C.c_int, P, P, I32, I32, I32, P, P, P],
+    "sb_count_transpose_cols_ell": [C.c_int, P, P, I32, I32, C.POINTER(I32), P],
+    "sb_transpose_ell": [C.c_int, P, P, I32, I32, I32, P, P, P],
+    "sb_map_coo": [C.c_int, C.c_int, C.c_double, P, P, I64, P],
+    "sb_map_ell": [C.c_int, C.c_int, C.c_double, P, P, I32, I32, P],
+    "sb_map_dia": [C.c_int, C.c_int, C.c_double, P, P, P, I32, I32, I32, P],
 }
 _RESTYPE = {"sb_last_error": C.c_char_p, "sb_status_string": C.c_char_p}
 

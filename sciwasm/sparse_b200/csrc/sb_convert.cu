@@ -37,17 +37,6 @@ __global__ void coo_check(const int* __restrict__ row, const int* __restrict__ c
   }
 }
 
-// row_ptr from a row array sorted ascending: row_ptr[r] = first position of
-// a row >= r.  Every row_ptr entry is written exactly once.
-__global__ void row_ptr_from_sorted(const int* __restrict__ row, long long nnz, int N,
-                                    int* __restrict__ row_ptr) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > nnz) return;
-  const int prev = (i == 0) ? -1 : row[i - 1];
-  const int cur = (i == nnz) ? N : row[i];
-  for (int r = prev + 1; r <= cur; ++r) row_ptr[r] = (int)i;
-}
-
 __global__ void pack_keys(const int* __restrict__ row, const int* __restrict__ col,
                           long long nnz, unsigned long long* __restrict__ keys,
                           unsigned* __restrict__ idx) {
@@ -186,7 +175,7 @@ static int coo_csr_impl(const int* row, const int* col, const T* val, int N, lon
     // already in (row, col) order: the stable sort is the identity
     SB_CHECK_CUDA(cudaMemcpyAsync(csr_col, col, sizeof(int) * nnz, cudaMemcpyDeviceToDevice, st));
     SB_CHECK_CUDA(cudaMemcpyAsync(csr_val, val, sizeof(T) * nnz, cudaMemcpyDeviceToDevice, st));
-    row_ptr_from_sorted<<<grid_for(nnz + 1), kThreads, 0, st>>>(row, nnz, N, csr_row);
+    prim::row_ptr_from_sorted<<<grid_for(nnz + 1), kThreads, 0, st>>>(row, nnz, N, csr_row);
     SB_CHECK_LAUNCH("row_ptr_from_sorted");
     return SB_OK;
   }
@@ -216,7 +205,7 @@ static int coo_csr_impl(const int* row, const int* col, const T* val, int N, lon
     if (e != cudaSuccess) r = cuda_status(e, "unpack_sorted");
   }
   if (!r) {
-    row_ptr_from_sorted<<<grid_for(nnz + 1), kThreads, 0, st>>>(rows_sorted, nnz, N, csr_row);
+    prim::row_ptr_from_sorted<<<grid_for(nnz + 1), kThreads, 0, st>>>(rows_sorted, nnz, N, csr_row);
     e = cudaGetLastError();
     if (e != cudaSuccess) r = cuda_status(e, "row_ptr_from_sorted");
   }

@@ -103,6 +103,24 @@ inline int exclusive_scan(const int* in, int* out, long long n, cudaStream_t st)
   return r;
 }
 
+// row_ptr from a row array sorted ascending: row_ptr[r] = first position of
+// a row >= r.  Every row_ptr entry (0..N) is written exactly once.
+__global__ void row_ptr_from_sorted(const int* __restrict__ row, long long nnz, int N,
+                                    int* __restrict__ row_ptr) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > nnz) return;
+  const int prev = (i == 0) ? -1 : row[i - 1];
+  const int cur = (i == nnz) ? N : row[i];
+  for (int r = prev + 1; r <= cur; ++r) row_ptr[r] = (int)i;
+}
+
+// Row index of every CSR entry.
+__global__ void expand_rows(const int* __restrict__ row_ptr, int N, int* __restrict__ row_of) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (int j = row_ptr[i]; j < row_ptr[i + 1]; ++j) row_of[j] = i;
+}
+
 // ------------------------------------------------------------ radix sort
 
 constexpr int kRadixThreads = 256;

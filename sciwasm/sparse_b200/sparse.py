@@ -390,6 +390,174 @@ def csr_dia(A_csr, stream=None):
     return D
 
 
+# --------------------------------------------------------------- transpose / eliminate_zeros
+
+
+def _d(arr):
+    return arr.ptr
+
+
+def transpose(A, stream=None):
+    """transpose (src/sequential/src/sparse32.js:1106-1138): a new object."""
+    dt, sp = _dtcode(A.dtype), _sp(stream)
+    if isinstance(A, sparse_COO_t):
+        B = allocate_COO(A.N, A.nnz, A.dtype)
+        call("sb_transpose_coo", dt, _d(A.row_index), _d(A.col_index), _d(A.val_index), A.nnz,
+             _d(B.row_index), _d(B.col_index), _d(B.val_index), sp)
+        return B
+    if isinstance(A, sparse_CSR_t):
+        B = allocate_CSR(A.N, A.nnz, A.dtype)
+        call("sb_transpose_csr", dt, _d(A.row_index), _d(A.col_index), _d(A.val_index), A.N,
+             A.nnz, _d(B.row_index), _d(B.col_index), _d(B.val_index), sp)
+        return B
+    if isinstance(A, sparse_DIA_t):
+        B = allocate_DIA(A.N, A.nnz, A.ndiags, A.stride, A.dtype)
+        call("sb_transpose_dia", dt, _d(A.offset_index), _d(A.data_index), A.ndiags, A.stride,
+             A.N, _d(B.offset_index), _d(B.data_index), sp)
+        return B
+    if isinstance(A, sparse_ELL_t):
+        cc = C.c_int32(0)
+        call("sb_count_transpose_cols_ell", dt, _d(A.data_index), _d(A.indices_index), A.ncols,
+             A.N, C.byref(cc), sp)
+        B = allocate_ELL(A.N, A.nnz, int(cc.value), A.dtype)
+        call("sb_transpose_ell", dt, _d(A.data_index), _d(A.indices_index), A.ncols, A.N,
+             B.ncols, _d(B.data_index), _d(B.indices_index), sp)
+        return B
+    raise TypeError(f"transpose: unsupported object {type(A).__name__}")
+
+
+def _copy_arrays(pairs, stream):
+    for src, dst in pairs:
+        call("sb_memcpy_dtod", dst.ptr, src.ptr, src.nbytes, _sp(stream))
+
+
+def eliminate_zeros(A, stream=None):
+    """eliminate_zeros (src/sequential/src/sparse32.js:1140-1207): a new object
+    without entries whose value is not (v > 0 || v < 0); an unchanged copy
+    when the nonzero count equals A.nnz."""
+    dt, sp = _dtcode(A.dtype), _sp(stream)
+    if isinstance(A, (sparse_COO_t, sparse_CSR_t)):
+        cnt = C.c_int64(0)
+        call("sb_count_nonzeros", dt, _d(A.val_index), A.nnz, C.byref(cnt), sp)
+        count = int(cnt.value)
+        if isinstance(A, sparse_COO_t):
+            B = allocate_COO(A.N, A.nnz if count == A.nnz else count, A.dtype)
+            if count == A.nnz:
+                _copy_arrays([(A.row_index, B.row_index), (A.col_index, B.col_index),
+                              (A.val_index, B.val_index)], stream)
+            else:
+                call("sb_copy_nonzeros_coo", dt, _d(A.row_index), _d(A.col_index),
+                     _d(A.val_index), A.nnz, _d(B.row_index), _d(B.col_index),
+                     _d(B.val_index), sp)
+            return B
+        B = allocate_CSR(A.N, A.nnz if count == A.nnz else count, A.dtype)
+        if count == A.nnz:
+            _copy_arrays([(A.row_index, B.row_index), (A.col_index, B.col_index),
+                          (A.val_index, B.val_index)], stream)
+        else:
+            call("sb_copy_nonzeros_csr", dt, _d(A.row_index), _d(A.col_index), _d(A.val_index),
+                 A.N, A.nnz, _d(B.row_index), _d(B.col_index), _d(B.val_index), sp)
+        return B
+    if isinstance(A, sparse_DIA_t):
+        cd = C.c_int32(0)
+        cnt = C.c_int64(0)
+        call("sb_count_nonzeros_dia", dt, _d(A.offset_index), _d(A.data_index), A.ndiags,
+             A.stride, A.N, C.byref(cd), C.byref(cnt), sp)
+        if int(cnt.value) == A.nnz:
+            B = allocate_DIA(A.N, A.nnz, A.ndiags, A.stride, A.dtype)
+            _copy_arrays([(A.offset_index, B.offset_index), (A.data_index, B.data_index)], stream)
+            return B
+        B = allocate_DIA(A.N, int(cnt.value), int(cd.value), A.stride, A.dtype)
+        call("sb_copy_nonzeros_dia", dt, _d(A.offset_index), _d(A.data_index), A.ndiags, A.stride,
+             A.N, _d(B.offset_index), _d(B.data_index), sp)
+        return B
+    if isinstance(A, sparse_ELL_t):
+        cc = C.c_int32(0)
+        cnt = C.c_int64(0)
+        call("sb_count_nonzeros_ell", dt, _d(A.data_index), A.ncols, A.N, C.byref(cc),
+             C.byref(cnt), sp)
+        if int(cnt.value) == A.nnz:
+            B = allocate_ELL(A.N, A.nnz, A.ncols, A.dtype)
+            _copy_arrays([(A.indices_index, B.indices_index), (A.data_index, B.data_index)],
+                         stream)
+            return B
+        B = allocate_ELL(A.N, int(cnt.value), int(cc.value), A.dtype)
+        call("sb_copy_nonzeros_ell", dt, _d(A.data_index), _d(A.indices_index), A.ncols, A.N,
+             B.ncols, _d(B.data_index), _d(B.indices_index), sp)
+        return B
+    raise TypeError(f"eliminate_zeros: unsupported object {type(A).__name__}")
+
+
+# --------------------------------------------------------------- element-wise maps
+# Functional forms (src/sequential/src/sparse32.js:671-1104) return a copy;
+# map_inplace is the self_* method form (:202-667).
+
+MAP_OPS = {"expm1": 0, "log1p": 1, "sin": 2, "tan": 3, "pow": 4, "deg2rad": 5, "rad2deg": 6,
+           "sign": 7, "abs": 8, "neg": 9, "sqrt": 10, "ceil": 11, "floor": 12, "trunc": 13,
+           "nearest": 14, "multiply": 15}
+
+
+def _map_into(A, B, op, p, stream):
+    dt, sp = _dtcode(A.dtype), _sp(stream)
+    code = MAP_OPS[op]
+    if isinstance(A, (sparse_COO_t, sparse_CSR_t)):
+        call("sb_map_coo", dt, code, float(p), _d(A.val_index), _d(B.val_index), A.nnz, sp)
+    elif isinstance(A, sparse_DIA_t):
+        call("sb_map_dia", dt, code, float(p), _d(A.offset_index), _d(A.data_index),
+             _d(B.data_index), A.ndiags, A.stride, A.N, sp)
+    elif isinstance(A, sparse_ELL_t):
+        call("sb_map_ell", dt, code, float(p), _d(A.data_index), _d(B.data_index), A.ncols, A.N,
+             sp)
+    else:
+        raise TypeError(f"{op}: unsupported object {type(A).__name__}")
+
+
+def _copy_structure(A, stream):
+    if isinstance(A, sparse_COO_t):
+        B = allocate_COO(A.N, A.nnz, A.dtype)
+        _copy_arrays([(A.row_index, B.row_index), (A.col_index, B.col_index)], stream)
+    elif isinstance(A, sparse_CSR_t):
+        B = allocate_CSR(A.N, A.nnz, A.dtype)
+        _copy_arrays([(A.row_index, B.row_index), (A.col_index, B.col_index)], stream)
+    elif isinstance(A, sparse_DIA_t):
+        B = allocate_DIA(A.N, A.nnz, A.ndiags, A.stride, A.dtype)
+        _copy_arrays([(A.offset_index, B.offset_index)], stream)
+    elif isinstance(A, sparse_ELL_t):
+        B = allocate_ELL(A.N, A.nnz, A.ncols, A.dtype)
+        _copy_arrays([(A.indices_index, B.indices_index)], stream)
+    else:
+        raise TypeError(type(A).__name__)
+    return B
+
+
+def map_copy(A, op, p=0.0, stream=None):
+    B = _copy_structure(A, stream)
+    _map_into(A, B, op, p, stream)
+    return B
+
+
+def map_inplace(A, op, p=0.0, stream=None):
+    _map_into(A, A, op, p, stream)
+
+
+def expm1(A): return map_copy(A, "expm1")
+def log1p(A): return map_copy(A, "log1p")
+def sin(A): return map_copy(A, "sin")
+def tan(A): return map_copy(A, "tan")
+def pow(A, p): return map_copy(A, "pow", p)  # noqa: A001
+def deg2rad(A): return map_copy(A, "deg2rad", np.pi)
+def rad2deg(A): return map_copy(A, "rad2deg", np.pi)
+def sign(A): return map_copy(A, "sign")
+def abs(A): return map_copy(A, "abs")  # noqa: A001
+def neg(A): return map_copy(A, "neg")
+def sqrt(A): return map_copy(A, "sqrt")
+def ceil(A): return map_copy(A, "ceil")
+def floor(A): return map_copy(A, "floor")
+def trunc(A): return map_copy(A, "trunc")
+def nearest(A): return map_copy(A, "nearest")
+def multiply(A, s): return map_copy(A, "multiply", s)
+
+
 # --------------------------------------------------------------- level sets / SpTS
 
 _SPTS_ALGO = {"level": _lib.SB_SPTS_LEVEL, "syncfree": _lib.SB_SPTS_SYNCFREE,
