@@ -666,6 +666,46 @@ def synchronize(stream=None) -> None:
     call("sb_stream_synchronize", _sp(stream))
 
 
+# --------------------------------------------------------------- partitioning
+
+
+def static_nnz(row_ptr, num_workers):
+    """static_nnz (src/parallel/src/sparse32.js:2769-2821) on host row
+    pointers: greedy contiguous row ranges, each taking rows while its running
+    nonzero count is below floor(remaining nnz / remaining workers); the last
+    range always ends at N.  Returns (row_start, row_end) int32 arrays.  Used
+    here to shard a matrix's rows across GPUs."""
+    rp = np.asarray(row_ptr, dtype=np.int64)
+    N = rp.size - 1
+    nw = int(num_workers)
+    rs = np.zeros(nw, np.int32)
+    re = np.zeros(nw, np.int32)
+    lens = np.diff(rp)
+    rem_nnz = int(rp[-1] - rp[0])
+    rem_nw = nw
+    index = 0
+    i = 0
+    for i in range(nw):
+        if index == N:
+            rs[i] = re[i] = N
+            continue
+        ideal = rem_nnz // rem_nw
+        rs[i] = index
+        # rows are taken while the running sum is below `ideal`: find the
+        # first prefix whose sum reaches it (the reference's loop, vectorised)
+        csum = np.cumsum(lens[index:])
+        k = int(np.searchsorted(csum, ideal, side="left")) if ideal > 0 else -1
+        taken = min(k + 1, N - index) if ideal > 0 else 0
+        s = int(csum[taken - 1]) if taken > 0 else 0
+        index += taken
+        if index < N:
+            re[i] = index
+        rem_nnz -= s
+        rem_nw -= 1
+    re[i] = N
+    return rs, re
+
+
 # --------------------------------------------------------------- checksum
 
 

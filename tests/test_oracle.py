@@ -201,3 +201,20 @@ def test_quick_sort_coo_sorts(oracle):
     assert np.all(np.diff(key) >= 0)
     assert sorted(zip(row.tolist(), col.tolist(), val.tolist())) == \
         sorted(zip(r.tolist(), c.tolist(), v.tolist()))
+
+
+def test_static_nnz_host_mirror_matches_oracle(oracle):
+    from sciwasm.sparse_b200.sparse import static_nnz
+    k = KAT["static_nnz"]
+    rs, re = static_nnz(np.array(k["row_ptr"]), k["nw"])
+    assert rs.tolist() == k["row_start"] and re.tolist() == k["row_end"]
+    for seed, nw in [(0, 1), (1, 3), (2, 5), (3, 8), (4, 64)]:
+        rp, col, val = synth.power_law(3000, seed=seed, cap=500)
+        a = static_nnz(rp, nw)
+        b = oracle.static_nnz(rp, nw)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), (seed, nw)
+    rp = np.array([0, 0, 0, 5, 5, 9], np.int32)  # empty rows
+    for nw in (1, 2, 4, 7):
+        a = static_nnz(rp, nw)
+        b = oracle.static_nnz(rp, nw)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), nw
