@@ -200,6 +200,23 @@ int sb_spts_syncfree_csr(int dtype, const int32_t* row_ptr, const int32_t* col, 
                          int32_t N, const void* b, void* y, int64_t spin_limit_cycles,
                          void* stream);
 
+/* No counterpart in the reference (its wasm memory is allocated by the JS
+ * host; this is an addition for callers that cannot allocate device memory).
+ * Same solve as sb_spts_syncfree_csr, but the ready flags, row ticket and
+ * status word live in a fixed 16 MiB device array inside the library, so the
+ * call makes no device allocation: for callers whose device memory is all
+ * reserved up front (a serving process that admitted its matrices against a
+ * fixed HBM budget, an embedding runtime that owns every device allocation)
+ * or that must not pay cudaMalloc's synchronisation in a latency-critical
+ * loop.  Limit: N <= 4,194,304 rows (larger N returns SB_EINVAL).  The first
+ * call on a device looks up the array's device address (do that call before
+ * any stream capture).  Every call on a device shares the array: calls that
+ * overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller.  Returns after the solve. */
+int sb_spts_syncfree_csr_noalloc(int dtype, const int32_t* row_ptr, const int32_t* col,
+                                 const void* val, int32_t N, const void* b, void* y,
+                                 int64_t spin_limit_cycles, void* stream);
+
 /* ---------------------------------------------------------------------- */
 /* eliminate_zeros and transpose (bit-exact with the reference's kernels). */
 /* The nonzero test is v > 0 || v < 0 (+0, -0 and NaN count as zeros).    */

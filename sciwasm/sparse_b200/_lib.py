@@ -75,6 +75,7 @@ SIGNATURES: dict[str, list] = {
     "sb_spts_plan_reordered": [P, P, P, P, P],
     "sb_spts_solve": [P, C.c_int, C.c_int, P, P, P],
     "sb_spts_syncfree_csr": [C.c_int, P, P, P, I32, P, P, I64, P],
+    "sb_spts_syncfree_csr_noalloc": [C.c_int, P, P, P, I32, P, P, I64, P],
     "sb_count_nonzeros": [C.c_int, P, I64, C.POINTER(I64), P],
     "sb_copy_nonzeros_coo": [C.c_int, P, P, P, I64, P, P, P, P],
     "sb_copy_nonzeros_csr": [C.c_int, P, P, P, I32, I64, P, P, P, P],

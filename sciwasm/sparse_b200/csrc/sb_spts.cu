@@ -24,6 +24,7 @@
 //                    row kernel's arithmetic, as the level/sync-free hybrid of
 //                    src/parallel/src/sparse_opt_32.wat:12846-13445
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "sb_common.cuh"
@@ -468,11 +469,92 @@ static int solve_impl(const sb_spts_plan* p, int algo, const T* b, T* y, long lo
   return SB_OK;
 }
 
+// ------------------------------------------------------------ no-allocation variant
+// Scratch of sb_spts_syncfree_csr_noalloc: one ready flag per row for up to
+// kNoAllocMaxRows rows, then the row ticket and the status word on their own
+// 128-byte lines.  It is a file-scope device array, so every GPU that loads
+// this library holds these 16 MiB until the process exits, and every call
+// shares them.
+constexpr int kNoAllocMaxRows = 1 << 22;  // 4,194,304 rows
+constexpr int kNoAllocTail = 64;          // ticket at +0, status at +32 (words)
+static __device__ __align__(256) unsigned g_noalloc_scratch[kNoAllocMaxRows + kNoAllocTail];
+
+// Device address of g_noalloc_scratch for the current device, looked up once
+// per device (with that device current) and cached.  The host-side symbol is
+// only a stand-in and must never be handed to a kernel.
+static unsigned* noalloc_scratch(int* status) {
+  static std::mutex mu;
+  static unsigned* addr[64] = {nullptr};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    *status = cuda_status(e == cudaSuccess ? cudaErrorInvalidDevice : e, "cudaGetDevice");
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      *status = cuda_status(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+      return nullptr;
+    }
+    addr[dev] = (unsigned*)p;
+  }
+  return addr[dev];
+}
+
 }  // namespace sb
 
 using namespace sb;
 
 extern "C" {
+
+int sb_spts_syncfree_csr_noalloc(int dtype, const int32_t* row_ptr, const int32_t* col,
+                                 const void* val, int32_t N, const void* b, void* y,
+                                 int64_t spin_limit_cycles, void* stream) {
+  SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_spts_syncfree_csr_noalloc: bad dtype");
+  SB_REQUIRE(N >= 0, "sb_spts_syncfree_csr_noalloc: negative size");
+  if (N > kNoAllocMaxRows) {
+    set_error("sb_spts_syncfree_csr_noalloc: N = %d exceeds the fixed scratch limit of %d rows "
+              "(use sb_spts_syncfree_csr)", N, kNoAllocMaxRows);
+    return SB_EINVAL;
+  }
+  if (N == 0) return SB_OK;
+  SB_REQUIRE(row_ptr && col && val && b && y, "sb_spts_syncfree_csr_noalloc: null pointer");
+  int r = ensure_device();
+  if (r) return r;
+  unsigned* scratch = noalloc_scratch(&r);
+  if (!scratch) return r;
+  cudaStream_t st = as_stream(stream);
+  unsigned* flags = scratch;
+  int* ticket = (int*)(scratch + kNoAllocMaxRows);
+  int* status = (int*)(scratch + kNoAllocMaxRows + 32);
+  // the array keeps the previous call's contents: clear what must start at 0
+  SB_CHECK_CUDA(cudaMemsetAsync(flags, 0, sizeof(unsigned) * (size_t)N, st));
+  SB_CHECK_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * kNoAllocTail, st));
+  const long long limit = spin_limit_cycles > 0 ? spin_limit_cycles : kDefaultSpin;
+  if (dtype == SB_F64) {
+    auto k = spts_syncfree_rows<double, double>;
+    k<<<resident_grid((const void*)k), kT, 0, st>>>(row_ptr, col, (const double*)val, N,
+                                                     (const double*)b, (double*)y, flags, ticket,
+                                                     limit, status);
+  } else {
+    auto k = spts_syncfree_rows<float, float>;
+    k<<<resident_grid((const void*)k), kT, 0, st>>>(row_ptr, col, (const float*)val, N,
+                                                     (const float*)b, (float*)y, flags, ticket,
+                                                     limit, status);
+  }
+  SB_CHECK_LAUNCH("spts_syncfree_rows");
+  int dstat = 0;
+  SB_CHECK_CUDA(cudaMemcpyAsync(&dstat, status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SB_CHECK_CUDA(cudaStreamSynchronize(st));
+  if (dstat) {
+    set_error("sb_spts_syncfree_csr_noalloc: a dependency wait ran out (row never became ready)");
+    return SB_ETIMEOUT;
+  }
+  return SB_OK;
+}
 
 int sb_spts_analyze(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                     int32_t N, int64_t nnz, void* stream, sb_spts_plan** plan) {

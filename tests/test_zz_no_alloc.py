@@ -1,0 +1,60 @@
+"""The no-allocation sync-free solve, sb_spts_syncfree_csr_noalloc.
+
+Some callers cannot allocate device memory when they solve: a serving process
+that reserved its whole HBM budget for resident matrices up front, or an
+embedding runtime that owns every device allocation.  This entry point keeps
+its scratch (ready flags, row ticket, status word) in a fixed device array
+inside the library instead.  The test calls it through the C ABI and checks
+its output against the allocating entry point, sb_spts_syncfree_csr, on two
+calls in a row (the shared array must be cleared between calls).  The file
+name makes pytest collect it last; it passes alone and after the others.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import TOL
+from sciwasm.sparse_b200 import _lib, synth
+
+pytestmark = pytest.mark.gpu
+
+MAX_ROWS = 1 << 22
+
+
+def _dev(arr):
+    from sciwasm.sparse_b200.sparse import DeviceArray
+    return DeviceArray.from_host(arr)
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_noalloc_matches_allocating_entry_point_twice(gpu, dt):
+    lib = _lib.load()
+    code = _lib.SB_F32 if dt == np.float32 else _lib.SB_F64
+    rp, col, val = synth.random_lower(200_000, seed=11, band=3000, dtype=dt)
+    N = rp.size - 1
+    d_rp, d_col, d_val = _dev(rp), _dev(col), _dev(val)
+    for call in range(2):
+        b = synth.uniform_vec(N, 20 + call, dtype=dt)
+        d_b = _dev(b)
+        ref_y = _dev(np.zeros(N, dt))
+        new_y = _dev(np.full(N, np.nan, dt))
+        st = lib.sb_spts_syncfree_csr(code, d_rp.ptr, d_col.ptr, d_val.ptr, N, d_b.ptr, ref_y.ptr,
+                                      0, None)
+        assert st == 0, lib.sb_last_error()
+        st = lib.sb_spts_syncfree_csr_noalloc(code, d_rp.ptr, d_col.ptr, d_val.ptr, N, d_b.ptr,
+                                              new_y.ptr, 0, None)
+        assert st == 0, lib.sb_last_error()
+        want, got = ref_y.to_host(), new_y.to_host()
+        err = np.max(np.abs(got.astype(np.float64) - want)) / np.max(np.abs(want))
+        assert err <= TOL[np.dtype(dt)], (call, err)
+        assert np.array_equal(got.view(np.uint8), want.view(np.uint8)), call
+
+
+def test_noalloc_rejects_sizes_beyond_its_limit(gpu):
+    lib = _lib.load()
+    tiny = _dev(np.zeros(4, np.int32))
+    st = lib.sb_spts_syncfree_csr_noalloc(_lib.SB_F64, tiny.ptr, tiny.ptr, tiny.ptr, MAX_ROWS + 1,
+                                          tiny.ptr, tiny.ptr, 0, None)
+    assert st == _lib.SB_EINVAL
+    assert b"4194304" in lib.sb_last_error()
