@@ -90,6 +90,31 @@ int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const voi
                 const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
                 void* stream);
 
+/* Kernel choice for CSR SpMV (no counterpart in the reference, whose
+ * parallel harness picks among unrolled CSR variants per run,
+ * src/parallel/tests/main32.js:150-313).  kernel 0 = row blocks (default),
+ * 1 = streamed nonzero tiles; lanes_per_row 1..32 (power of two) and
+ * unroll 2/4/8 tune the row-block kernel, 0 = chosen from the mean row
+ * length. */
+typedef struct sb_csr_opts {
+  int32_t kernel;
+  int32_t lanes_per_row;
+  int32_t unroll;
+  int32_t reserved;
+} sb_csr_opts;
+
+/* sb_spmv_csr with explicit kernel options (opts may be NULL). */
+int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                   const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
+                   const sb_csr_opts* opts, void* stream);
+
+/* Times the candidate kernel options around this matrix's row-length
+ * statistics (reps calls each, on a scratch y) and returns the fastest in
+ * *best (and its time per call in *best_ms).  Returns after timing. */
+int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                    const void* x, int32_t N, int64_t nnz, int32_t reps, sb_csr_opts* best,
+                    float* best_ms, void* stream);
+
 /* Replaces spmv_dia / spmv_dia_wrapper
  * (src/sequential/src/sparse_opt_32.wat:290-425; dispatch
  * src/sequential/src/sparse32.js:1272-1278).  offset[nd] diagonal offsets

@@ -92,6 +92,16 @@ SIGNATURES: dict[str, list] = {
     "sb_map_ell": [C.c_int, C.c_int, C.c_double, P, P, I32, I32, P],
     "sb_map_dia": [C.c_int, C.c_int, C.c_double, P, P, P, I32, I32, I32, P],
 }
+class CsrOpts(C.Structure):
+    _fields_ = [("kernel", I32), ("lanes_per_row", I32), ("unroll", I32), ("reserved", I32)]
+
+
+SIGNATURES.update({
+    "sb_spmv_csr_ex": [C.c_int, P, P, P, P, P, I32, I64, I32, C.POINTER(CsrOpts), P],
+    "sb_csr_autotune": [C.c_int, P, P, P, P, I32, I64, I32, C.POINTER(CsrOpts),
+                        C.POINTER(C.c_float), P],
+})
+
 _RESTYPE = {"sb_last_error": C.c_char_p, "sb_status_string": C.c_char_p}
 
 

@@ -376,15 +376,36 @@ static int launch_csr_rows_v(const int* row_ptr, const int* col, const S* val, c
   return SB_OK;
 }
 
-// V from the mean row length: about three items per lane per row.
+template <typename S, int V>
+static int launch_csr_rows_u(const int* row_ptr, const int* col, const S* val, const S* x, S* y,
+                             int N, int unroll, cudaStream_t st) {
+  if (unroll <= 2) return launch_csr_rows_v<S, V, 2>(row_ptr, col, val, x, y, N, st);
+  if (unroll >= 8) return launch_csr_rows_v<S, V, 8>(row_ptr, col, val, x, y, N, st);
+  return launch_csr_rows_v<S, V, 4>(row_ptr, col, val, x, y, N, st);
+}
+
+// Default lanes per row from the mean row length (about three items per lane).
+static int default_lanes(int N, long long nnz) {
+  const double avg = N ? (double)nnz / N : 0.0;
+  if (avg <= 6) return 2;
+  if (avg <= 14) return 4;
+  if (avg <= 28) return 8;
+  return 16;
+}
+
 template <typename S>
 static int launch_csr_rows(const int* row_ptr, const int* col, const S* val, const S* x, S* y,
-                           int N, long long nnz, cudaStream_t st) {
-  const double avg = N ? (double)nnz / N : 0.0;
-  if (avg <= 6) return launch_csr_rows_v<S, 2, 4>(row_ptr, col, val, x, y, N, st);
-  if (avg <= 14) return launch_csr_rows_v<S, 4, 4>(row_ptr, col, val, x, y, N, st);
-  if (avg <= 28) return launch_csr_rows_v<S, 8, 4>(row_ptr, col, val, x, y, N, st);
-  return launch_csr_rows_v<S, 16, 4>(row_ptr, col, val, x, y, N, st);
+                           int N, long long nnz, int lanes, int unroll, cudaStream_t st) {
+  if (lanes <= 0) lanes = default_lanes(N, nnz);
+  if (unroll <= 0) unroll = 4;
+  switch (lanes) {
+    case 1: return launch_csr_rows_u<S, 1>(row_ptr, col, val, x, y, N, unroll, st);
+    case 2: return launch_csr_rows_u<S, 2>(row_ptr, col, val, x, y, N, unroll, st);
+    case 4: return launch_csr_rows_u<S, 4>(row_ptr, col, val, x, y, N, unroll, st);
+    case 8: return launch_csr_rows_u<S, 8>(row_ptr, col, val, x, y, N, unroll, st);
+    case 16: return launch_csr_rows_u<S, 16>(row_ptr, col, val, x, y, N, unroll, st);
+    default: return launch_csr_rows_u<S, 32>(row_ptr, col, val, x, y, N, unroll, st);
+  }
 }
 
 // ------------------------------------------------------------ COO
@@ -592,17 +613,20 @@ static int csr_stream_tile() {
   return v;
 }
 
-// CSR dispatch: the row-block kernel by default; SB_CSR_KERNEL=s selects the
-// bulk-copy streamed-tile kernel (needs 16-byte aligned col/val).
+// CSR dispatch.  opts (may be null): kernel 0 = row blocks, 1 = streamed
+// tiles (needs 16-byte aligned col/val); lanes_per_row / unroll 0 = default.
+// SB_CSR_KERNEL=s in the environment selects the streamed kernel by default.
 template <typename S, typename A>
 static int launch_csr(const int* row_ptr, const int* col, const S* val, const S* x, S* y, int N,
-                      long long nnz, cudaStream_t st) {
-  if (csr_kernel_choice() == 2 && aligned16(col) && aligned16(val)) {
-    if (csr_stream_tile() == 2048)
-      return launch_csr_stream<S, 2048, 3>(row_ptr, col, val, x, y, N, nnz, st);
+                      long long nnz, const sb_csr_opts* opts, cudaStream_t st) {
+  const int kernel = opts ? opts->kernel : (csr_kernel_choice() == 2 ? 1 : 0);
+  if (kernel == 1 && aligned16(col) && aligned16(val)) {
+    const int tile = (opts && opts->unroll == 2048) ? 2048 : csr_stream_tile();
+    if (tile == 2048) return launch_csr_stream<S, 2048, 3>(row_ptr, col, val, x, y, N, nnz, st);
     return launch_csr_stream<S, 1024, 4>(row_ptr, col, val, x, y, N, nnz, st);
   }
-  return launch_csr_rows<S>(row_ptr, col, val, x, y, N, nnz, st);
+  return launch_csr_rows<S>(row_ptr, col, val, x, y, N, nnz, opts ? opts->lanes_per_row : 0,
+                            opts ? opts->unroll : 0, st);
 }
 
 template <typename S, typename A>
@@ -636,13 +660,20 @@ using namespace sb;
 
 extern "C" {
 
-int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
-                const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
-                void* stream) {
+int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                   const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
+                   const sb_csr_opts* opts, void* stream) {
   int r = check_dtype(dtype, "sb_spmv_csr");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nnz >= 0 && inner_max >= 0, "sb_spmv_csr: negative size");
   SB_REQUIRE(nnz <= 0x7fffffffLL, "sb_spmv_csr: nnz exceeds int32 row_ptr range");
+  if (opts) {
+    SB_REQUIRE(opts->kernel == 0 || opts->kernel == 1, "sb_spmv_csr: unknown kernel %d",
+               opts->kernel);
+    const int l = opts->lanes_per_row;
+    SB_REQUIRE(l == 0 || l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32,
+               "sb_spmv_csr: lanes_per_row must be 0 or a power of two <= 32");
+  }
   if (N == 0 || nnz == 0 || inner_max == 0) return SB_OK;
   SB_REQUIRE(row_ptr && col && val && x && y, "sb_spmv_csr: null pointer");
   if ((r = ensure_device())) return r;
@@ -650,13 +681,76 @@ int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const voi
   for (int it = 0; it < inner_max; ++it) {
     if (dtype == SB_F32)
       r = launch_csr<float, float>(row_ptr, col, (const float*)val, (const float*)x, (float*)y, N,
-                                   nnz, st);
+                                   nnz, opts, st);
     else
       r = launch_csr<double, double>(row_ptr, col, (const double*)val, (const double*)x,
-                                     (double*)y, N, nnz, st);
+                                     (double*)y, N, nnz, opts, st);
     if (r) return r;
   }
   return SB_OK;
+}
+
+int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
+                void* stream) {
+  return sb_spmv_csr_ex(dtype, row_ptr, col, val, x, y, N, nnz, inner_max, nullptr, stream);
+}
+
+int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                    const void* x, int32_t N, int64_t nnz, int32_t reps, sb_csr_opts* best,
+                    float* best_ms, void* stream) {
+  int r = check_dtype(dtype, "sb_csr_autotune");
+  if (r) return r;
+  SB_REQUIRE(best && N >= 0 && nnz >= 0, "sb_csr_autotune: bad argument");
+  best->kernel = 0;
+  best->lanes_per_row = default_lanes(N, nnz);
+  best->unroll = 4;
+  best->reserved = 0;
+  if (best_ms) *best_ms = 0.f;
+  if (N == 0 || nnz == 0) return SB_OK;
+  SB_REQUIRE(row_ptr && col && val && x, "sb_csr_autotune: null pointer");
+  if ((r = ensure_device())) return r;
+  if (reps <= 0) reps = 5;
+  cudaStream_t st = as_stream(stream);
+  // candidates around the mean row length: lanes in {d/2, d, 2d}, unroll {2, 4, 8},
+  // plus the streamed-tile kernel
+  const int d = default_lanes(N, nnz);
+  sb_csr_opts cand[16];
+  int nc = 0;
+  for (int lanes : {d / 2, d, d * 2}) {
+    if (lanes < 1 || lanes > 32) continue;
+    for (int u : {2, 4, 8}) cand[nc++] = sb_csr_opts{0, lanes, u, 0};
+  }
+  cand[nc++] = sb_csr_opts{1, 0, 1024, 0};
+  void* ywork = nullptr;
+  if ((r = scratch_alloc(&ywork, dtype_size(dtype) * (size_t)N, st))) return r;
+  SB_CHECK_CUDA(cudaMemsetAsync(ywork, 0, dtype_size(dtype) * (size_t)N, st));
+  cudaEvent_t e0, e1;
+  SB_CHECK_CUDA(cudaEventCreate(&e0));
+  SB_CHECK_CUDA(cudaEventCreate(&e1));
+  float best_t = 3.0e38f;
+  for (int c = 0; c < nc && !r; ++c) {
+    r = sb_spmv_csr_ex(dtype, row_ptr, col, val, x, ywork, N, nnz, 1, &cand[c], stream);
+    if (r) break;
+    cudaEventRecord(e0, st);
+    r = sb_spmv_csr_ex(dtype, row_ptr, col, val, x, ywork, N, nnz, reps, &cand[c], stream);
+    cudaEventRecord(e1, st);
+    if (r) break;
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) { r = cuda_status(e, "sb_csr_autotune"); break; }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= reps;
+    if (ms < best_t) {
+      best_t = ms;
+      *best = cand[c];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  scratch_free(ywork, st);
+  if (best_ms) *best_ms = best_t;
+  return r;
 }
 
 int sb_spmv_coo(int dtype, const int32_t* row, const int32_t* col, const void* val,

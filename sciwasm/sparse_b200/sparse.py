@@ -302,6 +302,19 @@ def free(obj) -> None:
 # --------------------------------------------------------------- SpMV
 
 
+def csr_autotune(A_csr, x_view, reps=5, stream=None):
+    """Pick the fastest CSR kernel options for this matrix (timed on a scratch
+    y; the choice is cached on the object and used by spmv)."""
+    best = _lib.CsrOpts()
+    ms = C.c_float(0)
+    call("sb_csr_autotune", _dtcode(A_csr.dtype), A_csr.row_index.ptr, A_csr.col_index.ptr,
+         A_csr.val_index.ptr, x_view.vec_index.ptr, A_csr.N, A_csr.nnz, int(reps), C.byref(best),
+         C.byref(ms), _sp(stream))
+    A_csr.opts = best
+    return {"kernel": best.kernel, "lanes_per_row": best.lanes_per_row, "unroll": best.unroll,
+            "ms": float(ms.value)}
+
+
 def spmv(A, x_view, y_view, inner_max=1, stream=None):
     """y <- y + A x, inner_max times (src/sequential/src/sparse32.js:1232-1286).
 
@@ -320,8 +333,13 @@ def spmv(A, x_view, y_view, inner_max=1, stream=None):
         call("sb_spmv_coo", dt, A.row_index.ptr, A.col_index.ptr, A.val_index.ptr, x, y, A.N,
              A.nnz, inner_max, s)
     elif isinstance(A, sparse_CSR_t):
-        call("sb_spmv_csr", dt, A.row_index.ptr, A.col_index.ptr, A.val_index.ptr, x, y, A.N,
-             A.nnz, inner_max, s)
+        opts = getattr(A, "opts", None)
+        if opts is None:
+            call("sb_spmv_csr", dt, A.row_index.ptr, A.col_index.ptr, A.val_index.ptr, x, y, A.N,
+                 A.nnz, inner_max, s)
+        else:
+            call("sb_spmv_csr_ex", dt, A.row_index.ptr, A.col_index.ptr, A.val_index.ptr, x, y,
+                 A.N, A.nnz, inner_max, C.byref(opts), s)
     elif isinstance(A, sparse_DIA_t):
         call("sb_spmv_dia", dt, A.offset_index.ptr, A.data_index.ptr, A.N, A.ndiags, A.stride, x,
              y, inner_max, s)
