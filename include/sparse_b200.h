@@ -115,6 +115,14 @@ int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const
                     const void* x, int32_t N, int64_t nnz, int32_t reps, sb_csr_opts* best,
                     float* best_ms, void* stream);
 
+/* Reduced-precision storage (no counterpart in the reference, which keeps
+ * f32 or f64 values): sb_spmv_csr / sb_spmv_csr_ex accept dtype SB_BF16 for
+ * BF16-stored values with f32 x, y and f32 accumulation (long rows use
+ * compensated sums).  sb_convert_values converts a value array between
+ * SB_F32, SB_F64 and SB_BF16 (round to nearest even). */
+int sb_convert_values(int src_dtype, const void* src, int dst_dtype, void* dst, int64_t n,
+                      void* stream);
+
 /* Replaces spmv_dia / spmv_dia_wrapper
  * (src/sequential/src/sparse_opt_32.wat:290-425; dispatch
  * src/sequential/src/sparse32.js:1272-1278).  offset[nd] diagonal offsets
@@ -128,6 +136,40 @@ int sb_spmv_dia(int dtype, const int32_t* offset, const void* data, int32_t N, i
  * nc*N slots; padding slots (data 0, index 0) are applied like the reference. */
 int sb_spmv_ell(int dtype, const int32_t* indices, const void* data, int32_t N, int32_t nc,
                 const void* x, void* y, int32_t inner_max, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* Batched SpMV (no counterpart in the reference, which calls spmv once per  */
+/* matrix and vector, src/sequential/src/sparse32.js:1232-1286).            */
+/* ---------------------------------------------------------------------- */
+
+/* One CSR matrix of a batch: y <- y + A x for nrhs (1..8) right-hand sides,
+ * x and y stored N x nrhs row-major (x[col*nrhs + j]).  lanes: lanes per row
+ * (1..32, power of two), 0 = chosen from nnz/N.  The y ranges of different
+ * items must not overlap (x may be shared). */
+typedef struct sb_batch_item {
+  const int32_t* row_ptr;
+  const int32_t* col;
+  const void* val;
+  const void* x;
+  void* y;
+  int32_t N;
+  int32_t nrhs;
+  int32_t lanes;
+  int32_t reserved;
+  int64_t nnz;
+} sb_batch_item;
+
+typedef struct sb_batch_exec sb_batch_exec;
+
+/* An executor for batches of up to `capacity` matrices whose values are
+ * stored as dtype (SB_F32, SB_F64 or SB_BF16 with f32 vectors).  It captures
+ * one CUDA graph: descriptor upload, work-counter reset and the persistent
+ * kernel over all 32-row blocks of the batch. */
+int sb_batch_exec_create(int dtype, int32_t capacity, sb_batch_exec** exec);
+int sb_batch_exec_destroy(sb_batch_exec* exec);
+/* Launch the graph for items[0..n) on `stream` (stream-ordered; the call
+ * waits only for the executor's previous run to have read its staging). */
+int sb_batch_exec_run(sb_batch_exec* exec, const sb_batch_item* items, int32_t n, void* stream);
 
 /* ---------------------------------------------------------------------- */
 /* Format conversions (bit-exact with the reference).  These calls return */

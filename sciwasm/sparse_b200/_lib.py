@@ -96,7 +96,16 @@ class CsrOpts(C.Structure):
     _fields_ = [("kernel", I32), ("lanes_per_row", I32), ("unroll", I32), ("reserved", I32)]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("row_ptr", P), ("col", P), ("val", P), ("x", P), ("y", P), ("N", I32),
+                ("nrhs", I32), ("lanes", I32), ("reserved", I32), ("nnz", I64)]
+
+
 SIGNATURES.update({
+    "sb_batch_exec_create": [C.c_int, I32, C.POINTER(P)],
+    "sb_batch_exec_destroy": [P],
+    "sb_batch_exec_run": [P, C.POINTER(BatchItem), I32, P],
+    "sb_convert_values": [C.c_int, P, C.c_int, P, I64, P],
     "sb_spmv_csr_ex": [C.c_int, P, P, P, P, P, I32, I64, I32, C.POINTER(CsrOpts), P],
     "sb_csr_autotune": [C.c_int, P, P, P, P, I32, I64, I32, C.POINTER(CsrOpts),
                         C.POINTER(C.c_float), P],

@@ -101,11 +101,55 @@ static int launch_map(int op, double p, const void* in, void* out, long long n, 
   return SB_OK;
 }
 
+template <typename A, typename B> __device__ __forceinline__ B conv(A v) { return (B)v; }
+template <> __device__ __forceinline__ __nv_bfloat16 conv(float v) { return __float2bfloat16_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 conv(double v) {
+  return __float2bfloat16_rn(__double2float_rn(v));
+}
+template <> __device__ __forceinline__ float conv(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <> __device__ __forceinline__ double conv(__nv_bfloat16 v) {
+  return (double)__bfloat162float(v);
+}
+template <> __device__ __forceinline__ float conv(double v) { return __double2float_rn(v); }
+
+template <typename A, typename B>
+__global__ void convert_kernel(const A* __restrict__ in, B* __restrict__ out, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = conv<A, B>(in[i]);
+}
+
+template <typename A>
+static int convert_from(const A* in, int dst, void* out, long long n, cudaStream_t st) {
+  const unsigned g = (unsigned)std::min<long long>((n + kMT - 1) / kMT, (long long)sm_count() * 16);
+  if (dst == SB_F32) convert_kernel<A, float><<<g, kMT, 0, st>>>(in, (float*)out, n);
+  else if (dst == SB_F64) convert_kernel<A, double><<<g, kMT, 0, st>>>(in, (double*)out, n);
+  else convert_kernel<A, __nv_bfloat16><<<g, kMT, 0, st>>>(in, (__nv_bfloat16*)out, n);
+  SB_CHECK_LAUNCH("convert_kernel");
+  return SB_OK;
+}
+
 }  // namespace sb
 
 using namespace sb;
 
 extern "C" {
+
+int sb_convert_values(int src_dtype, const void* src, int dst_dtype, void* dst, int64_t n,
+                      void* stream) {
+  const bool ok = (src_dtype >= SB_F32 && src_dtype <= SB_BF16) &&
+                  (dst_dtype >= SB_F32 && dst_dtype <= SB_BF16);
+  SB_REQUIRE(ok, "sb_convert_values: dtypes must be SB_F32, SB_F64 or SB_BF16");
+  SB_REQUIRE(n >= 0, "sb_convert_values: negative size");
+  if (n == 0) return SB_OK;
+  SB_REQUIRE(src && dst, "sb_convert_values: null pointer");
+  int r = ensure_device();
+  if (r) return r;
+  cudaStream_t st = as_stream(stream);
+  if (src_dtype == SB_F32) return convert_from<float>((const float*)src, dst_dtype, dst, n, st);
+  if (src_dtype == SB_F64) return convert_from<double>((const double*)src, dst_dtype, dst, n, st);
+  return convert_from<__nv_bfloat16>((const __nv_bfloat16*)src, dst_dtype, dst, n, st);
+}
 
 int sb_map_coo(int dtype, int op, double p, const void* in, void* out, int64_t n, void* stream) {
   int r = map_check(dtype, op, "sb_map_coo");

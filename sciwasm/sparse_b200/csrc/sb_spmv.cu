@@ -279,20 +279,39 @@ __global__ void __launch_bounds__(kStreamThreads)
 
 // ------------------------------------------------------------ CSR (rows)
 
+// Stored value -> accumulation type (BF16 storage widens exactly to f32).
+template <typename T> __device__ __forceinline__ T widen(float v) { return (T)v; }
+__device__ __forceinline__ float ld_val(const float* p) { return ld_stream(p); }
+__device__ __forceinline__ double ld_val(const double* p) { return ld_stream(p); }
+__device__ __forceinline__ float ld_val(const __nv_bfloat16* p) {
+  return __bfloat162float(__ushort_as_bfloat16(ld_stream(reinterpret_cast<const unsigned short*>(p))));
+}
+
+// Neumaier-compensated accumulation (used for long rows with f32 sums).
+template <typename T>
+__device__ __forceinline__ void comp_add(T& s, T& c, T v) {
+  const T t = s + v;
+  c += (fabs(s) >= fabs(v)) ? ((s - t) + v) : ((v - t) + s);
+  s = t;
+}
+
 // Row-block CSR: each warp owns 32 consecutive rows.  It reads their row_ptr
 // entries once (one per lane), then reduces the short rows in batches of
 // 32/V rows, V lanes per row, each lane issuing UNROLL independent col/val
 // loads before the dependent x gathers and one shuffle reduction per batch;
-// rows longer than the short limit are reduced afterwards by the whole warp.
-// V is picked per matrix from its mean row length.  No shared memory and no
-// block barrier: occupancy and unrolled loads keep the loads in flight.
-template <typename S, int V, int UNROLL>
+// rows longer than the short limit are reduced afterwards by the whole warp
+// (with compensated f32 sums when the accumulation type is f32).  V is picked
+// per matrix from its mean row length.  No shared memory and no block
+// barrier: occupancy and unrolled loads keep the loads in flight.  SV is the
+// stored value type (f32, f64 or BF16); x, y and the sums are T.
+template <typename SV, typename T, int V, int UNROLL>
 __global__ void __launch_bounds__(256)
     csr_rows_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
-                    const S* __restrict__ val, const S* __restrict__ x, S* __restrict__ y,
+                    const SV* __restrict__ val, const T* __restrict__ x, T* __restrict__ y,
                     int N) {
   constexpr int RPB = kWarp / V;           // rows per batch
   constexpr int SHORT = V * UNROLL;        // a short row needs one unrolled pass
+  constexpr bool COMP = sizeof(T) == 4;    // compensate long f32 sums
   const int lane = threadIdx.x & (kWarp - 1);
   const int g = lane / V;
   const int q = lane - g * V;
@@ -304,22 +323,22 @@ __global__ void __launch_bounds__(256)
     const int s_l = rr < N ? __ldg(row_ptr + rr) : 0;
     const int e_l = rr < N ? __ldg(row_ptr + rr + 1) : 0;
     const int len_l = e_l - s_l;
-    const S y_l = (rr < N && len_l > 0) ? y[rr] : (S)0;
+    const T y_l = (rr < N && len_l > 0) ? y[rr] : (T)0;
 #pragma unroll
     for (int b = 0; b < V; ++b) {
       const int j = b * RPB + g;  // row of this group within the block
       const int s = __shfl_sync(kFull, s_l, j);
       const int e = __shfl_sync(kFull, e_l, j);
       const int len = e - s;
-      S sum = 0;
+      T sum = 0;
       if (len <= SHORT) {
         int cc[UNROLL];
-        S vv[UNROLL];
+        T vv[UNROLL];
 #pragma unroll
         for (int u = 0; u < UNROLL; ++u) {
           const int k = s + q + u * V;
           cc[u] = k < e ? ld_stream(col + k) : 0;
-          vv[u] = k < e ? ld_stream(val + k) : (S)0;
+          vv[u] = k < e ? (T)ld_val(val + k) : (T)0;
         }
 #pragma unroll
         for (int u = 0; u < UNROLL; ++u) {
@@ -329,7 +348,7 @@ __global__ void __launch_bounds__(256)
       }
 #pragma unroll
       for (int off = V >> 1; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
-      const S yj = __shfl_sync(kFull, y_l, j);
+      const T yj = __shfl_sync(kFull, y_l, j);
       if (q == 0 && len > 0 && len <= SHORT && r0 + j < N) y[r0 + j] = yj + sum;
     }
     // long rows of the block: whole warp each
@@ -339,34 +358,45 @@ __global__ void __launch_bounds__(256)
       longm &= longm - 1;
       const int s = __shfl_sync(kFull, s_l, j);
       const int e = __shfl_sync(kFull, e_l, j);
-      S sum = 0;
+      T sum = 0, comp = 0;
       for (int k0 = s; k0 < e; k0 += kWarp * 4) {
         int cc[4];
-        S vv[4];
+        T vv[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int k = k0 + lane + u * kWarp;
           cc[u] = k < e ? ld_stream(col + k) : 0;
-          vv[u] = k < e ? ld_stream(val + k) : (S)0;
+          vv[u] = k < e ? (T)ld_val(val + k) : (T)0;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int k = k0 + lane + u * kWarp;
-          if (k < e) sum += vv[u] * ld_ro(x + cc[u]);
+          if (k < e) {
+            if (COMP) comp_add(sum, comp, vv[u] * ld_ro(x + cc[u]));
+            else sum += vv[u] * ld_ro(x + cc[u]);
+          }
         }
       }
 #pragma unroll
-      for (int off = kWarp / 2; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
-      const S yj = __shfl_sync(kFull, y_l, j);
-      if (lane == 0) y[r0 + j] = yj + sum;
+      for (int off = kWarp / 2; off > 0; off >>= 1) {
+        const T o = __shfl_xor_sync(kFull, sum, off);
+        if (COMP) {
+          comp += __shfl_xor_sync(kFull, comp, off);
+          comp_add(sum, comp, o);
+        } else {
+          sum += o;
+        }
+      }
+      const T yj = __shfl_sync(kFull, y_l, j);
+      if (lane == 0) y[r0 + j] = COMP ? yj + (sum + comp) : yj + sum;
     }
   }
 }
 
-template <typename S, int V, int UNROLL>
-static int launch_csr_rows_v(const int* row_ptr, const int* col, const S* val, const S* x, S* y,
+template <typename SV, typename T, int V, int UNROLL>
+static int launch_csr_rows_v(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
                              int N, cudaStream_t st) {
-  auto kern = csr_rows_kernel<S, V, UNROLL>;
+  auto kern = csr_rows_kernel<SV, T, V, UNROLL>;
   const long long warps_needed = ((long long)N + kWarp - 1) / kWarp;
   const long long max_warps = (long long)resident_ctas(kern, 256) * 8;
   const long long warps = std::min(warps_needed, max_warps);
@@ -376,12 +406,12 @@ static int launch_csr_rows_v(const int* row_ptr, const int* col, const S* val, c
   return SB_OK;
 }
 
-template <typename S, int V>
-static int launch_csr_rows_u(const int* row_ptr, const int* col, const S* val, const S* x, S* y,
+template <typename SV, typename T, int V>
+static int launch_csr_rows_u(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
                              int N, int unroll, cudaStream_t st) {
-  if (unroll <= 2) return launch_csr_rows_v<S, V, 2>(row_ptr, col, val, x, y, N, st);
-  if (unroll >= 8) return launch_csr_rows_v<S, V, 8>(row_ptr, col, val, x, y, N, st);
-  return launch_csr_rows_v<S, V, 4>(row_ptr, col, val, x, y, N, st);
+  if (unroll <= 2) return launch_csr_rows_v<SV, T, V, 2>(row_ptr, col, val, x, y, N, st);
+  if (unroll >= 8) return launch_csr_rows_v<SV, T, V, 8>(row_ptr, col, val, x, y, N, st);
+  return launch_csr_rows_v<SV, T, V, 4>(row_ptr, col, val, x, y, N, st);
 }
 
 // Default lanes per row from the mean row length (about three items per lane).
@@ -393,18 +423,18 @@ static int default_lanes(int N, long long nnz) {
   return 16;
 }
 
-template <typename S>
-static int launch_csr_rows(const int* row_ptr, const int* col, const S* val, const S* x, S* y,
+template <typename SV, typename T>
+static int launch_csr_rows(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
                            int N, long long nnz, int lanes, int unroll, cudaStream_t st) {
   if (lanes <= 0) lanes = default_lanes(N, nnz);
   if (unroll <= 0) unroll = 4;
   switch (lanes) {
-    case 1: return launch_csr_rows_u<S, 1>(row_ptr, col, val, x, y, N, unroll, st);
-    case 2: return launch_csr_rows_u<S, 2>(row_ptr, col, val, x, y, N, unroll, st);
-    case 4: return launch_csr_rows_u<S, 4>(row_ptr, col, val, x, y, N, unroll, st);
-    case 8: return launch_csr_rows_u<S, 8>(row_ptr, col, val, x, y, N, unroll, st);
-    case 16: return launch_csr_rows_u<S, 16>(row_ptr, col, val, x, y, N, unroll, st);
-    default: return launch_csr_rows_u<S, 32>(row_ptr, col, val, x, y, N, unroll, st);
+    case 1: return launch_csr_rows_u<SV, T, 1>(row_ptr, col, val, x, y, N, unroll, st);
+    case 2: return launch_csr_rows_u<SV, T, 2>(row_ptr, col, val, x, y, N, unroll, st);
+    case 4: return launch_csr_rows_u<SV, T, 4>(row_ptr, col, val, x, y, N, unroll, st);
+    case 8: return launch_csr_rows_u<SV, T, 8>(row_ptr, col, val, x, y, N, unroll, st);
+    case 16: return launch_csr_rows_u<SV, T, 16>(row_ptr, col, val, x, y, N, unroll, st);
+    default: return launch_csr_rows_u<SV, T, 32>(row_ptr, col, val, x, y, N, unroll, st);
   }
 }
 
@@ -625,8 +655,8 @@ static int launch_csr(const int* row_ptr, const int* col, const S* val, const S*
     if (tile == 2048) return launch_csr_stream<S, 2048, 3>(row_ptr, col, val, x, y, N, nnz, st);
     return launch_csr_stream<S, 1024, 4>(row_ptr, col, val, x, y, N, nnz, st);
   }
-  return launch_csr_rows<S>(row_ptr, col, val, x, y, N, nnz, opts ? opts->lanes_per_row : 0,
-                            opts ? opts->unroll : 0, st);
+  return launch_csr_rows<S, S>(row_ptr, col, val, x, y, N, nnz, opts ? opts->lanes_per_row : 0,
+                               opts ? opts->unroll : 0, st);
 }
 
 template <typename S, typename A>
@@ -663,7 +693,7 @@ extern "C" {
 int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                    const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
                    const sb_csr_opts* opts, void* stream) {
-  int r = check_dtype(dtype, "sb_spmv_csr");
+  int r = dtype == SB_BF16 ? SB_OK : check_dtype(dtype, "sb_spmv_csr");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nnz >= 0 && inner_max >= 0, "sb_spmv_csr: negative size");
   SB_REQUIRE(nnz <= 0x7fffffffLL, "sb_spmv_csr: nnz exceeds int32 row_ptr range");
@@ -679,7 +709,12 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
   if ((r = ensure_device())) return r;
   cudaStream_t st = as_stream(stream);
   for (int it = 0; it < inner_max; ++it) {
-    if (dtype == SB_F32)
+    if (dtype == SB_BF16)
+      r = launch_csr_rows<__nv_bfloat16, float>(row_ptr, col, (const __nv_bfloat16*)val,
+                                                (const float*)x, (float*)y, N, nnz,
+                                                opts ? opts->lanes_per_row : 0,
+                                                opts ? opts->unroll : 0, st);
+    else if (dtype == SB_F32)
       r = launch_csr<float, float>(row_ptr, col, (const float*)val, (const float*)x, (float*)y, N,
                                    nnz, opts, st);
     else

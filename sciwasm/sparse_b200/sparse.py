@@ -19,14 +19,22 @@ import numpy as np
 from . import _lib
 from ._lib import call
 
-_DT_CODE = {np.dtype(np.float32): _lib.SB_F32, np.dtype(np.float64): _lib.SB_F64}
+# BF16 value arrays are held as uint16 words (numpy has no bfloat16).
+_DT_CODE = {np.dtype(np.float32): _lib.SB_F32, np.dtype(np.float64): _lib.SB_F64,
+            np.dtype(np.uint16): _lib.SB_BF16}
+_STORAGE = {"f32": np.float32, "f64": np.float64, "bf16": np.uint16}
 
 
 def _dtcode(dtype) -> int:
     dt = np.dtype(dtype)
     if dt not in _DT_CODE:
-        raise TypeError(f"value dtype must be float32 or float64, got {dt}")
+        raise TypeError(f"value dtype must be float32, float64 or bf16 (uint16), got {dt}")
     return _DT_CODE[dt]
+
+
+def _vec_dtype(A):
+    """dtype of x and y for matrix A (f32 for BF16-stored values)."""
+    return np.dtype(np.float32) if A.dtype == np.uint16 else A.dtype
 
 
 def _sp(stream) -> Optional[int]:
@@ -322,8 +330,10 @@ def spmv(A, x_view, y_view, inner_max=1, stream=None):
     logging (the reference prints "spmv input : undefined" and returns)."""
     if A is None:
         raise ValueError("spmv input : undefined")
-    if x_view.dtype != A.dtype or y_view.dtype != A.dtype:
-        raise TypeError("x, y and A must share one value dtype")
+    if x_view.dtype != _vec_dtype(A) or y_view.dtype != _vec_dtype(A):
+        raise TypeError("x and y must have the matrix's value dtype (f32 for BF16 storage)")
+    if A.dtype == np.uint16 and not isinstance(A, sparse_CSR_t):
+        raise TypeError("BF16 storage is supported for CSR SpMV")
     if x_view.vec_nelem < A.N or y_view.vec_nelem < A.N:
         raise ValueError("x and y must hold N values")
     dt = _dtcode(A.dtype)
@@ -348,6 +358,63 @@ def spmv(A, x_view, y_view, inner_max=1, stream=None):
              inner_max, s)
     else:
         raise TypeError(f"spmv: unsupported matrix object {type(A).__name__}")
+
+
+def convert_values(src, storage, stream=None):
+    """A new device array holding src's values in `storage` ("f32", "f64",
+    "bf16"), rounded to nearest even."""
+    out = DeviceArray(src.n, _STORAGE[storage])
+    call("sb_convert_values", _dtcode(src.dtype), src.ptr, _dtcode(out.dtype), out.ptr, src.n,
+         _sp(stream))
+    return out
+
+
+def csr_with_storage(A_csr, storage, stream=None):
+    """The same CSR structure with values stored as `storage` (shares
+    row_index/col_index with A_csr)."""
+    return sparse_CSR_t(A_csr.row_index, A_csr.col_index,
+                        convert_values(A_csr.val_index, storage, stream), A_csr.N, A_csr.nnz)
+
+
+# --------------------------------------------------------------- batched SpMV
+
+
+class BatchExecutor:
+    """Batched CSR SpMV over many matrices and right-hand sides in one
+    graph-replayed persistent launch (values stored as `storage`)."""
+
+    def __init__(self, storage="f32", capacity=1024):
+        self.storage = storage
+        self.capacity = int(capacity)
+        p = C.c_void_p()
+        call("sb_batch_exec_create", _dtcode(_STORAGE[storage]), self.capacity, C.byref(p))
+        self.ptr = p.value
+        self._items = (_lib.BatchItem * self.capacity)()
+        self._keep = []
+
+    def run(self, jobs, stream=None):
+        """jobs: iterable of (A_csr, x DeviceArray N*k, y DeviceArray N*k, k)."""
+        n = 0
+        self._keep = []
+        for A, x, y, k in jobs:
+            it = self._items[n]
+            it.row_ptr, it.col, it.val = A.row_index.ptr, A.col_index.ptr, A.val_index.ptr
+            it.x, it.y = x.ptr, y.ptr
+            it.N, it.nrhs, it.lanes, it.reserved, it.nnz = A.N, int(k), 0, 0, A.nnz
+            self._keep.append((A, x, y))
+            n += 1
+        call("sb_batch_exec_run", self.ptr, self._items, n, _sp(stream))
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            try:
+                _lib.load().sb_batch_exec_destroy(self.ptr)
+            except Exception:
+                pass
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
 
 
 # --------------------------------------------------------------- conversions
