@@ -66,6 +66,14 @@ int sb_stream_create(void** stream);
 int sb_stream_destroy(void* stream);
 int sb_stream_synchronize(void* stream);
 int sb_mem_info(size_t* free_bytes, size_t* total_bytes);
+/* CUDA events for stream-ordered completion tracking and timing
+ * (sb_event_query returns 1 when complete, 0 when not yet, < 0 on error). */
+int sb_event_create(void** event);
+int sb_event_destroy(void* event);
+int sb_event_record(void* event, void* stream);
+int sb_event_query(void* event);
+int sb_event_synchronize(void* event);
+int sb_event_elapsed_ms(void* start, void* end, float* ms);
 /* Synchronises the device, returns and clears its status word: 0, or the code
  * of a kernel whose bounded wait gave up (1 = bulk copy, 2 = dependency). */
 int sb_device_status(int* code);
@@ -144,7 +152,8 @@ int sb_spmv_ell(int dtype, const int32_t* indices, const void* data, int32_t N, 
 
 /* One CSR matrix of a batch: y <- y + A x for nrhs (1..8) right-hand sides,
  * x and y stored N x nrhs row-major (x[col*nrhs + j]).  lanes: lanes per row
- * (1..32, power of two), 0 = chosen from nnz/N.  The y ranges of different
+ * (1..32, power of two), 0 = chosen from nnz/N.  flags bit 0 set: y <- A x
+ * (y is overwritten, rows without entries get 0).  The y ranges of different
  * items must not overlap (x may be shared). */
 typedef struct sb_batch_item {
   const int32_t* row_ptr;
@@ -155,7 +164,7 @@ typedef struct sb_batch_item {
   int32_t N;
   int32_t nrhs;
   int32_t lanes;
-  int32_t reserved;
+  int32_t flags;
   int64_t nnz;
 } sb_batch_item;
 

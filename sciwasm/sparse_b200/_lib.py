@@ -57,6 +57,12 @@ SIGNATURES: dict[str, list] = {
     "sb_stream_synchronize": [P],
     "sb_mem_info": [C.POINTER(SZ), C.POINTER(SZ)],
     "sb_device_status": [C.POINTER(C.c_int)],
+    "sb_event_create": [C.POINTER(P)],
+    "sb_event_destroy": [P],
+    "sb_event_record": [P, P],
+    "sb_event_query": [P],
+    "sb_event_synchronize": [P],
+    "sb_event_elapsed_ms": [P, P, C.POINTER(C.c_float)],
     "sb_spmv_coo": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
     "sb_spmv_csr": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
     "sb_spmv_dia": [C.c_int, P, P, I32, I32, I32, P, P, I32, P],
@@ -98,7 +104,7 @@ class CsrOpts(C.Structure):
 
 class BatchItem(C.Structure):
     _fields_ = [("row_ptr", P), ("col", P), ("val", P), ("x", P), ("y", P), ("N", I32),
-                ("nrhs", I32), ("lanes", I32), ("reserved", I32), ("nnz", I64)]
+                ("nrhs", I32), ("lanes", I32), ("flags", I32), ("nnz", I64)]
 
 
 SIGNATURES.update({

@@ -57,6 +57,7 @@ __device__ __forceinline__ void batch_block(const sb_batch_item& it, int r0, int
   const T* __restrict__ x = (const T*)it.x;
   T* __restrict__ y = (T*)it.y;
   const int K = it.nrhs;
+  const bool overwrite = (it.flags & 1) != 0;
   for (int b = 0; b < V; ++b) {
     const int row = r0 + b * RPB + g;
     const bool ok = row < it.N && row < r0 + 32;
@@ -77,7 +78,10 @@ __device__ __forceinline__ void batch_block(const sb_batch_item& it, int r0, int
       if (j < K) {
         T a = acc[j];
         for (int off = V >> 1; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
-        if (ok && q == 0 && e > s) y[(long long)row * K + j] += a;
+        if (ok && q == 0) {
+          if (overwrite) y[(long long)row * K + j] = a;
+          else if (e > s) y[(long long)row * K + j] += a;
+        }
       }
     }
   }

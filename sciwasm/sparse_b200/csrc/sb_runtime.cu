@@ -202,6 +202,52 @@ int sb_stream_synchronize(void* stream) {
   return SB_OK;
 }
 
+int sb_event_create(void** ev) {
+  SB_REQUIRE(ev, "sb_event_create: null output");
+  int r = ensure_device();
+  if (r) return r;
+  cudaEvent_t e;
+  SB_CHECK_CUDA(cudaEventCreate(&e));
+  *ev = reinterpret_cast<void*>(e);
+  return SB_OK;
+}
+
+int sb_event_destroy(void* ev) {
+  if (!ev) return SB_OK;
+  SB_CHECK_CUDA(cudaEventDestroy(reinterpret_cast<cudaEvent_t>(ev)));
+  return SB_OK;
+}
+
+int sb_event_record(void* ev, void* stream) {
+  SB_REQUIRE(ev, "sb_event_record: null event");
+  SB_CHECK_CUDA(cudaEventRecord(reinterpret_cast<cudaEvent_t>(ev), as_stream(stream)));
+  return SB_OK;
+}
+
+int sb_event_query(void* ev) {
+  SB_REQUIRE(ev, "sb_event_query: null event");
+  cudaError_t e = cudaEventQuery(reinterpret_cast<cudaEvent_t>(ev));
+  if (e == cudaSuccess) return 1;
+  if (e == cudaErrorNotReady) {
+    cudaGetLastError();
+    return 0;
+  }
+  return cuda_status(e, "cudaEventQuery");
+}
+
+int sb_event_synchronize(void* ev) {
+  SB_REQUIRE(ev, "sb_event_synchronize: null event");
+  SB_CHECK_CUDA(cudaEventSynchronize(reinterpret_cast<cudaEvent_t>(ev)));
+  return SB_OK;
+}
+
+int sb_event_elapsed_ms(void* start, void* end, float* ms) {
+  SB_REQUIRE(start && end && ms, "sb_event_elapsed_ms: null argument");
+  SB_CHECK_CUDA(cudaEventElapsedTime(ms, reinterpret_cast<cudaEvent_t>(start),
+                                     reinterpret_cast<cudaEvent_t>(end)));
+  return SB_OK;
+}
+
 int sb_device_status(int* code) {
   SB_REQUIRE(code, "sb_device_status: null output");
   *code = 0;

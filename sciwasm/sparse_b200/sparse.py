@@ -392,15 +392,16 @@ class BatchExecutor:
         self._items = (_lib.BatchItem * self.capacity)()
         self._keep = []
 
-    def run(self, jobs, stream=None):
-        """jobs: iterable of (A_csr, x DeviceArray N*k, y DeviceArray N*k, k)."""
+    def run(self, jobs, stream=None, overwrite=False):
+        """jobs: iterable of (A_csr, x DeviceArray N*k, y DeviceArray N*k, k);
+        y += A x, or y = A x with overwrite=True."""
         n = 0
         self._keep = []
         for A, x, y, k in jobs:
             it = self._items[n]
             it.row_ptr, it.col, it.val = A.row_index.ptr, A.col_index.ptr, A.val_index.ptr
             it.x, it.y = x.ptr, y.ptr
-            it.N, it.nrhs, it.lanes, it.reserved, it.nnz = A.N, int(k), 0, 0, A.nnz
+            it.N, it.nrhs, it.lanes, it.flags, it.nnz = A.N, int(k), 0, 1 if overwrite else 0, A.nnz
             self._keep.append((A, x, y))
             n += 1
         call("sb_batch_exec_run", self.ptr, self._items, n, _sp(stream))
