@@ -35,7 +35,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "SpMV HBM GB/s at <=1e-5 rel err"
+METRIC = "served SpMV/SpTS req/s + p99 vs plain path; SpMV HBM GB/s at \u22641e-5 rel err"
 UNIT = "GB/s"
 
 
@@ -462,8 +462,174 @@ def run_ours(args, jobs, config, rank, world, local_rank):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(jobs)
+    if world == 1 and not args.no_serving:
+        line["serving"] = run_serving(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ serving
+
+SERVE_STRUCT_MV = ("banded", "powerlaw", "laplacian2d")
+SERVE_STRUCT_TS = ("laplacian3d_lower", "random_lower")
+
+
+def build_serving_pool(n_mats, min_rows, max_rows, seed=11):
+    """Resident pool of the serving workload, generated on the device: rows
+    log-uniform in [min_rows, max_rows]; two thirds SpMV matrices (banded /
+    power-law / 2-D Laplacian, f32 and bf16 values), one third triangular
+    factors (3-D Laplacian lower / random lower, f32 values with a level-set
+    plan; f64 accumulation where the growth estimate exceeds 1)."""
+    from sciwasm.sparse_b200 import serve, synth_device as sd
+    rng = np.random.default_rng(seed)
+    pool = serve.ResidentPool(budget_bytes=150 * 10**9)
+    mv, ts = [], []
+    nrows = np.exp(rng.uniform(np.log(min_rows), np.log(max_rows), n_mats)).astype(np.int64)
+    for i, N in enumerate(nrows):
+        N = int(N)
+        name = f"m{i}"
+        if i % 3 == 2:
+            kind = SERVE_STRUCT_TS[(i // 3) % 2]
+            if kind == "laplacian3d_lower":
+                A = sd.laplacian_3d_lower(max(2, int(round(N ** (1 / 3)))))
+            else:
+                A = sd.random_lower(N, per_row=7, band=5000, seed=seed + i)
+            pool.add_csr(name, A, spmv_storages=(), spts_dtypes=("f32",))
+            ts.append(name)
+        else:
+            kind = SERVE_STRUCT_MV[(i // 3 * 2 + i % 3) % 3]
+            if kind == "banded":
+                A = sd.banded(N, half=5, seed=seed + i)
+            elif kind == "powerlaw":
+                A = sd.power_law(N, seed=seed + i)
+            else:
+                A = sd.laplacian_2d(max(2, int(round(N ** 0.5))))
+            pool.add_csr(name, A, spmv_storages=("f32", "bf16"))
+            mv.append(name)
+    return pool, mv, ts
+
+
+def serving_requests(pool, mv, ts, rate, seconds, in_ring, out_ring, seed=12):
+    """Poisson arrivals; 70% SpMV (f32 or bf16 values, even odds) on a
+    uniformly drawn SpMV matrix, 30% SpTS on a uniformly drawn factor.
+    Inputs and outputs are consecutive slices of pinned rings (wrapping)."""
+    from sciwasm.sparse_b200 import serve
+    rng = np.random.default_rng(seed)
+    t = serve.poisson_arrivals(rate, seconds, seed=seed)
+    is_mv = rng.random(t.size) < 0.7
+    pick_mv = rng.integers(0, len(mv), t.size)
+    pick_ts = rng.integers(0, len(ts), t.size)
+    bf = rng.random(t.size) < 0.5
+    reqs = []
+    io = oo = 0
+    for k in range(t.size):
+        if is_mv[k]:
+            name, op, st = mv[pick_mv[k]], "spmv", ("bf16" if bf[k] else "f32")
+        else:
+            name, op, st = ts[pick_ts[k]], "spts", "f32"
+        N = pool.mats[name].N
+        nb = serve._al(4 * N)
+        if io + nb > in_ring.nbytes:
+            io = 0
+        if oo + nb > out_ring.nbytes:
+            oo = 0
+        x = in_ring.view(io, N, np.float32)
+        y = out_ring.view(oo, N, np.float32)
+        io += nb
+        oo += nb
+        reqs.append(serve.Request(k, float(t[k]), name, op, st, x, y))
+    return reqs
+
+
+def serving_errors(pool, srv, mv, ts, n_check=24, seed=13):
+    """Max relative error (max norm) against an FP64 host computation (scipy)
+    of a sample of requests served in one batched mix: SpMV on the stored
+    values (f32, or bf16 widened), SpTS on the f32 factor."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as sl
+    from sciwasm.sparse_b200 import serve
+    rng = np.random.default_rng(seed)
+    small_mv = [n for n in mv if pool.mats[n].N <= 400_000] or mv
+    small_ts = [n for n in ts if pool.mats[n].N <= 400_000] or ts
+    reqs = []
+    for k in range(n_check):
+        if k % 3 == 2:
+            name, op, st = small_ts[rng.integers(len(small_ts))], "spts", "f32"
+        else:
+            name, op, st = small_mv[rng.integers(len(small_mv))], "spmv", ("f32", "bf16")[k % 2]
+        N = pool.mats[name].N
+        x = rng.uniform(-1, 1, N).astype(np.float32)
+        reqs.append(serve.Request(k, 0.0, name, op, st, x, np.zeros(N, np.float32)))
+    srv.serve(reqs, "batched")
+    errs = {"spmv_f32": 0.0, "spmv_bf16": 0.0, "spts_f32": 0.0}
+    for r in reqs:
+        A = pool.mats[r.matrix].csr[r.storage]
+        rp, col = A.row_array(), A.col_array()
+        v = A.val_array()
+        if r.storage == "bf16":
+            v = (v.astype(np.uint32) << 16).view(np.float32)
+        M = sp.csr_matrix((v.astype(np.float64), col, rp), shape=(A.N, A.N))
+        if r.op == "spmv":
+            t = M @ r.x.astype(np.float64)
+        else:
+            t = sl.spsolve_triangular(M, r.x.astype(np.float64), lower=True)
+        e = float(np.max(np.abs(r.y - t)) / max(np.max(np.abs(t)), 1e-300))
+        key = f"{r.op}_{r.storage}"
+        errs[key] = max(errs[key], e)
+    return errs
+
+
+def run_serving(args):
+    """Batched (continuous batching) and plain per-call serving of the same
+    request stream; returns the statistics of both and the sampled errors."""
+    from sciwasm.sparse_b200 import serve
+    from sciwasm.sparse_b200.sparse import PinnedBuffer
+    t0 = time.perf_counter()
+    pool, mv, ts = build_serving_pool(args.serve_pool, 1000, args.serve_max_rows)
+    build_s = time.perf_counter() - t0
+    in_ring = PinnedBuffer(1 << 30)
+    out_ring = PinnedBuffer(1 << 30)
+    xs = in_ring.view(0, in_ring.nbytes // 4, np.float32)
+    np.random.default_rng(5).random(out=xs, dtype=np.float32)
+    xs *= 2
+    xs -= 1
+    reqs = serving_requests(pool, mv, ts, args.serve_rate, args.serve_seconds, in_ring,
+                            out_ring)
+    srv = serve.Server(pool, max_batch=args.serve_batch, slots=args.serve_slots)
+    # warm-up: executors, graphs and first-touch costs
+    srv.serve([serve.Request(r.rid, 0.0, r.matrix, r.op, r.storage, r.x, r.y)
+               for r in reqs[:200]], "batched")
+    srv.serve([serve.Request(r.rid, 0.0, r.matrix, r.op, r.storage, r.x, r.y)
+               for r in reqs[:50]], "plain")
+    batched = srv.serve(reqs, "batched")
+    for r in reqs:
+        r.t_done = -1.0
+    plain = srv.serve(reqs, "plain")
+    errs = serving_errors(pool, srv, mv, ts)
+    rows = np.array([pool.mats[r.matrix].N for r in reqs])
+    bytes_io = int(np.sum(rows) * 8)
+    out = {
+        "workload": (f"{args.serve_pool} resident matrices, rows log-uniform in "
+                     f"[1000, {args.serve_max_rows}] (2/3 banded / power-law / 2-D Laplacian "
+                     "with f32 and bf16 values, 1/3 triangular factors: 3-D Laplacian lower / "
+                     "random lower, f32 with f64 accumulation where growth > 1); "
+                     f"Poisson arrivals at {args.serve_rate:g} req/s for "
+                     f"{args.serve_seconds:g} s, 70% SpMV (f32 or bf16 by request), 30% SpTS; "
+                     "vectors in pinned host memory, copies inside the measured latency"),
+        "requests": len(reqs), "mean_rows": float(rows.mean()),
+        "h2d_plus_d2h_bytes": bytes_io,
+        "pool_bytes": pool.admission.used, "pool_build_s": round(build_s, 2),
+        "flagged_f64_factors": sum(1 for n in ts if pool.mats[n].policy["f32"] == "f64"),
+        "batched": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in batched.items()},
+        "plain": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in plain.items()},
+        "max_rel_err_vs_fp64": errs,
+        "slots": args.serve_slots, "max_batch": args.serve_batch,
+        "timing": "host wall clock from each request's arrival to the host seeing its result",
+    }
+    pool.close()
+    in_ring.free()
+    out_ring.free()
+    return out
 
 
 def _pinned(nbytes):
@@ -491,6 +657,13 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="quarter-size matrices (profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-pool", type=int, default=2000)
+    ap.add_argument("--serve-max-rows", type=int, default=2_000_000)
+    ap.add_argument("--serve-rate", type=float, default=20_000.0)
+    ap.add_argument("--serve-seconds", type=float, default=5.0)
+    ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-batch", type=int, default=64)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -74,6 +74,8 @@ int sb_event_record(void* event, void* stream);
 int sb_event_query(void* event);
 int sb_event_synchronize(void* event);
 int sb_event_elapsed_ms(void* start, void* end, float* ms);
+/* Later work on `stream` waits for the event's recorded work. */
+int sb_stream_wait_event(void* stream, void* event);
 /* Synchronises the device, returns and clears its status word: 0, or the code
  * of a kernel whose bounded wait gave up (1 = bulk copy, 2 = dependency). */
 int sb_device_status(int* code);
@@ -292,6 +294,34 @@ int sb_spts_syncfree_csr(int dtype, const int32_t* row_ptr, const int32_t* col, 
 int sb_spts_syncfree_csr_noalloc(int dtype, const int32_t* row_ptr, const int32_t* col,
                                  const void* val, int32_t N, const void* b, void* y,
                                  int64_t spin_limit_cycles, void* stream);
+
+/* Growth estimate of a triangular factor (no counterpart in the reference):
+ * max over rows of sum_{j<i} |L_ij| / |L_ii| (inf for a zero diagonal).  Below
+ * 1 the factor is row diagonally dominant and a solve in the value type does
+ * not amplify rounding; above a threshold the caller flags the factor for
+ * SB_SPTS_ACC_F64.  Returns after the reduction. */
+int sb_spts_plan_growth(const sb_spts_plan* plan, double* growth, void* stream);
+
+/* Batched solves (no counterpart in the reference, which solves one system
+ * per call): many independent systems, each with its own analysed plan, in
+ * one persistent launch replayed from a captured CUDA graph.  Every row is
+ * solved with the arithmetic of SB_SPTS_HYBRID, so each result is
+ * bit-identical to sb_spts_solve(plan, SB_SPTS_HYBRID, policy, b, y).  An
+ * executor serves one value dtype (SB_F32 or SB_F64) and one accumulation
+ * policy; a plan may appear once per run, and the solves of one plan must be
+ * ordered (one stream, or events) because they share its work vector and
+ * ready flags.  Stream-ordered; a dependency wait that runs out is reported
+ * by sb_device_status (code 2). */
+typedef struct sb_spts_batch sb_spts_batch;
+typedef struct sb_spts_batch_item {
+  sb_spts_plan* plan;
+  const void* b; /* right-hand side, natural row order */
+  void* y;       /* solution, natural row order        */
+} sb_spts_batch_item;
+int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch** out);
+int sb_spts_batch_destroy(sb_spts_batch* e);
+int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t n,
+                      void* stream);
 
 /* ---------------------------------------------------------------------- */
 /* eliminate_zeros and transpose (bit-exact with the reference's kernels). */

@@ -63,6 +63,7 @@ SIGNATURES: dict[str, list] = {
     "sb_event_query": [P],
     "sb_event_synchronize": [P],
     "sb_event_elapsed_ms": [P, P, C.POINTER(C.c_float)],
+    "sb_stream_wait_event": [P, P],
     "sb_spmv_coo": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
     "sb_spmv_csr": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
     "sb_spmv_dia": [C.c_int, P, P, I32, I32, I32, P, P, I32, P],
@@ -107,7 +108,15 @@ class BatchItem(C.Structure):
                 ("nrhs", I32), ("lanes", I32), ("flags", I32), ("nnz", I64)]
 
 
+class SptsBatchItem(C.Structure):
+    _fields_ = [("plan", P), ("b", P), ("y", P)]
+
+
 SIGNATURES.update({
+    "sb_spts_plan_growth": [P, C.POINTER(C.c_double), P],
+    "sb_spts_batch_create": [C.c_int, C.c_int, I32, C.POINTER(P)],
+    "sb_spts_batch_destroy": [P],
+    "sb_spts_batch_run": [P, C.POINTER(SptsBatchItem), I32, P],
     "sb_batch_exec_create": [C.c_int, I32, C.POINTER(P)],
     "sb_batch_exec_destroy": [P],
     "sb_batch_exec_run": [P, C.POINTER(BatchItem), I32, P],

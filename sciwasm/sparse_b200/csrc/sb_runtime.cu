@@ -241,6 +241,12 @@ int sb_event_synchronize(void* ev) {
   return SB_OK;
 }
 
+int sb_stream_wait_event(void* stream, void* ev) {
+  SB_REQUIRE(ev, "sb_stream_wait_event: null event");
+  SB_CHECK_CUDA(cudaStreamWaitEvent(as_stream(stream), reinterpret_cast<cudaEvent_t>(ev), 0));
+  return SB_OK;
+}
+
 int sb_event_elapsed_ms(void* start, void* end, float* ms) {
   SB_REQUIRE(start && end && ms, "sb_event_elapsed_ms: null argument");
   SB_CHECK_CUDA(cudaEventElapsedTime(ms, reinterpret_cast<cudaEvent_t>(start),

@@ -24,6 +24,8 @@
 //                    row kernel's arithmetic, as the level/sync-free hybrid of
 //                    src/parallel/src/sparse_opt_32.wat:12846-13445
 #include <algorithm>
+#include <cstring>
+#include <type_traits>
 #include <mutex>
 #include <vector>
 
@@ -48,7 +50,6 @@ struct sb_spts_plan {
   int* rcol = nullptr;
   void* rval = nullptr;
   void* ywork = nullptr;
-  unsigned* flags = nullptr;
   int* ticket = nullptr;
   std::vector<int> h_level_ptr;
   std::vector<void*> owned;
@@ -59,31 +60,47 @@ namespace sb {
 constexpr int kT = 256;
 constexpr long long kDefaultSpin = 1LL << 31;  // SM cycles (about a second)
 
+// Polling back-off of the dependency waits: the sleep between two polls of a
+// ready flag starts at SB_SPTS_SLEEP_MIN_NS and doubles up to
+// SB_SPTS_SLEEP_MAX_NS, trading a little latency per level for less L2
+// traffic from the many waiting threads.
+#ifndef SB_SPTS_SLEEP_MIN_NS
+#define SB_SPTS_SLEEP_MIN_NS 32u
+#endif
+#ifndef SB_SPTS_SLEEP_MAX_NS
+#define SB_SPTS_SLEEP_MAX_NS 1024u
+#endif
+
 static unsigned grid1(long long n) {
   long long g = (n + kT - 1) / kT;
   return (unsigned)std::max(1LL, std::min(g, 0x7fffffffLL));
 }
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
   unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
   return v;
 }
+__device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 // Wait until flags[c] != 0 or the clock bound passes (then record a timeout
 // in the status word and carry on, so that the kernel always terminates).
-__device__ __forceinline__ void wait_ready(const unsigned* flags, int c, long long limit,
-                                           int* status) {
-  if (ld_acquire(flags + c)) return;
+// Polls with relaxed loads: the caller issues an acquire fence before it
+// reads what the flag publishes.
+__device__ __noinline__ void wait_ready(const unsigned* flags, int c, long long limit,
+                                        int* status) {
   const long long t0 = clock64();
-  while (!ld_acquire(flags + c)) {
-    if (clock64() - t0 > limit) {
+  unsigned ns = SB_SPTS_SLEEP_MIN_NS;
+  while (!ld_relaxed_u32(flags + c)) {
+    // once any wait has given up, the others give up at once
+    if (clock64() - t0 > limit || *(volatile const int*)status) {
       atomicExch(status, SB_DEV_TIMEOUT_DEP);
       return;
     }
-    __nanosleep(64);
+    __nanosleep(ns);
+    ns = ns < SB_SPTS_SLEEP_MAX_NS ? 2 * ns : ns;
   }
 }
 
@@ -107,6 +124,99 @@ template <typename T> __device__ __forceinline__ T div_rn(T a, T b);
 template <> __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
 template <> __device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
 
+// ------------------------------------------------------------ pending values
+// The plan-based solves and the level analysis publish each row's result in a
+// work array that starts filled with all-one bits ("pending").  One relaxed
+// load of a dependency then gives both its readiness and its value: no ready
+// flag, no fence, and the loads of a row's dependencies go out together
+// (kG per round trip).  A result that happens to have the pending bits is
+// stored as a canonical NaN instead, so a written result is never pending.
+__device__ __forceinline__ float ld_relaxed(const float* p) {
+  float v;
+  asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_relaxed(const double* p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(float* p, float v) {
+  asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(int* p, int v) {
+  asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ bool pending(float v) { return __float_as_uint(v) == 0xffffffffu; }
+__device__ __forceinline__ bool pending(double v) { return __double_as_longlong(v) == -1LL; }
+__device__ __forceinline__ bool pending(int v) { return v < 0; }
+__device__ __forceinline__ float settled(float v) {
+  return pending(v) ? __uint_as_float(0x7fffffffu) : v;
+}
+__device__ __forceinline__ double settled(double v) {
+  return pending(v) ? __longlong_as_double(0x7fffffffffffffffLL) : v;
+}
+
+// Poll *p until it is no longer pending or the clock bound passes (then
+// record a timeout in the status word and return the pending value, so that
+// the kernel always terminates); once any wait has given up, the others give
+// up at once.
+template <typename V>
+__device__ __noinline__ V wait_pending(const V* p, long long limit, int* status) {
+  const long long t0 = clock64();
+  unsigned ns = SB_SPTS_SLEEP_MIN_NS;
+  while (true) {
+    __nanosleep(ns);
+    ns = ns < SB_SPTS_SLEEP_MAX_NS ? 2 * ns : ns;
+    const V v = ld_relaxed(p);
+    if (!pending(v)) return v;
+    if (clock64() - t0 > limit || *(volatile const int*)status) {
+      atomicExch(status, SB_DEV_TIMEOUT_DEP);
+      return v;
+    }
+  }
+}
+
+constexpr int kG = 8;  // dependencies loaded per round trip
+
+// acc (+|-)= val[j] * w[col[j]] for j in [s, e), in storage order, waiting
+// for each w[col[j]] to be published (SUB selects the sync-free form).
+template <typename T, typename A, bool SUB>
+__device__ __forceinline__ A dot_published(const int* __restrict__ col, const T* __restrict__ val,
+                                           int s, int e, const T* w, A acc, long long limit,
+                                           int* status) {
+  for (int j0 = s; j0 < e; j0 += kG) {
+    int c[kG];
+    A a[kG];
+    T v[kG];
+#pragma unroll
+    for (int k = 0; k < kG; ++k)
+      if (j0 + k < e) {
+        c[k] = col[j0 + k];
+        a[k] = (A)val[j0 + k];
+      }
+#pragma unroll
+    for (int k = 0; k < kG; ++k)
+      if (j0 + k < e) v[k] = ld_relaxed(w + c[k]);
+#pragma unroll
+    for (int k = 0; k < kG; ++k)
+      if (j0 + k < e) {
+        T x = v[k];
+        if (pending(x)) x = wait_pending(w + c[k], limit, status);
+        acc = SUB ? sub_rn(acc, mul_rn(a[k], (A)x)) : add_rn(acc, mul_rn(a[k], (A)x));
+      }
+  }
+  return acc;
+}
+
 // ------------------------------------------------------------ analysis
 
 // flags[0] = 1 unless every row is non-empty, ends with its diagonal and has
@@ -122,8 +232,8 @@ __global__ void lower_check(const int* __restrict__ row_ptr, const int* __restri
 }
 
 __global__ void level_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col, int N,
-                             int* __restrict__ level, unsigned* __restrict__ done,
-                             int* __restrict__ ticket, long long limit, int* __restrict__ status) {
+                             int* level, int* __restrict__ ticket, long long limit,
+                             int* __restrict__ status) {
   while (true) {
     const int base = next_rows(ticket);
     if (base >= N) return;
@@ -135,18 +245,22 @@ __global__ void level_kernel(const int* __restrict__ row_ptr, const int* __restr
         lv = 0;
       } else {
         int m = 0;
-        for (int j = s; j < e - 1; ++j) {
-          const int c = col[j];
-          if (c >= 0 && c < i) {
-            wait_ready(done, c, limit, status);
-            const int lc = *(volatile const int*)(level + c);
-            m = lc > m ? lc : m;
+        for (int j0 = s; j0 < e - 1; j0 += kG) {
+          int c[kG], v[kG];
+#pragma unroll
+          for (int k = 0; k < kG; ++k) c[k] = (j0 + k < e - 1) ? col[j0 + k] : -1;
+#pragma unroll
+          for (int k = 0; k < kG; ++k) v[k] = (c[k] >= 0 && c[k] < i) ? ld_relaxed(level + c[k]) : 0;
+#pragma unroll
+          for (int k = 0; k < kG; ++k) {
+            int x = v[k];
+            if (x < 0) x = wait_pending(level + c[k], limit, status);
+            m = x > m ? x : m;
           }
         }
         lv = 1 + m;
       }
-      level[i] = lv;
-      st_release(done + i, 1u);
+      st_relaxed(level + i, lv);
     }
   }
 }
@@ -228,11 +342,13 @@ __global__ void spts_level_rows(const int* __restrict__ rrow, const int* __restr
   }
 }
 
-// Level-ordered rows with ready flags (hybrid): same arithmetic as above.
+// Level-ordered rows (hybrid): same arithmetic as above, dependencies read
+// from the pending-initialised work vector yw (level order); each row also
+// writes its natural-order output y[perm[i]].
 template <typename T, typename A>
 __global__ void spts_hybrid_rows(const int* __restrict__ rrow, const int* __restrict__ rcol,
                                  const T* __restrict__ rval, int N, const int* __restrict__ perm,
-                                 const T* __restrict__ b, T* yw, unsigned* __restrict__ done,
+                                 const T* __restrict__ b, T* yw, T* __restrict__ y,
                                  int* __restrict__ ticket, long long limit, int* status) {
   while (true) {
     const int base = next_rows(ticket);
@@ -240,26 +356,47 @@ __global__ void spts_hybrid_rows(const int* __restrict__ rrow, const int* __rest
     const int i = base + (threadIdx.x & 31);
     if (i < N) {
       const int s = rrow[i], end = rrow[i + 1] - 1;
-      const A bi = (A)b[perm[i]];
+      const int pi = perm[i];
+      const A bi = (A)b[pi];
       T yi;
       if (end > s) {
-        A t = 0;
-        for (int j = s; j < end; ++j) {
-          const int c = rcol[j];
-          wait_ready(done, c, limit, status);
-          t = add_rn(t, mul_rn((A)rval[j], (A)*(volatile const T*)(yw + c)));
-        }
+        const A t = dot_published<T, A, false>(rcol, rval, s, end, yw, A(0), limit, status);
         yi = (T)div_rn(sub_rn(bi, t), (A)rval[end]);
       } else {
         yi = (T)div_rn(bi, (A)rval[end]);
       }
-      yw[i] = yi;
-      st_release(done + i, 1u);
+      st_relaxed(yw + i, settled(yi));
+      y[pi] = yi;
     }
   }
 }
 
-// Sync-free solve in natural order (t = b_i; t -= L_ij*y_j; y_i = t/L_ii).
+// Sync-free solve of an analysed (lower, diagonal last) matrix in natural
+// order, the sync-free kernel's arithmetic (t = b_i; t -= L_ij*y_j;
+// y_i = t/L_ii), dependencies read from the pending-initialised yw.
+template <typename T, typename A>
+__global__ void spts_syncfree_plan_rows(const int* __restrict__ row_ptr,
+                                        const int* __restrict__ col, const T* __restrict__ val,
+                                        int N, const T* __restrict__ b, T* yw, T* __restrict__ y,
+                                        int* __restrict__ ticket, long long limit, int* status) {
+  while (true) {
+    const int base = next_rows(ticket);
+    if (base >= N) return;
+    const int i = base + (threadIdx.x & 31);
+    if (i < N) {
+      const int s = row_ptr[i], e = row_ptr[i + 1];
+      const A t = dot_published<T, A, true>(col, val, s, e - 1, yw, (A)b[i], limit, status);
+      const T yi = (T)div_rn(t, (A)val[e - 1]);
+      st_relaxed(yw + i, settled(yi));
+      y[i] = yi;
+    }
+  }
+}
+
+// Sync-free solve in natural order (t = b_i; t -= L_ij*y_j; y_i = t/L_ii) on
+// the caller's arrays with ready flags: a row first waits for the flags of
+// all its in-range dependencies (kG relaxed loads per round trip), then one
+// acquire fence orders the value loads after them.
 template <typename T, typename A>
 __global__ void spts_syncfree_rows(const int* __restrict__ row_ptr, const int* __restrict__ col,
                                    const T* __restrict__ val, int N, const T* __restrict__ b, T* y,
@@ -274,12 +411,29 @@ __global__ void spts_syncfree_rows(const int* __restrict__ row_ptr, const int* _
       A t = (A)b[i];
       T yi;
       if (e > s + 1) {
-        for (int j = s; j < e - 1; ++j) {
-          const int c = col[j];
-          if (c >= 0 && c < N) {
-            wait_ready(done, c, limit, status);
-            t = sub_rn(t, mul_rn((A)val[j], (A)*(volatile const T*)(y + c)));
-          }
+        for (int j0 = s; j0 < e - 1; j0 += kG) {
+          int c[kG];
+          unsigned f[kG];
+#pragma unroll
+          for (int k = 0; k < kG; ++k) c[k] = (j0 + k < e - 1) ? col[j0 + k] : -1;
+#pragma unroll
+          for (int k = 0; k < kG; ++k) f[k] = (c[k] >= 0 && c[k] < N) ? ld_relaxed_u32(done + c[k]) : 1u;
+#pragma unroll
+          for (int k = 0; k < kG; ++k)
+            if (!f[k]) wait_ready(done, c[k], limit, status);
+        }
+        fence_acquire();
+        for (int j0 = s; j0 < e - 1; j0 += kG) {
+          int c[kG];
+          T v[kG];
+#pragma unroll
+          for (int k = 0; k < kG; ++k) c[k] = (j0 + k < e - 1) ? col[j0 + k] : -1;
+#pragma unroll
+          for (int k = 0; k < kG; ++k)
+            if (c[k] >= 0 && c[k] < N) v[k] = ld_relaxed(y + c[k]);
+#pragma unroll
+          for (int k = 0; k < kG; ++k)
+            if (c[k] >= 0 && c[k] < N) t = sub_rn(t, mul_rn((A)val[j0 + k], (A)v[k]));
         }
         yi = (T)div_rn(t, (A)val[e - 1]);
       } else {
@@ -296,6 +450,104 @@ __global__ void scatter_by_perm(const T* __restrict__ yw, const int* __restrict_
                                 T* __restrict__ y) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p < N) y[perm[p]] = yw[p];
+}
+
+// ------------------------------------------------------------ batched solves
+// Many independent systems in one persistent launch.  Each system hands out
+// its own 32-row chunks in level order through its own ticket counter; warp
+// w starts on system w mod M and moves to the next system once the current
+// one has no chunk left, so all systems of a batch advance at the same time
+// (the launch takes about the deepest system's time, not the sum of all).
+// A row waits only on rows of its own system with a smaller level-order
+// index, i.e. on chunks of that system already claimed by running warps, so
+// the launch always makes progress.  Rows are solved as in spts_hybrid_rows.
+struct SptsDesc {
+  const int* rrow;
+  const int* rcol;
+  const void* rval;
+  const int* perm;
+  void* yw;
+  const void* b;
+  void* y;
+  int N;
+  int pad;
+};
+
+// Every item's work vector to the pending bits.
+template <typename T>
+__global__ void spts_batch_reset(const SptsDesc* __restrict__ items, const int* __restrict__ count) {
+  using U = typename std::conditional<sizeof(T) == 4, unsigned, unsigned long long>::type;
+  const int M = count[0];
+  for (int k = 0; k < M; ++k) {
+    U* w = (U*)items[k].yw;
+    const long long N = items[k].N;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x)
+      w[i] = ~U(0);
+  }
+}
+
+template <typename T, typename A>
+__global__ void __launch_bounds__(kT)
+    spts_batch_kernel(const SptsDesc* __restrict__ items, const int* __restrict__ count,
+                      int* __restrict__ tickets, long long limit, int* status) {
+  const int lane = threadIdx.x & 31;
+  const int M = count[0];
+  if (M <= 0) return;
+  const int gw = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  for (int k = 0; k < M; ++k) {
+    const int sys = (int)(((long long)gw + k) % M);
+    const SptsDesc d = items[sys];
+    const int nch = (d.N + 31) >> 5;
+    const T* __restrict__ rval = (const T*)d.rval;
+    T* yw = (T*)d.yw;
+    while (true) {
+      int t = 0;
+      if (lane == 0) t = atomicAdd(tickets + sys, 1);
+      t = __shfl_sync(0xffffffffu, t, 0);
+      if (t >= nch) break;
+      const int i = t * 32 + lane;
+      if (i < d.N) {
+        const int s = d.rrow[i], end = d.rrow[i + 1] - 1;
+        const int pi = d.perm[i];
+        const A bi = (A)((const T*)d.b)[pi];
+        T yi;
+        if (end > s) {
+          const A acc = dot_published<T, A, false>(d.rcol, rval, s, end, yw, A(0), limit, status);
+          yi = (T)div_rn(sub_rn(bi, acc), (A)rval[end]);
+        } else {
+          yi = (T)div_rn(bi, (A)rval[end]);
+        }
+        st_relaxed(yw + i, settled(yi));
+        ((T*)d.y)[pi] = yi;
+      }
+    }
+  }
+}
+
+// max over rows of sum_{j < diag} |L_ij| / |L_ii| (inf for a zero diagonal),
+// as the bits of a non-negative double so that an integer max orders them.
+template <typename T>
+__global__ void growth_kernel(const int* __restrict__ row_ptr, const T* __restrict__ val, int N,
+                              unsigned long long* __restrict__ out) {
+  double m = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int s = row_ptr[i], e = row_ptr[i + 1];
+    if (e <= s) continue;
+    double off = 0.0;
+    for (int j = s; j < e - 1; ++j) off += fabs((double)val[j]);
+    const double dg = fabs((double)val[e - 1]);
+    const double r = off / dg;  // 0/0 -> NaN, x/0 -> inf
+    const double rr = (r != r) ? __longlong_as_double(0x7ff0000000000000LL) : r;
+    m = rr > m ? rr : m;
+  }
+  unsigned long long b = (unsigned long long)__double_as_longlong(m);
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long v = __shfl_xor_sync(0xffffffffu, b, o);
+    b = v > b ? v : b;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, b);
 }
 
 static int resident_grid(const void* kern) {
@@ -333,7 +585,6 @@ static int analyze_impl(sb_spts_plan* p, cudaStream_t st) {
   SB_PA(p->rcol, sizeof(int) * (size_t)nnz);
   SB_PA(p->rval, sizeof(T) * (size_t)nnz);
   SB_PA(p->ywork, sizeof(T) * N);
-  SB_PA(p->flags, sizeof(unsigned) * N);
   SB_PA(p->ticket, sizeof(int) * 4);
 #undef SB_PA
   int* status = device_status_word();
@@ -346,10 +597,10 @@ static int analyze_impl(sb_spts_plan* p, cudaStream_t st) {
   SB_CHECK_CUDA(cudaMemsetAsync(tmp, 0, 4 * sizeof(int), st));
   lower_check<<<grid1(N), kT, 0, st>>>(p->row_ptr, p->col, N, tmp);
   SB_CHECK_LAUNCH("lower_check");
-  SB_CHECK_CUDA(cudaMemsetAsync(p->flags, 0, sizeof(unsigned) * N, st));
+  SB_CHECK_CUDA(cudaMemsetAsync(p->level, 0xff, sizeof(int) * N, st));
   SB_CHECK_CUDA(cudaMemsetAsync(p->ticket, 0, sizeof(int), st));
   level_kernel<<<resident_grid((const void*)level_kernel), kT, 0, st>>>(
-      p->row_ptr, p->col, N, p->level, p->flags, p->ticket, kDefaultSpin, status);
+      p->row_ptr, p->col, N, p->level, p->ticket, kDefaultSpin, status);
   SB_CHECK_LAUNCH("level_kernel");
   max_kernel<<<std::min<unsigned>(grid1(N), (unsigned)sm_count() * 4), kT, 0, st>>>(p->level, N,
                                                                                     tmp + 1);
@@ -437,32 +688,30 @@ static int solve_impl(const sb_spts_plan* p, int algo, const T* b, T* y, long lo
     set_error("sb_spts_solve: device status word unavailable");
     return SB_ENOMEM;
   }
-  if (algo == SB_SPTS_SYNCFREE) {
-    SB_CHECK_CUDA(cudaMemsetAsync(p->flags, 0, sizeof(unsigned) * N, st));
+  T* yw = (T*)p->ywork;
+  if (algo == SB_SPTS_SYNCFREE || algo == SB_SPTS_HYBRID) {
+    SB_CHECK_CUDA(cudaMemsetAsync(yw, 0xff, sizeof(T) * N, st));
     SB_CHECK_CUDA(cudaMemsetAsync(p->ticket, 0, sizeof(int), st));
-    auto k = spts_syncfree_rows<T, A>;
-    k<<<resident_grid((const void*)k), kT, 0, st>>>(p->row_ptr, p->col, (const T*)p->val, N, b, y,
-                                                     p->flags, p->ticket, limit, status);
-    SB_CHECK_LAUNCH("spts_syncfree_rows");
+    if (algo == SB_SPTS_SYNCFREE) {
+      auto k = spts_syncfree_plan_rows<T, A>;
+      k<<<resident_grid((const void*)k), kT, 0, st>>>(p->row_ptr, p->col, (const T*)p->val, N, b,
+                                                       yw, y, p->ticket, limit, status);
+      SB_CHECK_LAUNCH("spts_syncfree_plan_rows");
+    } else {
+      auto k = spts_hybrid_rows<T, A>;
+      k<<<resident_grid((const void*)k), kT, 0, st>>>(p->rrow, p->rcol, (const T*)p->rval, N,
+                                                       p->perm, b, yw, y, p->ticket, limit,
+                                                       status);
+      SB_CHECK_LAUNCH("spts_hybrid_rows");
+    }
     return SB_OK;
   }
-  T* yw = (T*)p->ywork;
-  if (algo == SB_SPTS_HYBRID) {
-    SB_CHECK_CUDA(cudaMemsetAsync(p->flags, 0, sizeof(unsigned) * N, st));
-    SB_CHECK_CUDA(cudaMemsetAsync(p->ticket, 0, sizeof(int), st));
-    auto k = spts_hybrid_rows<T, A>;
-    k<<<resident_grid((const void*)k), kT, 0, st>>>(p->rrow, p->rcol, (const T*)p->rval, N,
-                                                     p->perm, b, yw, p->flags, p->ticket, limit,
-                                                     status);
-    SB_CHECK_LAUNCH("spts_hybrid_rows");
-  } else {
-    for (int l = 0; l < p->nlevels; ++l) {
-      const int r0 = p->h_level_ptr[l], r1 = p->h_level_ptr[l + 1];
-      if (r1 <= r0) continue;
-      spts_level_rows<T, A><<<grid1(r1 - r0), kT, 0, st>>>(p->rrow, p->rcol, (const T*)p->rval,
-                                                           r0, r1, p->perm, b, yw);
-      SB_CHECK_LAUNCH("spts_level_rows");
-    }
+  for (int l = 0; l < p->nlevels; ++l) {
+    const int r0 = p->h_level_ptr[l], r1 = p->h_level_ptr[l + 1];
+    if (r1 <= r0) continue;
+    spts_level_rows<T, A><<<grid1(r1 - r0), kT, 0, st>>>(p->rrow, p->rcol, (const T*)p->rval,
+                                                         r0, r1, p->perm, b, yw);
+    SB_CHECK_LAUNCH("spts_level_rows");
   }
   scatter_by_perm<T><<<grid1(N), kT, 0, st>>>(yw, p->perm, N, y);
   SB_CHECK_LAUNCH("scatter_by_perm");
@@ -508,7 +757,190 @@ static unsigned* noalloc_scratch(int* status) {
 
 using namespace sb;
 
+struct sb_spts_batch {
+  int dtype = 0;
+  int policy = 0;
+  int capacity = 0;
+  int device = 0;
+  int grid = 0;
+  SptsDesc* h_items = nullptr;  // pinned
+  int* h_count = nullptr;       // pinned: [0] items
+  SptsDesc* d_items = nullptr;
+  int* d_count = nullptr;       // [0] items
+  int* d_tickets = nullptr;     // one chunk counter per item
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t capture_stream = nullptr;
+  cudaEvent_t done = nullptr;
+  bool pending = false;
+};
+
+static void spts_batch_release(sb_spts_batch* e) {
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->capture_stream) cudaStreamDestroy(e->capture_stream);
+  if (e->done) cudaEventDestroy(e->done);
+  if (e->h_items) cudaFreeHost(e->h_items);
+  if (e->h_count) cudaFreeHost(e->h_count);
+  if (e->d_items) cudaFree(e->d_items);
+  if (e->d_count) cudaFree(e->d_count);
+  if (e->d_tickets) cudaFree(e->d_tickets);
+  delete e;
+}
+
+static const void* spts_batch_kernel_for(int dtype, int policy) {
+  if (dtype == SB_F64) return (const void*)spts_batch_kernel<double, double>;
+  if (policy == SB_SPTS_ACC_F64) return (const void*)spts_batch_kernel<float, double>;
+  return (const void*)spts_batch_kernel<float, float>;
+}
+
 extern "C" {
+
+int sb_spts_plan_growth(const sb_spts_plan* plan, double* growth, void* stream) {
+  SB_REQUIRE(plan && growth, "sb_spts_plan_growth: null argument");
+  *growth = 0.0;
+  if (plan->N == 0) return SB_OK;
+  cudaStream_t st = as_stream(stream);
+  unsigned long long* d = nullptr;
+  int r = scratch_alloc((void**)&d, sizeof(unsigned long long), st);
+  if (r) return r;
+  SB_CHECK_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), st));
+  const unsigned g = std::min<unsigned>(grid1(plan->N), (unsigned)sm_count() * 8);
+  if (plan->dtype == SB_F64)
+    growth_kernel<double><<<g, kT, 0, st>>>(plan->row_ptr, (const double*)plan->val, plan->N, d);
+  else
+    growth_kernel<float><<<g, kT, 0, st>>>(plan->row_ptr, (const float*)plan->val, plan->N, d);
+  SB_CHECK_LAUNCH("growth_kernel");
+  unsigned long long h = 0;
+  SB_CHECK_CUDA(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, st));
+  SB_CHECK_CUDA(cudaStreamSynchronize(st));
+  scratch_free(d, st);
+  double v;
+  memcpy(&v, &h, sizeof(v));
+  *growth = v;
+  return SB_OK;
+}
+
+int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch** out) {
+  SB_REQUIRE(out, "sb_spts_batch_create: null output");
+  *out = nullptr;
+  SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_spts_batch_create: dtype must be F32 or F64");
+  SB_REQUIRE(policy == SB_SPTS_ACC_NATIVE || policy == SB_SPTS_ACC_F64,
+             "sb_spts_batch_create: bad accumulation policy");
+  SB_REQUIRE(capacity > 0, "sb_spts_batch_create: capacity must be positive");
+  int r = ensure_device();
+  if (r) return r;
+  int* status = device_status_word();
+  if (!status) {
+    set_error("sb_spts_batch_create: device status word unavailable");
+    return SB_ENOMEM;
+  }
+  sb_spts_batch* e = new sb_spts_batch();
+  e->dtype = dtype;
+  e->policy = dtype == SB_F64 ? SB_SPTS_ACC_F64 : policy;
+  e->capacity = capacity;
+  cudaGetDevice(&e->device);
+  cudaError_t ce = cudaSuccess;
+#define SB_E(call)                    \
+  if ((ce = (call)) != cudaSuccess) { \
+    r = cuda_status(ce, #call);       \
+    spts_batch_release(e);            \
+    return r;                         \
+  }
+  SB_E(cudaMallocHost(&e->h_items, sizeof(SptsDesc) * capacity));
+  SB_E(cudaMallocHost(&e->h_count, sizeof(int) * 4));
+  SB_E(cudaMalloc(&e->d_items, sizeof(SptsDesc) * capacity));
+  SB_E(cudaMalloc(&e->d_count, sizeof(int) * 4));
+  SB_E(cudaMalloc(&e->d_tickets, sizeof(int) * capacity));
+  SB_E(cudaStreamCreateWithFlags(&e->capture_stream, cudaStreamNonBlocking));
+  SB_E(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming));
+  const void* kern = spts_batch_kernel_for(dtype, e->policy);
+  e->grid = resident_grid(kern);
+  cudaGraph_t g = nullptr;
+  SB_E(cudaStreamBeginCapture(e->capture_stream, cudaStreamCaptureModeThreadLocal));
+  cudaMemcpyAsync(e->d_items, e->h_items, sizeof(SptsDesc) * capacity, cudaMemcpyHostToDevice,
+                  e->capture_stream);
+  cudaMemcpyAsync(e->d_count, e->h_count, sizeof(int) * 4, cudaMemcpyHostToDevice,
+                  e->capture_stream);
+  cudaMemsetAsync(e->d_tickets, 0, sizeof(int) * capacity, e->capture_stream);
+  {
+    const void* reset = dtype == SB_F64 ? (const void*)spts_batch_reset<double>
+                                        : (const void*)spts_batch_reset<float>;
+    void* rargs[] = {(void*)&e->d_items, (void*)&e->d_count};
+    cudaLaunchKernel(reset, dim3(sm_count() * 4), dim3(kT), rargs, 0, e->capture_stream);
+  }
+  long long limit = kDefaultSpin;
+  void* args[] = {(void*)&e->d_items, (void*)&e->d_count, (void*)&e->d_tickets, (void*)&limit,
+                  (void*)&status};
+  cudaLaunchKernel(kern, dim3(e->grid), dim3(kT), args, 0, e->capture_stream);
+  SB_E(cudaStreamEndCapture(e->capture_stream, &g));
+  ce = cudaGraphInstantiate(&e->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) {
+    r = cuda_status(ce, "cudaGraphInstantiate");
+    spts_batch_release(e);
+    return r;
+  }
+#undef SB_E
+  *out = e;
+  return SB_OK;
+}
+
+int sb_spts_batch_destroy(sb_spts_batch* e) {
+  if (!e) return SB_OK;
+  if (e->pending) cudaEventSynchronize(e->done);
+  spts_batch_release(e);
+  return SB_OK;
+}
+
+int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t n,
+                      void* stream) {
+  SB_REQUIRE(e, "sb_spts_batch_run: null executor");
+  SB_REQUIRE(n >= 0 && n <= e->capacity, "sb_spts_batch_run: %d items exceed capacity %d", n,
+             e->capacity);
+  SB_REQUIRE(n == 0 || items, "sb_spts_batch_run: null items");
+  for (int i = 0; i < n; ++i) {
+    const sb_spts_plan* p = items[i].plan;
+    SB_REQUIRE(p, "sb_spts_batch_run: item %d: null plan", i);
+    SB_REQUIRE(p->dtype == e->dtype, "sb_spts_batch_run: item %d: plan dtype differs", i);
+    SB_REQUIRE(p->device == e->device, "sb_spts_batch_run: item %d: plan on another device", i);
+    SB_REQUIRE(p->N == 0 || (items[i].b && items[i].y), "sb_spts_batch_run: item %d: null vector",
+               i);
+    if (p->N > 0 && !p->solvable) {
+      set_error("sb_spts_batch_run: item %d: matrix is not lower triangular with its diagonal "
+                "stored last", i);
+      return SB_EINVAL;
+    }
+  }
+  {
+    std::vector<const sb_spts_plan*> ps(n);
+    for (int i = 0; i < n; ++i) ps[i] = items[i].plan;
+    std::sort(ps.begin(), ps.end());
+    for (int i = 1; i < n; ++i)
+      SB_REQUIRE(ps[i] != ps[i - 1], "sb_spts_batch_run: a plan appears twice in one batch");
+  }
+  // the pinned staging buffers are read by the previous run's first node
+  if (e->pending) SB_CHECK_CUDA(cudaEventSynchronize(e->done));
+  cudaStream_t st = as_stream(stream);
+  for (int i = 0; i < n; ++i) {
+    sb_spts_plan* p = items[i].plan;
+    SptsDesc& d = e->h_items[i];
+    d.rrow = p->rrow;
+    d.rcol = p->rcol;
+    d.rval = p->rval;
+    d.perm = p->perm;
+    d.yw = p->ywork;
+    d.b = items[i].b;
+    d.y = items[i].y;
+    d.N = p->N;
+    d.pad = 0;
+  }
+  e->h_count[0] = n;
+  e->h_count[1] = e->h_count[2] = e->h_count[3] = 0;
+  SB_CHECK_CUDA(cudaGraphLaunch(e->graph, st));
+  SB_CHECK_CUDA(cudaEventRecord(e->done, st));
+  e->pending = true;
+  return SB_OK;
+}
+
 
 int sb_spts_syncfree_csr_noalloc(int dtype, const int32_t* row_ptr, const int32_t* col,
                                  const void* val, int32_t N, const void* b, void* y,

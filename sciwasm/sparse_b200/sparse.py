@@ -98,6 +98,34 @@ class DeviceArray:
         self.free()
 
 
+class PinnedBuffer:
+    """Page-locked host memory (sb_host_alloc) with a numpy byte view, for
+    copies that overlap with device work."""
+
+    def __init__(self, nbytes: int):
+        self.nbytes = int(nbytes)
+        p = C.c_void_p()
+        call("sb_host_alloc", C.byref(p), max(self.nbytes, 16))
+        self.ptr = int(p.value)
+        self.bytes = np.ctypeslib.as_array((C.c_uint8 * max(self.nbytes, 16)).from_address(self.ptr))
+
+    def view(self, offset: int, n: int, dtype) -> np.ndarray:
+        dt = np.dtype(dtype)
+        return self.bytes[offset:offset + n * dt.itemsize].view(dt)
+
+    def free(self) -> None:
+        if self.ptr:
+            self.bytes = None
+            try:
+                _lib.load().sb_host_free(self.ptr)
+            except Exception:
+                pass
+            self.ptr = 0
+
+    def __del__(self):
+        self.free()
+
+
 # --------------------------------------------------------------- objects
 # Shapes follow src/sequential/src/sparse32.js:29-198.
 
@@ -395,6 +423,9 @@ class BatchExecutor:
     def run(self, jobs, stream=None, overwrite=False):
         """jobs: iterable of (A_csr, x DeviceArray N*k, y DeviceArray N*k, k);
         y += A x, or y = A x with overwrite=True."""
+        jobs = list(jobs)
+        if len(jobs) > self.capacity:
+            raise ValueError(f"{len(jobs)} items exceed the executor capacity {self.capacity}")
         n = 0
         self._keep = []
         for A, x, y, k in jobs:
@@ -676,10 +707,58 @@ class SptsPlan:
         call("sb_stream_synchronize", _sp(stream))
         return lv, lp, perm, order
 
+    def growth(self, stream=None) -> float:
+        """max_i sum_{j<i} |L_ij| / |L_ii| (below 1: row diagonally dominant)."""
+        g = C.c_double(0.0)
+        call("sb_spts_plan_growth", self.ptr, C.byref(g), _sp(stream))
+        return float(g.value)
+
     def close(self):
         if getattr(self, "ptr", None):
             try:
                 _lib.load().sb_spts_plan_destroy(self.ptr)
+            except Exception:
+                pass
+            self.ptr = None
+
+    def __del__(self):
+        self.close()
+
+
+class SptsBatch:
+    """Many triangular solves, each on its own SptsPlan, in one graph-replayed
+    persistent launch; every result is bit-identical to
+    spts(L, b, y, algo="hybrid", policy=policy)."""
+
+    def __init__(self, dtype=np.float32, policy="native", capacity=256):
+        self.dtype = np.dtype(dtype)
+        self.policy = policy
+        self.capacity = int(capacity)
+        p = C.c_void_p()
+        call("sb_spts_batch_create", _dtcode(self.dtype), _SPTS_POLICY[policy], self.capacity,
+             C.byref(p))
+        self.ptr = p.value
+        self._items = (_lib.SptsBatchItem * self.capacity)()
+        self._keep = []
+
+    def run(self, jobs, stream=None):
+        """jobs: iterable of (SptsPlan, b DeviceArray, y DeviceArray), natural order."""
+        jobs = list(jobs)
+        if len(jobs) > self.capacity:
+            raise ValueError(f"{len(jobs)} solves exceed the executor capacity {self.capacity}")
+        n = 0
+        self._keep = []
+        for plan, b, y in jobs:
+            it = self._items[n]
+            it.plan, it.b, it.y = plan.ptr, b.ptr, y.ptr
+            self._keep.append((plan, b, y))
+            n += 1
+        call("sb_spts_batch_run", self.ptr, self._items, n, _sp(stream))
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            try:
+                _lib.load().sb_spts_batch_destroy(self.ptr)
             except Exception:
                 pass
             self.ptr = None
