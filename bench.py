@@ -509,14 +509,14 @@ def build_serving_pool(n_mats, min_rows, max_rows, seed=11):
     return pool, mv, ts
 
 
-def serving_requests(pool, mv, ts, rate, seconds, in_ring, out_ring, seed=12):
+def serving_requests(pool, mv, ts, rate, seconds, in_ring, out_ring, seed=12, spmv_frac=0.7):
     """Poisson arrivals; 70% SpMV (f32 or bf16 values, even odds) on a
     uniformly drawn SpMV matrix, 30% SpTS on a uniformly drawn factor.
     Inputs and outputs are consecutive slices of pinned rings (wrapping)."""
     from sciwasm.sparse_b200 import serve
     rng = np.random.default_rng(seed)
     t = serve.poisson_arrivals(rate, seconds, seed=seed)
-    is_mv = rng.random(t.size) < 0.7
+    is_mv = rng.random(t.size) < spmv_frac
     pick_mv = rng.integers(0, len(mv), t.size)
     pick_ts = rng.integers(0, len(ts), t.size)
     bf = rng.random(t.size) < 0.5
@@ -595,7 +595,8 @@ def run_serving(args):
     xs -= 1
     reqs = serving_requests(pool, mv, ts, args.serve_rate, args.serve_seconds, in_ring,
                             out_ring)
-    srv = serve.Server(pool, max_batch=args.serve_batch, slots=args.serve_slots)
+    srv = serve.Server(pool, max_batch=args.serve_batch, slots=args.serve_slots,
+                       spts_slots=args.serve_spts_slots, spts_batch=args.serve_spts_batch)
     # warm-up: executors, graphs and first-touch costs
     srv.serve([serve.Request(r.rid, 0.0, r.matrix, r.op, r.storage, r.x, r.y)
                for r in reqs[:200]], "batched")
@@ -623,7 +624,8 @@ def run_serving(args):
         "batched": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in batched.items()},
         "plain": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in plain.items()},
         "max_rel_err_vs_fp64": errs,
-        "slots": args.serve_slots, "max_batch": args.serve_batch,
+        "slots": {"spmv": args.serve_slots, "spts": args.serve_spts_slots},
+        "max_batch": {"spmv": args.serve_batch, "spts": args.serve_spts_batch},
         "timing": "host wall clock from each request's arrival to the host seeing its result",
     }
     pool.close()
@@ -664,6 +666,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=5.0)
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-batch", type=int, default=64)
+    ap.add_argument("--serve-spts-slots", type=int, default=1)
+    ap.add_argument("--serve-spts-batch", type=int, default=256)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -64,6 +64,11 @@ int sb_memcpy_dtod(void* dst, const void* src, size_t bytes, void* stream);
 int sb_memset(void* dst, int value, size_t bytes, void* stream);
 int sb_stream_create(void** stream);
 int sb_stream_destroy(void* stream);
+/* A non-blocking stream with a scheduling priority (CUDA convention: a
+ * numerically lower value is more urgent; clamped into the device's range,
+ * which sb_stream_priority_range returns). */
+int sb_stream_create_priority(void** stream, int priority);
+int sb_stream_priority_range(int* least, int* greatest);
 int sb_stream_synchronize(void* stream);
 int sb_mem_info(size_t* free_bytes, size_t* total_bytes);
 /* CUDA events for stream-ordered completion tracking and timing

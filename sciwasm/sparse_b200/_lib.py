@@ -53,6 +53,8 @@ SIGNATURES: dict[str, list] = {
     "sb_memcpy_dtod": [P, P, SZ, P],
     "sb_memset": [P, C.c_int, SZ, P],
     "sb_stream_create": [C.POINTER(P)],
+    "sb_stream_create_priority": [C.POINTER(P), C.c_int],
+    "sb_stream_priority_range": [C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "sb_stream_destroy": [P],
     "sb_stream_synchronize": [P],
     "sb_mem_info": [C.POINTER(SZ), C.POINTER(SZ)],

@@ -191,6 +191,28 @@ int sb_stream_create(void** stream) {
   return SB_OK;
 }
 
+int sb_stream_create_priority(void** stream, int priority) {
+  SB_REQUIRE(stream, "sb_stream_create_priority: null output");
+  int r = ensure_device();
+  if (r) return r;
+  int least = 0, greatest = 0;
+  SB_CHECK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  // clamp into [greatest, least] (numerically lower is more urgent)
+  const int p = priority < greatest ? greatest : (priority > least ? least : priority);
+  cudaStream_t s;
+  SB_CHECK_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, p));
+  *stream = reinterpret_cast<void*>(s);
+  return SB_OK;
+}
+
+int sb_stream_priority_range(int* least, int* greatest) {
+  SB_REQUIRE(least && greatest, "sb_stream_priority_range: null output");
+  int r = ensure_device();
+  if (r) return r;
+  SB_CHECK_CUDA(cudaDeviceGetStreamPriorityRange(least, greatest));
+  return SB_OK;
+}
+
 int sb_stream_destroy(void* stream) {
   if (!stream) return SB_OK;
   SB_CHECK_CUDA(cudaStreamDestroy(as_stream(stream)));

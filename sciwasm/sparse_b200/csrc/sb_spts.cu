@@ -453,14 +453,18 @@ __global__ void scatter_by_perm(const T* __restrict__ yw, const int* __restrict_
 }
 
 // ------------------------------------------------------------ batched solves
-// Many independent systems in one persistent launch.  Each system hands out
-// its own 32-row chunks in level order through its own ticket counter; warp
-// w starts on system w mod M and moves to the next system once the current
-// one has no chunk left, so all systems of a batch advance at the same time
-// (the launch takes about the deepest system's time, not the sum of all).
-// A row waits only on rows of its own system with a smaller level-order
-// index, i.e. on chunks of that system already claimed by running warps, so
-// the launch always makes progress.  Rows are solved as in spts_hybrid_rows.
+// Many independent systems in one launch of one warp per 32-row chunk (not
+// persistent: warps exit after their chunk, and the hardware dispatches the
+// blocks as SM slots free up).  Warps are laid out in rounds of one chunk per
+// unfinished system, so all systems of a batch advance at the same time and
+// the launch takes about the deepest system's time, not the sum.  A warp
+// takes its chunk from its system's ticket counter, i.e. chunks of a system
+// are claimed in level order by running warps; a row waits only on rows of
+// its own system with a smaller level-order index, all claimed by running
+// warps, so the launch always makes progress whatever order the hardware
+// runs the blocks in.  Rows are solved as in spts_hybrid_rows.
+constexpr int kTB = 128;  // threads per block of the batched solve
+
 struct SptsDesc {
   const int* rrow;
   const int* rcol;
@@ -473,11 +477,23 @@ struct SptsDesc {
   int pad;
 };
 
+// Schedule of one batch: systems sorted by chunk count (order[]), and the
+// warps in rounds of one chunk per system still unfinished.  Segment k holds
+// the rounds [nch(order[k-1]), nch(order[k])) of the M - k systems
+// order[k..M-1]; seg[k] is the first warp of segment k and `warps` the
+// number of warps (one per chunk of the batch).
+struct SptsSched {
+  int M;
+  int pad;
+  long long warps;
+};
+
 // Every item's work vector to the pending bits.
 template <typename T>
-__global__ void spts_batch_reset(const SptsDesc* __restrict__ items, const int* __restrict__ count) {
+__global__ void spts_batch_reset(const SptsDesc* __restrict__ items,
+                                 const SptsSched* __restrict__ sched) {
   using U = typename std::conditional<sizeof(T) == 4, unsigned, unsigned long long>::type;
-  const int M = count[0];
+  const int M = sched->M;
   for (int k = 0; k < M; ++k) {
     U* w = (U*)items[k].yw;
     const long long N = items[k].N;
@@ -488,41 +504,41 @@ __global__ void spts_batch_reset(const SptsDesc* __restrict__ items, const int* 
 }
 
 template <typename T, typename A>
-__global__ void __launch_bounds__(kT)
-    spts_batch_kernel(const SptsDesc* __restrict__ items, const int* __restrict__ count,
+__global__ void __launch_bounds__(kTB)
+    spts_batch_kernel(const SptsDesc* __restrict__ items, const SptsSched* __restrict__ sched,
+                      const int* __restrict__ order, const long long* __restrict__ seg,
                       int* __restrict__ tickets, long long limit, int* status) {
   const int lane = threadIdx.x & 31;
-  const int M = count[0];
-  if (M <= 0) return;
-  const int gw = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
-  for (int k = 0; k < M; ++k) {
-    const int sys = (int)(((long long)gw + k) % M);
-    const SptsDesc d = items[sys];
-    const int nch = (d.N + 31) >> 5;
-    const T* __restrict__ rval = (const T*)d.rval;
-    T* yw = (T*)d.yw;
-    while (true) {
-      int t = 0;
-      if (lane == 0) t = atomicAdd(tickets + sys, 1);
-      t = __shfl_sync(0xffffffffu, t, 0);
-      if (t >= nch) break;
-      const int i = t * 32 + lane;
-      if (i < d.N) {
-        const int s = d.rrow[i], end = d.rrow[i + 1] - 1;
-        const int pi = d.perm[i];
-        const A bi = (A)((const T*)d.b)[pi];
-        T yi;
-        if (end > s) {
-          const A acc = dot_published<T, A, false>(d.rcol, rval, s, end, yw, A(0), limit, status);
-          yi = (T)div_rn(sub_rn(bi, acc), (A)rval[end]);
-        } else {
-          yi = (T)div_rn(bi, (A)rval[end]);
-        }
-        st_relaxed(yw + i, settled(yi));
-        ((T*)d.y)[pi] = yi;
-      }
-    }
+  const int M = sched->M;
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (M <= 0 || gw >= sched->warps) return;
+  int lo = 0, hi = M - 1;  // last segment starting at or before gw
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (seg[mid] <= gw) lo = mid; else hi = mid - 1;
   }
+  const int sys = order[lo + (int)((gw - seg[lo]) % (M - lo))];
+  // the chunk itself comes from the system's ticket, in the order warps run
+  int t = 0;
+  if (lane == 0) t = atomicAdd(tickets + sys, 1);
+  t = __shfl_sync(0xffffffffu, t, 0);
+  const SptsDesc d = items[sys];
+  const int i = t * 32 + lane;
+  if (i >= d.N) return;
+  const T* __restrict__ rval = (const T*)d.rval;
+  T* yw = (T*)d.yw;
+  const int s = d.rrow[i], end = d.rrow[i + 1] - 1;
+  const int pi = d.perm[i];
+  const A bi = (A)((const T*)d.b)[pi];
+  T yi;
+  if (end > s) {
+    const A acc = dot_published<T, A, false>(d.rcol, rval, s, end, yw, A(0), limit, status);
+    yi = (T)div_rn(sub_rn(bi, acc), (A)rval[end]);
+  } else {
+    yi = (T)div_rn(bi, (A)rval[end]);
+  }
+  st_relaxed(yw + i, settled(yi));
+  ((T*)d.y)[pi] = yi;
 }
 
 // max over rows of sum_{j < diag} |L_ij| / |L_ii| (inf for a zero diagonal),
@@ -762,13 +778,22 @@ struct sb_spts_batch {
   int policy = 0;
   int capacity = 0;
   int device = 0;
-  int grid = 0;
-  SptsDesc* h_items = nullptr;  // pinned
-  int* h_count = nullptr;       // pinned: [0] items
+  SptsDesc* h_items = nullptr;   // pinned staging of the descriptors...
+  SptsSched* h_sched = nullptr;  // ...the schedule header...
+  int* h_order = nullptr;        // ...systems by chunk count...
+  long long* h_seg = nullptr;    // ...and segment starts (capacity + 1)
   SptsDesc* d_items = nullptr;
-  int* d_count = nullptr;       // [0] items
-  int* d_tickets = nullptr;     // one chunk counter per item
+  SptsSched* d_sched = nullptr;
+  int* d_order = nullptr;
+  long long* d_seg = nullptr;
+  int* d_tickets = nullptr;      // one chunk counter per item
+  cudaGraph_t graph_def = nullptr;
   cudaGraphExec_t graph = nullptr;
+  cudaGraphNode_t solve_node = nullptr;
+  cudaKernelNodeParams solve_params = {};
+  void* solve_args[7] = {};
+  long long limit = 0;
+  int* status = nullptr;
   cudaStream_t capture_stream = nullptr;
   cudaEvent_t done = nullptr;
   bool pending = false;
@@ -776,13 +801,14 @@ struct sb_spts_batch {
 
 static void spts_batch_release(sb_spts_batch* e) {
   if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->graph_def) cudaGraphDestroy(e->graph_def);
   if (e->capture_stream) cudaStreamDestroy(e->capture_stream);
   if (e->done) cudaEventDestroy(e->done);
-  if (e->h_items) cudaFreeHost(e->h_items);
-  if (e->h_count) cudaFreeHost(e->h_count);
-  if (e->d_items) cudaFree(e->d_items);
-  if (e->d_count) cudaFree(e->d_count);
-  if (e->d_tickets) cudaFree(e->d_tickets);
+  for (void* h : {(void*)e->h_items, (void*)e->h_sched, (void*)e->h_order, (void*)e->h_seg})
+    if (h) cudaFreeHost(h);
+  for (void* d : {(void*)e->d_items, (void*)e->d_sched, (void*)e->d_order, (void*)e->d_seg,
+                  (void*)e->d_tickets})
+    if (d) cudaFree(d);
   delete e;
 }
 
@@ -846,39 +872,71 @@ int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch*
     return r;                         \
   }
   SB_E(cudaMallocHost(&e->h_items, sizeof(SptsDesc) * capacity));
-  SB_E(cudaMallocHost(&e->h_count, sizeof(int) * 4));
+  SB_E(cudaMallocHost(&e->h_sched, sizeof(SptsSched)));
+  SB_E(cudaMallocHost(&e->h_order, sizeof(int) * capacity));
+  SB_E(cudaMallocHost(&e->h_seg, sizeof(long long) * (capacity + 1)));
   SB_E(cudaMalloc(&e->d_items, sizeof(SptsDesc) * capacity));
-  SB_E(cudaMalloc(&e->d_count, sizeof(int) * 4));
+  SB_E(cudaMalloc(&e->d_sched, sizeof(SptsSched)));
+  SB_E(cudaMalloc(&e->d_order, sizeof(int) * capacity));
+  SB_E(cudaMalloc(&e->d_seg, sizeof(long long) * (capacity + 1)));
   SB_E(cudaMalloc(&e->d_tickets, sizeof(int) * capacity));
   SB_E(cudaStreamCreateWithFlags(&e->capture_stream, cudaStreamNonBlocking));
   SB_E(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming));
-  const void* kern = spts_batch_kernel_for(dtype, e->policy);
-  e->grid = resident_grid(kern);
-  cudaGraph_t g = nullptr;
+  e->h_sched->M = 0;
+  e->h_sched->warps = 0;
+  e->limit = kDefaultSpin;
+  e->status = status;
+  // graph: descriptors and schedule (host -> device), tickets to 0, work
+  // vectors to pending, the solve (its grid is set per run)
   SB_E(cudaStreamBeginCapture(e->capture_stream, cudaStreamCaptureModeThreadLocal));
-  cudaMemcpyAsync(e->d_items, e->h_items, sizeof(SptsDesc) * capacity, cudaMemcpyHostToDevice,
-                  e->capture_stream);
-  cudaMemcpyAsync(e->d_count, e->h_count, sizeof(int) * 4, cudaMemcpyHostToDevice,
-                  e->capture_stream);
-  cudaMemsetAsync(e->d_tickets, 0, sizeof(int) * capacity, e->capture_stream);
+  const cudaStream_t cs = e->capture_stream;
+  cudaMemcpyAsync(e->d_items, e->h_items, sizeof(SptsDesc) * capacity, cudaMemcpyHostToDevice, cs);
+  cudaMemcpyAsync(e->d_sched, e->h_sched, sizeof(SptsSched), cudaMemcpyHostToDevice, cs);
+  cudaMemcpyAsync(e->d_order, e->h_order, sizeof(int) * capacity, cudaMemcpyHostToDevice, cs);
+  cudaMemcpyAsync(e->d_seg, e->h_seg, sizeof(long long) * (capacity + 1), cudaMemcpyHostToDevice,
+                  cs);
+  cudaMemsetAsync(e->d_tickets, 0, sizeof(int) * capacity, cs);
   {
     const void* reset = dtype == SB_F64 ? (const void*)spts_batch_reset<double>
                                         : (const void*)spts_batch_reset<float>;
-    void* rargs[] = {(void*)&e->d_items, (void*)&e->d_count};
-    cudaLaunchKernel(reset, dim3(sm_count() * 4), dim3(kT), rargs, 0, e->capture_stream);
+    void* rargs[] = {(void*)&e->d_items, (void*)&e->d_sched};
+    cudaLaunchKernel(reset, dim3(sm_count() * 4), dim3(kT), rargs, 0, cs);
   }
-  long long limit = kDefaultSpin;
-  void* args[] = {(void*)&e->d_items, (void*)&e->d_count, (void*)&e->d_tickets, (void*)&limit,
-                  (void*)&status};
-  cudaLaunchKernel(kern, dim3(e->grid), dim3(kT), args, 0, e->capture_stream);
-  SB_E(cudaStreamEndCapture(e->capture_stream, &g));
-  ce = cudaGraphInstantiate(&e->graph, g, 0);
-  cudaGraphDestroy(g);
-  if (ce != cudaSuccess) {
-    r = cuda_status(ce, "cudaGraphInstantiate");
-    spts_batch_release(e);
-    return r;
+  e->solve_args[0] = (void*)&e->d_items;
+  e->solve_args[1] = (void*)&e->d_sched;
+  e->solve_args[2] = (void*)&e->d_order;
+  e->solve_args[3] = (void*)&e->d_seg;
+  e->solve_args[4] = (void*)&e->d_tickets;
+  e->solve_args[5] = (void*)&e->limit;
+  e->solve_args[6] = (void*)&e->status;
+  const void* kern = spts_batch_kernel_for(dtype, e->policy);
+  cudaLaunchKernel(kern, dim3(1), dim3(kTB), e->solve_args, 0, cs);
+  SB_E(cudaStreamEndCapture(cs, &e->graph_def));
+  {
+    size_t nn = 0;
+    SB_E(cudaGraphGetNodes(e->graph_def, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    SB_E(cudaGraphGetNodes(e->graph_def, nodes.data(), &nn));
+    for (cudaGraphNode_t nd : nodes) {
+      cudaGraphNodeType ty;
+      SB_E(cudaGraphNodeGetType(nd, &ty));
+      if (ty != cudaGraphNodeTypeKernel) continue;
+      cudaKernelNodeParams kp = {};
+      SB_E(cudaGraphKernelNodeGetParams(nd, &kp));
+      if (kp.func == kern) {
+        e->solve_node = nd;
+        e->solve_params = kp;
+      }
+    }
+    if (!e->solve_node) {
+      set_error("sb_spts_batch_create: solve node not found in the captured graph");
+      spts_batch_release(e);
+      return SB_ECUDA;
+    }
+    e->solve_params.kernelParams = e->solve_args;
+    e->solve_params.extra = nullptr;
   }
+  SB_E(cudaGraphInstantiate(&e->graph, e->graph_def, 0));
 #undef SB_E
   *out = e;
   return SB_OK;
@@ -917,9 +975,10 @@ int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t
     for (int i = 1; i < n; ++i)
       SB_REQUIRE(ps[i] != ps[i - 1], "sb_spts_batch_run: a plan appears twice in one batch");
   }
-  // the pinned staging buffers are read by the previous run's first node
+  // the pinned staging buffers are read by the previous run's first nodes
   if (e->pending) SB_CHECK_CUDA(cudaEventSynchronize(e->done));
   cudaStream_t st = as_stream(stream);
+  std::vector<std::pair<int, int>> by_chunks(n);
   for (int i = 0; i < n; ++i) {
     sb_spts_plan* p = items[i].plan;
     SptsDesc& d = e->h_items[i];
@@ -932,9 +991,25 @@ int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t
     d.y = items[i].y;
     d.N = p->N;
     d.pad = 0;
+    by_chunks[i] = {(p->N + 31) / 32, i};
   }
-  e->h_count[0] = n;
-  e->h_count[1] = e->h_count[2] = e->h_count[3] = 0;
+  std::sort(by_chunks.begin(), by_chunks.end());
+  long long warps = 0;
+  int prev = 0;
+  for (int k = 0; k < n; ++k) {
+    e->h_order[k] = by_chunks[k].second;
+    e->h_seg[k] = warps;
+    warps += (long long)(by_chunks[k].first - prev) * (n - k);
+    prev = by_chunks[k].first;
+  }
+  e->h_seg[n] = warps;
+  e->h_sched->M = n;
+  e->h_sched->warps = warps;
+  const long long per_block = kTB / 32;
+  const long long blocks = std::max(1LL, (warps + per_block - 1) / per_block);
+  SB_REQUIRE(blocks <= 0x7fffffffLL, "sb_spts_batch_run: batch too large");
+  e->solve_params.gridDim = dim3((unsigned)blocks);
+  SB_CHECK_CUDA(cudaGraphExecKernelNodeSetParams(e->graph, e->solve_node, &e->solve_params));
   SB_CHECK_CUDA(cudaGraphLaunch(e->graph, st));
   SB_CHECK_CUDA(cudaEventRecord(e->done, st));
   e->pending = true;

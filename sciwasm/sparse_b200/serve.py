@@ -15,15 +15,16 @@ The pieces:
 * `Server.serve(requests, mode)`: a host loop over requests whose vectors
   live in host memory (pinned, so that copies overlap with device work).
   - "batched": continuous batching.  Requests are released as their arrival
-    times pass.  Whenever a slot is free, the pending requests that fit its
-    device arena (and whose factor has no solve in flight) are packed into
-    one batch: their inputs go up with one copy per contiguous host range,
-    all SpMVs of a storage run as one graph-replayed persistent launch, all
-    solves of a dtype as one more (on a second stream of the slot, so the
-    two kinds overlap), and the outputs come back the same way.  Slots
-    retire as their completion events fire, so batches in different slots
-    overlap on the device and requests that arrive meanwhile join the next
-    batch.
+    times pass into one queue per kind.  Whenever a slot of that kind is
+    free, the oldest pending requests that fit its device arena (and, for
+    solves, whose factor has no solve in flight) are packed into one batch:
+    their inputs go up with one copy per contiguous host range, all SpMVs of
+    a value storage run as one graph-replayed persistent launch (all solves
+    of a dtype and accumulation policy as one graph-replayed launch), and
+    the outputs come back the same way.  Slots retire as their completion
+    events fire, so batches in different slots overlap on the device and
+    requests that arrive meanwhile join the next batch.  SpMV and SpTS have
+    their own slots, so a short SpMV never waits behind a deep solve.
   - "plain": the per-call path.  Each request runs alone, in arrival order:
     copy in, one library call, copy out, synchronise.
   A request's latency is the time from its arrival until the host sees its
@@ -272,10 +273,19 @@ class _Event:
             self.ptr = None
 
 
-def _stream():
+def _stream(priority: Optional[int] = None):
     s = C.c_void_p()
-    call("sb_stream_create", C.byref(s))
+    if priority is None:
+        call("sb_stream_create", C.byref(s))
+    else:
+        call("sb_stream_create_priority", C.byref(s), int(priority))
     return s.value
+
+
+def _priority_range():
+    least, greatest = C.c_int(0), C.c_int(0)
+    call("sb_stream_priority_range", C.byref(least), C.byref(greatest))
+    return least.value, greatest.value
 
 
 def merge_runs(pairs) -> list:
@@ -300,42 +310,38 @@ def _copies(pairs, kind, stream) -> int:
 
 
 class _Slot:
-    def __init__(self, index, arena_bytes, max_batch):
+    """One stream with its device arena and executors; serves batches of one
+    kind ("spmv" or "spts")."""
+
+    def __init__(self, index, kind, arena_bytes, max_batch, priority=None):
         self.index = index
-        self.s_mv = _stream()
-        self.s_ts = _stream()
-        self.ev_in = _Event()
-        self.ev_ts = _Event()
+        self.kind = kind
+        self.stream = _stream(priority)
         self.ev_done = _Event()
         self.arena = DeviceArray(arena_bytes, np.uint8)
         self.arena_bytes = arena_bytes
         self.max_batch = max_batch
-        self.spmv = {}
-        self.spts = {}
+        self.execs = {}
         self.busy = False
         self.reqs = []
         self.plans = []
         self.copies = 0
         self.launches = 0
 
-    def spmv_exec(self, storage):
-        if storage not in self.spmv:
-            self.spmv[storage] = BatchExecutor(storage, capacity=self.max_batch)
-        return self.spmv[storage]
-
-    def spts_exec(self, dtype, policy):
-        k = (dtype, policy)
-        if k not in self.spts:
-            self.spts[k] = SptsBatch(_STORAGE[dtype], policy, capacity=self.max_batch)
-        return self.spts[k]
+    def executor(self, key):
+        if key not in self.execs:
+            if self.kind == "spmv":
+                self.execs[key] = BatchExecutor(key, capacity=self.max_batch)
+            else:
+                dtype, policy = key
+                self.execs[key] = SptsBatch(_STORAGE[dtype], policy, capacity=self.max_batch)
+        return self.execs[key]
 
     def close(self):
-        for e in list(self.spmv.values()) + list(self.spts.values()):
+        for e in self.execs.values():
             e.close()
-        for ev in (self.ev_in, self.ev_ts, self.ev_done):
-            ev.close()
-        for s in (self.s_mv, self.s_ts):
-            call("sb_stream_destroy", s)
+        self.ev_done.close()
+        call("sb_stream_destroy", self.stream)
         self.arena.free()
 
 
@@ -344,15 +350,27 @@ def _vec_bytes(m: ResidentMatrix, r: Request) -> int:
 
 
 class Server:
-    """Continuous-batching request loop over a ResidentPool."""
+    """Continuous-batching request loop over a ResidentPool.
+
+    SpMV and SpTS requests are batched separately, into `slots` SpMV slots
+    (at most `max_batch` requests each) and `spts_slots` SpTS slots (at most
+    `spts_batch` solves each), so that short SpMVs never wait behind a deep
+    solve.  One launch advances all solves of its batch together, so a few
+    large SpTS batches serve better than many small ones; SpMV streams have
+    the higher priority so that their blocks go before pending solve blocks."""
 
     def __init__(self, pool: ResidentPool, max_batch: int = 64, slots: int = 4,
-                 arena_bytes: Optional[int] = None):
+                 arena_bytes: Optional[int] = None, spts_slots: int = 1, spts_batch: int = 256,
+                 priorities: bool = True, spts_arena_bytes: Optional[int] = None):
         self.pool = pool
+        self.priorities = bool(priorities)
         self.max_batch = int(max_batch)
         self.nslots = int(slots)
+        self.spts_slots = int(spts_slots)
+        self.spts_batch = int(spts_batch)
         need = 2 * 8 * max(pool.max_rows, 1) + 2 * _ALIGN  # the largest single request
         self.arena_bytes = _al(max(int(arena_bytes or (256 << 20)), need))
+        self.spts_arena_bytes = _al(max(int(spts_arena_bytes or (1 << 30)), need))
 
     def _check(self, r: Request, m: ResidentMatrix):
         if r.op == "spmv":
@@ -382,47 +400,40 @@ class Server:
             yo.append(off)
             off += _al(_vec_bytes(m, r))
         h2d = [(base + o, r.x.ctypes.data, _vec_bytes(m, r)) for m, r, o in zip(mats, reqs, xo)]
-        slot.copies = _copies(h2d, "h2d", slot.s_mv)
-        mv = collections.defaultdict(list)
-        ts = collections.defaultdict(list)
+        slot.copies = _copies(h2d, "h2d", slot.stream)
+        groups = collections.defaultdict(list)
         for m, r, a, b in zip(mats, reqs, xo, yo):
             vt = _VEC[r.storage]
             xd = DeviceArray(m.N, vt, base + a)
             yd = DeviceArray(m.N, vt, base + b)
             if r.op == "spmv":
-                mv[r.storage].append((m.csr[r.storage], xd, yd, 1))
+                groups[r.storage].append((m.csr[r.storage], xd, yd, 1))
             else:
-                ts[(r.storage, m.policy[r.storage])].append((m.plans[r.storage], xd, yd))
-        launches = 0
-        if ts:
-            slot.ev_in.record(slot.s_mv)
-            call("sb_stream_wait_event", slot.s_ts, slot.ev_in.ptr)
-            for (st, pol), jobs in ts.items():
-                slot.spts_exec(st, pol).run(jobs, stream=slot.s_ts)
-                launches += 1
-            slot.ev_ts.record(slot.s_ts)
-        for st, jobs in mv.items():
-            slot.spmv_exec(st).run(jobs, stream=slot.s_mv, overwrite=True)
-            launches += 1
-        if ts:
-            call("sb_stream_wait_event", slot.s_mv, slot.ev_ts.ptr)
+                groups[(r.storage, m.policy[r.storage])].append((m.plans[r.storage], xd, yd))
+        for key, jobs in groups.items():
+            if slot.kind == "spmv":
+                slot.executor(key).run(jobs, stream=slot.stream, overwrite=True)
+            else:
+                slot.executor(key).run(jobs, stream=slot.stream)
         d2h = [(r.y.ctypes.data, base + o, _vec_bytes(m, r)) for m, r, o in zip(mats, reqs, yo)]
-        slot.copies += _copies(d2h, "d2h", slot.s_mv)
-        slot.ev_done.record(slot.s_mv)
-        slot.launches = launches
+        slot.copies += _copies(d2h, "d2h", slot.stream)
+        slot.ev_done.record(slot.stream)
+        slot.launches = len(groups)
         slot.busy = True
         slot.reqs = reqs
         slot.plans = [(r.matrix, r.storage) for r in reqs if r.op == "spts"]
         self.pool.busy.update(r.matrix for r in reqs)
 
-    def _take(self, pending: collections.deque, busy_plans: set, arena: int) -> list:
+    def _take(self, pending: collections.deque, busy_plans: set, arena: int,
+              max_batch: Optional[int] = None) -> list:
         """Pending requests for one batch, oldest first: at most max_batch,
         within the arena, at most one solve per plan and none on a plan with
         a solve in flight (those wait in order for a later batch)."""
+        max_batch = self.max_batch if max_batch is None else max_batch
         take, keep = [], []
         used = 0
         seen = set()
-        while pending and len(take) < self.max_batch:
+        while pending and len(take) < max_batch:
             r = pending.popleft()
             m = self.pool.mats[r.matrix]
             need = 2 * _al(_vec_bytes(m, r))
@@ -441,8 +452,16 @@ class Server:
         return take
 
     def _serve_batched(self, reqs: list) -> dict:
-        slots = [_Slot(i, self.arena_bytes, self.max_batch) for i in range(self.nslots)]
-        pending: collections.deque = collections.deque()
+        # SpMV streams are the more urgent: their blocks are dispatched before
+        # pending blocks of solves, whose waiting warps would otherwise hold
+        # the SMs
+        least, greatest = _priority_range() if self.priorities else (None, None)
+        kinds = {"spmv": ([_Slot(i, "spmv", self.arena_bytes, self.max_batch, greatest)
+                           for i in range(self.nslots)], collections.deque(), self.max_batch),
+                 "spts": ([_Slot(self.nslots + i, "spts", self.spts_arena_bytes,
+                                 self.spts_batch, least) for i in range(self.spts_slots)],
+                          collections.deque(), self.spts_batch)}
+        all_slots = kinds["spmv"][0] + kinds["spts"][0]
         busy_plans: set = set()
         n = len(reqs)
         i = done = batches = copies = launches = 0
@@ -451,9 +470,10 @@ class Server:
             while done < n:
                 now = time.perf_counter() - t0
                 while i < n and reqs[i].t_arrival <= now:
-                    pending.append(reqs[i])
+                    kinds[reqs[i].op][1].append(reqs[i])
                     i += 1
-                for sl in slots:
+                retired = False
+                for sl in all_slots:
                     if sl.busy and sl.ev_done.done():
                         t = time.perf_counter() - t0
                         for r in sl.reqs:
@@ -462,26 +482,29 @@ class Server:
                         busy_plans.difference_update(sl.plans)
                         sl.busy = False
                         sl.reqs = []
-                        self.pool.busy = {r.matrix for s in slots for r in s.reqs}
-                while pending:
-                    free = next((sl for sl in slots if not sl.busy), None)
-                    if free is None:
-                        break
-                    take = self._take(pending, busy_plans, free.arena_bytes)
-                    if not take:
-                        break
-                    self._launch(free, take)
-                    for r in take:
-                        r.slot = free.index
-                    busy_plans.update(free.plans)
-                    batches += 1
-                    copies += free.copies
-                    launches += free.launches
+                        retired = True
+                if retired:
+                    self.pool.busy = {r.matrix for s in all_slots for r in s.reqs}
+                for slots, pending, mb in kinds.values():
+                    while pending:
+                        free = next((sl for sl in slots if not sl.busy), None)
+                        if free is None:
+                            break
+                        take = self._take(pending, busy_plans, free.arena_bytes, mb)
+                        if not take:
+                            break
+                        self._launch(free, take)
+                        for r in take:
+                            r.slot = free.index
+                        busy_plans.update(free.plans)
+                        batches += 1
+                        copies += free.copies
+                        launches += free.launches
         finally:
-            for sl in slots:
+            for sl in all_slots:
                 if sl.busy:
                     sl.ev_done.wait()
-            for sl in slots:
+            for sl in all_slots:
                 sl.close()
             self.pool.busy = set()
         st = _stats(reqs, batches)
@@ -554,11 +577,17 @@ def _stats(reqs, batches) -> dict:
                 "mean_batch": 0.0, "span_s": 0.0}
     lat = np.array([r.t_done - r.t_arrival for r in reqs])
     span = max(r.t_done for r in reqs) - min(r.t_arrival for r in reqs)
-    return {"requests": len(reqs), "batches": int(batches),
-            "req_per_s": len(reqs) / span if span > 0 else 0.0,
-            "p50_ms": float(np.percentile(lat, 50) * 1e3),
-            "p99_ms": float(np.percentile(lat, 99) * 1e3),
-            "mean_batch": len(reqs) / max(batches, 1), "span_s": float(span)}
+    out = {"requests": len(reqs), "batches": int(batches),
+           "req_per_s": len(reqs) / span if span > 0 else 0.0,
+           "p50_ms": float(np.percentile(lat, 50) * 1e3),
+           "p99_ms": float(np.percentile(lat, 99) * 1e3),
+           "mean_batch": len(reqs) / max(batches, 1), "span_s": float(span)}
+    for op in ("spmv", "spts"):
+        lo = np.array([r.t_done - r.t_arrival for r in reqs if r.op == op])
+        if lo.size:
+            out[f"{op}_p50_ms"] = float(np.percentile(lo, 50) * 1e3)
+            out[f"{op}_p99_ms"] = float(np.percentile(lo, 99) * 1e3)
+    return out
 
 
 def poisson_arrivals(rate_hz: float, duration_s: float, seed: int = 6) -> np.ndarray:
