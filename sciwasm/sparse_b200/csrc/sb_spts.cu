@@ -165,27 +165,42 @@ __device__ __forceinline__ double settled(double v) {
   return pending(v) ? __longlong_as_double(0x7fffffffffffffffLL) : v;
 }
 
-// Poll *p until it is no longer pending or the clock bound passes (then
-// record a timeout in the status word and return the pending value, so that
-// the kernel always terminates); once any wait has given up, the others give
-// up at once.
+constexpr int kG = 8;  // dependencies loaded per round trip
+
+// Wait until none of v[k] (k < n, loaded from p[c[k]]) is pending: every
+// poll reloads all still-pending entries of the group at once (one round
+// trip).  The sleep between polls backs off; past the clock bound (or once
+// any other wait has given up) the wait records a timeout in the status
+// word and returns with the entries still pending, so that the kernel
+// always terminates.
 template <typename V>
-__device__ __noinline__ V wait_pending(const V* p, long long limit, int* status) {
+__device__ __forceinline__ void wait_group(const V* p, const int (&c)[kG], V (&v)[kG], int n,
+                                           long long limit, int* status) {
+  unsigned mask = 0;
+#pragma unroll
+  for (int k = 0; k < kG; ++k)
+    if (k < n && pending(v[k])) mask |= 1u << k;
+  if (!mask) return;
   const long long t0 = clock64();
   unsigned ns = SB_SPTS_SLEEP_MIN_NS;
   while (true) {
     __nanosleep(ns);
     ns = ns < SB_SPTS_SLEEP_MAX_NS ? 2 * ns : ns;
-    const V v = ld_relaxed(p);
-    if (!pending(v)) return v;
+#pragma unroll
+    for (int k = 0; k < kG; ++k)
+      if (mask & (1u << k)) v[k] = ld_relaxed(p + c[k]);
+    unsigned still = 0;
+#pragma unroll
+    for (int k = 0; k < kG; ++k)
+      if ((mask & (1u << k)) && pending(v[k])) still |= 1u << k;
+    mask = still;
+    if (!mask) return;
     if (clock64() - t0 > limit || *(volatile const int*)status) {
       atomicExch(status, SB_DEV_TIMEOUT_DEP);
-      return v;
+      return;
     }
   }
 }
-
-constexpr int kG = 8;  // dependencies loaded per round trip
 
 // acc (+|-)= val[j] * w[col[j]] for j in [s, e), in storage order, waiting
 // for each w[col[j]] to be published (SUB selects the sync-free form).
@@ -194,25 +209,23 @@ __device__ __forceinline__ A dot_published(const int* __restrict__ col, const T*
                                            int s, int e, const T* w, A acc, long long limit,
                                            int* status) {
   for (int j0 = s; j0 < e; j0 += kG) {
+    const int n = e - j0 < kG ? e - j0 : kG;
     int c[kG];
     A a[kG];
     T v[kG];
 #pragma unroll
     for (int k = 0; k < kG; ++k)
-      if (j0 + k < e) {
+      if (k < n) {
         c[k] = col[j0 + k];
         a[k] = (A)val[j0 + k];
       }
 #pragma unroll
     for (int k = 0; k < kG; ++k)
-      if (j0 + k < e) v[k] = ld_relaxed(w + c[k]);
+      if (k < n) v[k] = ld_relaxed(w + c[k]);
+    wait_group(w, c, v, n, limit, status);
 #pragma unroll
     for (int k = 0; k < kG; ++k)
-      if (j0 + k < e) {
-        T x = v[k];
-        if (pending(x)) x = wait_pending(w + c[k], limit, status);
-        acc = SUB ? sub_rn(acc, mul_rn(a[k], (A)x)) : add_rn(acc, mul_rn(a[k], (A)x));
-      }
+      if (k < n) acc = SUB ? sub_rn(acc, mul_rn(a[k], (A)v[k])) : add_rn(acc, mul_rn(a[k], (A)v[k]));
   }
   return acc;
 }
@@ -248,15 +261,16 @@ __global__ void level_kernel(const int* __restrict__ row_ptr, const int* __restr
         for (int j0 = s; j0 < e - 1; j0 += kG) {
           int c[kG], v[kG];
 #pragma unroll
-          for (int k = 0; k < kG; ++k) c[k] = (j0 + k < e - 1) ? col[j0 + k] : -1;
-#pragma unroll
-          for (int k = 0; k < kG; ++k) v[k] = (c[k] >= 0 && c[k] < i) ? ld_relaxed(level + c[k]) : 0;
-#pragma unroll
           for (int k = 0; k < kG; ++k) {
-            int x = v[k];
-            if (x < 0) x = wait_pending(level + c[k], limit, status);
-            m = x > m ? x : m;
+            // columns outside [0, i) read as level 0 (row 0's slot, never pending)
+            const int cc = (j0 + k < e - 1) ? col[j0 + k] : -1;
+            c[k] = (cc >= 0 && cc < i) ? cc : -1;
           }
+#pragma unroll
+          for (int k = 0; k < kG; ++k) v[k] = c[k] >= 0 ? ld_relaxed(level + c[k]) : 0;
+          wait_group(level, c, v, kG, limit, status);
+#pragma unroll
+          for (int k = 0; k < kG; ++k) m = v[k] > m ? v[k] : m;
         }
         lv = 1 + m;
       }
