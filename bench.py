@@ -462,6 +462,11 @@ def run_ours(args, jobs, config, rank, world, local_rank):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(jobs)
+    if world == 1 and not args.no_sections:
+        line["laplacian4096_fp32"] = run_laplacian_large(stream, peak)
+        line["batched"] = run_batched(stream, peak)
+        line["spts"] = run_spts_section(stream)
+        torch.cuda.empty_cache()
     if world == 1 and not args.no_serving:
         line["serving"] = run_serving(args)
     if rank == 0:
@@ -579,6 +584,212 @@ def serving_errors(pool, srv, mv, ts, n_check=24, seed=13):
     return errs
 
 
+# ------------------------------------------------------------------ other configs
+
+def _time_each_ms(stream, fn, reps):
+    """Mean device time of fn() over reps runs, each bracketed by CUDA events
+    on `stream` (host gaps between runs are not counted)."""
+    import torch
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(reps)]
+    with torch.cuda.stream(stream):
+        for e0, e1 in evs:
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+    torch.cuda.synchronize()
+    return float(np.mean([e0.elapsed_time(e1) for e0, e1 in evs]))
+
+
+def _vec(t):
+    import sciwasm.sparse_b200 as sb
+    n = t.numel()
+    dt = np.float64 if str(t.dtype) == "torch.float64" else np.float32
+    return sb.sparse_vec_t(sb.DeviceArray(n, dt, t.data_ptr()), n)
+
+
+def run_laplacian_large(stream, peak):
+    """CSR SpMV, FP32 and BF16 values, on the 5-point Laplacian of a 4096 x 4096
+    grid (16,777,216 rows, 83,869,696 nonzeros; 0.94 GB in FP32, above L2)."""
+    import torch
+    import sciwasm.sparse_b200 as sb
+    from sciwasm.sparse_b200 import synth_device as sd
+    n = 4096
+    A = sd.laplacian_2d(n)
+    N, nnz = A.N, A.nnz
+    g = torch.Generator(device="cuda").manual_seed(0)
+    xt = torch.rand(N, generator=g, device="cuda") * 2 - 1
+    yt = torch.zeros(N, device="cuda")
+    x, y = _vec(xt), _vec(yt)
+    sp = stream.cuda_stream
+    X = xt.double().reshape(n, n)
+    T = 4 * X
+    T[1:, :] -= X[:-1, :]
+    T[:-1, :] -= X[1:, :]
+    T[:, 1:] -= X[:, :-1]
+    T[:, :-1] -= X[:, 1:]
+    out = {"workload": "5-point Laplacian 4096^2, x ~ U[-1,1] seed 0, y <- y + A x",
+           "N": N, "nnz": nnz}
+    for storage in ("f32", "bf16"):
+        B = A if storage == "f32" else sb.csr_with_storage(A, "bf16")
+        yt.zero_()
+        with torch.cuda.stream(stream):
+            sb.spmv(B, x, y, stream=sp)
+        torch.cuda.synchronize()
+        err = float((yt.double().reshape(n, n) - T).abs().max() / T.abs().max())
+        for _ in range(3):
+            with torch.cuda.stream(stream):
+                sb.spmv(B, x, y, stream=sp)
+        ms = _time_each_ms(stream, lambda: sb.spmv(B, x, y, stream=sp), 20)
+        nbytes = algo_bytes("csr", N, nnz, 2 if storage == "bf16" else 4) + \
+            (3 * N * 4 - 3 * N * (2 if storage == "bf16" else 4))  # x, y stay f32
+        gbs = nbytes / (ms / 1e3) / 1e9
+        out[storage] = {"ms": round(ms, 4), "GB_s": round(gbs, 1), "frac": round(gbs / peak, 3),
+                        "algorithmic_bytes": nbytes, "rel_err_vs_fp64": err}
+    return out
+
+
+def run_batched(stream, peak, n_mats=512, seed=5):
+    """Batched CSR SpMV: n_mats matrices with rows log-uniform in [1e3, 2e5],
+    Poisson(12) off-diagonals plus the diagonal per row, values U[-1,1] stored
+    FP32 and BF16 (FP32 accumulation), 1-8 right-hand sides each; one
+    graph-replayed persistent launch for the whole batch against one
+    sb_spmv_csr call per (matrix, right-hand side)."""
+    import torch
+    import scipy.sparse as sps
+    import sciwasm.sparse_b200 as sb
+    from sciwasm.sparse_b200 import _lib, synth_device as sd
+    rng = np.random.default_rng(seed)
+    Ns = np.floor(np.exp(rng.uniform(np.log(1e3), np.log(2e5), n_mats))).astype(np.int64)
+    ks = rng.integers(1, 9, n_mats)
+    sp = stream.cuda_stream
+    mats = [sd.poisson_rows(int(N), 12.0, seed=seed * 1000 + i) for i, N in enumerate(Ns)]
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    xs = [torch.rand(int(N) * int(k), generator=g, device="cuda") * 2 - 1 for N, k in zip(Ns, ks)]
+    ys = [torch.zeros(int(N) * int(k), device="cuda") for N, k in zip(Ns, ks)]
+    xcols = [[x.reshape(int(N), int(k))[:, j].contiguous() for j in range(int(k))]
+             for x, N, k in zip(xs, Ns, ks)]
+    ycols = [[torch.zeros(int(N), device="cuda") for _ in range(int(k))] for N, k in zip(Ns, ks)]
+    nnz_tot = int(sum(A.nnz for A in mats))
+    out = {"workload": f"{n_mats} CSR matrices, rows log-uniform in [1e3, 2e5] "
+                       f"({int(Ns.sum())} rows), Poisson(12)+diagonal per row "
+                       f"({nnz_tot} nonzeros), 1-8 right-hand sides, y <- y + A x",
+           "matrices": n_mats, "rows": int(Ns.sum()), "nnz": nnz_tot,
+           "rhs": int(ks.sum())}
+    sample = list(range(0, n_mats, max(1, n_mats // 8)))
+    for storage in ("f32", "bf16"):
+        As = mats if storage == "f32" else [sb.csr_with_storage(A, "bf16") for A in mats]
+        s_v = 2 if storage == "bf16" else 4
+        ex = sb.BatchExecutor(storage, capacity=n_mats)
+        jobs = [(A, sb.DeviceArray(x.numel(), np.float32, x.data_ptr()),
+                 sb.DeviceArray(y.numel(), np.float32, y.data_ptr()), int(k))
+                for A, x, y, k in zip(As, xs, ys, ks)]
+        for y in ys:
+            y.zero_()
+        ex.run(jobs, stream=sp)
+        torch.cuda.synchronize()
+        err = 0.0
+        for i in sample:
+            A = As[i]
+            v = A.val_array()
+            if storage == "bf16":
+                v = (v.astype(np.uint32) << 16).view(np.float32)
+            M = sps.csr_matrix((v.astype(np.float64), A.col_array(), A.row_array()),
+                               shape=(A.N, A.N))
+            X = xs[i].double().cpu().numpy().reshape(A.N, int(ks[i]))
+            Y = ys[i].double().cpu().numpy().reshape(A.N, int(ks[i]))
+            T = M @ X
+            err = max(err, float(np.max(np.abs(Y - T)) / max(np.max(np.abs(T)), 1e-300)))
+        nbytes = sum(A.nnz * (s_v + 4) + 4 * (A.N + 1) + int(k) * A.N * 12
+                     for A, k in zip(As, ks))
+        for _ in range(3):
+            ex.run(jobs, stream=sp)
+        ms = _time_each_ms(stream, lambda: ex.run(jobs, stream=sp), 10)
+        dt = _lib.SB_BF16 if storage == "bf16" else _lib.SB_F32
+
+        def per_call():
+            for A, xc, yc in zip(As, xcols, ycols):
+                for xj, yj in zip(xc, yc):
+                    _lib.call("sb_spmv_csr", dt, A.row_index.ptr, A.col_index.ptr,
+                              A.val_index.ptr, xj.data_ptr(), yj.data_ptr(), A.N, A.nnz, 1, sp)
+        per_call()
+        ms_pc = _time_each_ms(stream, per_call, 3)
+        gbs = nbytes / (ms / 1e3) / 1e9
+        out[storage] = {"ms": round(ms, 4), "GB_s": round(gbs, 1), "frac": round(gbs / peak, 3),
+                        "per_call_ms": round(ms_pc, 4),
+                        "speedup_vs_per_call": round(ms_pc / ms, 2),
+                        "algorithmic_bytes": nbytes, "launches": 1,
+                        "per_call_launches": int(ks.sum()),
+                        "max_rel_err_vs_fp64": err, "error_sample_matrices": len(sample)}
+        ex.close()
+    return out
+
+
+def run_spts_section(stream):
+    """SpTS: lower triangle of the 3-D 7-point Laplacian on a 64^3 grid and a
+    random lower-triangular matrix (1M rows, 7 off-diagonals per row within
+    5,000 of the diagonal, diagonal U[2,4]), FP64 and FP32, b ~ U[-1,1];
+    analysis and the three solves, errors against an FP64 host solve (scipy)."""
+    import torch
+    import scipy.sparse as sps
+    import scipy.sparse.linalg as spl
+    import sciwasm.sparse_b200 as sb
+    from sciwasm.sparse_b200 import _lib, synth_device as sd
+    sp = stream.cuda_stream
+    from sciwasm.sparse_b200 import synth
+    npdt = {"f64": np.float64, "f32": np.float32}
+    cases = [("laplacian3d_64", lambda dt: sb.csr_from_host(
+                 *synth.laplacian_3d_lower(64, dtype=npdt[dt]))),
+             ("random_lower_1M", lambda dt: sb.csr_from_host(
+                 *synth.random_lower(1_000_000, 7, 5000, seed=3, dtype=npdt[dt])))]
+    algos = {"level": _lib.SB_SPTS_LEVEL, "syncfree": _lib.SB_SPTS_SYNCFREE,
+             "hybrid": _lib.SB_SPTS_HYBRID}
+    out = {}
+    for name, gen in cases:
+        for dt in ("f64", "f32"):
+            L = gen(dt)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            plan = sb.SptsPlan(L)
+            analysis_ms = (time.perf_counter() - t0) * 1e3
+            tdt = torch.float64 if dt == "f64" else torch.float32
+            g = torch.Generator(device="cuda").manual_seed(4)
+            bt = (torch.rand(L.N, generator=g, device="cuda", dtype=torch.float64) * 2 - 1).to(tdt)
+            yt = torch.zeros(L.N, device="cuda", dtype=tdt)
+            M = sps.csr_matrix((L.val_array().astype(np.float64), L.col_array(), L.row_array()),
+                               shape=(L.N, L.N))
+            M.sum_duplicates()
+            truth = spl.spsolve_triangular(M, bt.double().cpu().numpy(), lower=True)
+            s_v = 8 if dt == "f64" else 4
+            nbytes = L.nnz * (s_v + 4) + 4 * (L.N + 1) + 2 * L.N * s_v
+            row = {"N": L.N, "nnz": L.nnz, "levels": plan.nlevels,
+                   "analysis_ms": round(analysis_ms, 2), "algorithmic_bytes": nbytes}
+            runs = [(an, code, _lib.SB_SPTS_ACC_NATIVE) for an, code in algos.items()]
+            if dt == "f32":
+                runs.append(("hybrid_acc_f64", _lib.SB_SPTS_HYBRID, _lib.SB_SPTS_ACC_F64))
+            for an, code, pol in runs:
+                def solve():
+                    _lib.call("sb_spts_solve", plan.ptr, code, pol, bt.data_ptr(), yt.data_ptr(),
+                              sp)
+                yt.zero_()
+                with torch.cuda.stream(stream):
+                    solve()
+                torch.cuda.synchronize()
+                y = yt.double().cpu().numpy()
+                err = float(np.max(np.abs(y - truth)) / max(np.max(np.abs(truth)), 1e-300))
+                with torch.cuda.stream(stream):
+                    solve()
+                ms = _time_each_ms(stream, solve, 5)
+                row[an] = {"ms": round(ms, 4), "us_per_level": round(ms * 1e3 / plan.nlevels, 3),
+                           "rows_per_s": round(L.N / (ms / 1e3), 1), "rel_err_vs_fp64": err}
+            code = __import__("ctypes").c_int(0)
+            _lib.call("sb_device_status", __import__("ctypes").byref(code))
+            row["device_status"] = code.value
+            out[f"{name}/{dt}"] = row
+            plan.close()
+    return out
+
+
 def run_serving(args):
     """Batched (continuous batching) and plain per-call serving of the same
     request stream; returns the statistics of both and the sampled errors."""
@@ -660,6 +871,8 @@ def main():
                     help="quarter-size matrices (profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-sections", action="store_true",
+                    help="skip the 4096^2 Laplacian, batched and SpTS sections")
     ap.add_argument("--serve-pool", type=int, default=2000)
     ap.add_argument("--serve-max-rows", type=int, default=2_000_000)
     ap.add_argument("--serve-rate", type=float, default=20_000.0)

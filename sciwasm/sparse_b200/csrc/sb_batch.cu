@@ -4,12 +4,14 @@
 // No counterpart in the reference (it calls spmv once per matrix and vector,
 // src/sequential/src/sparse32.js:1232-1286).  Work is a flat list of 32-row
 // blocks over all matrices of the batch (block_offsets = exclusive scan of
-// ceil(N_i/32)); persistent warps take blocks from a device counter, map a
-// block index to its matrix by binary search, and reduce each row with V
-// lanes (V per matrix from its mean row length: the "rows per warp"
-// autotuning), accumulating all of the matrix's nrhs (1..8) right-hand sides
-// at once (x and y are N x nrhs, row-major).  Values are stored f32, f64 or
-// BF16 (f32 vectors and sums for f32/BF16).  The executor keeps descriptors
+// ceil(N_i/32)); persistent warps take four blocks at a time from a device
+// counter, map a block index to its matrix by binary search, and reduce each
+// short row with V lanes (V per matrix from its mean row length: the "rows
+// per warp" autotuning) and each long row with the whole warp (compensated
+// f32 sums); with several right-hand sides (x and y are N x nrhs, row-major,
+// nrhs <= 8) the right-hand sides go across lanes instead, so that one load
+// gathers all of a column's x values.  Values are stored f32, f64 or BF16
+// (f32 vectors and sums for f32/BF16).  The executor keeps descriptors
 // in pinned host and device buffers; one run = the graph [copy descriptors,
 // reset the counter, kernel] launched on the caller's stream.
 #include <algorithm>
@@ -38,6 +40,7 @@ namespace sb {
 
 constexpr int kBT = 256;
 constexpr int kMaxRhs = 8;
+constexpr int kBlocksPerTicket = 4;  // 32-row blocks a warp takes per work-counter update
 
 __device__ __forceinline__ float ldv(const float* p, long long i) { return ld_stream(p + i); }
 __device__ __forceinline__ double ldv(const double* p, long long i) { return ld_stream(p + i); }
@@ -46,10 +49,36 @@ __device__ __forceinline__ float ldv(const __nv_bfloat16* p, long long i) {
       __ushort_as_bfloat16(ld_stream(reinterpret_cast<const unsigned short*>(p) + i)));
 }
 
-// One 32-row block of one matrix, V lanes per row, K right-hand sides.
+// Neumaier-compensated accumulation (long rows with f32 sums).
+template <typename T>
+__device__ __forceinline__ void comp_add(T& s, T& c, T v) {
+  const T t = s + v;
+  c += (fabs(s) >= fabs(v)) ? ((s - t) + v) : ((v - t) + s);
+  s = t;
+}
+
+// y[row*K + j] for one finished row sum: y = A x (overwrite) or y += A x,
+// where a row without entries keeps y unless it is overwritten with 0.
+template <typename T>
+__device__ __forceinline__ void put_y(T* y, long long at, T sum, bool overwrite, bool nonempty) {
+  if (overwrite) y[at] = sum;
+  else if (nonempty) y[at] += sum;
+}
+
+// One 32-row block of one matrix, V lanes per row, K right-hand sides: the
+// block's row_ptr entries are read once (one per lane); rows of up to kLong
+// entries are reduced in batches of 32/V rows, each lane issuing UNROLL
+// independent col/val loads per pass before the x gathers (K consecutive
+// values per column), then one shuffle reduction per right-hand side; longer
+// rows are reduced by the whole warp, one right-hand side at a time, with
+// compensated f32 sums.
+constexpr int kLong = 128;
+
 template <typename SV, typename T, int V>
 __device__ __forceinline__ void batch_block(const sb_batch_item& it, int r0, int lane) {
+  constexpr int UNROLL = 4;
   constexpr int RPB = 32 / V;
+  constexpr bool COMP = sizeof(T) == 4;
   const int g = lane / V, q = lane - (lane / V) * V;
   const int* __restrict__ rp = it.row_ptr;
   const int* __restrict__ col = it.col;
@@ -57,32 +86,182 @@ __device__ __forceinline__ void batch_block(const sb_batch_item& it, int r0, int
   const T* __restrict__ x = (const T*)it.x;
   T* __restrict__ y = (T*)it.y;
   const int K = it.nrhs;
+  const int N = it.N;
   const bool overwrite = (it.flags & 1) != 0;
+  const int rr = r0 + lane;
+  const int s_l = rr < N ? __ldg(rp + rr) : 0;
+  const int e_l = rr < N ? __ldg(rp + rr + 1) : 0;
+  const int len_l = e_l - s_l;
+#pragma unroll
   for (int b = 0; b < V; ++b) {
-    const int row = r0 + b * RPB + g;
-    const bool ok = row < it.N && row < r0 + 32;
-    const int s = ok ? __ldg(rp + row) : 0;
-    const int e = ok ? __ldg(rp + row + 1) : 0;
+    const int j = b * RPB + g;
+    const int s = __shfl_sync(0xffffffffu, s_l, j);
+    const int e = __shfl_sync(0xffffffffu, e_l, j);
+    const int len = e - s;
     T acc[kMaxRhs];
 #pragma unroll
-    for (int j = 0; j < kMaxRhs; ++j) acc[j] = 0;
-    for (int k = s + q; k < e; k += V) {
-      const long long c = (long long)ld_stream(col + k) * K;
-      const T v = (T)ldv(val, k);
+    for (int h = 0; h < kMaxRhs; ++h) acc[h] = 0;
+    if (len <= kLong) {
+      for (int k0 = s + q; k0 < e; k0 += V * UNROLL) {
+        int cc[UNROLL];
+        T vv[UNROLL];
 #pragma unroll
-      for (int j = 0; j < kMaxRhs; ++j)
-        if (j < K) acc[j] += v * __ldg(x + c + j);
-    }
+        for (int u = 0; u < UNROLL; ++u) {
+          const int k = k0 + u * V;
+          cc[u] = k < e ? ld_stream(col + k) : 0;
+          vv[u] = k < e ? ldv(val, k) : (T)0;
+        }
 #pragma unroll
-    for (int j = 0; j < kMaxRhs; ++j) {
-      if (j < K) {
-        T a = acc[j];
-        for (int off = V >> 1; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
-        if (ok && q == 0) {
-          if (overwrite) y[(long long)row * K + j] = a;
-          else if (e > s) y[(long long)row * K + j] += a;
+        for (int u = 0; u < UNROLL; ++u) {
+          if (k0 + u * V < e) {
+            const T* xc = x + (long long)cc[u] * K;
+#pragma unroll
+            for (int h = 0; h < kMaxRhs; ++h)
+              if (h < K) acc[h] += vv[u] * __ldg(xc + h);
+          }
         }
       }
+    }
+#pragma unroll
+    for (int h = 0; h < kMaxRhs; ++h) {
+      if (h < K) {
+        T a = acc[h];
+#pragma unroll
+        for (int off = V >> 1; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+        if (q == 0 && len <= kLong && r0 + j < N)
+          put_y(y, (long long)(r0 + j) * K + h, a, overwrite, len > 0);
+      }
+    }
+  }
+  // long rows of the block: the whole warp, one right-hand side at a time
+  unsigned longm = __ballot_sync(0xffffffffu, rr < N && len_l > kLong);
+  while (longm) {
+    const int j = __ffs(longm) - 1;
+    longm &= longm - 1;
+    const int s = __shfl_sync(0xffffffffu, s_l, j);
+    const int e = __shfl_sync(0xffffffffu, e_l, j);
+    for (int h = 0; h < K; ++h) {
+      T sum = 0, comp = 0;
+      for (int k0 = s; k0 < e; k0 += 32 * UNROLL) {
+        int cc[UNROLL];
+        T vv[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          const int k = k0 + lane + u * 32;
+          cc[u] = k < e ? ld_stream(col + k) : 0;
+          vv[u] = k < e ? ldv(val, k) : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          const int k = k0 + lane + u * 32;
+          if (k < e) {
+            const T p = vv[u] * __ldg(x + (long long)cc[u] * K + h);
+            if (COMP) comp_add(sum, comp, p);
+            else sum += p;
+          }
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const T o = __shfl_xor_sync(0xffffffffu, sum, off);
+        if (COMP) {
+          comp += __shfl_xor_sync(0xffffffffu, comp, off);
+          comp_add(sum, comp, o);
+        } else {
+          sum += o;
+        }
+      }
+      if (lane == 0) put_y(y, (long long)(r0 + j) * K + h, COMP ? sum + comp : sum, overwrite, true);
+    }
+  }
+}
+
+// Several right-hand sides (K = 2..8): one 32-row block, the right-hand
+// sides across lanes.  KP = K rounded up to a power of two lanes share a row,
+// lane h of the group accumulating right-hand side h over the row's entries
+// in storage order (UNROLL entries per pass), so one load instruction gathers
+// the K consecutive x values of 32/KP columns (one L1 tag per nonzero instead
+// of K) and the col/val loads of a row are shared by its KP lanes.  Rows
+// longer than kLong go to the whole-warp path of batch_block.
+template <typename SV, typename T, int KP>
+__device__ __forceinline__ void batch_block_rhs(const sb_batch_item& it, int r0, int lane) {
+  constexpr int UNROLL = 4;
+  constexpr int R = 32 / KP;  // rows per pass
+  constexpr bool COMP = sizeof(T) == 4;
+  const int r = lane / KP, h = lane - (lane / KP) * KP;
+  const int* __restrict__ rp = it.row_ptr;
+  const int* __restrict__ col = it.col;
+  const SV* __restrict__ val = (const SV*)it.val;
+  const T* __restrict__ x = (const T*)it.x;
+  T* __restrict__ y = (T*)it.y;
+  const int K = it.nrhs;
+  const int N = it.N;
+  const bool overwrite = (it.flags & 1) != 0;
+  const int rr = r0 + lane;
+  const int s_l = rr < N ? __ldg(rp + rr) : 0;
+  const int e_l = rr < N ? __ldg(rp + rr + 1) : 0;
+  const int len_l = e_l - s_l;
+#pragma unroll
+  for (int b = 0; b < KP; ++b) {
+    const int j = b * R + r;
+    const int s = __shfl_sync(0xffffffffu, s_l, j);
+    const int e = __shfl_sync(0xffffffffu, e_l, j);
+    const int len = e - s;
+    if (len <= kLong) {
+      T acc = 0;
+      for (int k0 = s; k0 < e; k0 += UNROLL) {
+        int cc[UNROLL];
+        T vv[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          cc[u] = k0 + u < e ? ld_stream(col + k0 + u) : 0;
+          vv[u] = k0 + u < e ? ldv(val, k0 + u) : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u)
+          if (k0 + u < e && h < K) acc += vv[u] * __ldg(x + (long long)cc[u] * K + h);
+      }
+      if (h < K && r0 + j < N) put_y(y, (long long)(r0 + j) * K + h, acc, overwrite, len > 0);
+    }
+  }
+  unsigned longm = __ballot_sync(0xffffffffu, rr < N && len_l > kLong);
+  while (longm) {
+    const int j = __ffs(longm) - 1;
+    longm &= longm - 1;
+    const int s = __shfl_sync(0xffffffffu, s_l, j);
+    const int e = __shfl_sync(0xffffffffu, e_l, j);
+    for (int hh = 0; hh < K; ++hh) {
+      T sum = 0, comp = 0;
+      for (int k0 = s; k0 < e; k0 += 32 * 4) {
+        int cc[4];
+        T vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = k0 + lane + u * 32;
+          cc[u] = k < e ? ld_stream(col + k) : 0;
+          vv[u] = k < e ? ldv(val, k) : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = k0 + lane + u * 32;
+          if (k < e) {
+            const T p = vv[u] * __ldg(x + (long long)cc[u] * K + hh);
+            if (COMP) comp_add(sum, comp, p);
+            else sum += p;
+          }
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const T o = __shfl_xor_sync(0xffffffffu, sum, off);
+        if (COMP) {
+          comp += __shfl_xor_sync(0xffffffffu, comp, off);
+          comp_add(sum, comp, o);
+        } else {
+          sum += o;
+        }
+      }
+      if (lane == 0) put_y(y, (long long)(r0 + j) * K + hh, COMP ? sum + comp : sum, overwrite, true);
     }
   }
 }
@@ -96,25 +275,34 @@ __global__ void __launch_bounds__(kBT)
   if (M <= 0) return;
   const long long total = offsets[M];
   while (true) {
-    long long w = 0;
-    if (lane == 0) w = atomicAdd((unsigned long long*)(count + 2), 1ull);
-    w = __shfl_sync(0xffffffffu, w, 0);
-    if (w >= total) return;
-    // matrix of block w: last m with offsets[m] <= w
-    int lo = 0, hi = M - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (offsets[mid] <= w) lo = mid; else hi = mid - 1;
-    }
-    const sb_batch_item it = items[lo];
-    const int r0 = (int)((w - offsets[lo]) * 32);
-    switch (it.lanes) {
-      case 1: batch_block<SV, T, 1>(it, r0, lane); break;
-      case 2: batch_block<SV, T, 2>(it, r0, lane); break;
-      case 4: batch_block<SV, T, 4>(it, r0, lane); break;
-      case 8: batch_block<SV, T, 8>(it, r0, lane); break;
-      case 16: batch_block<SV, T, 16>(it, r0, lane); break;
-      default: batch_block<SV, T, 32>(it, r0, lane); break;
+    long long w0 = 0;
+    if (lane == 0) w0 = (long long)atomicAdd((unsigned long long*)(count + 2), 1ull) * kBlocksPerTicket;
+    w0 = __shfl_sync(0xffffffffu, w0, 0);
+    if (w0 >= total) return;
+    const long long w1 = min(w0 + kBlocksPerTicket, total);
+    for (long long w = w0; w < w1; ++w) {
+      // matrix of block w: last m with offsets[m] <= w
+      int lo = 0, hi = M - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(offsets + mid) <= w) lo = mid; else hi = mid - 1;
+      }
+      const sb_batch_item it = items[lo];
+      const int r0 = (int)((w - __ldg(offsets + lo)) * 32);
+      if (it.nrhs > 1) {
+        if (it.nrhs == 2) batch_block_rhs<SV, T, 2>(it, r0, lane);
+        else if (it.nrhs <= 4) batch_block_rhs<SV, T, 4>(it, r0, lane);
+        else batch_block_rhs<SV, T, 8>(it, r0, lane);
+        continue;
+      }
+      switch (it.lanes) {
+        case 1: batch_block<SV, T, 1>(it, r0, lane); break;
+        case 2: batch_block<SV, T, 2>(it, r0, lane); break;
+        case 4: batch_block<SV, T, 4>(it, r0, lane); break;
+        case 8: batch_block<SV, T, 8>(it, r0, lane); break;
+        case 16: batch_block<SV, T, 16>(it, r0, lane); break;
+        default: batch_block<SV, T, 32>(it, r0, lane); break;
+      }
     }
   }
 }

@@ -4,8 +4,9 @@ Laplacian, power-law rows, and the lower-triangular factors of the SpTS
 workloads (3-D 7-point Laplacian lower triangle, band-limited random lower).
 The structures follow synth.py; random draws use torch's generator, so the
 values differ from the host versions while shapes and distributions match.
-Column indices are sorted within each row and a factor's diagonal is stored
-last.  The returned sparse_CSR_t objects view torch tensors (kept alive on
+Column indices are distinct and sorted within each row (repeated draws are
+merged, so a row can come out a little shorter than drawn) and a factor's
+diagonal is stored last.  The returned sparse_CSR_t objects view torch tensors (kept alive on
 the object as `_torch`)."""
 from __future__ import annotations
 
@@ -98,6 +99,18 @@ def laplacian_3d_lower(n: int, dtype="f32"):
     return _wrap(rp, col, val)
 
 
+def _csr_from_keys(key, N):
+    """Sorted, de-duplicated keys row * N + col -> (row_ptr i32, col i32, row i64)."""
+    torch = _torch()
+    key = torch.unique_consecutive(key)
+    row = key // N
+    col = (key % N).to(torch.int32)
+    counts = torch.bincount(row, minlength=N)
+    rp = torch.zeros(N + 1, device=key.device, dtype=torch.int64)
+    torch.cumsum(counts, 0, out=rp[1:])
+    return rp.to(torch.int32), col, row
+
+
 def _rows_from_counts(counts):
     torch = _torch()
     N = counts.numel()
@@ -109,8 +122,8 @@ def _rows_from_counts(counts):
 
 def power_law(N: int, s: float = 2.0, cap: int = 2000, shift: int = 15, seed: int = 2,
               dtype="f32"):
-    """Row lengths min(cap, Zipf(s) + shift, N), uniform columns (sorted within
-    the row, repeats possible), values ~ U[-1, 1]."""
+    """Row lengths min(cap, Zipf(s) + shift, N), uniform distinct columns,
+    values ~ U[-1, 1]."""
     torch = _torch()
     dev = torch.device("cuda")
     rng = np.random.default_rng(seed)
@@ -120,15 +133,15 @@ def power_law(N: int, s: float = 2.0, cap: int = 2000, shift: int = 15, seed: in
     gen = torch.Generator(device=dev).manual_seed(seed)
     c = torch.randint(0, N, (row.numel(),), generator=gen, device=dev, dtype=torch.int64)
     key, _ = torch.sort(row * N + c)
-    col = (key % N).to(torch.int32)
+    rp, col, _ = _csr_from_keys(key, N)
     tdt = torch.float64 if dtype == "f64" else torch.float32
     val = (torch.rand(col.numel(), generator=gen, device=dev, dtype=tdt) * 2 - 1)
-    return _wrap(rp.to(torch.int32), col, val)
+    return _wrap(rp, col, val)
 
 
 def random_lower(N: int, per_row: int = 7, band: int = 5000, seed: int = 3, dtype="f32"):
-    """Row i: min(per_row, i) columns uniform in [max(0, i - band), i) (sorted,
-    repeats possible) with values ~ U[-0.5, 0.5], then the diagonal ~ U[2, 4]."""
+    """Row i: min(per_row, i) distinct columns uniform in [max(0, i - band), i)
+    with values ~ U[-0.5, 0.5], then the diagonal ~ U[2, 4]."""
     torch = _torch()
     dev = torch.device("cuda")
     gen = torch.Generator(device=dev).manual_seed(seed)
@@ -144,10 +157,31 @@ def random_lower(N: int, per_row: int = 7, band: int = 5000, seed: int = 3, dtyp
     last = torch.zeros(nnz, device=dev, dtype=torch.bool)
     last[rp[1:] - 1] = True
     c = torch.where(last, row, c)
-    key, order = torch.sort(row * N + c, stable=True)
-    col = (key % N).to(torch.int32)
+    key, _ = torch.sort(row * N + c)
+    rp, col, row = _csr_from_keys(key, N)
     tdt = torch.float64 if dtype == "f64" else torch.float32
-    off = torch.rand(nnz, generator=gen, device=dev, dtype=tdt) - 0.5
-    dg = torch.rand(nnz, generator=gen, device=dev, dtype=tdt) * 2 + 2
-    val = torch.where(last, dg, off)[order]
-    return _wrap(rp.to(torch.int32), col, val)
+    off = torch.rand(col.numel(), generator=gen, device=dev, dtype=tdt) - 0.5
+    dg = torch.rand(col.numel(), generator=gen, device=dev, dtype=tdt) * 2 + 2
+    val = torch.where(col.to(torch.int64) == row, dg, off)
+    return _wrap(rp, col, val)
+
+
+def poisson_rows(N: int, mean: float = 12.0, seed: int = 5, dtype="f32"):
+    """Row i: Poisson(mean) distinct columns uniform in [0, N) plus the
+    diagonal, values ~ U[-1, 1]."""
+    torch = _torch()
+    dev = torch.device("cuda")
+    rng = np.random.default_rng(seed)
+    lens = (rng.poisson(mean, N) + 1).astype(np.int32)
+    counts = torch.from_numpy(lens).to(dev)
+    rp, row = _rows_from_counts(counts)
+    gen = torch.Generator(device=dev).manual_seed(seed)
+    c = torch.randint(0, N, (row.numel(),), generator=gen, device=dev, dtype=torch.int64)
+    last = torch.zeros(row.numel(), device=dev, dtype=torch.bool)
+    last[rp[1:] - 1] = True
+    c = torch.where(last, row, c)
+    key, _ = torch.sort(row * N + c)
+    rp, col, _ = _csr_from_keys(key, N)
+    tdt = torch.float64 if dtype == "f64" else torch.float32
+    val = torch.rand(col.numel(), generator=gen, device=dev, dtype=tdt) * 2 - 1
+    return _wrap(rp, col, val)
