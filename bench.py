@@ -35,6 +35,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+SECTIONS = ("batched", "laplacian4096_fp32", "spts", "serving")
 METRIC = "served SpMV/SpTS req/s + p99 vs plain path; SpMV HBM GB/s at \u22641e-5 rel err"
 UNIT = "GB/s"
 
@@ -866,7 +867,11 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="format_sweep_fp64")
+    ap.add_argument("--workload", default="format_sweep_fp64",
+                    help="format_sweep_fp64 (the bench line), laplacian_fp32, or one section "
+                         "alone: " + ", ".join(SECTIONS))
+    ap.add_argument("--batch-mats", type=int, default=512,
+                    help="matrices of the batched section when run alone")
     ap.add_argument("--small", action="store_true",
                     help="quarter-size matrices (profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -895,6 +900,27 @@ def main():
     if args.workload == "laplacian_fp32":
         config["l2"] = "3.7 MB working set stays L2-resident (reported, not a roofline claim)"
     dtype = config["dtype"]
+
+    if args.workload in SECTIONS:
+        # one configuration alone, one GPU (profiling and focused runs)
+        if args.impl == "reference" or rank != 0:
+            return
+        import torch
+        import sciwasm.sparse_b200 as sb
+        sb.load_library()
+        torch.cuda.set_device(local_rank)
+        stream = torch.cuda.Stream()
+        peak, _ = measured_peak()
+        if args.workload == "batched":
+            out = run_batched(stream, peak, n_mats=args.batch_mats)
+        elif args.workload == "laplacian4096_fp32":
+            out = run_laplacian_large(stream, peak)
+        elif args.workload == "spts":
+            out = run_spts_section(stream)
+        else:
+            out = run_serving(args)
+        print(json.dumps({"workload": args.workload, "result": out}), flush=True)
+        return
 
     if args.impl == "reference":
         if rank != 0:
