@@ -397,9 +397,10 @@ template <typename SV, typename T, int V, int UNROLL>
 static int launch_csr_rows_v(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
                              int N, cudaStream_t st) {
   auto kern = csr_rows_kernel<SV, T, V, UNROLL>;
-  const long long warps_needed = ((long long)N + kWarp - 1) / kWarp;
-  const long long max_warps = (long long)resident_ctas(kern, 256) * 8;
-  const long long warps = std::min(warps_needed, max_warps);
+  // one warp per 32-row block (up to 2^31 blocks): the hardware hands blocks
+  // to SMs as they free up, so blocks holding long rows do not hold back a
+  // fixed share of the others
+  const long long warps = ((long long)N + kWarp - 1) / kWarp;
   const unsigned ctas = (unsigned)((warps + 7) / 8);
   kern<<<ctas, 256, 0, st>>>(row_ptr, col, val, x, y, N);
   SB_CHECK_LAUNCH("csr_rows_kernel");
