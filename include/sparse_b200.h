@@ -110,12 +110,13 @@ int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const voi
  * src/parallel/tests/main32.js:150-313).  kernel 0 = row blocks (default),
  * 1 = streamed nonzero tiles; lanes_per_row 1..32 (power of two) and
  * unroll 2/4/8 tune the row-block kernel, 0 = chosen from the mean row
- * length. */
+ * length; grid 0 = a resident grid striding over 32-row blocks (regular
+ * rows), 1 = one warp per 32-row block (skewed row lengths). */
 typedef struct sb_csr_opts {
   int32_t kernel;
   int32_t lanes_per_row;
   int32_t unroll;
-  int32_t reserved;
+  int32_t grid;
 } sb_csr_opts;
 
 /* sb_spmv_csr with explicit kernel options (opts may be NULL). */

@@ -102,7 +102,7 @@ SIGNATURES: dict[str, list] = {
     "sb_map_dia": [C.c_int, C.c_int, C.c_double, P, P, P, I32, I32, I32, P],
 }
 class CsrOpts(C.Structure):
-    _fields_ = [("kernel", I32), ("lanes_per_row", I32), ("unroll", I32), ("reserved", I32)]
+    _fields_ = [("kernel", I32), ("lanes_per_row", I32), ("unroll", I32), ("grid", I32)]
 
 
 class BatchItem(C.Structure):

@@ -393,14 +393,18 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// grid 0: a resident grid whose warps stride over the 32-row blocks (best for
+// regular rows); grid 1: one warp per block, the hardware handing blocks to
+// SMs as they free up, so blocks holding long rows do not hold back a fixed
+// share of the others (best for skewed row lengths).
 template <typename SV, typename T, int V, int UNROLL>
 static int launch_csr_rows_v(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
-                             int N, cudaStream_t st) {
+                             int N, int grid, cudaStream_t st) {
   auto kern = csr_rows_kernel<SV, T, V, UNROLL>;
-  // one warp per 32-row block (up to 2^31 blocks): the hardware hands blocks
-  // to SMs as they free up, so blocks holding long rows do not hold back a
-  // fixed share of the others
-  const long long warps = ((long long)N + kWarp - 1) / kWarp;
+  const long long warps_needed = ((long long)N + kWarp - 1) / kWarp;
+  const long long warps =
+      grid == 1 ? warps_needed
+                : std::min(warps_needed, (long long)resident_ctas(kern, 256) * 8);
   const unsigned ctas = (unsigned)((warps + 7) / 8);
   kern<<<ctas, 256, 0, st>>>(row_ptr, col, val, x, y, N);
   SB_CHECK_LAUNCH("csr_rows_kernel");
@@ -409,10 +413,10 @@ static int launch_csr_rows_v(const int* row_ptr, const int* col, const SV* val, 
 
 template <typename SV, typename T, int V>
 static int launch_csr_rows_u(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
-                             int N, int unroll, cudaStream_t st) {
-  if (unroll <= 2) return launch_csr_rows_v<SV, T, V, 2>(row_ptr, col, val, x, y, N, st);
-  if (unroll >= 8) return launch_csr_rows_v<SV, T, V, 8>(row_ptr, col, val, x, y, N, st);
-  return launch_csr_rows_v<SV, T, V, 4>(row_ptr, col, val, x, y, N, st);
+                             int N, int unroll, int grid, cudaStream_t st) {
+  if (unroll <= 2) return launch_csr_rows_v<SV, T, V, 2>(row_ptr, col, val, x, y, N, grid, st);
+  if (unroll >= 8) return launch_csr_rows_v<SV, T, V, 8>(row_ptr, col, val, x, y, N, grid, st);
+  return launch_csr_rows_v<SV, T, V, 4>(row_ptr, col, val, x, y, N, grid, st);
 }
 
 // Default lanes per row from the mean row length (about three items per lane).
@@ -426,16 +430,17 @@ static int default_lanes(int N, long long nnz) {
 
 template <typename SV, typename T>
 static int launch_csr_rows(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
-                           int N, long long nnz, int lanes, int unroll, cudaStream_t st) {
+                           int N, long long nnz, int lanes, int unroll, int grid,
+                           cudaStream_t st) {
   if (lanes <= 0) lanes = default_lanes(N, nnz);
   if (unroll <= 0) unroll = 4;
   switch (lanes) {
-    case 1: return launch_csr_rows_u<SV, T, 1>(row_ptr, col, val, x, y, N, unroll, st);
-    case 2: return launch_csr_rows_u<SV, T, 2>(row_ptr, col, val, x, y, N, unroll, st);
-    case 4: return launch_csr_rows_u<SV, T, 4>(row_ptr, col, val, x, y, N, unroll, st);
-    case 8: return launch_csr_rows_u<SV, T, 8>(row_ptr, col, val, x, y, N, unroll, st);
-    case 16: return launch_csr_rows_u<SV, T, 16>(row_ptr, col, val, x, y, N, unroll, st);
-    default: return launch_csr_rows_u<SV, T, 32>(row_ptr, col, val, x, y, N, unroll, st);
+    case 1: return launch_csr_rows_u<SV, T, 1>(row_ptr, col, val, x, y, N, unroll, grid, st);
+    case 2: return launch_csr_rows_u<SV, T, 2>(row_ptr, col, val, x, y, N, unroll, grid, st);
+    case 4: return launch_csr_rows_u<SV, T, 4>(row_ptr, col, val, x, y, N, unroll, grid, st);
+    case 8: return launch_csr_rows_u<SV, T, 8>(row_ptr, col, val, x, y, N, unroll, grid, st);
+    case 16: return launch_csr_rows_u<SV, T, 16>(row_ptr, col, val, x, y, N, unroll, grid, st);
+    default: return launch_csr_rows_u<SV, T, 32>(row_ptr, col, val, x, y, N, unroll, grid, st);
   }
 }
 
@@ -657,7 +662,7 @@ static int launch_csr(const int* row_ptr, const int* col, const S* val, const S*
     return launch_csr_stream<S, 1024, 4>(row_ptr, col, val, x, y, N, nnz, st);
   }
   return launch_csr_rows<S, S>(row_ptr, col, val, x, y, N, nnz, opts ? opts->lanes_per_row : 0,
-                               opts ? opts->unroll : 0, st);
+                               opts ? opts->unroll : 0, opts ? opts->grid : 0, st);
 }
 
 template <typename S, typename A>
@@ -704,6 +709,7 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
     const int l = opts->lanes_per_row;
     SB_REQUIRE(l == 0 || l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32,
                "sb_spmv_csr: lanes_per_row must be 0 or a power of two <= 32");
+    SB_REQUIRE(opts->grid == 0 || opts->grid == 1, "sb_spmv_csr: grid must be 0 or 1");
   }
   if (N == 0 || nnz == 0 || inner_max == 0) return SB_OK;
   SB_REQUIRE(row_ptr && col && val && x && y, "sb_spmv_csr: null pointer");
@@ -714,7 +720,8 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
       r = launch_csr_rows<__nv_bfloat16, float>(row_ptr, col, (const __nv_bfloat16*)val,
                                                 (const float*)x, (float*)y, N, nnz,
                                                 opts ? opts->lanes_per_row : 0,
-                                                opts ? opts->unroll : 0, st);
+                                                opts ? opts->unroll : 0, opts ? opts->grid : 0,
+                                                st);
     else if (dtype == SB_F32)
       r = launch_csr<float, float>(row_ptr, col, (const float*)val, (const float*)x, (float*)y, N,
                                    nnz, opts, st);
@@ -735,32 +742,35 @@ int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const voi
 int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                     const void* x, int32_t N, int64_t nnz, int32_t reps, sb_csr_opts* best,
                     float* best_ms, void* stream) {
-  int r = check_dtype(dtype, "sb_csr_autotune");
+  int r = dtype == SB_BF16 ? SB_OK : check_dtype(dtype, "sb_csr_autotune");
   if (r) return r;
   SB_REQUIRE(best && N >= 0 && nnz >= 0, "sb_csr_autotune: bad argument");
   best->kernel = 0;
   best->lanes_per_row = default_lanes(N, nnz);
   best->unroll = 4;
-  best->reserved = 0;
+  best->grid = 0;
   if (best_ms) *best_ms = 0.f;
   if (N == 0 || nnz == 0) return SB_OK;
   SB_REQUIRE(row_ptr && col && val && x, "sb_csr_autotune: null pointer");
   if ((r = ensure_device())) return r;
   if (reps <= 0) reps = 5;
   cudaStream_t st = as_stream(stream);
-  // candidates around the mean row length: lanes in {d/2, d, 2d}, unroll {2, 4, 8},
+  // candidates around the mean row length: lanes in {d/4, d/2, d, 2d}, unroll {2, 4, 8},
+  // both grids,
   // plus the streamed-tile kernel
   const int d = default_lanes(N, nnz);
-  sb_csr_opts cand[16];
+  sb_csr_opts cand[32];
   int nc = 0;
-  for (int lanes : {d / 2, d, d * 2}) {
+  for (int lanes : {d / 4, d / 2, d, d * 2}) {
     if (lanes < 1 || lanes > 32) continue;
-    for (int u : {2, 4, 8}) cand[nc++] = sb_csr_opts{0, lanes, u, 0};
+    for (int u : {2, 4, 8})
+      for (int g : {0, 1}) cand[nc++] = sb_csr_opts{0, lanes, u, g};
   }
   cand[nc++] = sb_csr_opts{1, 0, 1024, 0};
   void* ywork = nullptr;
-  if ((r = scratch_alloc(&ywork, dtype_size(dtype) * (size_t)N, st))) return r;
-  SB_CHECK_CUDA(cudaMemsetAsync(ywork, 0, dtype_size(dtype) * (size_t)N, st));
+  const size_t ysize = dtype == SB_BF16 ? sizeof(float) : dtype_size(dtype);  // y is f32 for BF16
+  if ((r = scratch_alloc(&ywork, ysize * (size_t)N, st))) return r;
+  SB_CHECK_CUDA(cudaMemsetAsync(ywork, 0, ysize * (size_t)N, st));
   cudaEvent_t e0, e1;
   SB_CHECK_CUDA(cudaEventCreate(&e0));
   SB_CHECK_CUDA(cudaEventCreate(&e1));

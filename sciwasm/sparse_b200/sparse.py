@@ -348,7 +348,7 @@ def csr_autotune(A_csr, x_view, reps=5, stream=None):
          C.byref(ms), _sp(stream))
     A_csr.opts = best
     return {"kernel": best.kernel, "lanes_per_row": best.lanes_per_row, "unroll": best.unroll,
-            "ms": float(ms.value)}
+            "grid": best.grid, "ms": float(ms.value)}
 
 
 def spmv(A, x_view, y_view, inner_max=1, stream=None):
