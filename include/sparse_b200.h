@@ -330,6 +330,48 @@ int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t
                       void* stream);
 
 /* ---------------------------------------------------------------------- */
+/* Matrix Market input: replaces mmread / read_matrix_MM_files /            */
+/* create_COO_from_MM / create_LCOO_from_MM                                  */
+/* (src/sequential/src/sparse32.js:1889-2172, 2499-2510).                    */
+/* ---------------------------------------------------------------------- */
+#define SB_MM_REAL 0
+#define SB_MM_INTEGER 1
+#define SB_MM_PATTERN 2
+#define SB_MM_COMPLEX 3 /* the real part is read, as the reference's Number() of field 3 */
+
+typedef struct sb_mm_header {
+  int64_t nrows;
+  int64_t ncols;
+  int64_t nentries;    /* entry lines in the file */
+  int32_t field;       /* SB_MM_* */
+  int32_t symmetric;   /* 1 for the symmetry "symmetric"; anything else reads as general */
+  int64_t data_offset; /* byte offset of the first line after the size line */
+} sb_mm_header;
+
+/* Host only (no device work): parses the banner ("%%MatrixMarket matrix
+ * coordinate <field> <symmetry>", read_MM_header :1889-1911), skips comment
+ * and blank lines and reads the size line.  Refuses more than 2^27 entries
+ * (the reference throws, :1963-1965). */
+int sb_mm_read_header(const char* text, size_t len, sb_mm_header* header);
+/* Host only: parses the entry lines after the size line into host arrays
+ * (1-based row/col as in the file, f64 values; val unused for pattern),
+ * splitting the text across nthreads threads (<= 0: all hardware threads).
+ * The number of entry lines must equal header->nentries. */
+int sb_mm_read_entries(const char* text, size_t len, const sb_mm_header* header, int32_t* row,
+                       int32_t* col, double* val, int32_t nthreads);
+/* Device: the COO of create_COO_from_MM (lower = 0: explicit zeros dropped,
+ * off-diagonal entries of symmetric files mirrored, :2103-2172) or of
+ * create_LCOO_from_MM (lower = 1: the strictly lower part, upper entries of
+ * symmetric files mirrored, then a unit diagonal, :1983-2099), sorted by
+ * (row, col) in place of quick_sort_COO.  row/col/val are the device copies
+ * of sb_mm_read_entries' arrays.  With out_row == NULL only *nnz is computed
+ * (allocate, then call again).  Refuses more than 2^28 nonzeros.  Returns
+ * after the device work is complete. */
+int sb_mm_coo(int dtype, int lower, const sb_mm_header* header, const int32_t* row,
+              const int32_t* col, const double* val, int32_t* out_row, int32_t* out_col,
+              void* out_val, int64_t* nnz, void* stream);
+
+/* ---------------------------------------------------------------------- */
 /* eliminate_zeros and transpose (bit-exact with the reference's kernels). */
 /* The nonzero test is v > 0 || v < 0 (+0, -0 and NaN count as zeros).    */
 /* Calls that return a count return after the device work is complete.    */

@@ -71,6 +71,9 @@ _SIG = {
     "or_map_dia": ([C.c_int, C.c_int, C.c_double, _P, _P, _P, _I32, _I32, _I32], None),
     "or_fletcher_f32": ([_P, _I64], _I64),
     "or_fletcher_f64": ([_P, _I64], _I64),
+    "or_mm_read": ([_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P], C.c_int),
+    "or_mm_coo": ([C.c_int, C.c_int, _I32, _I32, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P],
+                  _I64),
 }
 
 _lib = None
@@ -409,3 +412,39 @@ def map_dia(offset, data, N, op, p=0.0, out=None, stride=None):
     lib().or_map_dia(data.dtype.itemsize, op, float(p), _p(offset), _p(data), _p(out), offset.size,
                      stride, N)
     return out
+
+
+# ------------------------------------------------------------------ Matrix Market
+
+def mm_read(text: bytes) -> dict:
+    """read_matrix_MM_files on the file's bytes: header, 1-based entries, nnz."""
+    buf = np.frombuffer(bytes(text), dtype=np.uint8)
+    nr, nc, ne = C.c_int64(), C.c_int64(), C.c_int64()
+    field, sym = C.c_int32(), C.c_int32()
+    nnz = C.c_int64()
+    L = lib()
+    if L.or_mm_read(_p(buf), buf.size, C.byref(nr), C.byref(nc), C.byref(ne), C.byref(field),
+                    C.byref(sym), None, None, None, None):
+        raise ValueError("entries : invalid length, cannot allocate")
+    row = np.zeros(ne.value, np.int32)
+    col = np.zeros(ne.value, np.int32)
+    val = np.zeros(ne.value, np.float64)
+    if L.or_mm_read(_p(buf), buf.size, C.byref(nr), C.byref(nc), C.byref(ne), C.byref(field),
+                    C.byref(sym), _p(row), _p(col), _p(val), C.byref(nnz)):
+        raise ValueError("nnz : invalid length, cannot allocate")
+    return dict(nrows=nr.value, ncols=nc.value, nentries=ne.value, field=field.value,
+                symmetric=sym.value, row=row, col=col, val=val, nnz=nnz.value)
+
+
+def mm_coo(info: dict, dtype=np.float32, lower=False):
+    """create_COO_from_MM (lower=False) or create_LCOO_from_MM (lower=True),
+    sorted by quick_sort_COO.  Returns (row, col, val)."""
+    dt = np.dtype(dtype)
+    cap = info["nnz"] if not lower else info["nrows"] + 2 * info["nentries"]
+    row = np.zeros(max(cap, 1), np.int32)
+    col = np.zeros(max(cap, 1), np.int32)
+    val = np.zeros(max(cap, 1), dt)
+    n = lib().or_mm_coo(dt.itemsize, int(lower), info["field"], info["symmetric"], info["nrows"],
+                        info["nentries"], info["nnz"], _p(info["row"]), _p(info["col"]),
+                        _p(info["val"]), _p(row), _p(col), _p(val))
+    return row[:n], col[:n], val[:n]

@@ -952,3 +952,151 @@ void or_map_dia(int w, int op, double p, const int32_t* offset, const void* in, 
                         (char*)out + (size_t)w * (base + lo), hi - lo);
   }
 }
+
+/* ======================= Matrix Market input ======================= */
+
+/* The i-th field of a line split at single spaces (JavaScript split(" ")),
+ * copied into buf; empty when absent. */
+static void mm_field(const char* line, int64_t n, int idx, char* buf, int cap) {
+  int k = 0;
+  int64_t i = 0;
+  while (k < idx && i < n) {
+    if (line[i] == ' ') ++k;
+    ++i;
+  }
+  int m = 0;
+  if (k == idx)
+    while (i < n && line[i] != ' ' && m < cap - 1) buf[m++] = line[i++];
+  buf[m] = 0;
+}
+
+/* JavaScript Number() of a decimal field (the test inputs are plain
+ * decimal numbers, for which strtod is the same correctly rounded parse). */
+static double mm_number(const char* line, int64_t n, int idx) {
+  char buf[128];
+  mm_field(line, n, idx, buf, (int)sizeof(buf));
+  return strtod(buf, NULL);
+}
+
+/* read_MM_header (:1889-1911) + read_matrix_MM_files (:1956-1981) with
+ * calculate_actual_nnz (:1914-1954). */
+int or_mm_read(const char* text, int64_t len, int64_t* nrows, int64_t* ncols, int64_t* nentries,
+               int32_t* field, int32_t* symmetric, int32_t* row, int32_t* col, double* val,
+               int64_t* nnz) {
+  /* lines: up to the last '\n' (load_file keeps the text after it for the
+   * next slice, and the last slice's remainder is dropped) */
+  int64_t end = len;
+  while (end > 0 && text[end - 1] != '\n') --end;
+  int64_t pos = 0;
+  /* first line: field and symmetry */
+  int64_t e0 = pos;
+  while (e0 < end && text[e0] != '\n') ++e0;
+  char f[64], sy[64];
+  mm_field(text, e0, 3, f, sizeof f);
+  mm_field(text, e0, 4, sy, sizeof sy);
+  *field = !strcmp(f, "real") ? 0 : !strcmp(f, "integer") ? 1 : !strcmp(f, "pattern") ? 2
+           : !strcmp(f, "complex") ? 3 : -1;
+  *symmetric = !strcmp(sy, "symmetric");
+  /* skip comment lines (the first line starts with '%' too) */
+  while (pos < end && text[pos] == '%') {
+    while (pos < end && text[pos] != '\n') ++pos;
+    ++pos;
+  }
+  int64_t le = pos;
+  while (le < end && text[le] != '\n') ++le;
+  *nrows = (int64_t)mm_number(text + pos, le - pos, 0);
+  *ncols = (int64_t)mm_number(text + pos, le - pos, 1);
+  *nentries = (int64_t)mm_number(text + pos, le - pos, 2);
+  pos = le + 1;
+  if (*nentries > ((int64_t)1 << 27)) return -1;
+  if (!row) return 0;
+  int64_t count = 0, j = 0;
+  const int pattern = *field == 2, sym = *symmetric;
+  while (pos < end) {
+    le = pos;
+    while (le < end && text[le] != '\n') ++le;
+    const char* ln = text + pos;
+    const int64_t n = le - pos;
+    const int32_t r = (int32_t)mm_number(ln, n, 0), c = (int32_t)mm_number(ln, n, 1);
+    if (j < *nentries) {
+      row[j] = r;
+      col[j] = c;
+    }
+    if (sym) {
+      if (!pattern) {
+        const double v = mm_number(ln, n, 2);
+        if (j < *nentries) val[j] = v;
+        if (v < 0 || v > 0) count += (r == c) ? 1 : 2;
+      } else {
+        count += (r == c) ? 1 : 2;
+      }
+    } else if (!pattern) {
+      const double v = mm_number(ln, n, 2);
+      if (j < *nentries) val[j] = v;
+      if (v < 0 || v > 0) count++;
+    }
+    j++;
+    pos = le + 1;
+  }
+  if (count == 0) count = *nentries;
+  *nnz = count;
+  if (count > ((int64_t)1 << 28)) return -1;
+  return 0;
+}
+
+static void mm_put(int w, void* out_val, int64_t i, double v) {
+  if (w == 4) ((float*)out_val)[i] = (float)v;
+  else ((double*)out_val)[i] = v;
+}
+
+int64_t or_mm_coo(int w, int lower, int32_t field, int32_t symmetric, int64_t nrows,
+                  int64_t nentries, int64_t nnz, const int32_t* row, const int32_t* col,
+                  const double* val, int32_t* out_row, int32_t* out_col, void* out_val) {
+  const int pattern = field == 2;
+  int64_t i = 0;
+  if (!lower) {
+    /* create_COO_from_MM :2103-2172 */
+    for (int64_t n = 0; n < nentries; ++n) {
+      const double v = pattern ? 1.0 : val[n];
+      if (!pattern && !(v < 0 || v > 0)) continue;
+      out_row[i] = row[n] - 1;
+      out_col[i] = col[n] - 1;
+      mm_put(w, out_val, i, v);
+      if (symmetric && row[n] != col[n]) {
+        out_row[i + 1] = col[n] - 1;
+        out_col[i + 1] = row[n] - 1;
+        mm_put(w, out_val, i + 1, v);
+        i += 2;
+      } else {
+        i += 1;
+      }
+    }
+  } else {
+    /* create_LCOO_from_MM :1983-2099: strictly lower part (mirrored upper
+     * entries when symmetric), then the unit diagonal */
+    for (int64_t n = 0; n < nentries; ++n) {
+      const double v = pattern ? 1.0 : val[n];
+      if (!pattern && !(v < 0 || v > 0)) continue;
+      if (row[n] > col[n]) {
+        out_row[i] = row[n] - 1;
+        out_col[i] = col[n] - 1;
+      } else if (symmetric && row[n] < col[n]) {
+        out_row[i] = col[n] - 1;
+        out_col[i] = row[n] - 1;
+      } else {
+        continue;
+      }
+      mm_put(w, out_val, i, v);
+      i++;
+    }
+    for (int64_t n = 0; n < nrows; ++n) {
+      out_row[i] = (int32_t)n;
+      out_col[i] = (int32_t)n;
+      mm_put(w, out_val, i, 1.0);
+      i++;
+    }
+    nnz = i;
+  }
+  if (nnz > 0) or_quick_sort_coo(w, out_row, out_col, out_val, 0, nnz - 1);
+  return nnz;
+}

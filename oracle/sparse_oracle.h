@@ -207,6 +207,31 @@ void or_map(int val_bytes, int kind, int op, double p, const void* in, void* out
 void or_map_dia(int val_bytes, int op, double p, const int32_t* offset, const void* in,
                 void* out, int32_t nd, int32_t stride, int32_t N);
 
+/* ---------------- Matrix Market input ---------------- */
+/* read_MM_header / calculate_actual_nnz / read_matrix_MM_files:
+ * src/sequential/src/sparse32.js:1889-1981, on text split into lines at
+ * '\n' and fields at single spaces (load_file :2454-2497).  Header: field =
+ * token 3 and symmetry = token 4 of the first line; lines starting with '%'
+ * skipped; then "nrows ncols nentries".  Returns 0, or -1 when nentries
+ * exceeds 2^27 / the counted nnz exceeds 2^28 (the reference throws).
+ * field: 0 real, 1 integer, 2 pattern, 3 complex, -1 other; symmetric = 1
+ * for the symmetry token "symmetric".  The first call (row == NULL) reads
+ * the header only; the second fills row/col (1-based, as in the file) and
+ * val (f64; not written for pattern) and the counted nnz, including the
+ * reference's fallback nnz = nentries when the count is 0. */
+int or_mm_read(const char* text, int64_t len, int64_t* nrows, int64_t* ncols, int64_t* nentries,
+               int32_t* field, int32_t* symmetric, int32_t* row, int32_t* col, double* val,
+               int64_t* nnz);
+/* create_COO_from_MM :2103-2172 (lower = 0; nnz from or_mm_read) and
+ * create_LCOO_from_MM :1983-2099 (lower = 1: strictly lower entries, the
+ * upper ones mirrored for "symmetric", explicit zeros dropped, then a unit
+ * diagonal appended; returns its nnz), both followed by quick_sort_COO.
+ * Values are stored with val_bytes (4: the Float32Array of sparse32.js,
+ * 8: sparse64.js).  out arrays hold nnz entries. */
+int64_t or_mm_coo(int val_bytes, int lower, int32_t field, int32_t symmetric, int64_t nrows,
+                  int64_t nentries, int64_t nnz, const int32_t* row, const int32_t* col,
+                  const double* val, int32_t* out_row, int32_t* out_col, void* out_val);
+
 #ifdef __cplusplus
 }
 #endif

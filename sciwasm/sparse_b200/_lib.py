@@ -110,11 +110,22 @@ class BatchItem(C.Structure):
                 ("nrhs", I32), ("lanes", I32), ("flags", I32), ("nnz", I64)]
 
 
+class MMHeader(C.Structure):
+    _fields_ = [("nrows", I64), ("ncols", I64), ("nentries", I64), ("field", I32),
+                ("symmetric", I32), ("data_offset", I64)]
+
+
+SB_MM_REAL, SB_MM_INTEGER, SB_MM_PATTERN, SB_MM_COMPLEX = 0, 1, 2, 3
+
+
 class SptsBatchItem(C.Structure):
     _fields_ = [("plan", P), ("b", P), ("y", P)]
 
 
 SIGNATURES.update({
+    "sb_mm_read_header": [P, SZ, C.POINTER(MMHeader)],
+    "sb_mm_read_entries": [P, SZ, C.POINTER(MMHeader), P, P, P, I32],
+    "sb_mm_coo": [C.c_int, C.c_int, C.POINTER(MMHeader), P, P, P, P, P, P, C.POINTER(I64), P],
     "sb_spts_plan_growth": [P, C.POINTER(C.c_double), P],
     "sb_spts_batch_create": [C.c_int, C.c_int, I32, C.POINTER(P)],
     "sb_spts_batch_destroy": [P],

@@ -324,6 +324,86 @@ def ell_from_host(indices, data, ncols, N, nnz=None):
                         nnz if nnz is not None else int(np.count_nonzero(data)))
 
 
+# --------------------------------------------------------------- Matrix Market
+
+
+class sparse_MM_info:
+    """sparse_MM_info (src/sequential/src/sparse32.js:14-25): the header of a
+    Matrix Market file and its entries (1-based, device arrays), with nnz as
+    read_matrix_MM_files counts it."""
+
+    _FIELDS = {_lib.SB_MM_REAL: "real", _lib.SB_MM_INTEGER: "integer",
+               _lib.SB_MM_PATTERN: "pattern", _lib.SB_MM_COMPLEX: "complex"}
+
+    def __init__(self, header, row, col, val):
+        self.header = header
+        self.field = self._FIELDS[header.field]
+        self.symmetry = "symmetric" if header.symmetric else "general"
+        self.nrows, self.ncols, self.nentries = header.nrows, header.ncols, header.nentries
+        self.row, self.col, self.val = row, col, val
+        self.nnz = self._count(0)
+
+    def _count(self, lower, stream=None):
+        n = C.c_int64(0)
+        call("sb_mm_coo", _lib.SB_F32, int(lower), C.byref(self.header), self.row.ptr,
+             self.col.ptr, self.val.ptr if self.val is not None else None, None, None, None,
+             C.byref(n), _sp(stream))
+        return int(n.value)
+
+
+def read_matrix_MM(source, nthreads=0, stream=None) -> sparse_MM_info:
+    """read_matrix_MM_files (src/sequential/src/sparse32.js:1956-1981) on a
+    file path or the file's bytes: the text is parsed on the host (entry
+    lines across nthreads threads), the entries are uploaded to the device."""
+    if isinstance(source, (bytes, bytearray, memoryview)):
+        text = np.frombuffer(bytes(source), dtype=np.uint8)
+    else:
+        text = np.fromfile(source, dtype=np.uint8)
+    hdr = _lib.MMHeader()
+    call("sb_mm_read_header", text.ctypes.data, text.size, C.byref(hdr))
+    n = int(hdr.nentries)
+    row = np.empty(n, np.int32)
+    col = np.empty(n, np.int32)
+    pattern = hdr.field == _lib.SB_MM_PATTERN
+    val = None if pattern else np.empty(n, np.float64)
+    call("sb_mm_read_entries", text.ctypes.data, text.size, C.byref(hdr), row.ctypes.data,
+         col.ctypes.data, None if pattern else val.ctypes.data, int(nthreads))
+    return sparse_MM_info(hdr, DeviceArray.from_host(row), DeviceArray.from_host(col),
+                          None if pattern else DeviceArray.from_host(val))
+
+
+def _coo_from_mm(mm_info, lower, dtype, stream):
+    nnz = mm_info._count(lower, stream)
+    A = allocate_COO(mm_info.nrows, nnz, dtype)
+    n = C.c_int64(0)
+    call("sb_mm_coo", _dtcode(dtype), int(lower), C.byref(mm_info.header), mm_info.row.ptr,
+         mm_info.col.ptr, mm_info.val.ptr if mm_info.val is not None else None,
+         A.row_index.ptr, A.col_index.ptr, A.val_index.ptr, C.byref(n), _sp(stream))
+    return A
+
+
+def create_COO_from_MM(mm_info, dtype=np.float32, stream=None):
+    """create_COO_from_MM (src/sequential/src/sparse32.js:2103-2172): a new
+    COO with explicit zeros dropped and symmetric entries mirrored, sorted
+    by (row, col).  Values in `dtype` (f32 as sparse32.js, f64 as
+    sparse64.js)."""
+    return _coo_from_mm(mm_info, 0, dtype, stream)
+
+
+def create_LCOO_from_MM(mm_info, dtype=np.float32, stream=None):
+    """create_LCOO_from_MM (src/sequential/src/sparse32.js:1983-2099): the
+    strictly lower triangle (symmetric upper entries mirrored, zeros
+    dropped) plus a unit diagonal, sorted by (row, col) so that each row's
+    diagonal is its last entry."""
+    return _coo_from_mm(mm_info, 1, dtype, stream)
+
+
+def mmread(filename, dtype=np.float32, nthreads=0):
+    """mmread (src/sequential/src/sparse32.js:2499-2510): read a Matrix
+    Market file into a new device COO."""
+    return create_COO_from_MM(read_matrix_MM(filename, nthreads), dtype)
+
+
 def free(obj) -> None:
     """free (src/sequential/src/sparse32.js:2204-2231)."""
     if obj is None:
