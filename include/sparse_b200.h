@@ -330,6 +330,35 @@ int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t
                       void* stream);
 
 /* ---------------------------------------------------------------------- */
+/* Reductions over a row-sorted COO (rows non-decreasing, as the           */
+/* reference's quick-sorted objects are; unsorted rows return SB_EINVAL).  */
+/* Each returns after a sortedness check that reads back one flag.         */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces diagonal_coo (src/sequential/src/sparse_opt_32.wat:1707-1798;
+ * JS A.diagonal(offset), src/sequential/src/sparse32.js:314-321): diag[i] =
+ * the first entry of row start+i in column start+i+k (start = max(0, -k)),
+ * else 0, for N - |k| slots.  |k| >= N returns SB_EINVAL (the reference
+ * returns no vector). */
+int sb_diagonal_coo(int dtype, int32_t k, const int32_t* row, const int32_t* col,
+                    const void* val, void* diag, int32_t N, int64_t nnz, void* stream);
+/* Replaces min_coo (src/sequential/src/sparse_opt_32.wat:1847-1946; JS
+ * A.min(axis), src/sequential/src/sparse32.js:323-328): axis 1 gives each
+ * row's minimum, 0 when the row has fewer than N entries and its minimum is
+ * positive, with the reference's walk reproduced exactly (an empty row
+ * repeats the previous stored minimum when that is <= 0; the last entry's
+ * row stays 0 when it holds one entry; later rows stay 0).  Other axes leave
+ * out unchanged (the caller zero-fills it, as create_vec does). */
+int sb_min_coo(int dtype, int32_t axis, const int32_t* row, const int32_t* col, const void* val,
+               void* out, int32_t N, int64_t nnz, void* stream);
+/* sum_coo (src/sequential/src/sparse_opt_32.wat:1800-1845), axis 1: the sum
+ * of each row in storage order.  The reference's export advances its row
+ * counter for every entry it adds as well, so its output is not this row
+ * sum (it is not reachable from the JS API). */
+int sb_sum_coo(int dtype, int32_t axis, const int32_t* row, const int32_t* col, const void* val,
+               void* out, int32_t N, int64_t nnz, void* stream);
+
+/* ---------------------------------------------------------------------- */
 /* Matrix Market input: replaces mmread / read_matrix_MM_files /            */
 /* create_COO_from_MM / create_LCOO_from_MM                                  */
 /* (src/sequential/src/sparse32.js:1889-2172, 2499-2510).                    */

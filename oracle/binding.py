@@ -71,6 +71,9 @@ _SIG = {
     "or_map_dia": ([C.c_int, C.c_int, C.c_double, _P, _P, _P, _I32, _I32, _I32], None),
     "or_fletcher_f32": ([_P, _I64], _I64),
     "or_fletcher_f64": ([_P, _I64], _I64),
+    "or_diagonal_coo": ([C.c_int, _I32, _P, _P, _P, _P, _I32, _I64], None),
+    "or_min_coo": ([C.c_int, _I32, _P, _P, _P, _I32, _I64], None),
+    "or_sum_coo_rows": ([C.c_int, _I32, _P, _P, _P, _I32, _I64], None),
     "or_mm_read": ([_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P], C.c_int),
     "or_mm_coo": ([C.c_int, C.c_int, _I32, _I32, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P],
                   _I64),
@@ -120,36 +123,34 @@ def _i32(a):
 def spmv_csr(row_ptr, col, val, x, y):
     """y + A x in the reference's serial order; returns a new array."""
     y = np.array(y, dtype=val.dtype, copy=True)
-    row_ptr, col = _i32(row_ptr), _i32(col)
+    row_ptr, col, x = _i32(row_ptr), _i32(col), np.ascontiguousarray(x, val.dtype)
     getattr(lib(), "or_spmv_csr_" + _sfx(val.dtype))(
-        _p(row_ptr), _p(col), _p(val), _p(np.ascontiguousarray(x, val.dtype)), _p(y),
-        row_ptr.size - 1)
+        _p(row_ptr), _p(col), _p(val), _p(x), _p(y), row_ptr.size - 1)
     return y
 
 
 def spmv_coo(row, col, val, x, y):
     y = np.array(y, dtype=val.dtype, copy=True)
-    row, col = _i32(row), _i32(col)
+    row, col, x = _i32(row), _i32(col), np.ascontiguousarray(x, val.dtype)
     getattr(lib(), "or_spmv_coo_" + _sfx(val.dtype))(
-        _p(row), _p(col), _p(val), _p(np.ascontiguousarray(x, val.dtype)), _p(y), row.size)
+        _p(row), _p(col), _p(val), _p(x), _p(y), row.size)
     return y
 
 
 def spmv_dia(offset, data, N, x, y, stride=None):
     y = np.array(y, dtype=data.dtype, copy=True)
-    offset = _i32(offset)
+    offset, x = _i32(offset), np.ascontiguousarray(x, data.dtype)
     stride = N if stride is None else stride
     getattr(lib(), "or_spmv_dia_" + _sfx(data.dtype))(
-        _p(offset), _p(data), N, offset.size, stride, _p(np.ascontiguousarray(x, data.dtype)),
-        _p(y))
+        _p(offset), _p(data), N, offset.size, stride, _p(x), _p(y))
     return y
 
 
 def spmv_ell(indices, data, N, nc, x, y):
     y = np.array(y, dtype=data.dtype, copy=True)
-    indices = _i32(indices)
+    indices, x = _i32(indices), np.ascontiguousarray(x, data.dtype)
     getattr(lib(), "or_spmv_ell_" + _sfx(data.dtype))(
-        _p(indices), _p(data), N, nc, _p(np.ascontiguousarray(x, data.dtype)), _p(y))
+        _p(indices), _p(data), N, nc, _p(x), _p(y))
     return y
 
 
@@ -289,26 +290,32 @@ def level_sets(row_ptr, col, val):
                 row_ptr=nr, col=nc, val=nv, nlevels=int(nl))
 
 
+def _spts_args(row_ptr, col, val, b):
+    """Contiguous operands, held by the caller for the duration of the call."""
+    val = np.ascontiguousarray(val)
+    return _i32(row_ptr), _i32(col), val, np.ascontiguousarray(b, val.dtype)
+
+
 def spts_csr(row_ptr, col, val, b):
-    y = np.zeros(row_ptr.size - 1, val.dtype)
-    getattr(lib(), "or_spts_csr_" + _sfx(val.dtype))(
-        _p(_i32(row_ptr)), _p(_i32(col)), _p(val), _p(np.ascontiguousarray(b, val.dtype)), _p(y),
-        row_ptr.size - 1)
+    rp, c, v, bb = _spts_args(row_ptr, col, val, b)
+    y = np.zeros(rp.size - 1, v.dtype)
+    getattr(lib(), "or_spts_csr_" + _sfx(v.dtype))(_p(rp), _p(c), _p(v), _p(bb), _p(y),
+                                                    rp.size - 1)
     return y
 
 
 def spts_syncfree(row_ptr, col, val, b):
-    y = np.zeros(row_ptr.size - 1, val.dtype)
-    getattr(lib(), "or_spts_syncfree_" + _sfx(val.dtype))(
-        _p(_i32(row_ptr)), _p(_i32(col)), _p(val), _p(np.ascontiguousarray(b, val.dtype)), _p(y),
-        row_ptr.size - 1)
+    rp, c, v, bb = _spts_args(row_ptr, col, val, b)
+    y = np.zeros(rp.size - 1, v.dtype)
+    getattr(lib(), "or_spts_syncfree_" + _sfx(v.dtype))(_p(rp), _p(c), _p(v), _p(bb), _p(y),
+                                                         rp.size - 1)
     return y
 
 
 def truth_spts(row_ptr, col, val, b):
-    y = np.zeros(row_ptr.size - 1, np.float64)
-    lib().or_truth_spts(val.dtype.itemsize, _p(_i32(row_ptr)), _p(_i32(col)), _p(val),
-                        _p(np.ascontiguousarray(b, val.dtype)), _p(y), row_ptr.size - 1)
+    rp, c, v, bb = _spts_args(row_ptr, col, val, b)
+    y = np.zeros(rp.size - 1, np.float64)
+    lib().or_truth_spts(v.dtype.itemsize, _p(rp), _p(c), _p(v), _p(bb), _p(y), rp.size - 1)
     return y
 
 
@@ -448,3 +455,26 @@ def mm_coo(info: dict, dtype=np.float32, lower=False):
                         info["nentries"], info["nnz"], _p(info["row"]), _p(info["col"]),
                         _p(info["val"]), _p(row), _p(col), _p(val))
     return row[:n], col[:n], val[:n]
+
+
+# ------------------------------------------------------------------ COO reductions
+
+def diagonal_coo(k, row, col, val, N):
+    row, col, val = _i32(row), _i32(col), np.ascontiguousarray(val)
+    out = np.zeros(max(N - abs(k), 0), val.dtype)
+    lib().or_diagonal_coo(val.dtype.itemsize, k, _p(row), _p(col), _p(val), _p(out), N, row.size)
+    return out
+
+
+def min_coo(axis, row, val, N):
+    row, val = _i32(row), np.ascontiguousarray(val)
+    out = np.zeros(N, val.dtype)
+    lib().or_min_coo(val.dtype.itemsize, axis, _p(row), _p(val), _p(out), N, row.size)
+    return out
+
+
+def sum_coo_rows(axis, row, val, N):
+    row, val = _i32(row), np.ascontiguousarray(val)
+    out = np.zeros(N, val.dtype)
+    lib().or_sum_coo_rows(val.dtype.itemsize, axis, _p(row), _p(val), _p(out), N, row.size)
+    return out

@@ -1100,3 +1100,91 @@ int64_t or_mm_coo(int w, int lower, int32_t field, int32_t symmetric, int64_t nr
   if (nnz > 0) or_quick_sort_coo(w, out_row, out_col, out_val, 0, nnz - 1);
   return nnz;
 }
+
+/* ======================= COO reductions ======================= */
+
+#define OR_REDUCE(T, SFX)                                                                      \
+  static void diag_##SFX(int32_t k, const int32_t* row, const int32_t* col, const T* val,     \
+                         T* diag, int32_t N, int64_t nnz) {                                    \
+    int32_t start = k < 0 ? -k : 0, end = k < 0 ? N : N - k;                                  \
+    int64_t i = 0;                                                                             \
+    /* $init: bring the pointer to the first row >= start */                                   \
+    while (start > row[i]) {                                                                   \
+      if (++i == nnz) return;                                                                  \
+    }                                                                                          \
+    for (;;) { /* $diag_loop */                                                                \
+      while (row[i] == start) { /* $row_loop */                                                \
+        if (col[i] - row[i] != k) {                                                            \
+          if (++i == nnz) return;                                                              \
+          continue;                                                                            \
+        }                                                                                      \
+        *diag = val[i]; /* found: skip the rest of the row */                                  \
+        while (row[i] == start) {                                                              \
+          if (++i == nnz) return;                                                              \
+        }                                                                                      \
+      }                                                                                        \
+      diag++;                                                                                  \
+      if (++start == end) return;                                                              \
+    }                                                                                          \
+  }                                                                                            \
+  static void min_##SFX(int32_t axis, const int32_t* row, const T* val, T* out, int32_t N,     \
+                        int64_t nnz) {                                                         \
+    int64_t j = 0;                                                                             \
+    T temp = 0;                                                                                \
+    if (axis != 1) return;                                                                     \
+    for (int32_t i = 0;;) { /* $min_loop_1 */                                                  \
+      int32_t n = 0;                                                                           \
+      if (row[j] == i) {                                                                       \
+        temp = val[j];                                                                         \
+        j++;                                                                                   \
+        n++;                                                                                   \
+        if (j == nnz) return;                                                                  \
+      }                                                                                        \
+      while (row[j] == i) { /* $row_loop_1 */                                                  \
+        if (temp > val[j]) temp = val[j];                                                      \
+        j++;                                                                                   \
+        n++;                                                                                   \
+        if (j == nnz) {                                                                        \
+          if (n < N && 0 < temp) temp = 0;                                                     \
+          *out = temp;                                                                         \
+          return;                                                                              \
+        }                                                                                      \
+      }                                                                                        \
+      if (n < N && 0 < temp) temp = 0;                                                         \
+      *out = temp;                                                                             \
+      out++;                                                                                   \
+      if (++i == N) return;                                                                    \
+    }                                                                                          \
+  }                                                                                            \
+  static void sumr_##SFX(int32_t axis, const int32_t* row, const T* val, T* out, int32_t N,    \
+                         int64_t nnz) {                                                        \
+    if (axis != 1) return;                                                                     \
+    for (int32_t i = 0; i < N; ++i) out[i] = 0;                                                \
+    for (int64_t e = 0; e < nnz; ++e) out[row[e]] = out[row[e]] + val[e];                      \
+  }
+
+OR_REDUCE(float, f32)
+OR_REDUCE(double, f64)
+
+void or_diagonal_coo(int w, int32_t k, const int32_t* row, const int32_t* col, const void* val,
+                     void* diag, int32_t N, int64_t nnz) {
+  if (nnz <= 0 || (int64_t)N - (k < 0 ? -(int64_t)k : k) <= 0) return;
+  if (w == 4) diag_f32(k, row, col, (const float*)val, (float*)diag, N, nnz);
+  else diag_f64(k, row, col, (const double*)val, (double*)diag, N, nnz);
+}
+
+void or_min_coo(int w, int32_t axis, const int32_t* row, const void* val, void* out, int32_t N,
+                int64_t nnz) {
+  if (N <= 0) return;
+  if (nnz <= 0) { /* every row empty: the accumulator stays 0 */
+    return;
+  }
+  if (w == 4) min_f32(axis, row, (const float*)val, (float*)out, N, nnz);
+  else min_f64(axis, row, (const double*)val, (double*)out, N, nnz);
+}
+
+void or_sum_coo_rows(int w, int32_t axis, const int32_t* row, const void* val, void* out,
+                     int32_t N, int64_t nnz) {
+  if (w == 4) sumr_f32(axis, row, (const float*)val, (float*)out, N, nnz);
+  else sumr_f64(axis, row, (const double*)val, (double*)out, N, nnz);
+}

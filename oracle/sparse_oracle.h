@@ -207,6 +207,20 @@ void or_map(int val_bytes, int kind, int op, double p, const void* in, void* out
 void or_map_dia(int val_bytes, int op, double p, const int32_t* offset, const void* in,
                 void* out, int32_t nd, int32_t stride, int32_t N);
 
+/* ---------------- COO reductions ---------------- */
+/* diagonal_coo :1707-1798: the pointer walk over a row-sorted COO; diag
+ * holds N - |k| slots and must be zero-filled (create_vec). */
+void or_diagonal_coo(int val_bytes, int32_t k, const int32_t* row, const int32_t* col,
+                     const void* val, void* diag, int32_t N, int64_t nnz);
+/* min_coo :1847-1946 (axis 1; out zero-filled, as create_vec leaves it),
+ * including its accumulator carried into empty rows and its early returns. */
+void or_min_coo(int val_bytes, int32_t axis, const int32_t* row, const void* val, void* out,
+                int32_t N, int64_t nnz);
+/* Row sums in storage order (axis 1): what sum_coo :1800-1845 computes when
+ * its row counter is not also advanced per entry. */
+void or_sum_coo_rows(int val_bytes, int32_t axis, const int32_t* row, const void* val,
+                     void* out, int32_t N, int64_t nnz);
+
 /* ---------------- Matrix Market input ---------------- */
 /* read_MM_header / calculate_actual_nnz / read_matrix_MM_files:
  * src/sequential/src/sparse32.js:1889-1981, on text split into lines at

@@ -150,6 +150,41 @@ class sparse_COO_t:
     def val_array(self):
         return self.val_index.to_host()
 
+    def diagonal(self, offset=0, stream=None):
+        """sparse_self_diagonal_coo (src/sequential/src/sparse32.js:314-321):
+        the k-th diagonal as a new vector of N - |k| values (None when
+        N - |k| <= 0, where the reference returns undefined); rows must be
+        sorted, as the reference's COO objects are."""
+        k = int(offset)
+        count = self.N - (k if k >= 0 else -k)  # (this module's abs is the element-wise map)
+        if count <= 0:
+            return None
+        v = create_vec(count, 0, self.dtype)
+        call("sb_diagonal_coo", _dtcode(self.dtype), int(offset), self.row_index.ptr,
+             self.col_index.ptr, self.val_index.ptr, v.vec_index.ptr, self.N, self.nnz,
+             _sp(stream))
+        return v
+
+    def min(self, axis=1, stream=None):
+        """sparse_self_min_coo (src/sequential/src/sparse32.js:323-328): per
+        row minimum for axis 1 (a zero vector for other axes), with the
+        reference's implicit-zero rule and walk."""
+        v = create_vec(self.N, 0, self.dtype)
+        call("sb_min_coo", _dtcode(self.dtype), int(axis), self.row_index.ptr,
+             self.col_index.ptr, self.val_index.ptr, v.vec_index.ptr, self.N, self.nnz,
+             _sp(stream))
+        return v
+
+
+def sum_coo(A_coo, axis=1, stream=None):
+    """Row sums of a row-sorted COO for axis 1 (sum_coo,
+    src/sequential/src/sparse_opt_32.wat:1800-1845), a zero vector otherwise."""
+    v = create_vec(A_coo.N, 0, A_coo.dtype)
+    call("sb_sum_coo", _dtcode(A_coo.dtype), int(axis), A_coo.row_index.ptr,
+         A_coo.col_index.ptr, A_coo.val_index.ptr, v.vec_index.ptr, A_coo.N, A_coo.nnz,
+         _sp(stream))
+    return v
+
 
 class sparse_CSR_t:
     """CSR matrix: row_index (N+1), col_index / val_index (nnz)."""
