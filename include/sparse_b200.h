@@ -359,6 +359,30 @@ int sb_sum_coo(int dtype, int32_t axis, const int32_t* row, const int32_t* col, 
                void* out, int32_t N, int64_t nnz, void* stream);
 
 /* ---------------------------------------------------------------------- */
+/* Row reordering (src/parallel/src/sparse32.js:2148-2269).                */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces sort_rows_by_nnz (:2148-2218): the rows stably sorted by their
+ * number of nonzeros (ascending) into a new CSR (columns unchanged);
+ * permutation[new] = old row, nnz_per_row = the new matrix's row lengths,
+ * small_rows[q] (host, may be NULL) = rows with at most q nonzeros, q = 0..3
+ * (num_zero_rows .. num_three_rows).  Returns after the device work. */
+int sb_sort_rows_by_nnz(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                        int32_t N, int64_t nnz, int32_t* out_row_ptr, int32_t* out_col,
+                        void* out_val, int32_t* nnz_per_row, int32_t* permutation,
+                        int32_t* small_rows, void* stream);
+/* Replaces sort_y_rows_by_nnz (:2220-2235): out[permutation[i]] = in[i]
+ * (a result of the reordered matrix back in the original row order). */
+int sb_unpermute_rows(int dtype, const int32_t* permutation, const void* in, void* out,
+                      int32_t N, void* stream);
+/* Replaces calculate_csr_locality_index (:2238-2269): the percentage of
+ * accesses whose 16-column line was last touched fewer than 16 rows before
+ * (NaN for an empty matrix, as the reference's 0/0).  Returns after the
+ * device work. */
+int sb_csr_locality_index(const int32_t* row_ptr, const int32_t* col, int32_t N, int64_t nnz,
+                          double* index, void* stream);
+
+/* ---------------------------------------------------------------------- */
 /* Matrix Market input: replaces mmread / read_matrix_MM_files /            */
 /* create_COO_from_MM / create_LCOO_from_MM                                  */
 /* (src/sequential/src/sparse32.js:1889-2172, 2499-2510).                    */

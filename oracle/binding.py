@@ -74,6 +74,9 @@ _SIG = {
     "or_diagonal_coo": ([C.c_int, _I32, _P, _P, _P, _P, _I32, _I64], None),
     "or_min_coo": ([C.c_int, _I32, _P, _P, _P, _I32, _I64], None),
     "or_sum_coo_rows": ([C.c_int, _I32, _P, _P, _P, _I32, _I64], None),
+    "or_sort_rows_by_nnz": ([C.c_int, _P, _P, _P, _I32, _P, _P, _P, _P, _P, _P], None),
+    "or_unpermute_rows": ([C.c_int, _P, _P, _P, _I32], None),
+    "or_csr_locality_index": ([_P, _P, _I32, _I64], C.c_double),
     "or_mm_read": ([_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P], C.c_int),
     "or_mm_coo": ([C.c_int, C.c_int, _I32, _I32, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P],
                   _I64),
@@ -478,3 +481,32 @@ def sum_coo_rows(axis, row, val, N):
     out = np.zeros(N, val.dtype)
     lib().or_sum_coo_rows(val.dtype.itemsize, axis, _p(row), _p(val), _p(out), N, row.size)
     return out
+
+
+# ------------------------------------------------------------------ row reordering
+
+def sort_rows_by_nnz(row_ptr, col, val):
+    row_ptr, col, val = _i32(row_ptr), _i32(col), np.ascontiguousarray(val)
+    N = row_ptr.size - 1
+    nrp = np.zeros(N + 1, np.int32)
+    ncol = np.zeros(col.size, np.int32)
+    nval = np.zeros(col.size, val.dtype)
+    npr = np.zeros(N, np.int32)
+    perm = np.zeros(N, np.int32)
+    small = np.zeros(4, np.int32)
+    lib().or_sort_rows_by_nnz(val.dtype.itemsize, _p(row_ptr), _p(col), _p(val), N, _p(nrp),
+                              _p(ncol), _p(nval), _p(npr), _p(perm), _p(small))
+    return dict(row_ptr=nrp, col=ncol, val=nval, nnz_per_row=npr, permutation=perm,
+                small_rows=small)
+
+
+def unpermute_rows(permutation, y):
+    permutation, y = _i32(permutation), np.ascontiguousarray(y)
+    out = np.zeros_like(y)
+    lib().or_unpermute_rows(y.dtype.itemsize, _p(permutation), _p(y), _p(out), y.size)
+    return out
+
+
+def csr_locality_index(row_ptr, col):
+    row_ptr, col = _i32(row_ptr), _i32(col)
+    return lib().or_csr_locality_index(_p(row_ptr), _p(col), row_ptr.size - 1, col.size)

@@ -1188,3 +1188,65 @@ void or_sum_coo_rows(int w, int32_t axis, const int32_t* row, const void* val, v
   if (w == 4) sumr_f32(axis, row, (const float*)val, (float*)out, N, nnz);
   else sumr_f64(axis, row, (const double*)val, (double*)out, N, nnz);
 }
+
+/* ======================= row reordering ======================= */
+
+void or_sort_rows_by_nnz(int w, const int32_t* row_ptr, const int32_t* col, const void* val,
+                         int32_t N, int32_t* nrow_ptr, int32_t* ncol, void* nval,
+                         int32_t* nnz_per_row, int32_t* permutation, int32_t* small_rows) {
+  int32_t* freq = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
+  int32_t* start = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
+  for (int32_t i = 0; i < N; ++i) {
+    nnz_per_row[i] = row_ptr[i + 1] - row_ptr[i];
+    freq[nnz_per_row[i]]++;
+  }
+  start[0] = 0;
+  for (int32_t i = 1; i <= N; ++i) start[i] = start[i - 1] + freq[i - 1];
+  small_rows[0] = N > 0 ? freq[0] : 0;
+  for (int q = 1; q < 4; ++q) small_rows[q] = small_rows[q - 1] + (q <= N ? freq[q] : 0);
+  for (int32_t i = 0; i < N; ++i) permutation[start[nnz_per_row[i]]++] = i;
+  int64_t j = 0;
+  nrow_ptr[0] = 0;
+  for (int32_t i = 0; i < N; ++i) {
+    int64_t k = row_ptr[permutation[i]];
+    int32_t t = nnz_per_row[permutation[i]];
+    nrow_ptr[i + 1] = nrow_ptr[i] + t;
+    for (; t != 0; --t, ++j, ++k) {
+      ncol[j] = col[k];
+      memcpy((char*)nval + j * w, (const char*)val + k * w, (size_t)w);
+    }
+  }
+  /* the reference's nnz_per_row array holds the lengths in the original
+   * row order; the reordered matrix's lengths follow the permutation */
+  for (int32_t i = 0; i < N; ++i) nnz_per_row[i] = nrow_ptr[i + 1] - nrow_ptr[i];
+  free(freq);
+  free(start);
+}
+
+void or_unpermute_rows(int w, const int32_t* permutation, const void* in, void* out, int32_t N) {
+  for (int32_t i = 0; i < N; ++i)
+    memcpy((char*)out + (size_t)permutation[i] * w, (const char*)in + (size_t)i * w, (size_t)w);
+}
+
+double or_csr_locality_index(const int32_t* row_ptr, const int32_t* col, int32_t N, int64_t nnz) {
+  const int64_t lines = N / 16 + 1;
+  int32_t* last_used = (int32_t*)malloc(sizeof(int32_t) * (size_t)lines);
+  int32_t* reuse = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
+  for (int64_t l = 0; l < lines; ++l) last_used[l] = -1;
+  for (int32_t i = 0; i < N; ++i)
+    for (int32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j) {
+      const int64_t l = col[j] / 16;
+      if (last_used[l] == -1) {
+        last_used[l] = i;
+        continue;
+      }
+      const int32_t d = i - last_used[l];
+      if (d <= i) reuse[d]++;
+      last_used[l] = i;
+    }
+  double sum = 0;
+  for (int32_t d = 0; d < 16 && d <= N; ++d) sum += reuse[d];
+  free(last_used);
+  free(reuse);
+  return (sum * 100) / (double)nnz;
+}

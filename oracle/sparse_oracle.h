@@ -221,6 +221,21 @@ void or_min_coo(int val_bytes, int32_t axis, const int32_t* row, const void* val
 void or_sum_coo_rows(int val_bytes, int32_t axis, const int32_t* row, const void* val,
                      void* out, int32_t N, int64_t nnz);
 
+/* ---------------- row reordering ---------------- */
+/* sort_rows_by_nnz: src/parallel/src/sparse32.js:2148-2218 (stable counting
+ * sort of rows by length; new CSR with rows in that order, columns kept).
+ * small_rows[q] = rows with at most q nonzeros (num_zero_rows ...
+ * num_three_rows). */
+void or_sort_rows_by_nnz(int val_bytes, const int32_t* row_ptr, const int32_t* col,
+                         const void* val, int32_t N, int32_t* nrow_ptr, int32_t* ncol,
+                         void* nval, int32_t* nnz_per_row, int32_t* permutation,
+                         int32_t* small_rows);
+/* sort_y_rows_by_nnz :2220-2235: y_new[permutation[i]] = y[i]. */
+void or_unpermute_rows(int val_bytes, const int32_t* permutation, const void* in, void* out,
+                       int32_t N);
+/* calculate_csr_locality_index :2238-2269. */
+double or_csr_locality_index(const int32_t* row_ptr, const int32_t* col, int32_t N, int64_t nnz);
+
 /* ---------------- Matrix Market input ---------------- */
 /* read_MM_header / calculate_actual_nnz / read_matrix_MM_files:
  * src/sequential/src/sparse32.js:1889-1981, on text split into lines at

@@ -359,6 +359,46 @@ def ell_from_host(indices, data, ncols, N, nnz=None):
                         nnz if nnz is not None else int(np.count_nonzero(data)))
 
 
+# --------------------------------------------------------------- row reordering
+
+
+def sort_rows_by_nnz(A_csr, stream=None):
+    """sort_rows_by_nnz (src/parallel/src/sparse32.js:2148-2218): a new CSR
+    with the rows stably sorted by their number of nonzeros, carrying
+    permutation_index (new -> old row), nnz_row_index and num_zero_rows ..
+    num_three_rows."""
+    N, nnz = A_csr.N, A_csr.nnz
+    B = allocate_CSR(N, nnz, A_csr.dtype)
+    B.nnz_row_index = DeviceArray(N, np.int32)
+    B.permutation_index = DeviceArray(N, np.int32)
+    small = (C.c_int32 * 4)()
+    call("sb_sort_rows_by_nnz", _dtcode(A_csr.dtype), A_csr.row_index.ptr, A_csr.col_index.ptr,
+         A_csr.val_index.ptr, N, nnz, B.row_index.ptr, B.col_index.ptr, B.val_index.ptr,
+         B.nnz_row_index.ptr, B.permutation_index.ptr, small, _sp(stream))
+    B.num_zero_rows, B.num_one_rows, B.num_two_rows, B.num_three_rows = (int(v) for v in small)
+    return B
+
+
+def sort_y_rows_by_nnz(y_view, A_csr, stream=None):
+    """sort_y_rows_by_nnz (src/parallel/src/sparse32.js:2220-2235): y_view
+    (computed with the reordered matrix) back in the original row order; the
+    view is given a new array, as the reference replaces y's buffer."""
+    N = A_csr.N
+    out = DeviceArray(N, y_view.dtype)
+    call("sb_unpermute_rows", _dtcode(y_view.dtype), A_csr.permutation_index.ptr,
+         y_view.vec_index.ptr, out.ptr, N, _sp(stream))
+    y_view.vec_index = out
+    return y_view
+
+
+def calculate_csr_locality_index(A_csr, stream=None) -> float:
+    """calculate_csr_locality_index (src/parallel/src/sparse32.js:2238-2269)."""
+    v = C.c_double(0.0)
+    call("sb_csr_locality_index", A_csr.row_index.ptr, A_csr.col_index.ptr, A_csr.N, A_csr.nnz,
+         C.byref(v), _sp(stream))
+    return float(v.value)
+
+
 # --------------------------------------------------------------- Matrix Market
 
 
