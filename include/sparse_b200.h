@@ -202,6 +202,13 @@ int sb_batch_exec_run(sb_batch_exec* exec, const sb_batch_item* items, int32_t n
 int sb_coo_csr(int dtype, const int32_t* row, const int32_t* col, const void* val, int32_t N,
                int64_t nnz, int32_t* csr_row_ptr, int32_t* csr_col, void* csr_val, void* stream);
 
+/* Replaces coo_csc (src/sequential/src/sparse32.js:1629-1671): the CSC
+ * (col_ptr[N+1], row[nnz], val[nnz]) with entries stably ordered by
+ * (col, row), as the reference's count / scatter / per-column stable sort. */
+int sb_coo_csc(int dtype, const int32_t* row, const int32_t* col, const void* val, int32_t N,
+               int64_t nnz, int32_t* csc_col_ptr, int32_t* csc_row, void* csc_val,
+               void* stream);
+
 /* Replaces num_cols (src/sequential/src/sparse32.js:1436-1447): the maximum
  * row length, returned to the host in *nc. */
 int sb_num_cols(const int32_t* row_ptr, int32_t N, int32_t* nc, void* stream);
@@ -274,6 +281,18 @@ int sb_spts_plan_reordered(const sb_spts_plan* plan, int32_t* row_ptr, int32_t* 
  * dependency wait that runs out is reported by sb_device_status (code 2). */
 int sb_spts_solve(const sb_spts_plan* plan, int algo, int policy, const void* b, void* y,
                   void* stream);
+
+/* Replaces spts_csc / spts_csc_wrapper (src/sequential/src/sparse_opt_32.wat:11-148;
+ * test driver src/sequential/src/sparse32.js:1845-1870): y = x, then for
+ * each column j, y_j /= L_jj (the column's first entry) and y_r -= L_rj*y_j
+ * for the rest of the column.  Every row thus subtracts in increasing column
+ * order before its division, the sync-free kernel's arithmetic on L in CSR,
+ * which is what runs here (after a device transpose); results are
+ * bit-identical to the reference's column sweep.  The matrix must be a CSC
+ * lower triangle with each column starting at its diagonal (SB_EINVAL
+ * otherwise).  Returns after the solve. */
+int sb_spts_csc(int dtype, const int32_t* col_ptr, const int32_t* row, const void* val,
+                int32_t N, int64_t nnz, const void* x, void* y, void* stream);
 
 /* Replaces the raw spts_csr_sync_free export on caller arrays without any
  * structural check: every dependency wait is bounded by spin_limit_cycles

@@ -71,6 +71,7 @@ _SIG = {
     "or_map_dia": ([C.c_int, C.c_int, C.c_double, _P, _P, _P, _I32, _I32, _I32], None),
     "or_fletcher_f32": ([_P, _I64], _I64),
     "or_fletcher_f64": ([_P, _I64], _I64),
+    "or_spts_csc": ([C.c_int, _P, _P, _P, _P, _P, _I32], None),
     "or_diagonal_coo": ([C.c_int, _I32, _P, _P, _P, _P, _I32, _I64], None),
     "or_min_coo": ([C.c_int, _I32, _P, _P, _P, _I32, _I64], None),
     "or_sum_coo_rows": ([C.c_int, _I32, _P, _P, _P, _I32, _I64], None),
@@ -510,3 +511,12 @@ def unpermute_rows(permutation, y):
 def csr_locality_index(row_ptr, col):
     row_ptr, col = _i32(row_ptr), _i32(col)
     return lib().or_csr_locality_index(_p(row_ptr), _p(col), row_ptr.size - 1, col.size)
+
+
+def spts_csc(col_ptr, row, val, x):
+    col_ptr, row, val = _i32(col_ptr), _i32(row), np.ascontiguousarray(val)
+    x = np.ascontiguousarray(x, val.dtype)
+    y = np.zeros(col_ptr.size - 1, val.dtype)
+    lib().or_spts_csc(val.dtype.itemsize, _p(col_ptr), _p(row), _p(val), _p(x), _p(y),
+                      col_ptr.size - 1)
+    return y

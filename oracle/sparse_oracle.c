@@ -1250,3 +1250,25 @@ double or_csr_locality_index(const int32_t* row_ptr, const int32_t* col, int32_t
   free(reuse);
   return (sum * 100) / (double)nnz;
 }
+
+/* ======================= CSC SpTS ======================= */
+
+#define OR_SPTS_CSC(T, SFX)                                                                   \
+  static void spts_csc_##SFX(const int32_t* cp, const int32_t* row, const T* val, const T* x, \
+                             T* y, int32_t N) {                                               \
+    for (int32_t j = 0; j < N; ++j) y[j] = x[j];                                              \
+    for (int32_t j = 0; j < N; ++j) {                                                         \
+      const int32_t s = cp[j], e = cp[j + 1];                                                 \
+      y[j] = y[j] / val[s];                                                                   \
+      for (int32_t q = s + 1; q < e; ++q) y[row[q]] = y[row[q]] - val[q] * y[j];              \
+    }                                                                                         \
+  }
+OR_SPTS_CSC(float, f32)
+OR_SPTS_CSC(double, f64)
+
+void or_spts_csc(int w, const int32_t* cp, const int32_t* row, const void* val, const void* x,
+                 void* y, int32_t N) {
+  if (N <= 0) return;
+  if (w == 4) spts_csc_f32(cp, row, (const float*)val, (const float*)x, (float*)y, N);
+  else spts_csc_f64(cp, row, (const double*)val, (const double*)x, (double*)y, N);
+}

@@ -207,6 +207,12 @@ void or_map(int val_bytes, int kind, int op, double p, const void* in, void* out
 void or_map_dia(int val_bytes, int op, double p, const int32_t* offset, const void* in,
                 void* out, int32_t nd, int32_t stride, int32_t N);
 
+/* spts_csc: src/sequential/src/sparse_opt_32.wat:11-148 (y = x; per column
+ * j: y_j /= first entry; y_r -= L_rj*y_j for the rest of the column; the
+ * 4-wide SIMD body rounds each lane like the scalar one). */
+void or_spts_csc(int val_bytes, const int32_t* col_ptr, const int32_t* row, const void* val,
+                 const void* x, void* y, int32_t N);
+
 /* ---------------- COO reductions ---------------- */
 /* diagonal_coo :1707-1798: the pointer walk over a row-sorted COO; diag
  * holds N - |k| slots and must be zero-filled (create_vec). */

@@ -382,4 +382,11 @@ int sb_csr_dia(int dtype, const int32_t* row_ptr, const int32_t* col, const void
   return SB_OK;
 }
 
+int sb_coo_csc(int dtype, const int32_t* row, const int32_t* col, const void* val, int32_t N,
+               int64_t nnz, int32_t* csc_col_ptr, int32_t* csc_row, void* csc_val,
+               void* stream) {
+  // coo_csc is coo_csr with the roles of rows and columns swapped
+  return sb_coo_csr(dtype, col, row, val, N, nnz, csc_col_ptr, csc_row, csc_val, stream);
+}
+
 }  // extern "C"

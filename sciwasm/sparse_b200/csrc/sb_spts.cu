@@ -580,6 +580,18 @@ __global__ void growth_kernel(const int* __restrict__ row_ptr, const T* __restri
   if ((threadIdx.x & 31) == 0) atomicMax(out, b);
 }
 
+// flags[0] = 1 unless every column j of a CSC lower triangle is non-empty,
+// starts with its diagonal (row j) and has all other rows in (j, N).
+__global__ void csc_lower_check(const int* __restrict__ col_ptr, const int* __restrict__ row,
+                                int N, int* __restrict__ flags) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  const int s = col_ptr[j], e = col_ptr[j + 1];
+  bool ok = e > s && row[s] == j;
+  for (int q = s + 1; ok && q < e; ++q) ok = row[q] > j && row[q] < N;
+  if (!ok) flags[0] = 1;
+}
+
 static int resident_grid(const void* kern) {
   int per = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kT, 0);
@@ -1217,6 +1229,45 @@ int sb_spts_syncfree_csr(int dtype, const int32_t* row_ptr, const int32_t* col, 
     return SB_ETIMEOUT;
   }
   return SB_OK;
+}
+
+int sb_spts_csc(int dtype, const int32_t* col_ptr, const int32_t* row, const void* val,
+                int32_t N, int64_t nnz, const void* x, void* y, void* stream) {
+  SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_spts_csc: dtype must be F32 or F64");
+  SB_REQUIRE(N >= 0 && nnz >= 0 && nnz <= 0x7fffffffLL, "sb_spts_csc: bad size");
+  if (N == 0) return SB_OK;
+  SB_REQUIRE(col_ptr && row && val && x && y, "sb_spts_csc: null pointer");
+  int r = ensure_device();
+  if (r) return r;
+  cudaStream_t st = as_stream(stream);
+  const size_t vb = dtype_size(dtype);
+  void* mem = nullptr;
+  // [flag] [CSR row_ptr N+1] [CSR col nnz] [CSR val nnz]
+  const size_t off_rp = 16, off_col = off_rp + sizeof(int) * ((size_t)N + 1);
+  const size_t off_val = (off_col + sizeof(int) * (size_t)nnz + 15) / 16 * 16;
+  if ((r = scratch_alloc(&mem, off_val + vb * (size_t)nnz, st))) return r;
+  char* p = (char*)mem;
+  int* flag = (int*)p;
+  int* rp = (int*)(p + off_rp);
+  int* col = (int*)(p + off_col);
+  void* cval = p + off_val;
+  SB_CHECK_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
+  csc_lower_check<<<grid1(N), kT, 0, st>>>(col_ptr, row, N, flag);
+  SB_CHECK_LAUNCH("csc_lower_check");
+  int h = 0;
+  SB_CHECK_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SB_CHECK_CUDA(cudaStreamSynchronize(st));
+  if (h) {
+    scratch_free(mem, st);
+    set_error("sb_spts_csc: every column must start with its diagonal, the other rows below it");
+    return SB_EINVAL;
+  }
+  // the CSC arrays are the CSR of L^T; its transpose is L in CSR with each
+  // row's entries in increasing column order (diagonal last)
+  r = sb_transpose_csr(dtype, col_ptr, row, val, N, nnz, rp, col, cval, stream);
+  if (!r) r = sb_spts_syncfree_csr(dtype, rp, col, cval, N, x, y, 0, stream);
+  scratch_free(mem, st);
+  return r;
 }
 
 }  // extern "C"

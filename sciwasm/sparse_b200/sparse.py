@@ -186,6 +186,28 @@ def sum_coo(A_coo, axis=1, stream=None):
     return v
 
 
+class sparse_CSC_t:
+    """CSC matrix (src/sequential/src/sparse32.js:112-121): col_index (ncols+1
+    column pointers), row_index / val_index (nnz)."""
+
+    def __init__(self, col_index, row_index, val_index, ncols, nnz):
+        self.col_index, self.row_index, self.val_index = col_index, row_index, val_index
+        self.ncols, self.nnz = int(ncols), int(nnz)
+
+    @property
+    def dtype(self):
+        return self.val_index.dtype
+
+    def col_array(self):
+        return self.col_index.to_host()
+
+    def row_array(self):
+        return self.row_index.to_host()
+
+    def val_array(self):
+        return self.val_index.to_host()
+
+
 class sparse_CSR_t:
     """CSR matrix: row_index (N+1), col_index / val_index (nnz)."""
 
@@ -616,6 +638,28 @@ def coo_csr(A_coo, stream=None):
          A_coo.val_index.ptr, A_coo.N, A_coo.nnz, A.row_index.ptr, A.col_index.ptr,
          A.val_index.ptr, _sp(stream))
     return A
+
+
+def coo_csc(A_coo, stream=None):
+    """coo_csc (src/sequential/src/sparse32.js:1629-1671): a new CSC, entries
+    stably ordered by (col, row)."""
+    N, nnz = A_coo.N, A_coo.nnz
+    B = sparse_CSC_t(DeviceArray(N + 1, np.int32), DeviceArray(nnz, np.int32),
+                     DeviceArray(nnz, A_coo.dtype), N, nnz)
+    call("sb_coo_csc", _dtcode(A_coo.dtype), A_coo.row_index.ptr, A_coo.col_index.ptr,
+         A_coo.val_index.ptr, N, nnz, B.col_index.ptr, B.row_index.ptr, B.val_index.ptr,
+         _sp(stream))
+    return B
+
+
+def spts_csc(A_csc, x_view, y_view, stream=None):
+    """spts_csc (src/sequential/src/sparse_opt_32.wat:11-148): solve L y = x
+    for a CSC lower triangle whose columns start with their diagonal."""
+    if x_view.dtype != A_csc.dtype or y_view.dtype != A_csc.dtype:
+        raise TypeError("x, y and the matrix must share one value dtype")
+    call("sb_spts_csc", _dtcode(A_csc.dtype), A_csc.col_index.ptr, A_csc.row_index.ptr,
+         A_csc.val_index.ptr, A_csc.ncols, A_csc.nnz, x_view.vec_index.ptr,
+         y_view.vec_index.ptr, _sp(stream))
 
 
 def num_cols(A_csr, stream=None) -> int:
