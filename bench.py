@@ -277,6 +277,7 @@ def run_ours(args, jobs, config, rank, world, local_rank):
     import torch
     import sciwasm.sparse_b200 as sb
     from sciwasm.sparse_b200 import _lib, synth
+    from sciwasm.sparse_b200.dist import max_over_ranks
 
     sb.load_library()
     torch.cuda.set_device(local_rank)
@@ -384,10 +385,7 @@ def run_ours(args, jobs, config, rank, world, local_rank):
     elapsed_ms = t_start.elapsed_time(t_end)
     per_obj_ms = [float(np.mean([evs[s][k][0].elapsed_time(evs[s][k][1])
                                  for s in range(args.steps)])) for k in range(len(objs))]
-    if dist:
-        t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, device="cuda")
     value = bytes_step * args.steps * world / (elapsed_ms / 1e3) / 1e9
 
     # ---------------- e2e through the public API with host buffers
@@ -427,10 +425,7 @@ def run_ours(args, jobs, config, rank, world, local_rank):
         e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, device="cuda")
     e2e_value = bytes_step * args.steps * world / (e2e_ms / 1e3) / 1e9
     for xp, yp, yo, _ in host:
         for p in (xp, yp, yo):

@@ -1,0 +1,85 @@
+"""Row-sharded SpMV across processes (one per GPU) and the multi-process
+timing helper.
+
+SpMV shards by contiguous row blocks balanced by nonzeros, the partition the
+reference's worker pool uses (static_nnz, src/parallel/src/sparse32.js:2769-2821):
+every rank keeps its block of rows resident and the whole x, computes its own
+y rows with the library's kernels, and the y blocks are disjoint, so the
+data path needs no reduction; `gather_rows` assembles the full y where a
+caller needs it (one all-gather).  `max_over_ranks` is the timing rule of
+multi-GPU measurements: the slowest rank's time.
+
+The torch.distributed calls run on whatever backend the process group has
+(NCCL on GPUs, gloo for host-side tests).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .sparse import DeviceArray, sparse_CSR_t, spmv, static_nnz
+
+
+def shard_rows(row_ptr, world: int):
+    """(row_start, row_end) of every rank: static_nnz over `world` parts."""
+    return static_nnz(row_ptr, world)
+
+
+def local_block(row_ptr, col, val, r0: int, r1: int):
+    """Host arrays of rows [r0, r1) as a CSR of r1 - r0 rows (columns keep
+    their global numbering, so the block multiplies the full x)."""
+    row_ptr = np.asarray(row_ptr, np.int64)
+    s, e = int(row_ptr[r0]), int(row_ptr[r1])
+    rp = (row_ptr[r0:r1 + 1] - s).astype(np.int32)
+    return rp, np.asarray(col)[s:e], np.asarray(val)[s:e]
+
+
+class RowShardedCSR:
+    """This rank's row block of a CSR matrix, resident on its device.  The
+    block is a CSR of r1 - r0 rows whose columns keep their global numbers;
+    the kernels index x by column, so x holds all N entries and y only this
+    rank's rows."""
+
+    def __init__(self, row_ptr, col, val, rank: int, world: int):
+        starts, ends = shard_rows(row_ptr, world)
+        self.rank, self.world = int(rank), int(world)
+        self.starts, self.ends = starts, ends
+        self.r0, self.r1 = int(starts[rank]), int(ends[rank])
+        self.N = int(np.asarray(row_ptr).size - 1)
+        self.rows = self.r1 - self.r0
+        rp, c, v = local_block(row_ptr, col, val, self.r0, self.r1)
+        if c.size and (int(np.min(c)) < 0 or int(np.max(c)) >= self.N):
+            raise ValueError("column outside the matrix")
+        self.A = sparse_CSR_t(DeviceArray.from_host(rp), DeviceArray.from_host(c),
+                              DeviceArray.from_host(np.ascontiguousarray(v)), self.rows,
+                              c.size) if self.rows > 0 else None
+
+    def spmv(self, x_view, y_view, inner_max=1, stream=None):
+        """y_view (this rank's rows) += A[r0:r1, :] x_view (all N entries)."""
+        if self.A is not None:
+            spmv(self.A, x_view, y_view, inner_max, stream)
+
+
+def gather_rows(y_local, starts, ends, group=None):
+    """All-gather of the ranks' y blocks (torch tensors, 1-D) into the full y
+    on every rank; blocks may differ in length."""
+    import torch
+    import torch.distributed as dist
+    world = len(starts)
+    counts = [int(e - s) for s, e in zip(starts, ends)]
+    top = max(counts) if counts else 0
+    buf = torch.zeros(top, dtype=y_local.dtype, device=y_local.device)
+    buf[:y_local.numel()] = y_local
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    return torch.cat([p[:c] for p, c in zip(parts, counts)])
+
+
+def max_over_ranks(value: float, device=None, group=None) -> float:
+    """The largest `value` over all ranks (the time of the slowest rank)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
