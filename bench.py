@@ -35,7 +35,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-SECTIONS = ("batched", "laplacian4096_fp32", "spts", "serving")
+SECTIONS = ("batched", "laplacian4096_fp32", "spts", "serving", "powerlaw_csr")
 METRIC = "served SpMV/SpTS req/s + p99 vs plain path; SpMV HBM GB/s at \u22641e-5 rel err"
 UNIT = "GB/s"
 
@@ -656,6 +656,35 @@ def run_laplacian_large(stream, peak):
     return out
 
 
+def run_powerlaw_csr(stream, peak, opts=None, small=False):
+    """CSR SpMV, FP64, on the power-law matrix of the format sweep (2M rows,
+    ~41M nonzeros; 500k rows with small), autotuned or with fixed options
+    "lanes,unroll,grid"."""
+    import torch
+    import sciwasm.sparse_b200 as sb
+    from sciwasm.sparse_b200 import _lib, synth
+    n = 500_000 if small else 2_000_000
+    rp, col, val = synth.power_law(n, seed=2, dtype=np.float64)
+    A = sb.csr_from_host(rp, col, val)
+    x = sb.vec_from_host(synth.uniform_vec(n, 0))
+    y = sb.create_vec(n, 0, np.float64)
+    sp = stream.cuda_stream
+    if opts:
+        lanes, unroll, grid = (int(v) for v in opts.split(","))
+        A.opts = _lib.CsrOpts(0, lanes, unroll, grid)
+        tuned = {"kernel": 0, "lanes_per_row": lanes, "unroll": unroll, "grid": grid}
+    else:
+        tuned = sb.csr_autotune(A, x, stream=sp)
+    for _ in range(3):
+        with torch.cuda.stream(stream):
+            sb.spmv(A, x, y, stream=sp)
+    ms = _time_each_ms(stream, lambda: sb.spmv(A, x, y, stream=sp), 20)
+    nbytes = algo_bytes("csr", n, col.size, 8)
+    gbs = nbytes / (ms / 1e3) / 1e9
+    return {"N": n, "nnz": int(col.size), "ms": round(ms, 4), "GB_s": round(gbs, 1),
+            "frac": round(gbs / peak, 3), "opts": tuned}
+
+
 def run_batched(stream, peak, n_mats=512, seed=5):
     """Batched CSR SpMV: n_mats matrices with rows log-uniform in [1e3, 2e5],
     Poisson(12) off-diagonals plus the diagonal per row, values U[-1,1] stored
@@ -824,6 +853,14 @@ def run_serving(args):
     for r in reqs:
         r.t_done = -1.0
     plain = srv.serve(reqs, "plain")
+    # capacity: the same kind of requests all present at t = 0 (a backlog),
+    # so that the rate is the server's, not the arrival process's
+    burst = [serve.Request(r.rid, 0.0, r.matrix, r.op, r.storage, r.x, r.y) for r in reqs]
+    cap_b = srv.serve(burst, "batched")
+    cap_p = srv.serve(burst[:max(1, len(burst) // 10)], "plain")
+    capacity = {"batched_req_per_s": round(cap_b["req_per_s"], 1),
+                "plain_req_per_s": round(cap_p["req_per_s"], 1),
+                "batched_requests": cap_b["requests"], "plain_requests": cap_p["requests"]}
     errs = serving_errors(pool, srv, mv, ts)
     rows = np.array([pool.mats[r.matrix].N for r in reqs])
     bytes_io = int(np.sum(rows) * 8)
@@ -841,6 +878,7 @@ def run_serving(args):
         "flagged_f64_factors": sum(1 for n in ts if pool.mats[n].policy["f32"] == "f64"),
         "batched": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in batched.items()},
         "plain": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in plain.items()},
+        "capacity_backlog": capacity,
         "max_rel_err_vs_fp64": errs,
         "slots": {"spmv": args.serve_slots, "spts": args.serve_spts_slots},
         "max_batch": {"spmv": args.serve_batch, "spts": args.serve_spts_batch},
@@ -876,6 +914,8 @@ def main():
     ap.add_argument("--workload", default="format_sweep_fp64",
                     help="format_sweep_fp64 (the bench line), laplacian_fp32, or one section "
                          "alone: " + ", ".join(SECTIONS))
+    ap.add_argument("--csr-opts", default=None,
+                    help="powerlaw_csr: fixed CSR options lanes,unroll,grid (else autotuned)")
     ap.add_argument("--batch-mats", type=int, default=512,
                     help="matrices of the batched section when run alone")
     ap.add_argument("--small", action="store_true",
@@ -923,6 +963,8 @@ def main():
             out = run_laplacian_large(stream, peak)
         elif args.workload == "spts":
             out = run_spts_section(stream)
+        elif args.workload == "powerlaw_csr":
+            out = run_powerlaw_csr(stream, peak, args.csr_opts, args.small)
         else:
             out = run_serving(args)
         print(json.dumps({"workload": args.workload, "result": out}), flush=True)

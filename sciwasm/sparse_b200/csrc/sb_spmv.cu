@@ -559,10 +559,35 @@ template <typename T>
 __global__ void __launch_bounds__(256)
     dia_row_kernel(const int* __restrict__ offset, const T* __restrict__ data, int N, int nd,
                    int stride, const T* __restrict__ x, T* __restrict__ y) {
+  // smallest and largest offset (whatever their order), for the interior test
+  __shared__ int kext[2];
+  if (threadIdx.x == 0) {
+    kext[0] = 0x7fffffff;
+    kext[1] = -0x7fffffff - 1;
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < nd; d += blockDim.x) {
+    const int k = __ldg(offset + d);
+    atomicMin(&kext[0], k);
+    atomicMax(&kext[1], k);
+  }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   T t = y[i];
   const long long move = (long long)N - stride;
+  // interior rows (every diagonal in band) walk the diagonals with pointer
+  // increments and no predicates
+  const int kmin = kext[0], kmax = kext[1];
+  if (move == 0 && (long long)i + kmin >= 0 && (long long)i + kmax < N) {
+    const T* dp = data + i;
+    const T* xp = x + i;
+#pragma unroll 4
+    for (int d = 0; d < nd; ++d, dp += stride)
+      t = add_rn(mul_rn(ld_stream(dp), ld_ro(xp + __ldg(offset + d))), t);
+    y[i] = t;
+    return;
+  }
 #pragma unroll 4
   for (int d = 0; d < nd; ++d) {
     const int k = __ldg(offset + d);
