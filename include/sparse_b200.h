@@ -108,8 +108,10 @@ int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const voi
 /* Kernel choice for CSR SpMV (no counterpart in the reference, whose
  * parallel harness picks among unrolled CSR variants per run,
  * src/parallel/tests/main32.js:150-313).  kernel 0 = row blocks (default),
- * 1 = streamed nonzero tiles; lanes_per_row 1..32 (power of two) and
- * unroll 2/4/8 tune the row-block kernel, 0 = chosen from the mean row
+ * 1 = streamed nonzero tiles, 2 = nonzero tiles over row-aligned warp
+ * ranges (unroll = 256-nonzero tiles per warp, 1..64; F32, F64 and BF16;
+ * every row written once, no atomics); lanes_per_row 1..32 (power of two)
+ * and unroll 2/4/8 tune the row-block kernel, 0 = chosen from the mean row
  * length; grid 0 = a resident grid striding over 32-row blocks (regular
  * rows), 1 = one warp per 32-row block (skewed row lengths). */
 typedef struct sb_csr_opts {

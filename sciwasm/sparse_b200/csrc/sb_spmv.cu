@@ -9,13 +9,15 @@
 //     adaptive rows per warp) with unrolled independent loads and shuffle
 //     reductions, and the long ones with the whole warp.  An alternative
 //     streams fixed-size nonzero tiles into a shared-memory ring with bulk
-//     async copies (SB_CSR_KERNEL=s).
+//     async copies (SB_CSR_KERNEL=s); a third cuts the nonzeros into
+//     row-aligned warp ranges walked in 256-nonzero tiles (kernel 2).
 //   * COO is the same tile scheme keyed on the row array; every row segment
 //     is added with one atomic, so unsorted input is accepted.
 //   * DIA and ELL assign one row per thread and keep the reference's per-row
 //     addition order (separately rounded mul and add), so their results are
 //     bit-identical to the reference's serial loops.
 #include <algorithm>
+#include <climits>
 #include <stdlib.h>
 
 #include "sb_common.cuh"
@@ -542,6 +544,223 @@ __global__ void __launch_bounds__(kWarpsPerCta * kWarp)
   }
 }
 
+// ------------------------------------------------------------ CSR (nonzero tiles)
+
+// 8 consecutive stored values from a 16-byte aligned index k0 (a multiple of
+// 8), widened to the accumulation type.
+template <typename SV, typename T>
+__device__ __forceinline__ void load_vals8(const SV* __restrict__ val, long long k0, T (&v)[kItems]) {
+  if constexpr (sizeof(SV) == 8) {
+#pragma unroll
+    for (int h = 0; h < kItems; h += 2) {
+      const double2 w = ld_stream_v2(reinterpret_cast<const double*>(val) + k0 + h);
+      v[h] = w.x;
+      v[h + 1] = w.y;
+    }
+  } else if constexpr (sizeof(SV) == 4) {
+#pragma unroll
+    for (int h = 0; h < kItems; h += 4) {
+      const float4 w = ld_stream_v4(reinterpret_cast<const float*>(val) + k0 + h);
+      v[h] = w.x;
+      v[h + 1] = w.y;
+      v[h + 2] = w.z;
+      v[h + 3] = w.w;
+    }
+  } else {  // BF16: 8 values in one 16-byte word, element 2i in the low half of word i
+    const int4 w = ld_stream_v4(reinterpret_cast<const int*>(val) + k0 / 2);
+    const int ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      v[2 * h] = __uint_as_float((unsigned)ws[h] << 16);
+      v[2 * h + 1] = __uint_as_float((unsigned)ws[h] & 0xffff0000u);
+    }
+  }
+}
+
+// Nonzero-tile CSR: the nonzeros are cut into ranges of `items` (whole
+// 256-item warp tiles) and every cut is moved forward to the next row start,
+// so each row lies in exactly one warp's range and is written once, without
+// atomics, in an order fixed by the matrix and the range size
+// (y[row] += sum; rows without entries are not written).  A warp walks its
+// range in tiles of 256 nonzeros, 8 consecutive ones per lane loaded with
+// 16-byte vector loads and their 8 x gathers in flight together.  Each
+// item's row comes from row_ptr: the starts of the rows that begin inside
+// the tile are marked in a per-warp shared array (the largest row index wins
+// a position, which skips empty rows) and a prefix maximum over the
+// positions gives every item its row.  Row sums are combined by a segmented
+// scan across the lanes; the tile's last run is carried in registers into
+// the next tile.
+template <typename SV, typename T, bool VEC>
+__global__ void __launch_bounds__(kWarpsPerCta * kWarp)
+    csr_tile_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
+                    const SV* __restrict__ val, const T* __restrict__ x, T* __restrict__ y, int N,
+                    long long nnz, long long items) {
+  __shared__ __align__(16) int mark_all[kWarpsPerCta][kTile];
+  const int lane = threadIdx.x & (kWarp - 1);
+  int* mark = mark_all[threadIdx.x >> 5];
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long b_lo = gw * items;
+  if (b_lo >= nnz) return;
+  const long long b_hi = b_lo + items;
+  // The warp owns the rows whose start lies in [b_lo, b_hi): from r_lo, the
+  // first row starting at or after b_lo, up to the first row starting at or
+  // after b_hi, which is found while walking (its start is k_hi).
+  const int r_lo = b_lo == 0 ? 0 : row_of_item(row_ptr, N, b_lo - 1, lane) + 1;
+  if (r_lo >= N) return;
+  const long long k_lo = __ldg(row_ptr + r_lo);
+  if (k_lo >= b_hi || k_lo >= nnz) return;
+  long long k_hi = nnz;
+  bool hi_known = false;
+  int next_row = r_lo;  // first row whose start is not yet marked
+  int base_row = -1;    // row of the item before the tile
+  int carry_row = -1;   // row of the previous tile's last run, still open
+  T carry = 0;
+  for (long long kt = k_lo & ~7LL; kt < k_hi; kt += kTile) {
+    // the tile's col/val and x gathers first, so that they are in flight
+    // while the row starts are read (items found below to lie past the
+    // range end get a zero product)
+    const long long k0 = kt + (long long)kItems * lane;
+    int c[kItems];
+    T v[kItems];
+    if (VEC && k0 + kItems <= nnz) {
+      const int4 c0 = ld_stream_v4(col + k0), c1 = ld_stream_v4(col + k0 + 4);
+      c[0] = c0.x; c[1] = c0.y; c[2] = c0.z; c[3] = c0.w;
+      c[4] = c1.x; c[5] = c1.y; c[6] = c1.z; c[7] = c1.w;
+      load_vals8<SV, T>(val, k0, v);
+    } else {
+#pragma unroll
+      for (int e = 0; e < kItems; ++e) {
+        const long long k = k0 + e;
+        c[e] = k < nnz ? ld_stream(col + k) : 0;
+        v[e] = k < nnz ? (T)ld_val(val + k) : (T)0;
+      }
+    }
+    T p[kItems];
+#pragma unroll
+    for (int e = 0; e < kItems; ++e) {
+      const long long k = k0 + e;
+      p[e] = (k >= k_lo && k < k_hi) ? v[e] * ld_ro(x + c[e]) : (T)0;
+    }
+    *reinterpret_cast<int4*>(mark + kItems * lane) = make_int4(-1, -1, -1, -1);
+    *reinterpret_cast<int4*>(mark + kItems * lane + 4) = make_int4(-1, -1, -1, -1);
+    __syncwarp();
+    const long long lim = min(kt + kTile, k_hi);
+    while (true) {  // row starts are non-decreasing: the rows inside form a prefix
+      const int j = next_row + lane;
+      const long long s = j < N ? (long long)__ldg(row_ptr + j) : LLONG_MAX;
+      if (!hi_known) {
+        const unsigned h = __ballot_sync(kFull, s >= b_hi);
+        if (h) {
+          hi_known = true;
+          k_hi = min(__shfl_sync(kFull, s, __ffs(h) - 1), nnz);
+        }
+      }
+      const bool in = s < min(lim, k_hi);
+      if (in) atomicMax(mark + (int)(s - kt), j);
+      const unsigned b = __ballot_sync(kFull, in);
+      next_row += __popc(b);
+      if (b != kFull) break;
+    }
+#pragma unroll
+    for (int e = 0; e < kItems; ++e)
+      if (k0 + e >= k_hi) p[e] = 0;
+    __syncwarp();
+    // rows: prefix maximum of the marks (items outside [k_lo, k_hi) join the
+    // first or last row of the range with a zero product)
+    const int4 m0 = *reinterpret_cast<const int4*>(mark + kItems * lane);
+    const int4 m1 = *reinterpret_cast<const int4*>(mark + kItems * lane + 4);
+    int r[kItems] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+#pragma unroll
+    for (int e = 1; e < kItems; ++e) r[e] = max(r[e], r[e - 1]);
+    int incl = r[kItems - 1];
+#pragma unroll
+    for (int off = 1; off < kWarp; off <<= 1) {
+      const int t = __shfl_up_sync(kFull, incl, off);
+      if (lane >= off) incl = max(incl, t);
+    }
+    int before = __shfl_up_sync(kFull, incl, 1);
+    before = max(lane == 0 ? -1 : before, base_row);
+#pragma unroll
+    for (int e = 0; e < kItems; ++e) r[e] = max(r[e], before);
+    if (base_row < 0) {  // first tile: items before k_lo take the row that starts at k_lo
+      const int fr = mark[(int)(k_lo - kt)];
+#pragma unroll
+      for (int e = 0; e < kItems; ++e)
+        if (r[e] < 0) r[e] = fr;
+    }
+    __syncwarp();
+    // the open row of the previous tile: continued by lane 0, or finished
+    const int r00 = __shfl_sync(kFull, r[0], 0);
+    if (carry_row >= 0 && r00 != carry_row) {
+      if (lane == 0) y[carry_row] += carry;
+      carry_row = -1;
+    }
+    if (lane == 0 && carry_row >= 0) p[0] = carry + p[0];
+    // lane-local runs; the runs strictly inside a lane are whole rows
+    const int start_row = r[0];
+    int cur = start_row;
+    T acc = 0, first_val = 0;
+    bool internal = false;
+#pragma unroll
+    for (int e = 0; e < kItems; ++e) {
+      if (r[e] != cur) {
+        if (!internal) {
+          internal = true;
+          first_val = acc;
+        } else {
+          y[cur] += acc;
+        }
+        cur = r[e];
+        acc = 0;
+      }
+      acc += p[e];
+    }
+    const int end_row = cur;
+    const int prev_end = __shfl_up_sync(kFull, end_row, 1);
+    const bool cont_prev = lane > 0 && start_row == prev_end;
+    bool hf = internal || !cont_prev;  // this lane's last run does not continue the previous lane's
+    T sum = acc;
+#pragma unroll
+    for (int off = 1; off < kWarp; off <<= 1) {
+      const T o = __shfl_up_sync(kFull, sum, off);
+      const bool f = __shfl_up_sync(kFull, hf, off);
+      if (lane >= off) {
+        if (!hf) sum += o;
+        hf = hf || f;
+      }
+    }
+    const T from_prev = __shfl_up_sync(kFull, sum, 1);
+    if (internal) y[start_row] += first_val + (cont_prev ? from_prev : (T)0);
+    const int next_start = __shfl_down_sync(kFull, start_row, 1);
+    if (lane < kWarp - 1 && next_start != end_row) y[end_row] += sum;
+    carry_row = __shfl_sync(kFull, end_row, kWarp - 1);
+    carry = __shfl_sync(kFull, sum, kWarp - 1);
+    base_row = carry_row;
+  }
+  if (lane == 0 && carry_row >= 0) y[carry_row] += carry;
+}
+
+template <typename SV, typename T>
+static int launch_csr_tiles(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
+                            int N, long long nnz, int tiles_per_warp, cudaStream_t st) {
+  const long long items = (long long)std::max(1, std::min(tiles_per_warp, 64)) * kTile;
+  const long long warps = (nnz + items - 1) / items;
+  const long long ctas = (warps + kWarpsPerCta - 1) / kWarpsPerCta;
+  if (ctas > 0x7fffffffLL) {
+    set_error("sb_spmv_csr: too many nonzero tiles");
+    return SB_EINVAL;
+  }
+  const int threads = kWarpsPerCta * kWarp;
+  if (aligned16(col) && aligned16(val))
+    csr_tile_kernel<SV, T, true><<<(unsigned)ctas, threads, 0, st>>>(row_ptr, col, val, x, y, N,
+                                                                     nnz, items);
+  else
+    csr_tile_kernel<SV, T, false><<<(unsigned)ctas, threads, 0, st>>>(row_ptr, col, val, x, y, N,
+                                                                      nnz, items);
+  SB_CHECK_LAUNCH("csr_tile_kernel");
+  return SB_OK;
+}
+
 // ------------------------------------------------------------ DIA / ELL
 
 template <typename T> __device__ __forceinline__ T mul_rn(T a, T b);
@@ -681,6 +900,7 @@ template <typename S, typename A>
 static int launch_csr(const int* row_ptr, const int* col, const S* val, const S* x, S* y, int N,
                       long long nnz, const sb_csr_opts* opts, cudaStream_t st) {
   const int kernel = opts ? opts->kernel : (csr_kernel_choice() == 2 ? 1 : 0);
+  if (kernel == 2) return launch_csr_tiles<S, S>(row_ptr, col, val, x, y, N, nnz, opts->unroll, st);
   if (kernel == 1 && aligned16(col) && aligned16(val)) {
     const int tile = (opts && opts->unroll == 2048) ? 2048 : csr_stream_tile();
     if (tile == 2048) return launch_csr_stream<S, 2048, 3>(row_ptr, col, val, x, y, N, nnz, st);
@@ -729,7 +949,7 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
   SB_REQUIRE(N >= 0 && nnz >= 0 && inner_max >= 0, "sb_spmv_csr: negative size");
   SB_REQUIRE(nnz <= 0x7fffffffLL, "sb_spmv_csr: nnz exceeds int32 row_ptr range");
   if (opts) {
-    SB_REQUIRE(opts->kernel == 0 || opts->kernel == 1, "sb_spmv_csr: unknown kernel %d",
+    SB_REQUIRE(opts->kernel >= 0 && opts->kernel <= 2, "sb_spmv_csr: unknown kernel %d",
                opts->kernel);
     const int l = opts->lanes_per_row;
     SB_REQUIRE(l == 0 || l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32,
@@ -741,7 +961,11 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
   if ((r = ensure_device())) return r;
   cudaStream_t st = as_stream(stream);
   for (int it = 0; it < inner_max; ++it) {
-    if (dtype == SB_BF16)
+    if (dtype == SB_BF16 && opts && opts->kernel == 2)
+      r = launch_csr_tiles<__nv_bfloat16, float>(row_ptr, col, (const __nv_bfloat16*)val,
+                                                 (const float*)x, (float*)y, N, nnz, opts->unroll,
+                                                 st);
+    else if (dtype == SB_BF16)
       r = launch_csr_rows<__nv_bfloat16, float>(row_ptr, col, (const __nv_bfloat16*)val,
                                                 (const float*)x, (float*)y, N, nnz,
                                                 opts ? opts->lanes_per_row : 0,
@@ -781,8 +1005,8 @@ int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const
   if (reps <= 0) reps = 5;
   cudaStream_t st = as_stream(stream);
   // candidates around the mean row length: lanes in {d/4, d/2, d, 2d}, unroll {2, 4, 8},
-  // both grids,
-  // plus the streamed-tile kernel
+  // both grids, plus the streamed-tile kernel and the nonzero-tile kernel with
+  // 8 tiles per warp
   const int d = default_lanes(N, nnz);
   sb_csr_opts cand[32];
   int nc = 0;
@@ -792,6 +1016,7 @@ int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const
       for (int g : {0, 1}) cand[nc++] = sb_csr_opts{0, lanes, u, g};
   }
   cand[nc++] = sb_csr_opts{1, 0, 1024, 0};
+  cand[nc++] = sb_csr_opts{2, 0, 8, 0};
   void* ywork = nullptr;
   const size_t ysize = dtype == SB_BF16 ? sizeof(float) : dtype_size(dtype);  // y is f32 for BF16
   if ((r = scratch_alloc(&ywork, ysize * (size_t)N, st))) return r;

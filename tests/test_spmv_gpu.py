@@ -158,6 +158,35 @@ def _csr_check_all(sb, orc):
             assert err <= TOL[np.dtype(dt)], (name, dt, err)
 
 
+@pytest.mark.parametrize("storage", ["f32", "f64", "bf16"])
+@pytest.mark.parametrize("tiles", [1, 4, 16])
+def test_csr_nonzero_tile_kernel(gpu, oracle, storage, tiles):
+    """Kernel 2 (row-aligned nonzero ranges, 256-nonzero tiles): within the
+    tolerance of the exact result, rows without entries keep their bits, and
+    two runs give identical bits (every row is written once, no atomics)."""
+    from sciwasm.sparse_b200 import _lib
+    dt = np.float64 if storage == "f64" else np.float32
+    for name, (rp, col, val) in _mats(dt).items():
+        N = rp.size - 1
+        x, y0 = _x_y(N, dt)
+        A = gpu.csr_from_host(rp, col, val)
+        vals = val
+        if storage == "bf16":
+            A = gpu.csr_with_storage(A, "bf16")
+            vals = (A.val_array().astype(np.uint32) << 16).view(np.float32)
+        A.opts = _lib.CsrOpts(2, 0, tiles, 0)
+        outs = []
+        for _ in range(2):
+            xv, yv = gpu.vec_from_host(x), gpu.vec_from_host(y0)
+            gpu.spmv(A, xv, yv)
+            outs.append(yv.array())
+        truth = oracle.truth_csr(rp, col, vals, x, y0)
+        assert rel_err(outs[0], truth) <= TOL[np.dtype(dt)], (name, storage, tiles)
+        assert np.array_equal(outs[0].view(np.uint8), outs[1].view(np.uint8)), name
+        empty = np.diff(rp) == 0
+        assert np.array_equal(outs[0][empty].view(np.uint8), y0[empty].view(np.uint8)), name
+
+
 @pytest.mark.parametrize("tile", ["1024", "2048"])
 def test_csr_streamed_tile_kernel(gpu, tile):
     """The alternative bulk-copy streamed-tile CSR kernel (SB_CSR_KERNEL=s)."""
