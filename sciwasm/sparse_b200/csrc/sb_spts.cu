@@ -62,13 +62,15 @@ constexpr long long kDefaultSpin = 1LL << 31;  // SM cycles (about a second)
 
 // Polling back-off of the dependency waits: the sleep between two polls of a
 // ready flag starts at SB_SPTS_SLEEP_MIN_NS and doubles up to
-// SB_SPTS_SLEEP_MAX_NS, trading a little latency per level for less L2
-// traffic from the many waiting threads.
+// SB_SPTS_SLEEP_MAX_NS.  Measured on B200 over maxima of 64 to 2048 ns (and no
+// sleep), the wake-up delay of the longer sleeps costs more per level than
+// the extra polling traffic of the short ones, from 190-level to 100,000-level
+// factors; 64 ns was best or within 5% of best on every matrix tried.
 #ifndef SB_SPTS_SLEEP_MIN_NS
 #define SB_SPTS_SLEEP_MIN_NS 32u
 #endif
 #ifndef SB_SPTS_SLEEP_MAX_NS
-#define SB_SPTS_SLEEP_MAX_NS 1024u
+#define SB_SPTS_SLEEP_MAX_NS 64u
 #endif
 
 static unsigned grid1(long long n) {
