@@ -600,6 +600,24 @@ static int resident_grid(const void* kern) {
   return std::max(1, per) * sm_count();
 }
 
+// Grid of the plan-based polling solves.  Every warp that holds rows ahead
+// of the dependency frontier polls, and polling warps take issue slots and
+// L2 round trips from the warps at the frontier.  Measured on B200 from 74 to
+// 592 CTAs, on factors with 1 to 10^6 rows per level:
+//  * the level-ordered hybrid solve was fastest, or within 3%, with one CTA
+//    per SM on every factor (3-D Laplacian 64^3: 0.295 -> 0.246 ms; 1M-row
+//    random factor with 3470 levels: 9.5 -> 4.6 ms);
+//  * the natural-order sync-free solve needs the full resident grid when
+//    levels are wide (3-D Laplacians, >= 1380 rows per level: 5.6 ms at 444
+//    CTAs, 9.5 ms at 148 on 128^3) and one CTA per SM when they are narrow
+//    (288 rows per level: 9.5 -> 4.4 ms).
+static int polling_grid(const void* kern, int algo, int N, int nlevels) {
+  const int full = resident_grid(kern);
+  const bool wide = nlevels > 0 && (long long)N >= 1024LL * nlevels;
+  if (algo == SB_SPTS_SYNCFREE && wide) return full;
+  return std::min(full, sm_count());
+}
+
 static int plan_alloc(sb_spts_plan* p, void** out, size_t bytes) {
   *out = nullptr;
   cudaError_t e = cudaMalloc(out, bytes ? bytes : 16);
@@ -738,14 +756,13 @@ static int solve_impl(const sb_spts_plan* p, int algo, const T* b, T* y, long lo
     SB_CHECK_CUDA(cudaMemsetAsync(p->ticket, 0, sizeof(int), st));
     if (algo == SB_SPTS_SYNCFREE) {
       auto k = spts_syncfree_plan_rows<T, A>;
-      k<<<resident_grid((const void*)k), kT, 0, st>>>(p->row_ptr, p->col, (const T*)p->val, N, b,
-                                                       yw, y, p->ticket, limit, status);
+      k<<<polling_grid((const void*)k, algo, N, p->nlevels), kT, 0, st>>>(
+          p->row_ptr, p->col, (const T*)p->val, N, b, yw, y, p->ticket, limit, status);
       SB_CHECK_LAUNCH("spts_syncfree_plan_rows");
     } else {
       auto k = spts_hybrid_rows<T, A>;
-      k<<<resident_grid((const void*)k), kT, 0, st>>>(p->rrow, p->rcol, (const T*)p->rval, N,
-                                                       p->perm, b, yw, y, p->ticket, limit,
-                                                       status);
+      k<<<polling_grid((const void*)k, algo, N, p->nlevels), kT, 0, st>>>(
+          p->rrow, p->rcol, (const T*)p->rval, N, p->perm, b, yw, y, p->ticket, limit, status);
       SB_CHECK_LAUNCH("spts_hybrid_rows");
     }
     return SB_OK;
