@@ -42,11 +42,11 @@ constexpr int kBT = 256;
 constexpr int kMaxRhs = 8;
 constexpr int kBlocksPerTicket = 4;  // 32-row blocks a warp takes per work-counter update
 
-__device__ __forceinline__ float ldv(const float* p, long long i) { return ld_stream(p + i); }
-__device__ __forceinline__ double ldv(const double* p, long long i) { return ld_stream(p + i); }
+__device__ __forceinline__ float ldv(const float* p, long long i) { return ld_reuse(p + i); }
+__device__ __forceinline__ double ldv(const double* p, long long i) { return ld_reuse(p + i); }
 __device__ __forceinline__ float ldv(const __nv_bfloat16* p, long long i) {
   return __bfloat162float(
-      __ushort_as_bfloat16(ld_stream(reinterpret_cast<const unsigned short*>(p) + i)));
+      __ushort_as_bfloat16(ld_reuse(reinterpret_cast<const unsigned short*>(p) + i)));
 }
 
 // Neumaier-compensated accumulation (long rows with f32 sums).
@@ -108,7 +108,7 @@ __device__ __forceinline__ void batch_block(const sb_batch_item& it, int r0, int
 #pragma unroll
         for (int u = 0; u < UNROLL; ++u) {
           const int k = k0 + u * V;
-          cc[u] = k < e ? ld_stream(col + k) : 0;
+          cc[u] = k < e ? ld_reuse(col + k) : 0;
           vv[u] = k < e ? ldv(val, k) : (T)0;
         }
 #pragma unroll
@@ -148,7 +148,7 @@ __device__ __forceinline__ void batch_block(const sb_batch_item& it, int r0, int
 #pragma unroll
         for (int u = 0; u < UNROLL; ++u) {
           const int k = k0 + lane + u * 32;
-          cc[u] = k < e ? ld_stream(col + k) : 0;
+          cc[u] = k < e ? ld_reuse(col + k) : 0;
           vv[u] = k < e ? ldv(val, k) : (T)0;
         }
 #pragma unroll
@@ -214,7 +214,7 @@ __device__ __forceinline__ void batch_block_rhs(const sb_batch_item& it, int r0,
         T vv[UNROLL];
 #pragma unroll
         for (int u = 0; u < UNROLL; ++u) {
-          cc[u] = k0 + u < e ? ld_stream(col + k0 + u) : 0;
+          cc[u] = k0 + u < e ? ld_reuse(col + k0 + u) : 0;
           vv[u] = k0 + u < e ? ldv(val, k0 + u) : (T)0;
         }
 #pragma unroll
@@ -238,7 +238,7 @@ __device__ __forceinline__ void batch_block_rhs(const sb_batch_item& it, int r0,
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int k = k0 + lane + u * 32;
-          cc[u] = k < e ? ld_stream(col + k) : 0;
+          cc[u] = k < e ? ld_reuse(col + k) : 0;
           vv[u] = k < e ? ldv(val, k) : (T)0;
         }
 #pragma unroll

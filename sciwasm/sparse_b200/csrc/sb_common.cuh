@@ -56,6 +56,17 @@ __device__ __forceinline__ uint64_t evict_first_policy() {
   asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
   return pol;
 }
+// Read-only loads that allocate in L1, for arrays whose 32-byte sectors are
+// read by several load instructions of the same warp in a row (lanes that
+// interleave over a row's entries).  Measured on B200 against the streaming
+// form (no L1 allocation, L2 evict-first) in the CSR row-block kernel:
+// banded 4M FP64 0.125 -> 0.110 ms, Laplacian 4096^2 FP32 0.202 -> 0.175 ms,
+// power-law 2M FP64 0.242 -> 0.223 ms; keeping the L2 evict-first hint with
+// L1 allocation was slower than the default policy.
+__device__ __forceinline__ int ld_reuse(const int* p) { return __ldg(p); }
+__device__ __forceinline__ float ld_reuse(const float* p) { return __ldg(p); }
+__device__ __forceinline__ double ld_reuse(const double* p) { return __ldg(p); }
+__device__ __forceinline__ unsigned short ld_reuse(const unsigned short* p) { return __ldg(p); }
 __device__ __forceinline__ int4 ld_stream_v4(const int* p) {
   int4 r;
   const uint64_t pol = evict_first_policy();

@@ -285,6 +285,11 @@ __global__ void __launch_bounds__(kStreamThreads)
 template <typename T> __device__ __forceinline__ T widen(float v) { return (T)v; }
 __device__ __forceinline__ float ld_val(const float* p) { return ld_stream(p); }
 __device__ __forceinline__ double ld_val(const double* p) { return ld_stream(p); }
+__device__ __forceinline__ float ld_val_reuse(const float* p) { return ld_reuse(p); }
+__device__ __forceinline__ double ld_val_reuse(const double* p) { return ld_reuse(p); }
+__device__ __forceinline__ float ld_val_reuse(const __nv_bfloat16* p) {
+  return __bfloat162float(__ushort_as_bfloat16(ld_reuse(reinterpret_cast<const unsigned short*>(p))));
+}
 __device__ __forceinline__ float ld_val(const __nv_bfloat16* p) {
   return __bfloat162float(__ushort_as_bfloat16(ld_stream(reinterpret_cast<const unsigned short*>(p))));
 }
@@ -304,8 +309,11 @@ __device__ __forceinline__ void comp_add(T& s, T& c, T v) {
 // rows longer than the short limit are reduced afterwards by the whole warp
 // (with compensated f32 sums when the accumulation type is f32).  V is picked
 // per matrix from its mean row length.  No shared memory and no block
-// barrier: occupancy and unrolled loads keep the loads in flight.  SV is the
-// stored value type (f32, f64 or BF16); x, y and the sums are T.
+// barrier: occupancy and unrolled loads keep the loads in flight.  The V
+// lanes of a row interleave over its entries, so a 32-byte sector of col or
+// val is read by several consecutive load instructions: those loads
+// allocate in L1 (ld_reuse).  SV is the stored value type (f32, f64 or
+// BF16); x, y and the sums are T.
 template <typename SV, typename T, int V, int UNROLL>
 __global__ void __launch_bounds__(256)
     csr_rows_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
@@ -339,8 +347,8 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int u = 0; u < UNROLL; ++u) {
           const int k = s + q + u * V;
-          cc[u] = k < e ? ld_stream(col + k) : 0;
-          vv[u] = k < e ? (T)ld_val(val + k) : (T)0;
+          cc[u] = k < e ? ld_reuse(col + k) : 0;
+          vv[u] = k < e ? (T)ld_val_reuse(val + k) : (T)0;
         }
 #pragma unroll
         for (int u = 0; u < UNROLL; ++u) {
@@ -367,8 +375,8 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int k = k0 + lane + u * kWarp;
-          cc[u] = k < e ? ld_stream(col + k) : 0;
-          vv[u] = k < e ? (T)ld_val(val + k) : (T)0;
+          cc[u] = k < e ? ld_reuse(col + k) : 0;
+          vv[u] = k < e ? (T)ld_val_reuse(val + k) : (T)0;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
