@@ -358,6 +358,149 @@ __global__ void spts_level_rows(const int* __restrict__ rrow, const int* __restr
   }
 }
 
+// Grid barrier of a cooperative launch (every block resident).  Thread 0 of
+// each block reads the generation bar[1], then arrives on bar[0] with a
+// release add (ordered after the block's stores, which bar.sync made visible
+// to it); the last to arrive resets bar[0] and advances bar[1] with a release
+// add; the others poll bar[1] with acquire loads and a short sleep, bounded
+// by `limit` SM cycles (or by a timeout already recorded in the status
+// word).  Returns false after a timeout, which it records; the caller then
+// returns.
+__device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;"
+               : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, long long limit, int* status) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    const unsigned g = ld_relaxed_u32(bar + 1);
+    if (atom_add_release(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      atom_add_release(bar + 1, 1u);
+    } else {
+      const long long t0 = clock64();
+      unsigned ns = SB_SPTS_SLEEP_MIN_NS;
+      while (ld_acquire_u32(bar + 1) == g) {
+        if (clock64() - t0 > limit || *(volatile const int*)status) {
+          atomicExch(status, SB_DEV_TIMEOUT_DEP);
+          ok = 0;
+          break;
+        }
+        __nanosleep(ns);
+        ns = ns < SB_SPTS_SLEEP_MAX_NS ? 2 * ns : ns;
+      }
+    }
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// A thread's first row of a level, read ahead of the barrier that opens the
+// level: its structure, b, diagonal and up to kG off-diagonal columns and
+// values (the values of the columns are read after the barrier).
+template <typename T, typename A>
+struct LevelRow {
+  int i = -1, s = 0, end = 0, pi = 0;
+  A bi = 0, diag = 0;
+  int c[kG];
+  A v[kG];
+};
+
+template <typename T, typename A>
+__device__ __forceinline__ void level_row_load(LevelRow<T, A>& r, int i, const int* rrow,
+                                               const int* rcol, const T* rval, const int* perm,
+                                               const T* b) {
+  r.i = i;
+  r.s = rrow[i];
+  r.end = rrow[i + 1] - 1;
+  r.pi = perm[i];
+  r.bi = (A)b[r.pi];
+  r.diag = (A)rval[r.end];
+#pragma unroll
+  for (int k = 0; k < kG; ++k) {
+    const int j = r.s + k;
+    r.c[k] = j < r.end ? rcol[j] : 0;
+    r.v[k] = j < r.end ? (A)rval[j] : A(0);
+  }
+}
+
+// The level-set solve in one cooperative launch: the levels in order, the
+// rows of a level spread over all threads with the arithmetic of
+// spts_level_rows, a grid barrier after every level (the reference's
+// structure, src/parallel/src/spts_opt_32.wat:339-546).  Values of earlier
+// levels are read from L2 (__ldcg), since L1 is not kept coherent with other
+// SMs' stores inside a launch; each row also writes its natural-order
+// output, so no scatter pass follows.  Each thread reads its first row of
+// the next level before waiting at the barrier.  When every level fits in
+// one block of kLevelBlock1 threads, the launch is that one block and the
+// barrier is __syncthreads.
+constexpr int kLevelBlock1 = 512;  // threads of the single-block form
+
+template <typename T, typename A>
+__global__ void __launch_bounds__(kLevelBlock1)
+    spts_level_coop(const int* __restrict__ rrow, const int* __restrict__ rcol,
+                    const T* __restrict__ rval, const int* __restrict__ level_ptr, int nlevels,
+                    const int* __restrict__ perm, const T* __restrict__ b, T* yw,
+                    T* __restrict__ y, unsigned* bar, long long limit, int* status) {
+  const int nthreads = gridDim.x * blockDim.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  LevelRow<T, A> nx;
+  {
+    const int r0 = __ldg(level_ptr), r1 = __ldg(level_ptr + 1);
+    if (r0 + gt < r1) level_row_load(nx, r0 + gt, rrow, rcol, rval, perm, b);
+  }
+  for (int l = 0; l < nlevels; ++l) {
+    const int r0 = __ldg(level_ptr + l), r1 = __ldg(level_ptr + l + 1);
+    if (nx.i >= 0) {  // the prefetched first row (index r0 + gt)
+      A t = 0;
+      const int n = nx.end - nx.s;
+      T w[kG];
+#pragma unroll
+      for (int k = 0; k < kG; ++k)
+        if (k < n) w[k] = __ldcg(yw + nx.c[k]);
+#pragma unroll
+      for (int k = 0; k < kG; ++k)
+        if (k < n) t = add_rn(t, mul_rn(nx.v[k], (A)w[k]));
+      for (int j = nx.s + kG; j < nx.end; ++j)
+        t = add_rn(t, mul_rn((A)rval[j], (A)__ldcg(yw + rcol[j])));
+      const T yi = n > 0 ? (T)div_rn(sub_rn(nx.bi, t), nx.diag) : (T)div_rn(nx.bi, nx.diag);
+      __stcg(yw + nx.i, yi);
+      y[nx.pi] = yi;
+    }
+    for (int i = r0 + gt + nthreads; i < r1; i += nthreads) {
+      const int s = rrow[i], end = rrow[i + 1] - 1;
+      const int pi = perm[i];
+      const A bi = (A)b[pi];
+      T yi;
+      if (end > s) {
+        A t = 0;
+        for (int j = s; j < end; ++j) t = add_rn(t, mul_rn((A)rval[j], (A)__ldcg(yw + rcol[j])));
+        yi = (T)div_rn(sub_rn(bi, t), (A)rval[end]);
+      } else {
+        yi = (T)div_rn(bi, (A)rval[end]);
+      }
+      __stcg(yw + i, yi);
+      y[pi] = yi;
+    }
+    if (l + 1 < nlevels) {
+      const int q0 = r1, q1 = __ldg(level_ptr + l + 2);
+      nx.i = -1;
+      if (q0 + gt < q1) level_row_load(nx, q0 + gt, rrow, rcol, rval, perm, b);
+      if (gridDim.x == 1) __syncthreads();  // one block: its barrier orders the L2 accesses
+      else if (!grid_barrier(bar, limit, status)) return;
+    }
+  }
+}
+
 // Level-ordered rows (hybrid): same arithmetic as above, dependencies read
 // from the pending-initialised work vector yw (level order); each row also
 // writes its natural-order output y[perm[i]].
@@ -766,6 +909,40 @@ static int solve_impl(const sb_spts_plan* p, int algo, const T* b, T* y, long lo
       SB_CHECK_LAUNCH("spts_hybrid_rows");
     }
     return SB_OK;
+  }
+  {
+    // one cooperative launch: a single block of kLevelBlock1 threads when
+    // every level fits in it (no grid barrier), else blocks of kT threads for
+    // the widest level, at most one per SM (fewer blocks make each barrier
+    // cheaper), all of them resident
+    auto k = spts_level_coop<T, A>;
+    int widest = 0;
+    for (int l = 0; l < p->nlevels; ++l)
+      widest = std::max(widest, p->h_level_ptr[l + 1] - p->h_level_ptr[l]);
+    const int threads = widest <= kLevelBlock1 ? kLevelBlock1 : kT;
+    int per = 0, coop = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, threads, 0);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, p->device);
+    const int blocks =
+        threads == kLevelBlock1
+            ? std::min(1, per * sm_count())
+            : std::min(std::min((widest + kT - 1) / kT, sm_count()), std::max(per, 0) * sm_count());
+    if (coop && blocks >= 1) {
+      unsigned* bar = (unsigned*)(p->ticket + 2);
+      SB_CHECK_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
+      const int* rrow = p->rrow;
+      const int* rcol = p->rcol;
+      const T* rval = (const T*)p->rval;
+      const int* lptr = p->level_ptr;
+      int nl = p->nlevels;
+      const int* perm = p->perm;
+      void* args[] = {(void*)&rrow, (void*)&rcol, (void*)&rval, (void*)&lptr, (void*)&nl,
+                      (void*)&perm, (void*)&b,    (void*)&yw,   (void*)&y,    (void*)&bar,
+                      (void*)&limit, (void*)&status};
+      SB_CHECK_CUDA(
+          cudaLaunchCooperativeKernel((const void*)k, dim3(blocks), dim3(threads), args, 0, st));
+      return SB_OK;
+    }
   }
   for (int l = 0; l < p->nlevels; ++l) {
     const int r0 = p->h_level_ptr[l], r1 = p->h_level_ptr[l + 1];

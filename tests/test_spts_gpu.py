@@ -69,11 +69,45 @@ def test_level_sets_bitexact(gpu, oracle, name):
     _check_levels(gpu, oracle, rp, col, val)
 
 
+def _chain(n, dt):
+    """Lower bidiagonal: one row per level (a barrier per row in the level solve)."""
+    rp = np.concatenate([[0], np.cumsum([1] + [2] * (n - 1))]).astype(np.int32)
+    col = np.empty(rp[-1], np.int32)
+    val = np.empty(rp[-1], dt)
+    col[0], val[0] = 0, 2.0
+    i = np.arange(1, n)
+    col[rp[1:-1]] = i - 1
+    val[rp[1:-1]] = -0.5
+    col[rp[2:] - 1] = i
+    val[rp[2:] - 1] = 2.0
+    return rp, col, val
+
+
+def _two_levels(n, top, dt, seed=9):
+    """Rows >= top depend on 3 of the first `top` rows: level 1 holds n - top
+    rows, more than the threads of the level solve's grid."""
+    rng = np.random.default_rng(seed)
+    lens = np.ones(n, np.int64)
+    lens[top:] = 4
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    col = np.empty(rp[-1], np.int32)
+    col[rp[:top]] = np.arange(top)
+    offs = np.sort(rng.choice(top, size=(n - top, 3), replace=True), axis=1)
+    col[rp[top]:] = np.concatenate([offs, np.arange(top, n)[:, None]], axis=1).ravel()
+    val = rng.uniform(-0.3, 0.3, col.size).astype(dt)
+    val[rp[1:] - 1] = 3.0
+    return rp, col, val
+
+
 @pytest.mark.parametrize("dt", [np.float32, np.float64])
-@pytest.mark.parametrize("name", ["lap3d", "random_lower"])
+@pytest.mark.parametrize("name", ["lap3d", "random_lower", "chain", "two_levels"])
 def test_solves_bitexact(gpu, oracle, dt, name):
     if name == "lap3d":
         rp, col, val = synth.laplacian_3d_lower(24, dtype=dt)
+    elif name == "chain":
+        rp, col, val = _chain(20_000, dt)
+    elif name == "two_levels":
+        rp, col, val = _two_levels(300_000, 64, dt)
     else:
         rp, col, val = synth.random_lower(80_000, seed=3, band=2000, dtype=dt)
     N = rp.size - 1
