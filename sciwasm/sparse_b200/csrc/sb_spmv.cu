@@ -828,6 +828,71 @@ __global__ void __launch_bounds__(256)
   y[i] = t;
 }
 
+// dia_row_kernel with the diagonal count ND fixed at compile time (1..16):
+// the offsets and their extremes are held in registers (no shared memory, no
+// block barrier), and a row's ND data loads and ND x loads are all issued
+// before its additions, which keep the stored order (bit-identical to the
+// runtime-count kernel).
+template <typename T, int ND>
+__global__ void __launch_bounds__(256)
+    dia_rows_nd(const int* __restrict__ offset, const T* __restrict__ data, int N, int stride,
+                const T* __restrict__ x, T* __restrict__ y) {
+  int k[ND];
+  int kmin = 0x7fffffff, kmax = -0x7fffffff - 1;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    k[d] = __ldg(offset + d);
+    kmin = min(kmin, k[d]);
+    kmax = max(kmax, k[d]);
+  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  T t = y[i];
+  const long long move = (long long)N - stride;
+  T a[ND], b[ND];
+  if (move == 0 && (long long)i + kmin >= 0 && (long long)i + kmax < N) {
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      a[d] = ld_stream(data + (long long)d * stride + i);
+      b[d] = ld_ro(x + i + k[d]);
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d) t = add_rn(mul_rn(a[d], b[d]), t);
+    y[i] = t;
+    return;
+  }
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    const bool in = (unsigned)(i + k[d]) < (unsigned)N;
+    const long long idx = (long long)d * stride + i - (k[d] < 0 ? move : 0);
+    a[d] = in ? ld_stream(data + idx) : (T)0;
+    b[d] = in ? ld_ro(x + i + k[d]) : (T)0;
+  }
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    const bool in = (unsigned)(i + k[d]) < (unsigned)N;
+    const T p = mul_rn(a[d], b[d]);
+    t = in ? add_rn(p, t) : t;
+  }
+  y[i] = t;
+}
+
+template <typename T>
+static void launch_dia(const int* offset, const T* data, int N, int nd, int stride, const T* x,
+                       T* y, cudaStream_t st) {
+  const unsigned blocks = (unsigned)((N + 255) / 256);
+  switch (nd) {
+#define SB_DIA_ND(n) \
+  case n: dia_rows_nd<T, n><<<blocks, 256, 0, st>>>(offset, data, N, stride, x, y); return;
+    SB_DIA_ND(1) SB_DIA_ND(2) SB_DIA_ND(3) SB_DIA_ND(4) SB_DIA_ND(5) SB_DIA_ND(6) SB_DIA_ND(7)
+    SB_DIA_ND(8) SB_DIA_ND(9) SB_DIA_ND(10) SB_DIA_ND(11) SB_DIA_ND(12) SB_DIA_ND(13)
+    SB_DIA_ND(14) SB_DIA_ND(15) SB_DIA_ND(16)
+#undef SB_DIA_ND
+    default:
+      dia_row_kernel<T><<<blocks, 256, 0, st>>>(offset, data, N, nd, stride, x, y);
+  }
+}
+
 // One row per thread over the nc column-major slots, padding included
 // (src/sequential/src/sparse_opt_32.wat:427-479).
 template <typename T>
@@ -1089,14 +1154,12 @@ int sb_spmv_dia(int dtype, const int32_t* offset, const void* data, int32_t N, i
   SB_REQUIRE(offset && data && x && y, "sb_spmv_dia: null pointer");
   if ((r = ensure_device())) return r;
   cudaStream_t st = as_stream(stream);
-  const unsigned blocks = (unsigned)((N + 255) / 256);
   for (int it = 0; it < inner_max; ++it) {
     if (dtype == SB_F32)
-      dia_row_kernel<float><<<blocks, 256, 0, st>>>(offset, (const float*)data, N, nd, stride,
-                                                    (const float*)x, (float*)y);
+      launch_dia<float>(offset, (const float*)data, N, nd, stride, (const float*)x, (float*)y, st);
     else
-      dia_row_kernel<double><<<blocks, 256, 0, st>>>(offset, (const double*)data, N, nd, stride,
-                                                     (const double*)x, (double*)y);
+      launch_dia<double>(offset, (const double*)data, N, nd, stride, (const double*)x, (double*)y,
+                         st);
     SB_CHECK_LAUNCH("dia_row_kernel");
   }
   return SB_OK;

@@ -100,8 +100,11 @@ def test_coo_parity_sorted_and_unsorted(gpu, oracle, dt):
 
 @pytest.mark.parametrize("dt", DTYPES)
 def test_dia_ell_bitexact(gpu, oracle, dt):
-    for name in ("laplacian256", "banded"):
-        rp, col, val = _mats(dt)[name]
+    mats = _mats(dt)
+    # 21 diagonals: above the counts with a compile-time specialised kernel
+    mats["banded21"] = synth.banded(30_011, half=10, seed=4, dtype=dt)
+    for name in ("laplacian256", "banded", "banded21"):
+        rp, col, val = mats[name]
         N = rp.size - 1
         x, y0 = _x_y(N, dt, 9)
         off, dat, nd, stride = oracle.csr_dia(rp, col, val)
