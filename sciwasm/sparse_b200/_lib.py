@@ -26,6 +26,7 @@ SB_ETIMEOUT = -4
 SB_ECUDA = -5
 SB_ENODEV = -6
 SB_EALIGN = -7
+SB_COO_ROWS_SORTED = 1
 
 SB_F32 = 0
 SB_F64 = 1
@@ -67,6 +68,7 @@ SIGNATURES: dict[str, list] = {
     "sb_event_elapsed_ms": [P, P, C.POINTER(C.c_float)],
     "sb_stream_wait_event": [P, P],
     "sb_spmv_coo": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
+    "sb_spmv_coo_ex": [C.c_int, P, P, P, P, P, I32, I64, I32, I32, P],
     "sb_spmv_csr": [C.c_int, P, P, P, P, P, I32, I64, I32, P],
     "sb_spmv_dia": [C.c_int, P, P, I32, I32, I32, P, P, I32, P],
     "sb_spmv_ell": [C.c_int, P, P, I32, I32, P, P, I32, P],

@@ -456,7 +456,11 @@ static int launch_csr_rows(const int* row_ptr, const int* col, const SV* val, co
 
 // ------------------------------------------------------------ COO
 
-template <typename S, typename A, bool VEC>
+// SORTED: the caller guarantees non-decreasing rows.  A row that touches
+// neither end of a tile then has all its entries in that tile, so its sum
+// is added with a plain read-modify-write; only the rows of the tile's first
+// and last entries, which other tiles may share, keep the atomic.
+template <typename S, typename A, bool VEC, bool SORTED>
 __global__ void __launch_bounds__(kWarpsPerCta * kWarp)
     coo_tile_kernel(const int* __restrict__ row, const int* __restrict__ col,
                     const S* __restrict__ val, const S* __restrict__ x, S* __restrict__ y,
@@ -517,6 +521,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * kWarp)
       if (e < cnt) {
         if (r[e] != cur) {
           if (!internal) { internal = true; first_val = acc; }
+          else if (SORTED) y[cur] += (S)acc;  // strictly inside one lane: a whole row
           else atomicAdd(y + cur, (S)acc);
           cur = r[e];
           acc = 0;
@@ -525,6 +530,12 @@ __global__ void __launch_bounds__(kWarpsPerCta * kWarp)
       }
     }
     const int end_row = cur;
+    int tile_first = -1, tile_last = -1;
+    if (SORTED) {
+      tile_first = __shfl_sync(kFull, start_row, 0);
+      const unsigned have = __ballot_sync(kFull, cnt > 0);
+      tile_last = __shfl_sync(kFull, end_row, 31 - __clz(have));
+    }
     const int prev_end = __shfl_up_sync(kFull, end_row, 1);
     const bool cont_prev = lane > 0 && cnt > 0 && start_row == prev_end;
     // segment head for the scan: lane does not simply continue the previous one
@@ -542,13 +553,17 @@ __global__ void __launch_bounds__(kWarpsPerCta * kWarp)
     A carry = __shfl_up_sync(kFull, S_, 1);
     if (internal) {
       A v = first_val + (cont_prev ? carry : (A)0);
-      atomicAdd(y + start_row, (S)v);
+      if (SORTED && start_row != tile_first) y[start_row] += (S)v;
+      else atomicAdd(y + start_row, (S)v);
     }
     // tail run: emitted unless the next lane continues it
     const int next_start = __shfl_down_sync(kFull, start_row, 1);
     const int next_cnt = __shfl_down_sync(kFull, cnt, 1);
     const bool next_internal_or_diff = (lane == kWarp - 1) || next_cnt == 0 || next_start != end_row;
-    if (cnt > 0 && next_internal_or_diff) atomicAdd(y + end_row, (S)S_);
+    if (cnt > 0 && next_internal_or_diff) {
+      if (SORTED && end_row != tile_first && end_row != tile_last) y[end_row] += (S)S_;
+      else atomicAdd(y + end_row, (S)S_);
+    }
   }
 }
 
@@ -985,10 +1000,11 @@ static int launch_csr(const int* row_ptr, const int* col, const S* val, const S*
 
 template <typename S, typename A>
 static int launch_coo(const int* row, const int* col, const S* val, const S* x, S* y,
-                      long long nnz, cudaStream_t st) {
+                      long long nnz, bool sorted, cudaStream_t st) {
   const long long ntiles = (nnz + kTile - 1) / kTile;
   const bool vec = aligned16(row) && aligned16(col) && aligned16(val);
-  auto kern = vec ? coo_tile_kernel<S, A, true> : coo_tile_kernel<S, A, false>;
+  auto kern = vec ? (sorted ? coo_tile_kernel<S, A, true, true> : coo_tile_kernel<S, A, true, false>)
+                  : (sorted ? coo_tile_kernel<S, A, false, true> : coo_tile_kernel<S, A, false, false>);
   const int threads = kWarpsPerCta * kWarp;
   const long long max_warps = (long long)resident_ctas(kern, threads) * kWarpsPerCta;
   const long long warps = std::min(ntiles, max_warps);
@@ -1125,6 +1141,12 @@ int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const
 int sb_spmv_coo(int dtype, const int32_t* row, const int32_t* col, const void* val,
                 const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
                 void* stream) {
+  return sb_spmv_coo_ex(dtype, row, col, val, x, y, N, nnz, inner_max, 0, stream);
+}
+
+int sb_spmv_coo_ex(int dtype, const int32_t* row, const int32_t* col, const void* val,
+                   const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
+                   int32_t flags, void* stream) {
   int r = check_dtype(dtype, "sb_spmv_coo");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nnz >= 0 && inner_max >= 0, "sb_spmv_coo: negative size");
@@ -1135,10 +1157,10 @@ int sb_spmv_coo(int dtype, const int32_t* row, const int32_t* col, const void* v
   for (int it = 0; it < inner_max; ++it) {
     if (dtype == SB_F32)
       r = launch_coo<float, float>(row, col, (const float*)val, (const float*)x, (float*)y, nnz,
-                                   st);
+                                   (flags & SB_COO_ROWS_SORTED) != 0, st);
     else
       r = launch_coo<double, double>(row, col, (const double*)val, (const double*)x, (double*)y,
-                                     nnz, st);
+                                     nnz, (flags & SB_COO_ROWS_SORTED) != 0, st);
     if (r) return r;
   }
   return SB_OK;

@@ -131,11 +131,17 @@ class PinnedBuffer:
 
 
 class sparse_COO_t:
-    """COO matrix: row_index / col_index / val_index arrays of nnz entries."""
+    """COO matrix: row_index / col_index / val_index arrays of nnz entries.
 
-    def __init__(self, row_index, col_index, val_index, N, nnz):
+    rows_sorted is True when row_index is known to be non-decreasing: set by
+    coo_from_host (checked on the host) and by the Matrix Market constructors
+    (sorted by (row, col)); spmv then adds whole rows without atomics.  Code
+    that rewrites row_index in place must reset it."""
+
+    def __init__(self, row_index, col_index, val_index, N, nnz, rows_sorted=False):
         self.row_index, self.col_index, self.val_index = row_index, col_index, val_index
         self.N, self.nnz = int(N), int(nnz)
+        self.rows_sorted = bool(rows_sorted)
 
     @property
     def dtype(self):
@@ -338,7 +344,8 @@ def coo_from_host(row, col, val, N, dtype=None):
     _check_indices("row", row, N)
     _check_indices("col", col, N)
     return sparse_COO_t(DeviceArray.from_host(row), DeviceArray.from_host(col),
-                        DeviceArray.from_host(val), N, row.size)
+                        DeviceArray.from_host(val), N, row.size,
+                        rows_sorted=bool(row.size < 2 or np.all(row[1:] >= row[:-1])))
 
 
 def csr_from_host(row_ptr, col, val, dtype=None):
@@ -476,6 +483,7 @@ def _coo_from_mm(mm_info, lower, dtype, stream):
     call("sb_mm_coo", _dtcode(dtype), int(lower), C.byref(mm_info.header), mm_info.row.ptr,
          mm_info.col.ptr, mm_info.val.ptr if mm_info.val is not None else None,
          A.row_index.ptr, A.col_index.ptr, A.val_index.ptr, C.byref(n), _sp(stream))
+    A.rows_sorted = True  # sorted by (row, col) on the device
     return A
 
 
@@ -545,8 +553,9 @@ def spmv(A, x_view, y_view, inner_max=1, stream=None):
     s = _sp(stream)
     x, y = x_view.vec_index.ptr, y_view.vec_index.ptr
     if isinstance(A, sparse_COO_t):
-        call("sb_spmv_coo", dt, A.row_index.ptr, A.col_index.ptr, A.val_index.ptr, x, y, A.N,
-             A.nnz, inner_max, s)
+        flags = _lib.SB_COO_ROWS_SORTED if getattr(A, "rows_sorted", False) else 0
+        call("sb_spmv_coo_ex", dt, A.row_index.ptr, A.col_index.ptr, A.val_index.ptr, x, y, A.N,
+             A.nnz, inner_max, flags, s)
     elif isinstance(A, sparse_CSR_t):
         opts = getattr(A, "opts", None)
         if opts is None:

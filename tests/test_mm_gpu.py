@@ -23,6 +23,18 @@ def _check(gpu, oracle, text, dtype, tmp_path=None):
         assert A.N == oinfo["nrows"] and A.nnz == r.size
         assert np.array_equal(A.row_array(), r) and np.array_equal(A.col_array(), c)
         assert np.array_equal(A.val_array().view(np.uint8), v.view(np.uint8))
+        # the Matrix Market COO is row-sorted: its SpMV takes the sorted-rows kernel
+        assert A.rows_sorted
+        if A.nnz:
+            from conftest import TOL
+            # x covers every column (files may have more columns than rows)
+            nx = max(A.N, int(c.max()) + 1)
+            x = np.random.default_rng(2).uniform(-1, 1, nx).astype(dtype)
+            xv, yv = gpu.vec_from_host(x), gpu.create_vec(A.N, 0, dtype)
+            gpu.spmv(A, xv, yv)
+            rp = np.concatenate([[0], np.cumsum(np.bincount(r, minlength=A.N))]).astype(np.int32)
+            truth = oracle.truth_csr(rp, c, v, x)
+            assert rel_err(yv.array(), truth) <= TOL[np.dtype(dtype)]
 
 
 @pytest.mark.parametrize("name", FILES)

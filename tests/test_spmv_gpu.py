@@ -93,6 +93,8 @@ def test_coo_parity_sorted_and_unsorted(gpu, oracle, dt):
         perm = np.random.default_rng(1).permutation(row.size)
         for r, c, v in ((row, col, val), (row[perm], col[perm], val[perm])):
             A = gpu.coo_from_host(r, c, v, N)
+            # sorted rows take the kernel that adds whole rows without atomics
+            assert A.rows_sorted == bool(np.all(np.diff(r) >= 0)), name
             xv, yv = gpu.vec_from_host(x), gpu.vec_from_host(y0)
             gpu.spmv(A, xv, yv)
             assert rel_err(yv.array(), truth) <= TOL[np.dtype(dt)], name
