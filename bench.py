@@ -390,13 +390,13 @@ def run_ours(args, jobs, config, rank, world, local_rank):
 
     # ---------------- e2e through the public API with host buffers
     # Every call uploads its x and y from pinned host memory, runs spmv and
-    # reads y back.  Calls alternate over two streams, each call with its own
-    # device x and y, so one call's copies overlap another's kernel and the
-    # two copy directions overlap each other.
+    # reads y back.  Calls rotate over --e2e-streams streams, each call with
+    # its own device x and y, so one call's copies overlap another's kernel
+    # and the two copy directions overlap each other.
     h2d = 0
     d2h = 0
     host = []
-    e2e_streams = [stream, torch.cuda.Stream()]
+    e2e_streams = [stream] + [torch.cuda.Stream() for _ in range(max(1, args.e2e_streams) - 1)]
     for k, o in enumerate(objs):
         N = o["job"]["N"]
         dt = o["job"]["val"].dtype
@@ -405,7 +405,7 @@ def run_ours(args, jobs, config, rank, world, local_rank):
         _host_view(xp, N, dt)[:] = o["job"]["x"]
         _host_view(yp, N, dt)[:] = 0
         xd, yd = sb.create_vec(N, 0, dt), sb.create_vec(N, 0, dt)
-        host.append((xp, yp, yo, nb, xd, yd, e2e_streams[k % 2].cuda_stream))
+        host.append((xp, yp, yo, nb, xd, yd, e2e_streams[k % len(e2e_streams)].cuda_stream))
         h2d += 2 * nb
         d2h += nb
 
@@ -423,13 +423,15 @@ def run_ours(args, jobs, config, rank, world, local_rank):
         dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    side_done = torch.cuda.Event()
     e0.record(stream)
-    e2e_streams[1].wait_event(e0)
+    for sd in e2e_streams[1:]:
+        sd.wait_event(e0)
     for _ in range(args.steps):
         e2e_step()
-    side_done.record(e2e_streams[1])
-    stream.wait_event(side_done)
+    for sd in e2e_streams[1:]:
+        side_done = torch.cuda.Event()
+        side_done.record(sd)
+        stream.wait_event(side_done)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
@@ -476,7 +478,7 @@ def run_ours(args, jobs, config, rank, world, local_rank):
                 "d2h_bytes_per_step": d2h,
                 "path": "sciwasm.sparse_b200.spmv via the C ABI; per call x and y uploaded "
                         "from pinned host memory and y read back; matrices resident; calls "
-                        "alternate over two streams"},
+                        f"rotate over {len(e2e_streams)} streams"},
         "gpu_launches": len(objs) * args.steps,
         "clocks": clk,
     }
@@ -940,6 +942,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-sections", action="store_true",
                     help="skip the 4096^2 Laplacian, batched and SpTS sections")
+    ap.add_argument("--e2e-streams", type=int, default=2,
+                    help="streams the e2e calls rotate over")
     ap.add_argument("--serve-pool", type=int, default=2000)
     ap.add_argument("--serve-max-rows", type=int, default=2_000_000)
     ap.add_argument("--serve-rate", type=float, default=20_000.0)
