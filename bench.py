@@ -316,10 +316,22 @@ def run_ours(args, jobs, config, rank, world, local_rank):
                              bytes=algo_bytes(fmt, N, col.size, s_v, w)))
     bytes_step = sum(o["bytes"] for o in objs)
 
-    # the autotuner picks each CSR matrix's kernel options (setup, untimed)
+    # the autotuner picks each CSR matrix's kernel options (setup, untimed),
+    # unless --csr-fixed pins them (e.g. to profile the kernels a plain run
+    # chose: the tuning trials are not representative under a profiler)
+    fixed = {}
+    for item in (args.csr_fixed or "").split(";"):
+        if item.strip():
+            label, vals = item.split(":")
+            fixed[label.strip()] = [int(v) for v in vals.split(",")]
     for o in objs:
         if o["fmt"] == "csr":
-            o["tuned"] = sb.csr_autotune(o["A"], o["x"], stream=sptr)
+            label = o["label"].split("/")[0]
+            if label in fixed:
+                o["A"].opts = _lib.CsrOpts(*fixed[label])
+                o["tuned"] = dict(zip(("kernel", "lanes_per_row", "unroll", "grid"), fixed[label]))
+            else:
+                o["tuned"] = sb.csr_autotune(o["A"], o["x"], stream=sptr)
     torch.cuda.synchronize()
 
     # correctness gate: one call from y = 0 against an FP64 check
@@ -932,6 +944,9 @@ def main():
     ap.add_argument("--workload", default="format_sweep_fp64",
                     help="format_sweep_fp64 (the bench line), laplacian_fp32, or one section "
                          "alone: " + ", ".join(SECTIONS))
+    ap.add_argument("--csr-fixed", default=None,
+                    help="pinned CSR options of the default workload instead of the autotuner, "
+                         "e.g. 'banded:0,2,8,0;powerlaw:0,8,4,1' (kernel,lanes,unroll,grid)")
     ap.add_argument("--csr-opts", default=None,
                     help="powerlaw_csr: fixed CSR options lanes,unroll,grid (else autotuned)")
     ap.add_argument("--batch-mats", type=int, default=512,
