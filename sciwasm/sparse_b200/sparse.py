@@ -774,6 +774,7 @@ def eliminate_zeros(A, stream=None):
                 call("sb_copy_nonzeros_coo", dt, _d(A.row_index), _d(A.col_index),
                      _d(A.val_index), A.nnz, _d(B.row_index), _d(B.col_index),
                      _d(B.val_index), sp)
+            B.rows_sorted = A.rows_sorted  # the kept entries stay in order
             return B
         B = allocate_CSR(A.N, A.nnz if count == A.nnz else count, A.dtype)
         if count == A.nnz:
@@ -841,6 +842,7 @@ def _copy_structure(A, stream):
     if isinstance(A, sparse_COO_t):
         B = allocate_COO(A.N, A.nnz, A.dtype)
         _copy_arrays([(A.row_index, B.row_index), (A.col_index, B.col_index)], stream)
+        B.rows_sorted = A.rows_sorted
     elif isinstance(A, sparse_CSR_t):
         B = allocate_CSR(A.N, A.nnz, A.dtype)
         _copy_arrays([(A.row_index, B.row_index), (A.col_index, B.col_index)], stream)

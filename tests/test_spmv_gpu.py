@@ -101,6 +101,33 @@ def test_coo_parity_sorted_and_unsorted(gpu, oracle, dt):
 
 
 @pytest.mark.parametrize("dt", DTYPES)
+def test_coo_rows_sorted_carried(gpu, oracle, dt):
+    """Order-preserving operations keep a COO's rows_sorted flag (and its
+    sorted-rows SpMV), transpose drops it; results stay within tolerance."""
+    rp, col, val = synth.banded(50_021, half=4, seed=7, dtype=dt)
+    val = val.copy()
+    val[::7] = 0.0  # explicit zeros for eliminate_zeros to drop
+    N = rp.size - 1
+    row = synth.csr_to_coo_rows(rp)
+    A = gpu.coo_from_host(row, col, val, N)
+    assert A.rows_sorted
+    x, y0 = _x_y(N, dt, 8)
+    keep = val != 0
+    B = gpu.eliminate_zeros(A)
+    assert B.rows_sorted and B.nnz == int(keep.sum())
+    Nb = np.concatenate([[0], np.cumsum(np.bincount(row[keep], minlength=N))]).astype(np.int32)
+    cases = [(B, Nb, col[keep], val[keep]),
+             (gpu.neg(A), rp, col, -val)]
+    T = gpu.transpose(A)
+    assert not T.rows_sorted
+    for M, mrp, mcol, mval in cases:
+        assert M.rows_sorted
+        xv, yv = gpu.vec_from_host(x), gpu.vec_from_host(y0)
+        gpu.spmv(M, xv, yv)
+        assert rel_err(yv.array(), oracle.truth_csr(mrp, mcol, mval, x, y0)) <= TOL[np.dtype(dt)]
+
+
+@pytest.mark.parametrize("dt", DTYPES)
 def test_dia_ell_bitexact(gpu, oracle, dt):
     mats = _mats(dt)
     # 21 diagonals: above the counts with a compile-time specialised kernel
