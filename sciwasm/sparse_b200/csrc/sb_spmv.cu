@@ -11,11 +11,14 @@
 //     streams fixed-size nonzero tiles into a shared-memory ring with bulk
 //     async copies (SB_CSR_KERNEL=s); a third cuts the nonzeros into
 //     row-aligned warp ranges walked in 256-nonzero tiles (kernel 2).
-//   * COO is the same tile scheme keyed on the row array; every row segment
-//     is added with one atomic, so unsorted input is accepted.
+//   * COO walks 256-entry tiles, 8 entries per lane; every row segment is
+//     added with one atomic, so unsorted input is accepted.  With rows the
+//     caller declares sorted (and short on average), rows inside a tile are
+//     added without atomics.
 //   * DIA and ELL assign one row per thread and keep the reference's per-row
 //     addition order (separately rounded mul and add), so their results are
-//     bit-identical to the reference's serial loops.
+//     bit-identical to the reference's serial loops; DIA with up to 16
+//     diagonals runs a kernel with the count fixed at compile time.
 #include <algorithm>
 #include <climits>
 #include <stdlib.h>
