@@ -16,7 +16,8 @@
 // the results are bit-identical to the reference's row kernels):
 //   SB_SPTS_LEVEL    level by level on the reordered matrix, the row kernel
 //                    of src/parallel/src/sparse_opt_32.wat:11679-11757
-//                    (t = 0; t += L_ij*y_j; y_i = (b_i - t)/L_ii)
+//                    (t = 0; t += L_ij*y_j; y_i = (b_i - t)/L_ii), in one
+//                    cooperative launch with a grid barrier per level
 //   SB_SPTS_SYNCFREE natural order with per-row ready flags, the kernel of
 //                    src/parallel/src/spts_opt_32.wat:8-117
 //                    (t = b_i; t -= L_ij*y_j; y_i = t/L_ii)
