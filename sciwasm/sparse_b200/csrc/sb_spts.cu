@@ -755,6 +755,18 @@ static int resident_grid(const void* kern) {
 //    levels are wide (3-D Laplacians, >= 1380 rows per level: 5.6 ms at 444
 //    CTAs, 9.5 ms at 148 on 128^3) and one CTA per SM when they are narrow
 //    (288 rows per level: 9.5 -> 4.4 ms).
+// Grid of the natural-order polling kernels that run without level
+// information (the analysis itself and the sync-free solve on caller
+// arrays): two CTAs per SM.  Measured on B200 against the resident grid
+// (analysis / caller-array sync-free, ms): 3-D Laplacian 64^3 3.35 -> 3.16 /
+// 1.51 -> 1.50; 128^3 8.58 -> 8.15 / 15.2 -> 15.4; 1M-row random factor
+// 18.1 -> 8.1 / 41.0 -> 25.9; band-50 1M 425 -> 224 / 2048 -> 1368;
+// bidiagonal 100k 122 -> 81 / 265 -> 259.  One CTA per SM was faster still on
+// the narrow factors and 30-50% slower on the Laplacians.
+static int natural_order_grid(const void* kern) {
+  return std::min(resident_grid(kern), 2 * sm_count());
+}
+
 static int polling_grid(const void* kern, int algo, int N, int nlevels) {
   const int full = resident_grid(kern);
   const bool wide = nlevels > 0 && (long long)N >= 1024LL * nlevels;
@@ -805,7 +817,7 @@ static int analyze_impl(sb_spts_plan* p, cudaStream_t st) {
   SB_CHECK_LAUNCH("lower_check");
   SB_CHECK_CUDA(cudaMemsetAsync(p->level, 0xff, sizeof(int) * N, st));
   SB_CHECK_CUDA(cudaMemsetAsync(p->ticket, 0, sizeof(int), st));
-  level_kernel<<<resident_grid((const void*)level_kernel), kT, 0, st>>>(
+  level_kernel<<<natural_order_grid((const void*)level_kernel), kT, 0, st>>>(
       p->row_ptr, p->col, N, p->level, p->ticket, kDefaultSpin, status);
   SB_CHECK_LAUNCH("level_kernel");
   max_kernel<<<std::min<unsigned>(grid1(N), (unsigned)sm_count() * 4), kT, 0, st>>>(p->level, N,
@@ -1441,12 +1453,12 @@ int sb_spts_syncfree_csr(int dtype, const int32_t* row_ptr, const int32_t* col, 
   const long long limit = spin_limit_cycles > 0 ? spin_limit_cycles : kDefaultSpin;
   if (dtype == SB_F64) {
     auto k = spts_syncfree_rows<double, double>;
-    k<<<resident_grid((const void*)k), kT, 0, st>>>(row_ptr, col, (const double*)val, N,
+    k<<<natural_order_grid((const void*)k), kT, 0, st>>>(row_ptr, col, (const double*)val, N,
                                                      (const double*)b, (double*)y, flags, ticket,
                                                      limit, status);
   } else {
     auto k = spts_syncfree_rows<float, float>;
-    k<<<resident_grid((const void*)k), kT, 0, st>>>(row_ptr, col, (const float*)val, N,
+    k<<<natural_order_grid((const void*)k), kT, 0, st>>>(row_ptr, col, (const float*)val, N,
                                                      (const float*)b, (float*)y, flags, ticket,
                                                      limit, status);
   }
