@@ -44,7 +44,10 @@ def test_binding_covers_header(sb):
 def test_library_has_no_torch_dependency(sb):
     from sciwasm.sparse_b200 import _lib
     out = subprocess.run(["ldd", _lib.LIB_PATH], capture_output=True, text=True).stdout
-    assert "torch" not in out and "c10" not in out
+    # library names and paths only: the load addresses in parentheses are
+    # random hex that can contain "c10" by chance
+    libs = [line.split("(")[0] for line in out.splitlines()]
+    assert not any("torch" in lib or "c10" in lib for lib in libs), libs
 
 
 def test_status_strings(sb):
