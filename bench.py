@@ -273,6 +273,132 @@ def cpu_baseline_sample(jobs, budget_s=12.0):
 
 # ------------------------------------------------------------------ GPU arm
 
+def conversion_bytes(kind, N, nnz, s_v, width=0):
+    """Algorithmic bytes of one conversion: its input read plus its output
+    written (zero fill included)."""
+    csr = nnz * (4 + s_v) + 4 * (N + 1)
+    if kind == "coo_csr":
+        return nnz * (8 + s_v) + csr
+    if kind == "csr_dia":
+        return csr + width * N * s_v + 4 * width
+    if kind == "csr_ell":
+        return csr + width * N * (4 + s_v)
+    raise ValueError(kind)
+
+
+def _timed_call(stream, fn, reps=3):
+    """(median device ms over reps calls of fn bracketed by CUDA events on
+    `stream`, result of the last call); fn's own host synchronisations fall
+    inside the bracket."""
+    import torch
+    times, out = [], None
+    for _ in range(reps):
+        out = None
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return float(np.median(times)), out
+
+
+def device_conversions(jobs, stream):
+    """Objects of the format sweep built on the device.  For each matrix: a
+    COO sorted by (row, col) is uploaded (the "coo" object), coo_csr runs on
+    it (the copy-speed path) and on a shuffled copy (the stable radix-sort
+    path, whose output becomes the "csr" object), then csr_dia and csr_ell
+    run on the CSR (refused for the power-law matrix, as in the reference).
+    Returns (objects, timings, host copies of inputs and outputs for the
+    bit-exact check)."""
+    import sciwasm.sparse_b200 as sb
+    from sciwasm.sparse_b200 import synth
+    sp = stream.cuda_stream
+    objs, conv, check = [], {}, {}
+    for j in jobs:
+        N, rp, col, val = j["N"], j["rp"], j["col"], j["val"]
+        s_v, nnz = val.itemsize, col.size
+        x = sb.vec_from_host(j["x"])
+        row = synth.csr_to_coo_rows(rp)
+        Acoo = sb.coo_from_host(row, col, val, N)
+        c = {}
+        ms, Asorted = _timed_call(stream, lambda: sb.coo_csr(Acoo, stream=sp))
+        b = conversion_bytes("coo_csr", N, nnz, s_v)
+        c["coo_csr_sorted_input"] = {"ms": round(ms, 3), "GB_s": round(b / ms / 1e6, 1),
+                                     "algorithmic_bytes": b}
+        del Asorted
+        perm = np.random.default_rng(20 + len(conv)).permutation(nnz)
+        shuf = (row[perm], col[perm], val[perm])
+        del perm
+        Ashuf = sb.coo_from_host(*shuf, N)
+        ms, Acsr = _timed_call(stream, lambda: sb.coo_csr(Ashuf, stream=sp))
+        c["coo_csr_shuffled_input"] = {"ms": round(ms, 3), "GB_s": round(b / ms / 1e6, 1),
+                                       "algorithmic_bytes": b}
+        del Ashuf
+        chk = {"N": N, "shuffled": shuf, "csr": (Acsr.row_array(), Acsr.col_array(),
+                                                 Acsr.val_array())}
+        made = {"coo": (Acoo, 0), "csr": (Acsr, 0)}
+        for kind, fmt in (("csr_dia", "dia"), ("csr_ell", "ell")):
+            conv_fn = sb.csr_dia if fmt == "dia" else sb.csr_ell
+            ms, M = _timed_call(stream, lambda: conv_fn(Acsr, stream=sp))
+            if M is None:
+                c[kind] = {"refused": True, "ms": round(ms, 3)}
+                chk[fmt] = None
+                continue
+            w = M.ndiags if fmt == "dia" else M.ncols
+            b2 = conversion_bytes(kind, N, nnz, s_v, w)
+            c[kind] = {"ms": round(ms, 3), "GB_s": round(b2 / ms / 1e6, 1),
+                       "algorithmic_bytes": b2, "width": w}
+            chk[fmt] = ((M.offset_array(), M.data_array()) if fmt == "dia"
+                        else (M.indices_array(), M.data_array()))
+            made[fmt] = (M, w)
+        for fmt in j["formats"]:
+            if fmt not in made:
+                raise SystemExit(f"{j['label']}: {fmt} form was refused by the conversion")
+            A, w = made[fmt]
+            y = sb.create_vec(N, 0, val.dtype)
+            objs.append(dict(label=f"{j['label']}/{fmt}", fmt=fmt, A=A, x=x, y=y, job=j,
+                             bytes=algo_bytes(fmt, N, nnz, s_v, w)))
+        conv[j["label"]] = c
+        check[j["label"]] = chk
+    return objs, conv, check
+
+
+def conversions_cpu_check(conv, check):
+    """CPU-baseline leg of the conversions: the oracle's serial coo_csr,
+    csr_dia and csr_ell (the reference's conversions are serial JavaScript),
+    timed on the same inputs, and the device outputs compared with them bit
+    for bit."""
+    from oracle import binding as orc
+
+    def same(a, b):
+        a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+        return a.dtype == b.dtype and a.shape == b.shape and \
+            np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+    for label, chk in check.items():
+        c = conv[label]
+        t0 = time.perf_counter()
+        want = orc.coo_csr(*chk["shuffled"], chk["N"])
+        t_csr = time.perf_counter() - t0
+        ok = all(same(a, b) for a, b in zip(chk["csr"], want))
+        cpu = {"coo_csr_shuffled_input_ms": round(t_csr * 1e3, 1)}
+        for fmt, fn in (("dia", orc.csr_dia), ("ell", orc.csr_ell)):
+            t0 = time.perf_counter()
+            w = fn(*want)
+            cpu[f"csr_{fmt}_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
+            if w is None or chk[fmt] is None:
+                ok = ok and (w is None) and (chk[fmt] is None)
+            else:
+                ok = ok and same(chk[fmt][0], w[0]) and same(chk[fmt][1], w[1])
+        c["cpu_baseline"] = {**cpu, "cores": 1, "kind": "port",
+                             "sample": "one call each, serial C restatement of the "
+                                       "reference's conversions (JavaScript, serial)"}
+        c["bit_exact"] = bool(ok)
+
+
+
 def run_ours(args, jobs, config, rank, world, local_rank):
     import torch
     import sciwasm.sparse_b200 as sb
@@ -290,30 +416,10 @@ def run_ours(args, jobs, config, rank, world, local_rank):
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
 
-    # upload every (matrix, format) object
-    objs = []
-    for j in jobs:
-        N, rp, col, val = j["N"], j["rp"], j["col"], j["val"]
-        s_v = val.itemsize
-        x = sb.vec_from_host(j["x"])
-        for fmt in j["formats"]:
-            if fmt == "csr":
-                A = sb.csr_from_host(rp, col, val)
-                w = 0
-            elif fmt == "coo":
-                A = sb.coo_from_host(synth.csr_to_coo_rows(rp), col, val, N)
-                w = 0
-            elif fmt == "dia":
-                off, dat = synth.csr_to_dia_host(rp, col, val)
-                A = sb.dia_from_host(off, dat, N, nnz=col.size)
-                w = off.size
-            else:
-                ind, dat, nc = synth.csr_to_ell_host(rp, col, val)
-                A = sb.ell_from_host(ind, dat, nc, N, nnz=col.size)
-                w = nc
-            y = sb.create_vec(N, 0, val.dtype)
-            objs.append(dict(label=f"{j['label']}/{fmt}", fmt=fmt, A=A, x=x, y=y, job=j,
-                             bytes=algo_bytes(fmt, N, col.size, s_v, w)))
+    # every (matrix, format) object comes from the device conversions:
+    # COO (rows sorted, as the reference's reader leaves it) uploaded, then
+    # coo_csr -> csr_dia / csr_ell on the device, each timed
+    objs, conversions, conv_check = device_conversions(jobs, stream)
     bytes_step = sum(o["bytes"] for o in objs)
 
     # the autotuner picks each CSR matrix's kernel options (setup, untimed),
@@ -473,8 +579,6 @@ def run_ours(args, jobs, config, rank, world, local_rank):
                            **({"tuned": {k2: v for k2, v in o["tuned"].items() if k2 != "ms"}}
                               if "tuned" in o else {})}
               for k, o in enumerate(objs)}
-    config["per_call"] = detail
-    config["max_rel_err"] = max_err
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -493,13 +597,18 @@ def run_ours(args, jobs, config, rank, world, local_rank):
                         f"rotate over {len(e2e_streams)} streams"},
         "gpu_launches": len(objs) * args.steps,
         "clocks": clk,
+        "max_rel_err": max_err,
+        "per_call": detail,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(jobs)
+        conversions_cpu_check(conversions, conv_check)
+    del conv_check
+    line["conversions"] = conversions
     if world == 1 and not args.no_sections:
         line["laplacian4096_fp32"] = run_laplacian_large(stream, peak)
         line["batched"] = run_batched(stream, peak)
-        line["spts"] = run_spts_section(stream)
+        line["spts"] = run_spts_section(stream, cpu=not args.no_cpu_baseline)
         torch.cuda.empty_cache()
     if world == 1 and not args.no_serving:
         line["serving"] = run_serving(args)
@@ -791,57 +900,115 @@ def run_batched(stream, peak, n_mats=512, seed=5):
     return out
 
 
-def run_spts_section(stream):
+def _spts_cpu_baseline(rp, col, val, b, plan_levels, gpu_y, reps=3):
+    """CPU-baseline leg of one SpTS case: the oracle's serial analysis and row
+    kernel, and its pthread ports of the reference's parallel level-set and
+    sync-free solves on 5 threads (the published setting) and on every host
+    core, best of `reps` runs each.  The GPU's levels (level, level_ptr,
+    permutation, order) and its three solves are compared with the oracle's
+    bit for bit."""
+    from oracle import binding as orc
+    cores = os.cpu_count() or 1
+    N = rp.size - 1
+
+    def best(fn):
+        t = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            t.append((time.perf_counter() - t0) * 1e3)
+        return round(min(t), 3)
+
+    ls = {}
+
+    def analysis():
+        ls.update(orc.level_sets(rp, col, val))
+    out = {"analysis_ms_serial": best(analysis)}
+    out["row_kernel_ms_serial"] = best(lambda: orc.spts_csr(rp, col, val, b))
+    bp = np.ascontiguousarray(b[ls["permutation"]])
+    yl = np.zeros(N, val.dtype)
+    flag = np.zeros(N, np.int32)
+    ysf = np.zeros(N, val.dtype)
+    for nt in sorted({5, cores}):
+        out[f"level_ms_{nt}t"] = best(lambda: orc.par_spts_level(
+            nt, ls["level_ptr"], ls["row_ptr"], ls["col"], ls["val"], bp, yl))
+        out[f"syncfree_ms_{nt}t"] = best(lambda: orc.par_spts_syncfree(
+            nt, rp, col, val, b, ysf, flag))
+    out.update(cores=cores, kind="port",
+               sample="whole factor per run, best of 3: serial analysis and row kernel; "
+                      "pthread level-set (barrier per level) and sync-free (ready flags) "
+                      "solves on 5 threads and on all cores (C restatement of the "
+                      "reference's worker kernels, not V8/wasm)")
+
+    def same(a, c):
+        return np.array_equal(np.ascontiguousarray(a).view(np.uint8),
+                              np.ascontiguousarray(c).view(np.uint8))
+    lv, lp, perm, order = plan_levels
+    ok_levels = same(lv, ls["level"]) and same(lp, ls["level_ptr"]) and \
+        same(perm, ls["permutation"]) and same(order, ls["order"])
+    row_kernel = orc.spts_csr(rp, col, val, b)
+    syncfree = orc.spts_syncfree(rp, col, val, b)
+    ok_solves = {an: same(y, syncfree if an == "syncfree" else row_kernel)
+                 for an, y in gpu_y.items()}
+    ok_solves["syncfree_cpu_threads"] = same(ysf, syncfree)
+    return out, {"levels": ok_levels, **ok_solves}
+
+
+def run_spts_section(stream, cpu=True):
     """SpTS: lower triangle of the 3-D 7-point Laplacian on a 64^3 grid and a
     random lower-triangular matrix (1M rows, 7 off-diagonals per row within
     5,000 of the diagonal, diagonal U[2,4]), FP64 and FP32, b ~ U[-1,1];
-    analysis and the three solves, errors against an FP64 host solve (scipy)."""
+    analysis (device time from events around its kernels, and the host time
+    of the whole call) and the three solves, errors against an FP64 host
+    solve (scipy); with cpu, the CPU baselines and bit-exact checks."""
     import torch
     import scipy.sparse as sps
     import scipy.sparse.linalg as spl
     import sciwasm.sparse_b200 as sb
-    from sciwasm.sparse_b200 import _lib, synth_device as sd
+    from sciwasm.sparse_b200 import _lib, synth
     sp = stream.cuda_stream
-    from sciwasm.sparse_b200 import synth
     npdt = {"f64": np.float64, "f32": np.float32}
-    cases = [("laplacian3d_64", lambda dt: sb.csr_from_host(
-                 *synth.laplacian_3d_lower(64, dtype=npdt[dt]))),
-             ("random_lower_1M", lambda dt: sb.csr_from_host(
-                 *synth.random_lower(1_000_000, 7, 5000, seed=3, dtype=npdt[dt])))]
+    cases = [("laplacian3d_64", lambda dt: synth.laplacian_3d_lower(64, dtype=npdt[dt])),
+             ("random_lower_1M", lambda dt: synth.random_lower(1_000_000, 7, 5000, seed=3,
+                                                                dtype=npdt[dt]))]
     algos = {"level": _lib.SB_SPTS_LEVEL, "syncfree": _lib.SB_SPTS_SYNCFREE,
              "hybrid": _lib.SB_SPTS_HYBRID}
     out = {}
     for name, gen in cases:
         for dt in ("f64", "f32"):
-            L = gen(dt)
+            rp, col, val = gen(dt)
+            L = sb.csr_from_host(rp, col, val)
             torch.cuda.synchronize()
-            # analysis timed three times on the host (the first build also pays
-            # one-time allocation and module-load costs): median and first
-            ats = []
-            for rep in range(3):
-                if rep:
+            # five analyses: device time of the analysis kernels (events on
+            # the stream) and host time of the whole call; the first build
+            # also pays one-time module-load costs
+            dev_ms, host_ms = [], []
+            plan = None
+            for rep in range(5):
+                if plan is not None:
                     plan.close()
                 t0 = time.perf_counter()
-                plan = sb.SptsPlan(L)
+                plan = sb.SptsPlan(L, stream=sp)
                 torch.cuda.synchronize()
-                ats.append((time.perf_counter() - t0) * 1e3)
-            analysis_ms = float(np.median(ats))
-            tdt = torch.float64 if dt == "f64" else torch.float32
-            g = torch.Generator(device="cuda").manual_seed(4)
-            bt = (torch.rand(L.N, generator=g, device="cuda", dtype=torch.float64) * 2 - 1).to(tdt)
-            yt = torch.zeros(L.N, device="cuda", dtype=tdt)
-            M = sps.csr_matrix((L.val_array().astype(np.float64), L.col_array(), L.row_array()),
-                               shape=(L.N, L.N))
-            M.sum_duplicates()
-            truth = spl.spsolve_triangular(M, bt.double().cpu().numpy(), lower=True)
+                host_ms.append((time.perf_counter() - t0) * 1e3)
+                dev_ms.append(plan.analysis_ms)
+            b_host = synth.uniform_vec(L.N, 4, dtype=npdt[dt])
+            bt = torch.from_numpy(b_host).cuda()
+            yt = torch.zeros(L.N, device="cuda", dtype=bt.dtype)
+            M = sps.csr_matrix((val.astype(np.float64), col, rp), shape=(L.N, L.N))
+            truth = spl.spsolve_triangular(M, b_host.astype(np.float64), lower=True)
             s_v = 8 if dt == "f64" else 4
             nbytes = L.nnz * (s_v + 4) + 4 * (L.N + 1) + 2 * L.N * s_v
             row = {"N": L.N, "nnz": L.nnz, "levels": plan.nlevels,
-                   "analysis_ms": round(analysis_ms, 2), "analysis_first_ms": round(ats[0], 2),
+                   "analysis_device_ms": round(float(np.median(dev_ms)), 3),
+                   "analysis_device_ms_all": [round(v, 3) for v in dev_ms],
+                   "analysis_host_ms": round(float(np.median(host_ms)), 3),
+                   "analysis_host_ms_first": round(host_ms[0], 2),
                    "algorithmic_bytes": nbytes}
             runs = [(an, code, _lib.SB_SPTS_ACC_NATIVE) for an, code in algos.items()]
             if dt == "f32":
                 runs.append(("hybrid_acc_f64", _lib.SB_SPTS_HYBRID, _lib.SB_SPTS_ACC_F64))
+            gpu_y = {}
             for an, code, pol in runs:
                 def solve():
                     _lib.call("sb_spts_solve", plan.ptr, code, pol, bt.data_ptr(), yt.data_ptr(),
@@ -850,8 +1017,11 @@ def run_spts_section(stream):
                 with torch.cuda.stream(stream):
                     solve()
                 torch.cuda.synchronize()
-                y = yt.double().cpu().numpy()
-                err = float(np.max(np.abs(y - truth)) / max(np.max(np.abs(truth)), 1e-300))
+                y = yt.cpu().numpy()
+                if an in algos:
+                    gpu_y[an] = y.copy()
+                err = float(np.max(np.abs(y.astype(np.float64) - truth)) /
+                            max(np.max(np.abs(truth)), 1e-300))
                 with torch.cuda.stream(stream):
                     solve()
                 ms = _time_each_ms(stream, solve, 5)
@@ -860,6 +1030,10 @@ def run_spts_section(stream):
             code = __import__("ctypes").c_int(0)
             _lib.call("sb_device_status", __import__("ctypes").byref(code))
             row["device_status"] = code.value
+            if cpu:
+                levels = tuple(a.to_host() for a in plan.levels())
+                row["cpu_baseline"], row["bit_exact"] = _spts_cpu_baseline(
+                    rp, col, val, b_host, levels, gpu_y)
             out[f"{name}/{dt}"] = row
             plan.close()
     return out

@@ -120,8 +120,10 @@ int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const voi
 /* Kernel choice for CSR SpMV (no counterpart in the reference, whose
  * parallel harness picks among unrolled CSR variants per run,
  * src/parallel/tests/main32.js:150-313).  kernel 0 = row blocks (default),
- * 1 = streamed nonzero tiles, 2 = nonzero tiles over row-aligned warp
- * ranges (unroll = 256-nonzero tiles per warp, 1..64; F32, F64 and BF16;
+ * 1 = streamed nonzero tiles (1024 per tile, 2048 with unroll = 2048; F32
+ * and F64 with 16-byte aligned col/val, else row blocks), 2 = nonzero tiles
+ * over row-aligned warp ranges (unroll = 256-nonzero tiles per warp, 1..64;
+ * F32, F64 and BF16;
  * every row written once, no atomics); lanes_per_row 1..32 (power of two)
  * and unroll 2/4/8 tune the row-block kernel, 0 = chosen from the mean row
  * length; grid 0 = a resident grid striding over 32-row blocks (regular
@@ -278,6 +280,10 @@ int sb_spts_plan_destroy(sb_spts_plan* plan);
 /* nlevels; solvable = 1 when every row ends with its diagonal and all other
  * columns are below it (the solves' precondition). */
 int sb_spts_plan_info(const sb_spts_plan* plan, int32_t* nlevels, int32_t* solvable);
+/* Device time of the analysis (no counterpart in the reference): milliseconds
+ * between CUDA events recorded on the analysis stream before its first
+ * kernel and after its last, after the plan's one allocation. */
+int sb_spts_plan_analysis_ms(const sb_spts_plan* plan, float* ms);
 /* Device-to-device copies of the analysis results (any pointer may be NULL):
  * level[N], level_ptr[nlevels+1], permutation[N], order[N]. */
 int sb_spts_plan_levels(const sb_spts_plan* plan, int32_t* level, int32_t* level_ptr,

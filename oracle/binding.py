@@ -56,6 +56,8 @@ _SIG = {
     "or_truth_spts": ([C.c_int, _P, _P, _P, _P, _P, _I32], None),
     "or_par_spts_level_f32": ([C.c_int, _P, _I32, _P, _P, _P, _P, _P, _I32], None),
     "or_par_spts_level_f64": ([C.c_int, _P, _I32, _P, _P, _P, _P, _P, _I32], None),
+    "or_par_spts_syncfree_f32": ([C.c_int, _P, _P, _P, _P, _P, _I32, _P], C.c_int),
+    "or_par_spts_syncfree_f64": ([C.c_int, _P, _P, _P, _P, _P, _I32, _P], C.c_int),
     "or_count_nonzeros": ([C.c_int, _P, _I64], _I64),
     "or_copy_nonzeros_coo": ([C.c_int, _P, _P, _P, _I64, _P, _P, _P], _I64),
     "or_copy_nonzeros_csr": ([C.c_int, _P, _P, _P, _I32, _P, _P, _P], None),
@@ -327,6 +329,17 @@ def par_spts_level(nthreads, level_ptr, row_ptr, col, val, b, y):
     getattr(lib(), "or_par_spts_level_" + _sfx(val.dtype))(
         nthreads, _p(level_ptr), level_ptr.size - 1, _p(row_ptr), _p(col), _p(val), _p(b), _p(y),
         row_ptr.size - 1)
+
+
+def par_spts_syncfree(nthreads, row_ptr, col, val, b, y, flag=None):
+    """Parallel sync-free CPU baseline into y (in place); flag is an int32[N]
+    work array (allocated when None).  Raises if a bounded wait ran out."""
+    if flag is None:
+        flag = np.zeros(row_ptr.size - 1, np.int32)
+    st = getattr(lib(), "or_par_spts_syncfree_" + _sfx(val.dtype))(
+        nthreads, _p(row_ptr), _p(col), _p(val), _p(b), _p(y), row_ptr.size - 1, _p(flag))
+    if st != 0:
+        raise RuntimeError("or_par_spts_syncfree: a dependency wait ran out")
 
 
 def fletcher(y):

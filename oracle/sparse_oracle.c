@@ -15,6 +15,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <pthread.h>
+#include <sched.h>
 
 /* ======================= SpMV, serial storage order ======================= */
 
@@ -666,6 +667,70 @@ void or_truth_spts(int w, const int32_t* row_ptr, const int32_t* col, const void
   }
 DEF_PAR_SPTS(float, f32)
 DEF_PAR_SPTS(double, f64)
+
+/* spts_csr_sync_free + its wrapper: src/parallel/src/spts_opt_32.wat:8-260.
+ * Each worker copies its share of b into y and clears its share of the ready
+ * flags; after a barrier, worker id takes rows id, id + nt, ... in order:
+ * t = y[i], then for every off-diagonal (in storage order) it waits until
+ * flag[col] == 1 and subtracts val * y[col]; y[i] = t / diagonal (stored
+ * last), then flag[i] = 1.  Rows always wait on smaller rows, which their
+ * owners reach in increasing order, so the lowest unsolved row can always
+ * proceed.  The spins are bounded here (the reference's are not): a wait that
+ * runs out sets the job's error word and the worker stops; the caller gets
+ * -1.  Same arithmetic per row as or_spts_syncfree (bit-identical). */
+#define SF_SPIN_LIMIT (1LL << 34)
+#define DEF_PAR_SF(T, SFX)                                                          \
+  static void par_sf_##SFX(par_job* jb, int id) {                                   \
+    const int nt = jb->nt;                                                          \
+    const int32_t* row_ptr = (const int32_t*)jb->a[0];                              \
+    const int32_t* col = (const int32_t*)jb->a[1];                                  \
+    const T* val = (const T*)jb->a[2];                                              \
+    const T* b = (const T*)jb->a[3];                                                \
+    T* y = (T*)jb->m[0];                                                            \
+    int32_t* flag = (int32_t*)jb->m[1];                                             \
+    int32_t* err = (int32_t*)jb->m[2];                                              \
+    const int32_t N = (int32_t)jb->n[0];                                            \
+    const int32_t npw = N / nt, remN = N - npw * nt;                                \
+    const int32_t s0 = id * npw, e0 = (id + 1) * npw + (id == nt - 1 ? remN : 0);   \
+    for (int32_t i = s0; i < e0; ++i) {                                             \
+      y[i] = b[i];                                                                  \
+      __atomic_store_n(&flag[i], 0, __ATOMIC_RELAXED);                              \
+    }                                                                               \
+    pthread_barrier_wait(&jb->bar);                                                 \
+    for (int32_t i = id; i < N; i += nt) {                                          \
+      const int32_t s = row_ptr[i], end = row_ptr[i + 1];                           \
+      T t = y[i];                                                                   \
+      for (int32_t k = s; k < end - 1; ++k) {                                       \
+        const int32_t c = col[k];                                                   \
+        int64_t spins = 0;                                                          \
+        while (__atomic_load_n(&flag[c], __ATOMIC_ACQUIRE) != 1) {                  \
+          if (__atomic_load_n(err, __ATOMIC_RELAXED) || ++spins > SF_SPIN_LIMIT) {  \
+            __atomic_store_n(err, 1, __ATOMIC_RELAXED);                             \
+            return;                                                                 \
+          }                                                                         \
+          if ((spins & 1023) == 0) sched_yield();                                   \
+        }                                                                           \
+        T p = val[k] * y[c];                                                        \
+        t = t - p;                                                                  \
+      }                                                                             \
+      y[i] = t / val[end - 1];                                                      \
+      __atomic_store_n(&flag[i], 1, __ATOMIC_RELEASE);                              \
+    }                                                                               \
+  }                                                                                 \
+  int or_par_spts_syncfree_##SFX(int nthreads, const int32_t* row_ptr,              \
+                                 const int32_t* col, const T* val, const T* b, T* y, \
+                                 int32_t N, int32_t* flag) {                        \
+    par_job job;                                                                    \
+    int32_t err = 0;                                                                \
+    job.nt = clamp_threads(nthreads);                                               \
+    job.fn = par_sf_##SFX;                                                          \
+    job.a[0] = row_ptr; job.a[1] = col; job.a[2] = val; job.a[3] = b;               \
+    job.m[0] = y; job.m[1] = flag; job.m[2] = &err; job.n[0] = N;                   \
+    par_run(&job);                                                                  \
+    return err ? -1 : 0;                                                            \
+  }
+DEF_PAR_SF(float, f32)
+DEF_PAR_SF(double, f64)
 
 /* ======================= checksum ======================= */
 

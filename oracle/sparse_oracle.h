@@ -147,6 +147,15 @@ void or_par_spts_level_f64(int nthreads, const int32_t* level_ptr, int32_t nleve
 void or_par_spts_level_f32(int nthreads, const int32_t* level_ptr, int32_t nlevels,
                            const int32_t* row_ptr, const int32_t* col, const float* val,
                            const float* b, float* y, int32_t N);
+/* Parallel sync-free CPU baseline: cyclic rows per worker, per-row ready
+ * flags (flag[N], caller-owned), bounded spins; 0 on success, -1 when a wait
+ * ran out (src/parallel/src/spts_opt_32.wat:8-260). */
+int or_par_spts_syncfree_f64(int nthreads, const int32_t* row_ptr, const int32_t* col,
+                             const double* val, const double* b, double* y, int32_t N,
+                             int32_t* flag);
+int or_par_spts_syncfree_f32(int nthreads, const int32_t* row_ptr, const int32_t* col,
+                             const float* val, const float* b, float* y, int32_t N,
+                             int32_t* flag);
 
 /* ---------------- checksum ---------------- */
 /* fletcher_sum: src/sequential/src/sparse32.js:1286-1311 (matlab_modulo on

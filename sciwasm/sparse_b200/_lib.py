@@ -82,6 +82,7 @@ SIGNATURES: dict[str, list] = {
     "sb_spts_analyze": [C.c_int, P, P, P, I32, I64, P, C.POINTER(P)],
     "sb_spts_plan_destroy": [P],
     "sb_spts_plan_info": [P, C.POINTER(I32), C.POINTER(I32)],
+    "sb_spts_plan_analysis_ms": [P, C.POINTER(C.c_float)],
     "sb_spts_plan_levels": [P, P, P, P, P, P],
     "sb_spts_plan_reordered": [P, P, P, P, P],
     "sb_spts_solve": [P, C.c_int, C.c_int, P, P, P],

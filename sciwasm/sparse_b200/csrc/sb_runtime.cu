@@ -67,9 +67,32 @@ int* device_status_word() {
   return words[dev];
 }
 
+// Stream-ordered scratch comes from the device's default memory pool.  By
+// default the pool hands freed memory back to the driver at every
+// synchronisation, so each call that needs scratch would map fresh pages;
+// keeping up to kPoolKeep bytes of freed scratch lets later calls reuse it.
+constexpr uint64_t kPoolKeep = 2ull << 30;
+
+static void keep_pool_memory() {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = kPoolKeep;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done[dev] = true;
+}
+
 int scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
   *p = nullptr;
   if (bytes == 0) bytes = 16;
+  keep_pool_memory();
   cudaError_t e = cudaMallocAsync(p, bytes, s);
   if (e != cudaSuccess) return cuda_status(e, "cudaMallocAsync(scratch)");
   return SB_OK;

@@ -9,7 +9,7 @@
 //     adaptive rows per warp) with unrolled independent loads and shuffle
 //     reductions, and the long ones with the whole warp.  An alternative
 //     streams fixed-size nonzero tiles into a shared-memory ring with bulk
-//     async copies (SB_CSR_KERNEL=s); a third cuts the nonzeros into
+//     async copies (option kernel 1); a third cuts the nonzeros into
 //     row-aligned warp ranges walked in 256-nonzero tiles (kernel 2).
 //   * COO walks 256-entry tiles, 8 entries per lane; every row segment is
 //     added with one atomic, so unsorted input is accepted.  With rows the
@@ -21,7 +21,6 @@
 //     diagonals runs a kernel with the count fixed at compile time.
 #include <algorithm>
 #include <climits>
-#include <stdlib.h>
 
 #include "sb_common.cuh"
 
@@ -965,36 +964,17 @@ static int launch_csr_stream(const int* row_ptr, const int* col, const S* val, c
   return SB_OK;
 }
 
-// CSR dispatch: the streaming kernel when col/val are 16-byte aligned (bulk
-// copies need it), the warp-tile kernel otherwise.  SB_CSR_KERNEL=tile forces
-// the warp-tile kernel (tuning runs).
-static int csr_kernel_choice() {
-  static int v = [] {
-    const char* e = getenv("SB_CSR_KERNEL");
-    return (e && e[0] == 's') ? 2 : 0;  // 's': streamed tiles
-  }();
-  return v;
-}
-
-static int csr_stream_tile() {
-  static int v = [] {
-    const char* e = getenv("SB_CSR_T");
-    return (e && atoi(e) == 2048) ? 2048 : 1024;
-  }();
-  return v;
-}
-
-// CSR dispatch.  opts (may be null): kernel 0 = row blocks, 1 = streamed
-// tiles (needs 16-byte aligned col/val); lanes_per_row / unroll 0 = default.
-// SB_CSR_KERNEL=s in the environment selects the streamed kernel by default.
+// CSR dispatch.  opts (may be null = row blocks with default options):
+// kernel 0 = row blocks (lanes_per_row / unroll 0 = default), 1 = streamed
+// tiles of 1024 nonzeros, or 2048 with unroll = 2048 (needs 16-byte aligned
+// col/val, else row blocks), 2 = nonzero tiles (unroll = tiles per warp).
 template <typename S, typename A>
 static int launch_csr(const int* row_ptr, const int* col, const S* val, const S* x, S* y, int N,
                       long long nnz, const sb_csr_opts* opts, cudaStream_t st) {
-  const int kernel = opts ? opts->kernel : (csr_kernel_choice() == 2 ? 1 : 0);
+  const int kernel = opts ? opts->kernel : 0;
   if (kernel == 2) return launch_csr_tiles<S, S>(row_ptr, col, val, x, y, N, nnz, opts->unroll, st);
   if (kernel == 1 && aligned16(col) && aligned16(val)) {
-    const int tile = (opts && opts->unroll == 2048) ? 2048 : csr_stream_tile();
-    if (tile == 2048) return launch_csr_stream<S, 2048, 3>(row_ptr, col, val, x, y, N, nnz, st);
+    if (opts->unroll == 2048) return launch_csr_stream<S, 2048, 3>(row_ptr, col, val, x, y, N, nnz, st);
     return launch_csr_stream<S, 1024, 4>(row_ptr, col, val, x, y, N, nnz, st);
   }
   return launch_csr_rows<S, S>(row_ptr, col, val, x, y, N, nnz, opts ? opts->lanes_per_row : 0,

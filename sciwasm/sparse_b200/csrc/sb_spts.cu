@@ -54,6 +54,8 @@ struct sb_spts_plan {
   int* ticket = nullptr;
   std::vector<int> h_level_ptr;
   std::vector<void*> owned;
+  cudaEvent_t ev[2] = {nullptr, nullptr};  // bracket the analysis's device work
+  float analysis_ms = 0.f;
 };
 
 namespace sb {
@@ -774,17 +776,17 @@ static int polling_grid(const void* kern, int algo, int N, int nlevels) {
   return std::min(full, sm_count());
 }
 
-static int plan_alloc(sb_spts_plan* p, void** out, size_t bytes) {
-  *out = nullptr;
-  cudaError_t e = cudaMalloc(out, bytes ? bytes : 16);
-  if (e != cudaSuccess) return cuda_status(e, "sb_spts_analyze: cudaMalloc");
-  p->owned.push_back(*out);
-  return SB_OK;
-}
+// The plan's device arrays live in one allocation (one cudaMalloc per plan,
+// not one per array); level_ptr is sized for the largest possible level
+// count, N + 1 (a row's level is at most its index + 1).
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 static void plan_release(sb_spts_plan* p) {
   for (void* q : p->owned) cudaFree(q);
   p->owned.clear();
+  if (p->ev[0]) cudaEventDestroy(p->ev[0]);
+  if (p->ev[1]) cudaEventDestroy(p->ev[1]);
+  p->ev[0] = p->ev[1] = nullptr;
 }
 
 template <typename T>
@@ -792,24 +794,42 @@ static int analyze_impl(sb_spts_plan* p, cudaStream_t st) {
   const int N = p->N;
   const long long nnz = p->nnz;
   int r;
-  void* m;
-#define SB_PA(ptr, bytes)                       \
-  if ((r = plan_alloc(p, &m, (bytes)))) return r; \
-  ptr = (decltype(ptr))m;
-  SB_PA(p->level, sizeof(int) * N);
-  SB_PA(p->perm, sizeof(int) * N);
-  SB_PA(p->order, sizeof(int) * N);
-  SB_PA(p->rrow, sizeof(int) * ((size_t)N + 1));
-  SB_PA(p->rcol, sizeof(int) * (size_t)nnz);
-  SB_PA(p->rval, sizeof(T) * (size_t)nnz);
-  SB_PA(p->ywork, sizeof(T) * N);
-  SB_PA(p->ticket, sizeof(int) * 4);
-#undef SB_PA
+  {
+    const size_t sizes[9] = {sizeof(int) * (size_t)N,           sizeof(int) * (size_t)N,
+                             sizeof(int) * (size_t)N,           sizeof(int) * ((size_t)N + 1),
+                             sizeof(int) * (size_t)nnz,         sizeof(T) * (size_t)nnz,
+                             sizeof(T) * (size_t)N,             sizeof(int) * 4,
+                             sizeof(int) * ((size_t)N + 2)};
+    size_t total = 0;
+    for (size_t b : sizes) total += align256(b);
+    void* slab = nullptr;
+    cudaError_t e = cudaMalloc(&slab, total);
+    if (e != cudaSuccess) return cuda_status(e, "sb_spts_analyze: cudaMalloc");
+    p->owned.push_back(slab);
+    char* q = (char*)slab;
+    void* part[9];
+    for (int k = 0; k < 9; ++k) {
+      part[k] = q;
+      q += align256(sizes[k]);
+    }
+    p->level = (int*)part[0];
+    p->perm = (int*)part[1];
+    p->order = (int*)part[2];
+    p->rrow = (int*)part[3];
+    p->rcol = (int*)part[4];
+    p->rval = part[5];
+    p->ywork = part[6];
+    p->ticket = (int*)part[7];
+    p->level_ptr = (int*)part[8];
+    SB_CHECK_CUDA(cudaEventCreate(&p->ev[0]));
+    SB_CHECK_CUDA(cudaEventCreate(&p->ev[1]));
+  }
   int* status = device_status_word();
   if (!status) {
     set_error("sb_spts_analyze: device status word unavailable");
     return SB_ENOMEM;
   }
+  SB_CHECK_CUDA(cudaEventRecord(p->ev[0], st));
   int* tmp = nullptr;  // [0] lower-check flag, [1] max level
   if ((r = scratch_alloc((void**)&tmp, 4 * sizeof(int), st))) return r;
   SB_CHECK_CUDA(cudaMemsetAsync(tmp, 0, 4 * sizeof(int), st));
@@ -837,11 +857,6 @@ static int analyze_impl(sb_spts_plan* p, cudaStream_t st) {
   p->solvable = h[0] ? 0 : 1;
   p->nlevels = N ? h[1] + 1 : 0;
   const int L = p->nlevels;
-  {
-    void* lp = nullptr;
-    if ((r = plan_alloc(p, &lp, sizeof(int) * ((size_t)L + 1)))) return r;
-    p->level_ptr = (int*)lp;
-  }
   // level_ptr = exclusive scan of the per-level counts
   SB_CHECK_CUDA(cudaMemsetAsync(p->level_ptr, 0, sizeof(int) * ((size_t)L + 1), st));
   level_hist<<<grid1(N), kT, 0, st>>>(p->level, N, p->level_ptr);
@@ -888,9 +903,12 @@ static int analyze_impl(sb_spts_plan* p, cudaStream_t st) {
   }
   if (!r) {
     p->h_level_ptr.resize((size_t)L + 1);
-    e = cudaMemcpyAsync(p->h_level_ptr.data(), p->level_ptr, sizeof(int) * ((size_t)L + 1),
-                        cudaMemcpyDeviceToHost, st);
+    e = cudaEventRecord(p->ev[1], st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(p->h_level_ptr.data(), p->level_ptr, sizeof(int) * ((size_t)L + 1),
+                          cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&p->analysis_ms, p->ev[0], p->ev[1]);
     if (e != cudaSuccess) r = cuda_status(e, "sb_spts_analyze");
   }
   scratch_free(mem, st);
@@ -1313,14 +1331,14 @@ int sb_spts_syncfree_csr_noalloc(int dtype, const int32_t* row_ptr, const int32_
   const long long limit = spin_limit_cycles > 0 ? spin_limit_cycles : kDefaultSpin;
   if (dtype == SB_F64) {
     auto k = spts_syncfree_rows<double, double>;
-    k<<<resident_grid((const void*)k), kT, 0, st>>>(row_ptr, col, (const double*)val, N,
-                                                     (const double*)b, (double*)y, flags, ticket,
-                                                     limit, status);
+    k<<<natural_order_grid((const void*)k), kT, 0, st>>>(row_ptr, col, (const double*)val, N,
+                                                          (const double*)b, (double*)y, flags,
+                                                          ticket, limit, status);
   } else {
     auto k = spts_syncfree_rows<float, float>;
-    k<<<resident_grid((const void*)k), kT, 0, st>>>(row_ptr, col, (const float*)val, N,
-                                                     (const float*)b, (float*)y, flags, ticket,
-                                                     limit, status);
+    k<<<natural_order_grid((const void*)k), kT, 0, st>>>(row_ptr, col, (const float*)val, N,
+                                                          (const float*)b, (float*)y, flags,
+                                                          ticket, limit, status);
   }
   SB_CHECK_LAUNCH("spts_syncfree_rows");
   int dstat = 0;
@@ -1378,6 +1396,12 @@ int sb_spts_plan_info(const sb_spts_plan* plan, int32_t* nlevels, int32_t* solva
   SB_REQUIRE(plan && nlevels && solvable, "sb_spts_plan_info: null argument");
   *nlevels = plan->nlevels;
   *solvable = plan->solvable;
+  return SB_OK;
+}
+
+int sb_spts_plan_analysis_ms(const sb_spts_plan* plan, float* ms) {
+  SB_REQUIRE(plan && ms, "sb_spts_plan_analysis_ms: null argument");
+  *ms = plan->analysis_ms;
   return SB_OK;
 }
 

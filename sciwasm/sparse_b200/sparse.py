@@ -907,6 +907,9 @@ class SptsPlan:
         call("sb_spts_plan_info", self.ptr, C.byref(nl), C.byref(ok))
         self.nlevels = int(nl.value)
         self.solvable = bool(ok.value)
+        ms = C.c_float(0.0)
+        call("sb_spts_plan_analysis_ms", self.ptr, C.byref(ms))
+        self.analysis_ms = float(ms.value)
 
     def levels(self, stream=None):
         """(level, level_ptr, permutation, order) as device arrays."""

@@ -183,6 +183,21 @@ def test_level_solves_agree(oracle):
     assert np.array_equal(yp, y_lv)
 
 
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("nt", [1, 3, 5, 8])
+def test_parallel_syncfree_matches_serial(oracle, dt, nt):
+    """The pthread sync-free baseline (cyclic rows, ready flags) gives the
+    serial sync-free restatement's bits for any worker count."""
+    for rp, col, val in (synth.random_lower(20_000, seed=5, band=300, dtype=dt),
+                         synth.laplacian_3d_lower(12, dtype=dt)):
+        N = rp.size - 1
+        b = synth.uniform_vec(N, 6, dtype=dt)
+        want = oracle.spts_syncfree(rp, col, val, b)
+        y = np.full(N, np.nan, dt)
+        oracle.par_spts_syncfree(nt, rp, col, val, b, y)
+        assert np.array_equal(y.view(np.uint8), want.view(np.uint8))
+
+
 def test_laplacian3d_levels(oracle):
     rp, col, val = synth.laplacian_3d_lower(16)
     ls = oracle.level_sets(rp, col, val)

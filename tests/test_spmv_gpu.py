@@ -177,19 +177,6 @@ def test_zero_sized_calls_are_noops(gpu):
     assert yv.array().tolist() == [2.0, 2.0, 2.0]
 
 
-def _csr_check_all(sb, orc):
-    """Parity of every CSR case; run in a child process by the test below."""
-    for dt in DTYPES:
-        for name, (rp, col, val) in _mats(dt).items():
-            N = rp.size - 1
-            x, y0 = _x_y(N, dt)
-            A = sb.csr_from_host(rp, col, val)
-            xv, yv = sb.vec_from_host(x), sb.vec_from_host(y0)
-            sb.spmv(A, xv, yv)
-            err = rel_err(yv.array(), orc.truth_csr(rp, col, val, x, y0))
-            assert err <= TOL[np.dtype(dt)], (name, dt, err)
-
-
 @pytest.mark.parametrize("storage", ["f32", "f64", "bf16"])
 @pytest.mark.parametrize("tiles", [1, 4, 16])
 def test_csr_nonzero_tile_kernel(gpu, oracle, storage, tiles):
@@ -219,24 +206,18 @@ def test_csr_nonzero_tile_kernel(gpu, oracle, storage, tiles):
         assert np.array_equal(outs[0][empty].view(np.uint8), y0[empty].view(np.uint8)), name
 
 
-@pytest.mark.parametrize("tile", ["1024", "2048"])
-def test_csr_streamed_tile_kernel(gpu, tile):
-    """The alternative bulk-copy streamed-tile CSR kernel (SB_CSR_KERNEL=s)."""
-    import os
-    import subprocess
-    import sys
-    env = dict(os.environ, SB_CSR_KERNEL="s", SB_CSR_T=tile)
-    r = subprocess.run([sys.executable, __file__, "--csr-check"], env=env, capture_output=True,
-                       text=True, timeout=600)
-    assert r.returncode == 0, r.stdout + r.stderr
-
-
-if __name__ == "__main__":
-    import os
-    import sys
-    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-    if "--csr-check" in sys.argv:
-        import sciwasm.sparse_b200 as _sb
-        from oracle import binding as _orc
-        _csr_check_all(_sb, _orc)
-        print("ok")
+@pytest.mark.parametrize("tile", [1024, 2048])
+def test_csr_streamed_tile_kernel(gpu, oracle, tile):
+    """Kernel 1 (bulk-copy streamed tiles of 1024 or 2048 nonzeros through a
+    shared-memory ring), selected by the options struct."""
+    from sciwasm.sparse_b200 import _lib
+    for dt in DTYPES:
+        for name, (rp, col, val) in _mats(dt).items():
+            N = rp.size - 1
+            x, y0 = _x_y(N, dt)
+            A = gpu.csr_from_host(rp, col, val)
+            A.opts = _lib.CsrOpts(1, 0, tile, 0)
+            xv, yv = gpu.vec_from_host(x), gpu.vec_from_host(y0)
+            gpu.spmv(A, xv, yv)
+            err = rel_err(yv.array(), oracle.truth_csr(rp, col, val, x, y0))
+            assert err <= TOL[np.dtype(dt)], (name, dt, err)
