@@ -35,7 +35,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-SECTIONS = ("batched", "laplacian4096_fp32", "spts", "serving", "powerlaw_csr")
+SECTIONS = ("batched", "laplacian4096_fp32", "spts", "serving", "powerlaw_csr", "serving_sweep")
 METRIC = "served SpMV/SpTS req/s + p99 vs plain path; SpMV HBM GB/s at \u22641e-5 rel err"
 UNIT = "GB/s"
 
@@ -1103,6 +1103,70 @@ def run_serving(args):
     return out
 
 
+def run_serving_sweep(args):
+    """Serving at several arrival rates on one resident pool: for each rate
+    the same Poisson trace (args.sweep_seconds long) is served batched and
+    per call (the per-call path on at most its first args.plain_seconds,
+    since above its capacity its queue only grows); then one long batched
+    trace (args.serve_seconds) at args.serve_rate.  Per-op p50/p99 for both."""
+    from sciwasm.sparse_b200 import serve
+    from sciwasm.sparse_b200.sparse import PinnedBuffer
+    t0 = time.perf_counter()
+    pool, mv, ts = build_serving_pool(args.serve_pool, 1000, args.serve_max_rows)
+    build_s = time.perf_counter() - t0
+    in_ring = PinnedBuffer(1 << 30)
+    out_ring = PinnedBuffer(1 << 30)
+    xs = in_ring.view(0, in_ring.nbytes // 4, np.float32)
+    np.random.default_rng(5).random(out=xs, dtype=np.float32)
+    xs *= 2
+    xs -= 1
+    srv = serve.Server(pool, max_batch=args.serve_batch, slots=args.serve_slots,
+                       spts_slots=args.serve_spts_slots, spts_batch=args.serve_spts_batch)
+    warm = serving_requests(pool, mv, ts, 2000.0, 0.2, in_ring, out_ring, seed=99)
+    for mode in ("batched", "plain"):
+        srv.serve([serve.Request(r.rid, 0.0, r.matrix, r.op, r.storage, r.x, r.y)
+                   for r in warm], mode)
+    keys = ("requests", "req_per_s", "p50_ms", "p99_ms", "spmv_p50_ms", "spmv_p99_ms",
+            "spts_p50_ms", "spts_p99_ms", "mean_batch", "span_s")
+
+    def pick(st):
+        return {k: (round(st[k], 3) if isinstance(st[k], float) else st[k])
+                for k in keys if k in st}
+    sweep = {}
+    for rate in [float(v) for v in args.serve_rates.split(",")]:
+        reqs = serving_requests(pool, mv, ts, rate, args.sweep_seconds, in_ring, out_ring,
+                                seed=int(rate) % 1000 + 17)
+        b = srv.serve(reqs, "batched")
+        n_plain = max(1, min(len(reqs), int(rate * args.plain_seconds)))
+        prefix = reqs[:n_plain]
+        for r in prefix:
+            r.t_done = -1.0
+        p = srv.serve(prefix, "plain")
+        sweep[f"{int(rate)}"] = {"batched": pick(b), "plain": pick(p),
+                                 "plain_prefix_s": round(prefix[-1].t_arrival, 3)}
+        print(json.dumps({"rate": rate, **sweep[f"{int(rate)}"]}), file=sys.stderr, flush=True)
+    reqs = serving_requests(pool, mv, ts, args.serve_rate, args.serve_seconds, in_ring, out_ring)
+    long_b = srv.serve(reqs, "batched")
+    deepest = max(pool.mats[n].plans["f32"].nlevels for n in ts)
+    out = {"pool": f"{args.serve_pool} matrices, rows log-uniform in [1000, "
+                   f"{args.serve_max_rows}], 70% SpMV / 30% SpTS requests",
+           "pool_build_s": round(build_s, 2), "deepest_factor_levels": deepest,
+           "formats": dict(collections_counter(pool.mats[n].format for n in mv)),
+           "sweep_seconds": args.sweep_seconds, "plain_seconds": args.plain_seconds,
+           "sweep": sweep,
+           "long_trace": {"rate": args.serve_rate, "seconds": args.serve_seconds,
+                          "batched": pick(long_b)}}
+    pool.close()
+    in_ring.free()
+    out_ring.free()
+    return out
+
+
+def collections_counter(it):
+    import collections
+    return collections.Counter(it)
+
+
 def _pinned(nbytes):
     import ctypes
     from sciwasm.sparse_b200 import _lib
@@ -1150,6 +1214,12 @@ def main():
     ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--serve-spts-slots", type=int, default=1)
     ap.add_argument("--serve-spts-batch", type=int, default=256)
+    ap.add_argument("--serve-rates", default="1000,2000,3000,10000,20000",
+                    help="serving_sweep: arrival rates (req/s)")
+    ap.add_argument("--sweep-seconds", type=float, default=3.0,
+                    help="serving_sweep: trace length per rate")
+    ap.add_argument("--plain-seconds", type=float, default=2.0,
+                    help="serving_sweep: trace prefix served by the per-call path")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -1183,6 +1253,8 @@ def main():
             out = run_spts_section(stream)
         elif args.workload == "powerlaw_csr":
             out = run_powerlaw_csr(stream, peak, args.csr_opts, args.small)
+        elif args.workload == "serving_sweep":
+            out = run_serving_sweep(args)
         else:
             out = run_serving(args)
         print(json.dumps({"workload": args.workload, "result": out}), flush=True)

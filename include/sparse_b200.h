@@ -123,7 +123,8 @@ int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const voi
  * 1 = streamed nonzero tiles (1024 per tile, 2048 with unroll = 2048; F32
  * and F64 with 16-byte aligned col/val, else row blocks), 2 = nonzero tiles
  * over row-aligned warp ranges (unroll = 256-nonzero tiles per warp, 1..64;
- * F32, F64 and BF16;
+ * F32, F64 and BF16), 3 = block stream (a warp per 32-row block walks the
+ * block's nonzeros in 256-entry chunks with vector loads; F32, F64 and BF16;
  * every row written once, no atomics); lanes_per_row 1..32 (power of two)
  * and unroll 2/4/8 tune the row-block kernel, 0 = chosen from the mean row
  * length; grid 0 = a resident grid striding over 32-row blocks (regular
@@ -146,6 +147,58 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
 int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                     const void* x, int32_t N, int64_t nnz, int32_t reps, sb_csr_opts* best,
                     float* best_ms, void* stream);
+
+/* Format and kernel choice for SpMV on one CSR matrix (no counterpart in the
+ * reference, whose users pick coo_csr / csr_dia / csr_ell by hand,
+ * src/sequential/src/sparse32.js:1436-1720).  From the matrix's statistics
+ * (N, nnz, max row length nc, diagonal count nd) it records which of DIA and
+ * ELL the reference's admission test allows and the compulsory bytes of one
+ * y <- y + A x per format (bytes[]: CSR, DIA, ELL, COO).
+ *   mode SB_TUNE_MODEL: format = the admitted format with the fewest bytes,
+ *     csr = options from the row-length statistics; nothing is timed (x may
+ *     be NULL).
+ *   mode SB_TUNE_TIMED: every admitted format within twice the CSR bytes is
+ *     timed on the device (reps calls each on a scratch y; ms[] per format,
+ *     -1 when not timed): CSR with the options of sb_csr_autotune, DIA and
+ *     ELL built into scratch, COO with rows expanded from row_ptr; format =
+ *     the fastest, csr = the best CSR options.  BF16 values time CSR only.
+ * format is SB_FMT_CSR, SB_FMT_DIA, SB_FMT_ELL or SB_FMT_COO.  Returns when
+ * done; the matrix itself is not changed. */
+#define SB_TUNE_MODEL 0
+#define SB_TUNE_TIMED 1
+#define SB_FMT_CSR 0
+#define SB_FMT_DIA 1
+#define SB_FMT_ELL 2
+#define SB_FMT_COO 3
+typedef struct sb_spmv_choice {
+  int32_t format;
+  sb_csr_opts csr;
+  int32_t ndiags;
+  int32_t ncols;
+  int32_t dia_admitted;
+  int32_t ell_admitted;
+  float ms[4];
+  int64_t bytes[4];
+} sb_spmv_choice;
+int sb_spmv_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                     const void* x, int32_t N, int64_t nnz, int32_t mode, int32_t reps,
+                     sb_spmv_choice* choice, void* stream);
+
+/* The COO form of a CSR matrix (no counterpart in the reference): coo_row
+ * expanded from row_ptr (rows non-decreasing, so SB_COO_ROWS_SORTED holds),
+ * col and val copied; outputs caller-allocated, stream-ordered. */
+int sb_csr_coo(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val, int32_t N,
+               int64_t nnz, int32_t* coo_row, int32_t* coo_col, void* coo_val, void* stream);
+
+/* The floor of an SpMV on this matrix (no counterpart in the reference):
+ * *out += sum over k of val[k] * x[col[k]] (the sum of all entries of A x),
+ * accumulated per warp in the value type and added to *out (a device double)
+ * with one atomic per warp.  It reads the column and value streams an SpMV
+ * must read and gathers x once per entry, with no row structure, so its time
+ * bounds every SpMV kernel on the same col/val/x from below.  col and val
+ * must be 16-byte aligned. */
+int sb_gather_dot(int dtype, const int32_t* col, const void* val, const void* x, int64_t nnz,
+                  double* out, void* stream);
 
 /* Reduced-precision storage (no counterpart in the reference, which keeps
  * f32 or f64 values): sb_spmv_csr / sb_spmv_csr_ex accept dtype SB_BF16 for
@@ -174,11 +227,18 @@ int sb_spmv_ell(int dtype, const int32_t* indices, const void* data, int32_t N, 
 /* matrix and vector, src/sequential/src/sparse32.js:1232-1286).            */
 /* ---------------------------------------------------------------------- */
 
-/* One CSR matrix of a batch: y <- y + A x for nrhs (1..8) right-hand sides,
- * x and y stored N x nrhs row-major (x[col*nrhs + j]).  lanes: lanes per row
- * (1..32, power of two), 0 = chosen from nnz/N.  flags bit 0 set: y <- A x
- * (y is overwritten, rows without entries get 0).  The y ranges of different
- * items must not overlap (x may be shared). */
+/* One matrix of a batch: y <- y + A x for nrhs (1..8) right-hand sides, x
+ * and y stored N x nrhs row-major (x[col*nrhs + j]).  flags bit 0 set:
+ * y <- A x (y is overwritten, rows without entries get 0).  The y ranges of
+ * different items must not overlap (x may be shared).
+ *   format SB_FMT_CSR (0): row_ptr[N+1], col[nnz], val[nnz]; lanes: lanes
+ *     per row (1..32, power of two), 0 = chosen from nnz/N.
+ *   format SB_FMT_DIA (1): row_ptr = offsets[width] (ascending, as csr_dia
+ *     makes them), val = data[width*N] diagonal-major (stride N); each row is
+ *     bit-identical to sb_spmv_dia (the reference's per-row order).
+ *   format SB_FMT_ELL (2): col = indices[width*N] and val = data[width*N],
+ *     column-major; each row is bit-identical to sb_spmv_ell.
+ * Zero-initialised trailing fields (format 0, width 0) describe a CSR item. */
 typedef struct sb_batch_item {
   const int32_t* row_ptr;
   const int32_t* col;
@@ -190,6 +250,8 @@ typedef struct sb_batch_item {
   int32_t lanes;
   int32_t flags;
   int64_t nnz;
+  int32_t format;
+  int32_t width;
 } sb_batch_item;
 
 typedef struct sb_batch_exec sb_batch_exec;

@@ -110,7 +110,18 @@ class CsrOpts(C.Structure):
 
 class BatchItem(C.Structure):
     _fields_ = [("row_ptr", P), ("col", P), ("val", P), ("x", P), ("y", P), ("N", I32),
-                ("nrhs", I32), ("lanes", I32), ("flags", I32), ("nnz", I64)]
+                ("nrhs", I32), ("lanes", I32), ("flags", I32), ("nnz", I64), ("format", I32),
+                ("width", I32)]
+
+
+SB_FMT_CSR, SB_FMT_DIA, SB_FMT_ELL, SB_FMT_COO = 0, 1, 2, 3
+SB_TUNE_MODEL, SB_TUNE_TIMED = 0, 1
+
+
+class SpmvChoice(C.Structure):
+    _fields_ = [("format", I32), ("csr", CsrOpts), ("ndiags", I32), ("ncols", I32),
+                ("dia_admitted", I32), ("ell_admitted", I32), ("ms", C.c_float * 4),
+                ("bytes", I64 * 4)]
 
 
 class MMHeader(C.Structure):
@@ -146,6 +157,9 @@ SIGNATURES.update({
     "sb_batch_exec_run": [P, C.POINTER(BatchItem), I32, P],
     "sb_convert_values": [C.c_int, P, C.c_int, P, I64, P],
     "sb_spmv_csr_ex": [C.c_int, P, P, P, P, P, I32, I64, I32, C.POINTER(CsrOpts), P],
+    "sb_gather_dot": [C.c_int, P, P, P, I64, P, P],
+    "sb_spmv_autotune": [C.c_int, P, P, P, P, I32, I64, I32, I32, C.POINTER(SpmvChoice), P],
+    "sb_csr_coo": [C.c_int, P, P, P, I32, I64, P, P, P, P],
     "sb_csr_autotune": [C.c_int, P, P, P, P, I32, I64, I32, C.POINTER(CsrOpts),
                         C.POINTER(C.c_float), P],
 })

@@ -1,5 +1,6 @@
-// sb_batch.cu -- batched CSR SpMV: many matrices and right-hand sides in one
-// persistent launch, replayed from a captured CUDA graph.
+// sb_batch.cu -- batched SpMV: many matrices (CSR, DIA or ELL) and
+// right-hand sides in one persistent launch, replayed from a captured CUDA
+// graph.
 //
 // No counterpart in the reference (it calls spmv once per matrix and vector,
 // src/sequential/src/sparse32.js:1232-1286).  Work is a flat list of 32-row
@@ -10,7 +11,9 @@
 // per warp" autotuning) and each long row with the whole warp (compensated
 // f32 sums); with several right-hand sides (x and y are N x nrhs, row-major,
 // nrhs <= 8) the right-hand sides go across lanes instead, so that one load
-// gathers all of a column's x values.  Values are stored f32, f64 or BF16
+// gathers all of a column's x values.  DIA and ELL items take one row per
+// lane in the reference's per-row order (bit-identical to sb_spmv_dia /
+// sb_spmv_ell).  Values are stored f32, f64 or BF16
 // (f32 vectors and sums for f32/BF16).  The executor keeps descriptors
 // in pinned host and device buffers; one run = the graph [copy descriptors,
 // reset the counter, kernel] launched on the caller's stream.
@@ -266,8 +269,69 @@ __device__ __forceinline__ void batch_block_rhs(const sb_batch_item& it, int r0,
   }
 }
 
+template <typename T> __device__ __forceinline__ T bmul_rn(T a, T b);
+template <> __device__ __forceinline__ float bmul_rn(float a, float b) { return __fmul_rn(a, b); }
+template <> __device__ __forceinline__ double bmul_rn(double a, double b) { return __dmul_rn(a, b); }
+template <typename T> __device__ __forceinline__ T badd_rn(T a, T b);
+template <> __device__ __forceinline__ float badd_rn(float a, float b) { return __fadd_rn(a, b); }
+template <> __device__ __forceinline__ double badd_rn(double a, double b) { return __dadd_rn(a, b); }
+
+// One 32-row block of a DIA item, one row per lane: for each diagonal in
+// stored order, the separately rounded product of the in-band entry and x is
+// added to the row's running value (the order and rounding of sb_spmv_dia,
+// src/sequential/src/sparse_opt_32.wat:290-407), for every right-hand side.
 template <typename SV, typename T>
-__global__ void __launch_bounds__(kBT)
+__device__ __forceinline__ void batch_block_dia(const sb_batch_item& it, int r0, int lane) {
+  const int i = r0 + lane;
+  const int N = it.N;
+  if (i >= N) return;
+  const int K = it.nrhs;
+  const int nd = it.width;
+  const int* __restrict__ off = it.row_ptr;
+  const SV* __restrict__ data = (const SV*)it.val;
+  const T* __restrict__ x = (const T*)it.x;
+  T* __restrict__ y = (T*)it.y;
+  const bool overwrite = (it.flags & 1) != 0;
+  // one right-hand side at a time (few registers); the data re-reads of the
+  // later ones hit L1
+  for (int h = 0; h < K; ++h) {
+    T t = overwrite ? (T)0 : y[(long long)i * K + h];
+    for (int d = 0; d < nd; ++d) {
+      const int k = __ldg(off + d);
+      if ((unsigned)(i + k) >= (unsigned)N) continue;
+      t = badd_rn(bmul_rn((T)ldv(data, (long long)d * N + i), __ldg(x + (long long)(i + k) * K + h)),
+                  t);
+    }
+    y[(long long)i * K + h] = t;
+  }
+}
+
+// One 32-row block of an ELL item, one row per lane, slots in stored order
+// (padding included), as sb_spmv_ell (src/sequential/src/sparse_opt_32.wat:427-479).
+template <typename SV, typename T>
+__device__ __forceinline__ void batch_block_ell(const sb_batch_item& it, int r0, int lane) {
+  const int i = r0 + lane;
+  const int N = it.N;
+  if (i >= N) return;
+  const int K = it.nrhs;
+  const int nc = it.width;
+  const int* __restrict__ idx = it.col;
+  const SV* __restrict__ data = (const SV*)it.val;
+  const T* __restrict__ x = (const T*)it.x;
+  T* __restrict__ y = (T*)it.y;
+  const bool overwrite = (it.flags & 1) != 0;
+  for (int h = 0; h < K; ++h) {
+    T t = overwrite ? (T)0 : y[(long long)i * K + h];
+    for (int s = 0; s < nc; ++s) {
+      const long long o = (long long)s * N + i;
+      t = badd_rn(bmul_rn((T)ldv(data, o), __ldg(x + (long long)__ldg(idx + o) * K + h)), t);
+    }
+    y[(long long)i * K + h] = t;
+  }
+}
+
+template <typename SV, typename T>
+__global__ void __launch_bounds__(kBT, 5)
     batch_kernel(const sb_batch_item* __restrict__ items, const long long* __restrict__ offsets,
                  int* __restrict__ count) {
   const int lane = threadIdx.x & 31;
@@ -289,6 +353,14 @@ __global__ void __launch_bounds__(kBT)
       }
       const sb_batch_item it = items[lo];
       const int r0 = (int)((w - __ldg(offsets + lo)) * 32);
+      if (it.format == SB_FMT_DIA) {
+        batch_block_dia<SV, T>(it, r0, lane);
+        continue;
+      }
+      if (it.format == SB_FMT_ELL) {
+        batch_block_ell<SV, T>(it, r0, lane);
+        continue;
+      }
       if (it.nrhs > 1) {
         if (it.nrhs == 2) batch_block_rhs<SV, T, 2>(it, r0, lane);
         else if (it.nrhs <= 4) batch_block_rhs<SV, T, 4>(it, r0, lane);
@@ -417,10 +489,21 @@ int sb_batch_exec_run(sb_batch_exec* e, const sb_batch_item* items, int32_t n, v
     sb_batch_item it = items[i];
     SB_REQUIRE(it.N >= 0 && it.nrhs >= 1 && it.nrhs <= kMaxRhs,
                "sb_batch_exec_run: item %d: N >= 0 and 1 <= nrhs <= 8 required", i);
-    SB_REQUIRE(it.N == 0 || (it.row_ptr && it.x && it.y && (it.nnz == 0 || (it.col && it.val))),
-               "sb_batch_exec_run: item %d: null pointer", i);
-    if (it.lanes <= 0) it.lanes = lanes_for(it.nnz, it.N);
-    it.lanes = it.lanes > 32 ? 32 : it.lanes;
+    SB_REQUIRE(it.format == SB_FMT_CSR || it.format == SB_FMT_DIA || it.format == SB_FMT_ELL,
+               "sb_batch_exec_run: item %d: unknown format %d", i, it.format);
+    if (it.format == SB_FMT_CSR) {
+      SB_REQUIRE(it.N == 0 || (it.row_ptr && it.x && it.y && (it.nnz == 0 || (it.col && it.val))),
+                 "sb_batch_exec_run: item %d: null pointer", i);
+      if (it.lanes <= 0) it.lanes = lanes_for(it.nnz, it.N);
+      it.lanes = it.lanes > 32 ? 32 : it.lanes;
+    } else {
+      SB_REQUIRE(it.width >= 0, "sb_batch_exec_run: item %d: negative width", i);
+      const bool need_idx = it.width > 0 && it.N > 0;
+      SB_REQUIRE(it.N == 0 || (it.x && it.y), "sb_batch_exec_run: item %d: null vector", i);
+      SB_REQUIRE(!need_idx || (it.val && (it.format == SB_FMT_DIA ? it.row_ptr != nullptr
+                                                                 : it.col != nullptr)),
+                 "sb_batch_exec_run: item %d: null pointer", i);
+    }
     e->h_items[i] = it;
     e->h_offsets[i] = acc;
     acc += ((long long)it.N + 31) / 32;

@@ -786,6 +786,200 @@ static int launch_csr_tiles(const int* row_ptr, const int* col, const SV* val, c
   return SB_OK;
 }
 
+// ------------------------------------------------------------ CSR (block stream)
+
+// Block-stream CSR: a warp owns 32 consecutive rows, as in the row-block
+// kernel, but walks their nonzeros as one flat stream of 256-entry chunks:
+// 8 consecutive entries per lane loaded with 16-byte vector loads and their
+// 8 x gathers in flight together, whatever the row lengths.  Each entry's row
+// is found among the block's row starts, which the lanes hold one each (a
+// shuffle binary search for a lane's first entry, then shuffle steps across
+// row ends).  Rows are summed by lane-local runs and a warp segmented scan;
+// a row cut by a chunk boundary is carried into the next chunk.  Every
+// complete row sum lands once in a per-warp shared array, and the block's
+// rows are written at the end with one coalesced y[i] = y[i] + sum (rows
+// without entries are not written).  The summation order is fixed by the
+// matrix, so results are identical run to run.
+template <typename SV, typename T, bool VEC>
+__global__ void __launch_bounds__(kWarpsPerCta * kWarp)
+    csr_block_stream_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
+                            const SV* __restrict__ val, const T* __restrict__ x,
+                            T* __restrict__ y, int N, long long nnz) {
+  __shared__ T rowsum_all[kWarpsPerCta][kWarp];
+  const int lane = threadIdx.x & (kWarp - 1);
+  T* rowsum = rowsum_all[threadIdx.x >> 5];
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w * kWarp >= N) return;
+  const int r0 = (int)(w * kWarp);
+  const int rr = r0 + lane;
+  const int s_l = __ldg(row_ptr + min(rr, N));      // start of this lane's row
+  const int n_l = __ldg(row_ptr + min(rr + 1, N));  // its end (next row's start)
+  const bool has = rr < N && n_l > s_l;
+  const T y_l = has ? y[rr] : (T)0;
+  rowsum[lane] = (T)0;
+  __syncwarp();
+  const long long b_lo = __shfl_sync(kFull, s_l, 0);
+  const long long b_hi = __shfl_sync(kFull, n_l, kWarp - 1);
+  int carry_row = -1;
+  T carry = 0;
+  for (long long kb = b_lo & ~7LL; kb < b_hi; kb += kTile) {
+    const long long k0 = kb + (long long)kItems * lane;
+    int c[kItems];
+    T v[kItems];
+    if (VEC && k0 + kItems <= nnz) {
+      const int4 c0 = ld_stream_v4(col + k0), c1 = ld_stream_v4(col + k0 + 4);
+      c[0] = c0.x; c[1] = c0.y; c[2] = c0.z; c[3] = c0.w;
+      c[4] = c1.x; c[5] = c1.y; c[6] = c1.z; c[7] = c1.w;
+      load_vals8<SV, T>(val, k0, v);
+    } else {
+#pragma unroll
+      for (int e = 0; e < kItems; ++e) {
+        const long long k = k0 + e;
+        c[e] = k < nnz ? ld_stream(col + k) : 0;
+        v[e] = k < nnz ? (T)ld_val(val + k) : (T)0;
+      }
+    }
+    T p[kItems];
+#pragma unroll
+    for (int e = 0; e < kItems; ++e) {
+      const long long k = k0 + e;
+      p[e] = (k >= b_lo && k < b_hi) ? v[e] * ld_ro(x + c[e]) : (T)0;
+    }
+    // row of each entry: the largest j with start_j <= k (empty rows share
+    // their start with the next row and are skipped)
+    int j = 0;
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1) {
+      const long long sc = __shfl_sync(kFull, s_l, j + st);
+      if (sc <= k0) j += st;
+    }
+    long long nb = __shfl_sync(kFull, n_l, j);
+    int r[kItems];
+    r[0] = j;
+#pragma unroll
+    for (int e = 1; e < kItems; ++e) {
+      const long long k = k0 + e;
+      bool need = k >= nb && j < kWarp - 1;
+      while (__any_sync(kFull, need)) {
+        const int j2 = need ? j + 1 : j;
+        const long long nb2 = __shfl_sync(kFull, n_l, j2);
+        if (need) {
+          j = j2;
+          nb = nb2;
+        }
+        need = k >= nb && j < kWarp - 1;
+      }
+      r[e] = j;
+    }
+#pragma unroll
+    for (int e = 0; e < kItems; ++e) {
+      const long long k = k0 + e;
+      if (k < b_lo || k >= b_hi) r[e] = -1;  // not this block's entry (product 0)
+    }
+    // the open row of the previous chunk: continued by lane 0, or complete
+    const int r00 = __shfl_sync(kFull, r[0], 0);
+    if (carry_row >= 0 && r00 != carry_row) {
+      if (lane == 0) rowsum[carry_row] = carry;
+      carry_row = -1;
+    }
+    if (lane == 0 && carry_row >= 0) p[0] = carry + p[0];
+    // lane-local runs; a run strictly inside a lane is a whole row
+    const int start_row = r[0];
+    int cur = start_row;
+    T acc = 0, first_val = 0;
+    bool internal = false;
+#pragma unroll
+    for (int e = 0; e < kItems; ++e) {
+      if (r[e] != cur) {
+        if (!internal) {
+          internal = true;
+          first_val = acc;
+        } else if (cur >= 0) {
+          rowsum[cur] = acc;
+        }
+        cur = r[e];
+        acc = 0;
+      }
+      acc += p[e];
+    }
+    const int end_row = cur;
+    const int prev_end = __shfl_up_sync(kFull, end_row, 1);
+    const bool cont_prev = lane > 0 && start_row == prev_end;
+    bool hf = internal || !cont_prev;
+    T sum = acc;
+#pragma unroll
+    for (int off = 1; off < kWarp; off <<= 1) {
+      const T o = __shfl_up_sync(kFull, sum, off);
+      const bool f = __shfl_up_sync(kFull, hf, off);
+      if (lane >= off) {
+        if (!hf) sum += o;
+        hf = hf || f;
+      }
+    }
+    const T from_prev = __shfl_up_sync(kFull, sum, 1);
+    if (internal && start_row >= 0) rowsum[start_row] = first_val + (cont_prev ? from_prev : (T)0);
+    const int next_start = __shfl_down_sync(kFull, start_row, 1);
+    if (lane < kWarp - 1 && next_start != end_row && end_row >= 0) rowsum[end_row] = sum;
+    carry_row = __shfl_sync(kFull, end_row, kWarp - 1);
+    carry = __shfl_sync(kFull, sum, kWarp - 1);
+  }
+  if (lane == 0 && carry_row >= 0) rowsum[carry_row] = carry;
+  __syncwarp();
+  if (has) y[rr] = y_l + rowsum[lane];
+}
+
+template <typename SV, typename T>
+static int launch_csr_block_stream(const int* row_ptr, const int* col, const SV* val, const T* x,
+                                   T* y, int N, long long nnz, cudaStream_t st) {
+  const long long warps = ((long long)N + kWarp - 1) / kWarp;
+  const long long ctas = (warps + kWarpsPerCta - 1) / kWarpsPerCta;
+  const int threads = kWarpsPerCta * kWarp;
+  if (aligned16(col) && aligned16(val))
+    csr_block_stream_kernel<SV, T, true><<<(unsigned)ctas, threads, 0, st>>>(row_ptr, col, val, x,
+                                                                             y, N, nnz);
+  else
+    csr_block_stream_kernel<SV, T, false><<<(unsigned)ctas, threads, 0, st>>>(row_ptr, col, val,
+                                                                              x, y, N, nnz);
+  SB_CHECK_LAUNCH("csr_block_stream_kernel");
+  return SB_OK;
+}
+
+// ------------------------------------------------------------ gather floor
+
+// sum += val[k] * x[col[k]] over all entries: the column and value streams an
+// SpMV must read and its x gathers, without any row structure.  8 entries
+// per lane per step with vector loads, partial sums reduced per warp, one
+// atomic per warp.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    gather_dot_kernel(const int* __restrict__ col, const T* __restrict__ val,
+                      const T* __restrict__ x, long long nnz, double* __restrict__ out) {
+  const long long nthreads = (long long)gridDim.x * blockDim.x;
+  T acc = 0;
+  for (long long k0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * kItems; k0 < nnz;
+       k0 += nthreads * kItems) {
+    int c[kItems];
+    T v[kItems];
+    if (k0 + kItems <= nnz) {
+      const int4 c0 = ld_stream_v4(col + k0), c1 = ld_stream_v4(col + k0 + 4);
+      c[0] = c0.x; c[1] = c0.y; c[2] = c0.z; c[3] = c0.w;
+      c[4] = c1.x; c[5] = c1.y; c[6] = c1.z; c[7] = c1.w;
+      load_vals8<T, T>(val, k0, v);
+    } else {
+#pragma unroll
+      for (int e = 0; e < kItems; ++e) {
+        c[e] = k0 + e < nnz ? ld_stream(col + k0 + e) : 0;
+        v[e] = k0 + e < nnz ? ld_stream(val + k0 + e) : (T)0;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < kItems; ++e) acc += v[e] * ld_ro(x + c[e]);
+  }
+#pragma unroll
+  for (int off = kWarp / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFull, acc, off);
+  if ((threadIdx.x & (kWarp - 1)) == 0) atomicAdd(out, (double)acc);
+}
+
 // ------------------------------------------------------------ DIA / ELL
 
 template <typename T> __device__ __forceinline__ T mul_rn(T a, T b);
@@ -973,6 +1167,7 @@ static int launch_csr(const int* row_ptr, const int* col, const S* val, const S*
                       long long nnz, const sb_csr_opts* opts, cudaStream_t st) {
   const int kernel = opts ? opts->kernel : 0;
   if (kernel == 2) return launch_csr_tiles<S, S>(row_ptr, col, val, x, y, N, nnz, opts->unroll, st);
+  if (kernel == 3) return launch_csr_block_stream<S, S>(row_ptr, col, val, x, y, N, nnz, st);
   if (kernel == 1 && aligned16(col) && aligned16(val)) {
     if (opts->unroll == 2048) return launch_csr_stream<S, 2048, 3>(row_ptr, col, val, x, y, N, nnz, st);
     return launch_csr_stream<S, 1024, 4>(row_ptr, col, val, x, y, N, nnz, st);
@@ -1021,7 +1216,7 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
   SB_REQUIRE(N >= 0 && nnz >= 0 && inner_max >= 0, "sb_spmv_csr: negative size");
   SB_REQUIRE(nnz <= 0x7fffffffLL, "sb_spmv_csr: nnz exceeds int32 row_ptr range");
   if (opts) {
-    SB_REQUIRE(opts->kernel >= 0 && opts->kernel <= 2, "sb_spmv_csr: unknown kernel %d",
+    SB_REQUIRE(opts->kernel >= 0 && opts->kernel <= 3, "sb_spmv_csr: unknown kernel %d",
                opts->kernel);
     const int l = opts->lanes_per_row;
     SB_REQUIRE(l == 0 || l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32,
@@ -1037,6 +1232,9 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
       r = launch_csr_tiles<__nv_bfloat16, float>(row_ptr, col, (const __nv_bfloat16*)val,
                                                  (const float*)x, (float*)y, N, nnz, opts->unroll,
                                                  st);
+    else if (dtype == SB_BF16 && opts && opts->kernel == 3)
+      r = launch_csr_block_stream<__nv_bfloat16, float>(row_ptr, col, (const __nv_bfloat16*)val,
+                                                        (const float*)x, (float*)y, N, nnz, st);
     else if (dtype == SB_BF16)
       r = launch_csr_rows<__nv_bfloat16, float>(row_ptr, col, (const __nv_bfloat16*)val,
                                                 (const float*)x, (float*)y, N, nnz,
@@ -1089,6 +1287,7 @@ int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const
   }
   cand[nc++] = sb_csr_opts{1, 0, 1024, 0};
   cand[nc++] = sb_csr_opts{2, 0, 8, 0};
+  cand[nc++] = sb_csr_opts{3, 0, 0, 0};
   void* ywork = nullptr;
   const size_t ysize = dtype == SB_BF16 ? sizeof(float) : dtype_size(dtype);  // y is f32 for BF16
   if ((r = scratch_alloc(&ywork, ysize * (size_t)N, st))) return r;
@@ -1119,6 +1318,30 @@ int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const
   scratch_free(ywork, st);
   if (best_ms) *best_ms = best_t;
   return r;
+}
+
+int sb_gather_dot(int dtype, const int32_t* col, const void* val, const void* x, int64_t nnz,
+                  double* out, void* stream) {
+  int r = check_dtype(dtype, "sb_gather_dot");
+  if (r) return r;
+  SB_REQUIRE(nnz >= 0, "sb_gather_dot: negative size");
+  if (nnz == 0) return SB_OK;
+  SB_REQUIRE(col && val && x && out, "sb_gather_dot: null pointer");
+  SB_REQUIRE(aligned16(col) && aligned16(val), "sb_gather_dot: col and val must be 16-byte aligned");
+  if ((r = ensure_device())) return r;
+  cudaStream_t st = as_stream(stream);
+  const long long steps = (nnz + kItems - 1) / kItems;
+  const long long per = 256;
+  auto kf = gather_dot_kernel<float>;
+  auto kd = gather_dot_kernel<double>;
+  const long long maxc = dtype == SB_F32 ? resident_ctas(kf, 256) : resident_ctas(kd, 256);
+  const unsigned ctas = (unsigned)std::max(1LL, std::min((steps + per - 1) / per, maxc));
+  if (dtype == SB_F32)
+    kf<<<ctas, 256, 0, st>>>(col, (const float*)val, (const float*)x, nnz, out);
+  else
+    kd<<<ctas, 256, 0, st>>>(col, (const double*)val, (const double*)x, nnz, out);
+  SB_CHECK_LAUNCH("gather_dot_kernel");
+  return SB_OK;
 }
 
 int sb_spmv_coo(int dtype, const int32_t* row, const int32_t* col, const void* val,

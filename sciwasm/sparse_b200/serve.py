@@ -34,6 +34,7 @@ from __future__ import annotations
 
 import collections
 import ctypes as C
+import threading
 import time
 from dataclasses import dataclass, field
 from typing import Optional
@@ -43,7 +44,8 @@ import numpy as np
 from . import _lib
 from ._lib import call
 from .sparse import (BatchExecutor, DeviceArray, SptsBatch, SptsPlan, _STORAGE, _dtcode,
-                     csr_from_host, csr_with_storage, sparse_CSR_t)
+                     csr_from_host, csr_with_storage, sparse_CSR_t, sparse_DIA_t, sparse_ELL_t,
+                     spmv_autotune, with_storage)
 
 _ALIGN = 256
 _VEC = {"f32": np.float32, "bf16": np.float32, "f64": np.float64}
@@ -108,6 +110,13 @@ class AdmissionController:
         sz, _ = self.entries.pop(name)
         self.used -= sz
 
+    def grow(self, name: str, extra: int) -> None:
+        """Charge `extra` more bytes to a resident entry (after plan_admit of
+        those bytes has made room)."""
+        sz, pinned = self.entries[name]
+        self.entries[name] = (sz + int(extra), pinned)
+        self.used += int(extra)
+
 
 def device_free_bytes() -> int:
     free = C.c_size_t(0)
@@ -133,6 +142,18 @@ def matrix_bytes(N: int, nnz: int, spmv_storages=("f32",), spts_dtypes=(),
     return b
 
 
+def format_bytes(M, storages) -> int:
+    """Device bytes of a DIA or ELL form kept beside the CSR: its index array
+    once, its values once per storage."""
+    if isinstance(M, sparse_DIA_t):
+        idx, slots = 4 * M.ndiags, M.ndiags * M.N
+    elif isinstance(M, sparse_ELL_t):
+        idx, slots = 4 * M.ncols * M.N, M.ncols * M.N
+    else:
+        return 0
+    return idx + sum(np.dtype(_STORAGE[s]).itemsize * slots for s in set(storages))
+
+
 @dataclass
 class ResidentMatrix:
     name: str
@@ -143,6 +164,8 @@ class ResidentMatrix:
     policy: dict = field(default_factory=dict)  # "f32" / "f64" -> "native" | "f64"
     growth: float = 0.0
     nbytes: int = 0
+    fmt: dict = field(default_factory=dict)     # storage -> SpMV object (CSR, DIA or ELL)
+    format: str = "csr"                         # the SpMV format chosen at admission
 
 
 class ResidentPool:
@@ -150,10 +173,14 @@ class ResidentPool:
     device's free memory when that is less)."""
 
     def __init__(self, budget_bytes: Optional[int] = None, evict: bool = True,
-                 growth_threshold: float = 1.0, reserve_bytes: int = 1 << 30):
+                 growth_threshold: float = 1.0, reserve_bytes: int = 1 << 30,
+                 spmv_format: str = "auto"):
         if budget_bytes is None:
             budget_bytes = min(150 * 10**9, int(device_free_bytes() * 0.9))
+        if spmv_format not in ("auto", "csr"):
+            raise ValueError(f"spmv_format must be 'auto' or 'csr', not {spmv_format!r}")
         self.admission = AdmissionController(budget_bytes)
+        self.spmv_format = spmv_format
         self.evict = evict
         self.growth_threshold = float(growth_threshold)
         self.reserve = int(reserve_bytes)  # kept free for slot arenas and scratch
@@ -207,6 +234,9 @@ class ResidentPool:
                 csr[s] = csr_with_storage(A, s)
         m = ResidentMatrix(name, A.N, A.nnz, csr, nbytes=self.admission.entries[name][0])
         self.mats[name] = m
+        m.fmt = {s: csr[s] for s in spmv_storages}
+        if spmv_storages and self.spmv_format == "auto":
+            self._choose_format(m, A, spmv_storages)
         for s in spts_dtypes:
             plan = SptsPlan(csr[s])
             m.plans[s] = plan
@@ -220,6 +250,30 @@ class ResidentPool:
         self.max_rows = max(self.max_rows, A.N)
         return m
 
+    def _choose_format(self, m, A, storages) -> None:
+        """The SpMV format from the matrix's statistics (the admitted format
+        with the fewest compulsory bytes, sb_spmv_autotune's statistics mode).
+        A DIA or ELL form is kept beside the CSR (the per-call path of BF16
+        values and the solves use the CSR) when the budget has room for it;
+        otherwise the matrix stays CSR."""
+        M, info = spmv_autotune(A, timed=False)
+        if M is A:
+            return
+        extra = format_bytes(M, storages)
+        try:
+            free = device_free_bytes() - self.reserve
+            victims = self.admission.plan_admit(extra, self.evict, free,
+                                                self.busy | {m.name})
+        except AdmissionError:
+            return
+        for victim in victims:
+            self.drop(victim)
+        self.admission.grow(m.name, extra)
+        m.nbytes += extra
+        base = "f64" if A.dtype == np.float64 else "f32"
+        m.fmt = {s: (M if s == base else with_storage(M, s)) for s in storages}
+        m.format = info["format"]
+
     def drop(self, name) -> None:
         m = self.mats.pop(name, None)
         if m is not None:
@@ -227,6 +281,7 @@ class ResidentPool:
                 p.close()
             m.plans.clear()
             m.csr.clear()
+            m.fmt.clear()
         if name in self.admission.entries:
             self.admission.release(name)
 
@@ -250,6 +305,7 @@ class Request:
     y: np.ndarray        # host output, same length
     t_done: float = -1.0
     slot: int = -1
+    status: str = "pending"  # "done" or "cancelled" once served
 
 
 class _Event:
@@ -371,6 +427,20 @@ class Server:
         need = 2 * 8 * max(pool.max_rows, 1) + 2 * _ALIGN  # the largest single request
         self.arena_bytes = _al(max(int(arena_bytes or (256 << 20)), need))
         self.spts_arena_bytes = _al(max(int(spts_arena_bytes or (1 << 30)), need))
+        self._cancel_lock = threading.Lock()
+        self._cancelled: set = set()
+
+    def cancel(self, rid: int) -> None:
+        """Withdraw request `rid` (callable from any thread, also while serve()
+        runs).  A request that has not yet been put into a batch is dropped:
+        its y is not written and its status becomes "cancelled".  One already
+        on the device completes normally (its work cannot be recalled)."""
+        with self._cancel_lock:
+            self._cancelled.add(int(rid))
+
+    def _is_cancelled(self, r: Request) -> bool:
+        with self._cancel_lock:
+            return r.rid in self._cancelled
 
     def _check(self, r: Request, m: ResidentMatrix):
         if r.op == "spmv":
@@ -407,7 +477,7 @@ class Server:
             xd = DeviceArray(m.N, vt, base + a)
             yd = DeviceArray(m.N, vt, base + b)
             if r.op == "spmv":
-                groups[r.storage].append((m.csr[r.storage], xd, yd, 1))
+                groups[r.storage].append((m.fmt.get(r.storage, m.csr[r.storage]), xd, yd, 1))
             else:
                 groups[(r.storage, m.policy[r.storage])].append((m.plans[r.storage], xd, yd))
         for key, jobs in groups.items():
@@ -435,6 +505,9 @@ class Server:
         seen = set()
         while pending and len(take) < max_batch:
             r = pending.popleft()
+            if self._is_cancelled(r):
+                r.status = "cancelled"
+                continue
             m = self.pool.mats[r.matrix]
             need = 2 * _al(_vec_bytes(m, r))
             key = (r.matrix, r.storage)
@@ -456,17 +529,24 @@ class Server:
         # pending blocks of solves, whose waiting warps would otherwise hold
         # the SMs
         least, greatest = _priority_range() if self.priorities else (None, None)
-        kinds = {"spmv": ([_Slot(i, "spmv", self.arena_bytes, self.max_batch, greatest)
-                           for i in range(self.nslots)], collections.deque(), self.max_batch),
-                 "spts": ([_Slot(self.nslots + i, "spts", self.spts_arena_bytes,
-                                 self.spts_batch, least) for i in range(self.spts_slots)],
-                          collections.deque(), self.spts_batch)}
-        all_slots = kinds["spmv"][0] + kinds["spts"][0]
+        all_slots: list = []
         busy_plans: set = set()
         n = len(reqs)
         i = done = batches = copies = launches = 0
-        t0 = time.perf_counter()
         try:
+            # slots are created inside the try: if one of them cannot get its
+            # stream or arena, the ones already made are closed below
+            spmv_slots, spts_slots = [], []
+            for k in range(self.nslots):
+                spmv_slots.append(_Slot(k, "spmv", self.arena_bytes, self.max_batch, greatest))
+                all_slots.append(spmv_slots[-1])
+            for k in range(self.spts_slots):
+                spts_slots.append(_Slot(self.nslots + k, "spts", self.spts_arena_bytes,
+                                        self.spts_batch, least))
+                all_slots.append(spts_slots[-1])
+            kinds = {"spmv": (spmv_slots, collections.deque(), self.max_batch),
+                     "spts": (spts_slots, collections.deque(), self.spts_batch)}
+            t0 = time.perf_counter()
             while done < n:
                 now = time.perf_counter() - t0
                 while i < n and reqs[i].t_arrival <= now:
@@ -478,6 +558,7 @@ class Server:
                         t = time.perf_counter() - t0
                         for r in sl.reqs:
                             r.t_done = t
+                            r.status = "done"
                         done += len(sl.reqs)
                         busy_plans.difference_update(sl.plans)
                         sl.busy = False
@@ -490,7 +571,10 @@ class Server:
                         free = next((sl for sl in slots if not sl.busy), None)
                         if free is None:
                             break
+                        before = len(pending)
                         take = self._take(pending, busy_plans, free.arena_bytes, mb)
+                        # cancelled requests left the queue without a batch
+                        done += before - len(pending) - len(take)
                         if not take:
                             break
                         self._launch(free, take)
@@ -507,7 +591,8 @@ class Server:
             for sl in all_slots:
                 sl.close()
             self.pool.busy = set()
-        st = _stats(reqs, batches)
+        st = _stats([r for r in reqs if r.status == "done"], batches)
+        st["cancelled"] = sum(1 for r in reqs if r.status == "cancelled")
         st.update(copies=copies, gpu_launches=launches)
         return st
 
@@ -522,15 +607,16 @@ class Server:
             for r in reqs:
                 while time.perf_counter() - t0 < r.t_arrival:
                     pass
+                if self._is_cancelled(r):
+                    r.status = "cancelled"
+                    continue
                 m = self.pool.get(r.matrix)
                 nb = _vec_bytes(m, r)
                 xp, yp = dev.ptr, dev.ptr + _al(nb)
                 call("sb_memcpy_htod", xp, r.x.ctypes.data, nb, stream)
                 if r.op == "spmv":
-                    A = m.csr[r.storage]
                     call("sb_memset", yp, 0, nb, stream)
-                    call("sb_spmv_csr", _dtcode(A.dtype), A.row_index.ptr, A.col_index.ptr,
-                         A.val_index.ptr, xp, yp, A.N, A.nnz, 1, stream)
+                    _spmv_call(m, r.storage, xp, yp, stream)
                 else:
                     pol = _lib.SB_SPTS_ACC_F64 if m.policy[r.storage] == "f64" else \
                         _lib.SB_SPTS_ACC_NATIVE
@@ -541,13 +627,16 @@ class Server:
                 ev.record(stream)
                 ev.wait()
                 r.t_done = time.perf_counter() - t0
+                r.status = "done"
         finally:
             ev.close()
             call("sb_stream_synchronize", stream)
             call("sb_stream_destroy", stream)
             dev.free()
-        st = _stats(reqs, len(reqs))
-        st.update(copies=2 * len(reqs), gpu_launches=launches)
+        served = [r for r in reqs if r.status == "done"]
+        st = _stats(served, len(served))
+        st.update(copies=2 * len(served), gpu_launches=launches,
+                  cancelled=sum(1 for r in reqs if r.status == "cancelled"))
         return st
 
     def serve(self, requests: list, mode: str = "batched") -> dict:
@@ -556,6 +645,7 @@ class Server:
         reqs = sorted(requests, key=lambda r: r.t_arrival)
         for r in reqs:
             self._check(r, self.pool.get(r.matrix))
+            r.status = "pending"
         if mode == "plain":
             st = self._serve_plain(reqs)
         elif mode == "batched":
@@ -569,6 +659,25 @@ class Server:
                                    f"device status {code.value}: a dependency wait ran out")
         st["mode"] = mode
         return st
+
+
+def _spmv_call(m: ResidentMatrix, storage: str, xp: int, yp: int, stream) -> None:
+    """The per-call path's y += A x: the matrix's chosen format where a
+    single-call kernel takes its values (DIA and ELL: f32 and f64), else the
+    CSR."""
+    M = m.fmt.get(storage, m.csr[storage])
+    if isinstance(M, sparse_DIA_t) and storage != "bf16":
+        call("sb_spmv_dia", _dtcode(M.dtype), M.offset_index.ptr, M.data_index.ptr, M.N,
+             M.ndiags, M.stride, xp, yp, 1, stream)
+    elif isinstance(M, sparse_ELL_t) and storage != "bf16":
+        call("sb_spmv_ell", _dtcode(M.dtype), M.indices_index.ptr, M.data_index.ptr, M.N,
+             M.ncols, xp, yp, 1, stream)
+    else:
+        A = m.csr[storage]
+        opts = getattr(A, "opts", None)
+        call("sb_spmv_csr_ex", _dtcode(A.dtype), A.row_index.ptr, A.col_index.ptr,
+             A.val_index.ptr, xp, yp, A.N, A.nnz, 1, C.byref(opts) if opts is not None else None,
+             stream)
 
 
 def _stats(reqs, batches) -> dict:

@@ -536,6 +536,57 @@ def csr_autotune(A_csr, x_view, reps=5, stream=None):
             "grid": best.grid, "ms": float(ms.value)}
 
 
+def csr_coo(A_csr, stream=None):
+    """The COO form of a CSR matrix (rows expanded from row_ptr, so
+    rows_sorted holds); no counterpart in the reference."""
+    B = allocate_COO(A_csr.N, A_csr.nnz, A_csr.dtype)
+    call("sb_csr_coo", _dtcode(A_csr.dtype), A_csr.row_index.ptr, A_csr.col_index.ptr,
+         A_csr.val_index.ptr, A_csr.N, A_csr.nnz, B.row_index.ptr, B.col_index.ptr,
+         B.val_index.ptr, _sp(stream))
+    B.rows_sorted = True
+    return B
+
+
+_FORMAT_NAMES = ("csr", "dia", "ell", "coo")
+
+
+def spmv_autotune(A_csr, x_view=None, reps=5, timed=True, stream=None):
+    """Choose the SpMV format and kernel for a CSR matrix (sb_spmv_autotune):
+    the reference's admission test and the compulsory bytes of each format
+    decide what is tried; with timed=True device timing decides among them,
+    with timed=False the statistics alone (fewest bytes; x_view unused).
+    Returns (M, info): M is the matrix in the chosen format -- A_csr itself,
+    with its CSR kernel options set, when CSR wins; a new DIA, ELL or COO
+    object built on the device otherwise -- and info holds the statistics,
+    bytes and per-format times."""
+    ch = _lib.SpmvChoice()
+    if timed and x_view is None:
+        raise ValueError("spmv_autotune: the timed mode needs an x vector")
+    call("sb_spmv_autotune", _dtcode(A_csr.dtype), A_csr.row_index.ptr, A_csr.col_index.ptr,
+         A_csr.val_index.ptr, x_view.vec_index.ptr if x_view is not None else None, A_csr.N,
+         A_csr.nnz, _lib.SB_TUNE_TIMED if timed else _lib.SB_TUNE_MODEL, int(reps),
+         C.byref(ch), _sp(stream))
+    A_csr.opts = _lib.CsrOpts(ch.csr.kernel, ch.csr.lanes_per_row, ch.csr.unroll, ch.csr.grid)
+    fmt = _FORMAT_NAMES[ch.format]
+    if fmt == "dia":
+        M = csr_dia(A_csr, stream)
+    elif fmt == "ell":
+        M = csr_ell(A_csr, stream)
+    elif fmt == "coo":
+        M = csr_coo(A_csr, stream)
+    else:
+        M = A_csr
+    info = {"format": fmt,
+            "csr_opts": {"kernel": ch.csr.kernel, "lanes_per_row": ch.csr.lanes_per_row,
+                         "unroll": ch.csr.unroll, "grid": ch.csr.grid},
+            "ndiags": ch.ndiags, "ncols": ch.ncols, "dia_admitted": bool(ch.dia_admitted),
+            "ell_admitted": bool(ch.ell_admitted),
+            "ms": {n: (round(float(ch.ms[k]), 4) if ch.ms[k] >= 0 else None)
+                   for k, n in enumerate(_FORMAT_NAMES)},
+            "bytes": {n: int(ch.bytes[k]) for k, n in enumerate(_FORMAT_NAMES)}}
+    return M, info
+
+
 def spmv(A, x_view, y_view, inner_max=1, stream=None):
     """y <- y + A x, inner_max times (src/sequential/src/sparse32.js:1232-1286).
 
@@ -590,12 +641,28 @@ def csr_with_storage(A_csr, storage, stream=None):
                         convert_values(A_csr.val_index, storage, stream), A_csr.N, A_csr.nnz)
 
 
+def with_storage(A, storage, stream=None):
+    """A CSR, DIA or ELL matrix with its values stored as `storage` (the
+    index arrays are shared with A).  BF16 values serve the batched SpMV
+    (f32 vectors and sums); the single-call DIA and ELL kernels take f32 and
+    f64 only."""
+    if isinstance(A, sparse_CSR_t):
+        return csr_with_storage(A, storage, stream)
+    if isinstance(A, sparse_DIA_t):
+        return sparse_DIA_t(A.offset_index, convert_values(A.data_index, storage, stream),
+                            A.ndiags, A.stride, A.N, A.nnz)
+    if isinstance(A, sparse_ELL_t):
+        return sparse_ELL_t(A.indices_index, convert_values(A.data_index, storage, stream),
+                            A.ncols, A.N, A.nnz)
+    raise TypeError(f"with_storage: {type(A).__name__} is not CSR, DIA or ELL")
+
+
 # --------------------------------------------------------------- batched SpMV
 
 
 class BatchExecutor:
-    """Batched CSR SpMV over many matrices and right-hand sides in one
-    graph-replayed persistent launch (values stored as `storage`)."""
+    """Batched SpMV over many matrices (CSR, DIA or ELL, values stored as
+    `storage`) and right-hand sides in one graph-replayed persistent launch."""
 
     def __init__(self, storage="f32", capacity=1024):
         self.storage = storage
@@ -607,8 +674,9 @@ class BatchExecutor:
         self._keep = []
 
     def run(self, jobs, stream=None, overwrite=False):
-        """jobs: iterable of (A_csr, x DeviceArray N*k, y DeviceArray N*k, k);
-        y += A x, or y = A x with overwrite=True."""
+        """jobs: iterable of (A, x DeviceArray N*k, y DeviceArray N*k, k) with A
+        a CSR, DIA (stride N) or ELL matrix; y += A x, or y = A x with
+        overwrite=True."""
         jobs = list(jobs)
         if len(jobs) > self.capacity:
             raise ValueError(f"{len(jobs)} items exceed the executor capacity {self.capacity}")
@@ -616,9 +684,19 @@ class BatchExecutor:
         self._keep = []
         for A, x, y, k in jobs:
             it = self._items[n]
-            it.row_ptr, it.col, it.val = A.row_index.ptr, A.col_index.ptr, A.val_index.ptr
             it.x, it.y = x.ptr, y.ptr
             it.N, it.nrhs, it.lanes, it.flags, it.nnz = A.N, int(k), 0, 1 if overwrite else 0, A.nnz
+            if isinstance(A, sparse_DIA_t):
+                if A.stride != A.N:
+                    raise ValueError("batched DIA items need stride == N")
+                it.row_ptr, it.col, it.val = A.offset_index.ptr, None, A.data_index.ptr
+                it.format, it.width = _lib.SB_FMT_DIA, A.ndiags
+            elif isinstance(A, sparse_ELL_t):
+                it.row_ptr, it.col, it.val = None, A.indices_index.ptr, A.data_index.ptr
+                it.format, it.width = _lib.SB_FMT_ELL, A.ncols
+            else:
+                it.row_ptr, it.col, it.val = A.row_index.ptr, A.col_index.ptr, A.val_index.ptr
+                it.format, it.width = _lib.SB_FMT_CSR, 0
             self._keep.append((A, x, y))
             n += 1
         call("sb_batch_exec_run", self.ptr, self._items, n, _sp(stream))

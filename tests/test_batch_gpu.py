@@ -83,3 +83,63 @@ def test_batch_same_result_alone_and_in_mix(gpu):
         ex.run([(A, xd, yd, k)])
         gpu.synchronize()
         assert np.array_equal(yd.to_host(), ymix.to_host())
+
+
+@pytest.mark.parametrize("storage", ["f32", "f64", "bf16"])
+def test_batch_mixed_formats(gpu, oracle, storage):
+    """CSR, DIA and ELL items in one launch.  With one right-hand side a DIA
+    or ELL item is bit-identical to sb_spmv_dia / sb_spmv_ell on the same y;
+    with several, each right-hand side is bit-identical to the oracle's serial
+    DIA / ELL loop on that column; BF16 items are within tolerance of the FP64
+    product of their stored values."""
+    vdt = np.float64 if storage == "f64" else np.float32
+    ex = gpu.BatchExecutor(storage, capacity=16)
+    cases = []
+    for i, (rp, col, val) in enumerate([synth.banded(7_001, half=3, seed=3, dtype=vdt),
+                                        synth.laplacian_2d(90, dtype=vdt),
+                                        synth.banded(40_000, half=5, seed=4, dtype=vdt)]):
+        A = gpu.csr_from_host(rp, col, val)
+        for fmt in ("dia", "ell", "csr"):
+            M = {"dia": gpu.csr_dia, "ell": gpu.csr_ell, "csr": lambda a: a}[fmt](A)
+            assert M is not None
+            for k in (1, 3):
+                cases.append((fmt, M, rp, col, val, k, i))
+    jobs, host = [], []
+    for idx, (fmt, M, rp, col, val, k, i) in enumerate(cases):
+        N = rp.size - 1
+        Ms = gpu.with_storage(M, "bf16") if storage == "bf16" else M
+        X = synth.uniform_vec(N * k, 50 + idx, dtype=vdt).reshape(N, k)
+        Y0 = synth.uniform_vec(N * k, 90 + idx, dtype=vdt).reshape(N, k)
+        xd, yd = gpu.DeviceArray.from_host(X.ravel()), gpu.DeviceArray.from_host(Y0.ravel())
+        jobs.append((Ms, xd, yd, k))
+        host.append((fmt, M, Ms, rp, col, val, X, Y0))
+    ex.run(jobs)
+    gpu.synchronize()
+    for (Ms, xd, yd, k), (fmt, M, _, rp, col, val, X, Y0) in zip(jobs, host):
+        Y = yd.to_host().reshape(-1, k)
+        N = M.N
+        if storage == "bf16":
+            v = (gpu.csr_with_storage(gpu.csr_from_host(rp, col, val), "bf16").val_array()
+                 .astype(np.uint32) << 16).view(np.float32)
+            for j in range(k):
+                want = Y0[:, j].astype(np.float64) + oracle.truth_csr(
+                    rp, col, v.astype(np.float64), X[:, j].astype(np.float64))
+                assert rel_err(Y[:, j], want) <= 1e-4, (fmt, k)
+            continue
+        if fmt == "csr":
+            for j in range(k):
+                want = oracle.truth_csr(rp, col, val, X[:, j], Y0[:, j])
+                assert rel_err(Y[:, j], want) <= TOL[np.dtype(vdt)], (fmt, k)
+            continue
+        for j in range(k):
+            if fmt == "dia":
+                want = oracle.spmv_dia(M.offset_array(), M.data_array(), N,
+                                       np.ascontiguousarray(X[:, j]), Y0[:, j])
+            else:
+                want = oracle.spmv_ell(M.indices_array(), M.data_array(), N, M.ncols,
+                                       np.ascontiguousarray(X[:, j]), Y0[:, j])
+            assert np.array_equal(Y[:, j].view(np.uint8), want.view(np.uint8)), (fmt, k, j)
+        if k == 1:
+            xv, yv = gpu.vec_from_host(X[:, 0]), gpu.vec_from_host(Y0[:, 0])
+            gpu.spmv(M, xv, yv)
+            assert np.array_equal(yv.array().view(np.uint8), Y[:, 0].view(np.uint8)), fmt

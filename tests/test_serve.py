@@ -105,3 +105,67 @@ def test_poisson_arrivals():
     assert np.all(np.diff(t) > 0) and t[-1] < 2.0
     assert 1800 < t.size < 2200
     assert np.array_equal(t, serve.poisson_arrivals(1000.0, 2.0, seed=3))
+
+
+def test_take_drops_cancelled_requests():
+    pool = _FakePool({"A": 1000, "L": 2000})
+    srv = serve.Server(pool, max_batch=4, slots=2, arena_bytes=1 << 20)
+    reqs = [_req(0, "A"), _req(1, "L", "spts"), _req(2, "A"), _req(3, "A")]
+    srv.cancel(1)
+    srv.cancel(3)
+    pend = collections.deque(reqs)
+    take = srv._take(pend, set(), srv.arena_bytes)
+    assert [r.rid for r in take] == [0, 2] and not pend
+    assert [r.status for r in reqs] == ["pending", "cancelled", "pending", "cancelled"]
+
+
+class _Refused(Exception):
+    pass
+
+
+def test_pool_rolls_back_after_an_injected_allocation_failure(monkeypatch):
+    """A failed device allocation while a matrix is admitted leaves the pool's
+    accounting as it was (the reference's parallel calls resolve to -1 and
+    keep their state, src/parallel/src/sparse32.js:2640-2651)."""
+    from sciwasm.sparse_b200 import _lib
+    monkeypatch.setattr(serve, "device_free_bytes", lambda: 1 << 40)
+
+    def no_memory(*a, **k):
+        raise _lib.SparseError("sb_malloc", _lib.SB_ENOMEM, "injected allocation failure")
+    monkeypatch.setattr(serve, "csr_from_host", no_memory)
+    pool = serve.ResidentPool(budget_bytes=10**9)
+    rp = np.array([0, 1, 2], np.int32)
+    with pytest.raises(_lib.SparseError) as ei:
+        pool.add("m", rp, np.array([0, 1], np.int32), np.ones(2))
+    assert ei.value.status == _lib.SB_ENOMEM
+    assert pool.admission.used == 0 and not pool.admission.entries and not pool.mats
+    # the failure inside the attach step (e.g. a plan that cannot be built)
+    # is rolled back the same way, and a later admission still works
+    monkeypatch.setattr(serve, "csr_from_host", lambda *a, **k: object())
+
+    def attach_fails(*a, **k):
+        raise _Refused("plan allocation failed")
+    monkeypatch.setattr(pool, "_attach", attach_fails)
+    with pytest.raises(_Refused):
+        pool.add("m", rp, np.array([0, 1], np.int32), np.ones(2))
+    assert pool.admission.used == 0 and "m" not in pool.admission.entries
+
+
+def test_slot_creation_failure_closes_the_slots_already_made(monkeypatch):
+    made, closed = [], []
+
+    class FakeSlot:
+        def __init__(self, index, *a, **k):
+            if len(made) == 2:
+                raise _Refused("injected arena allocation failure")
+            self.index, self.busy = index, False
+            made.append(index)
+
+        def close(self):
+            closed.append(self.index)
+
+    monkeypatch.setattr(serve, "_Slot", FakeSlot)
+    srv = serve.Server(_FakePool({"A": 10}), slots=2, spts_slots=1, priorities=False)
+    with pytest.raises(_Refused):
+        srv._serve_batched([])
+    assert made == [0, 1] and sorted(closed) == [0, 1]

@@ -223,3 +223,41 @@ def test_pool_admission_evicts_lru_and_refuses_pinned(gpu):
         pool.add("c", rp, col, val)
     assert set(pool.mats) == {"a", "b"}
     pool.close()
+
+
+def test_serving_cancelled_requests_are_dropped(gpu, oracle):
+    """Requests withdrawn before they join a batch are not run (y keeps its
+    NaN fill, status "cancelled"); the others are served as usual, in both
+    modes, and a cancel from another thread while the loop runs is safe."""
+    import threading
+    pool, host = _serving_pool(gpu)
+    for mode in ("batched", "plain"):
+        reqs, buf = _requests(pool, 60, seed=7, rate_hz=2_000.0)
+        srv = serve.Server(pool, max_batch=16, slots=2)
+        drop = {r.rid for r in reqs if r.rid % 5 == 2}
+        for rid in sorted(drop)[:4]:
+            srv.cancel(rid)            # before the loop starts
+        # the rest arrive 0.3 s into the trace and are cancelled from another
+        # thread 0.05 s into it, while the loop runs
+        late = sorted(drop)[4:]
+        for r in reqs:
+            if r.rid in late:
+                r.t_arrival = 0.3 + 1e-4 * r.rid
+
+        def cancel_late():
+            import time
+            time.sleep(0.05)
+            for rid in late:
+                srv.cancel(rid)
+        th = threading.Thread(target=cancel_late)
+        th.start()
+        st = srv.serve(reqs, mode)
+        th.join()
+        assert st["cancelled"] == len(drop) and st["requests"] == 60 - len(drop)
+        for r in reqs:
+            if r.rid in drop:
+                assert r.status == "cancelled" and np.all(np.isnan(r.y)), r.rid
+            else:
+                assert r.status == "done", r.rid
+                assert rel_err(r.y, _truth(oracle, pool, host, r)) <= SERVE_TOL, r.rid
+    pool.close()

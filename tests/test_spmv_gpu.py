@@ -221,3 +221,143 @@ def test_csr_streamed_tile_kernel(gpu, oracle, tile):
             gpu.spmv(A, xv, yv)
             err = rel_err(yv.array(), oracle.truth_csr(rp, col, val, x, y0))
             assert err <= TOL[np.dtype(dt)], (name, dt, err)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f64", "bf16"])
+def test_csr_block_stream_kernel(gpu, oracle, storage):
+    """Kernel 3 (a warp per 32-row block streaming its nonzeros in 256-entry
+    chunks): within the tolerance of the exact result on regular, skewed,
+    ragged and empty-row matrices, rows without entries keep their bits, two
+    runs give identical bits, and a col/val pair that is not 16-byte aligned
+    takes the scalar-load form with the same result."""
+    from sciwasm.sparse_b200 import _lib
+    dt = np.float64 if storage == "f64" else np.float32
+    mats = _mats(dt)
+    mats["rows_over_blocks"] = synth.power_law(9_000, seed=8, dtype=dt, cap=3000, shift=0)
+    for name, (rp, col, val) in mats.items():
+        N = rp.size - 1
+        x, y0 = _x_y(N, dt)
+        A = gpu.csr_from_host(rp, col, val)
+        vals = val
+        if storage == "bf16":
+            A = gpu.csr_with_storage(A, "bf16")
+            vals = (A.val_array().astype(np.uint32) << 16).view(np.float32)
+        A.opts = _lib.CsrOpts(3, 0, 0, 0)
+        outs = []
+        for _ in range(2):
+            xv, yv = gpu.vec_from_host(x), gpu.vec_from_host(y0)
+            gpu.spmv(A, xv, yv)
+            outs.append(yv.array())
+        truth = oracle.truth_csr(rp, col, vals, x, y0)
+        assert rel_err(outs[0], truth) <= TOL[np.dtype(dt)], (name, storage)
+        assert np.array_equal(outs[0].view(np.uint8), outs[1].view(np.uint8)), name
+        empty = np.diff(rp) == 0
+        assert np.array_equal(outs[0][empty].view(np.uint8), y0[empty].view(np.uint8)), name
+        if storage != "bf16" and col.size > 1:
+            # col/val one element into a buffer: 4-byte (f32) or 8-byte (f64)
+            # aligned, not 16: the scalar-load form
+            from sciwasm.sparse_b200.sparse import DeviceArray
+            cbuf = DeviceArray.from_host(np.concatenate([[0], col]).astype(np.int32))
+            vbuf = DeviceArray.from_host(np.concatenate([[0], val]).astype(dt))
+            rpd = DeviceArray.from_host(rp)
+            xv, yv = gpu.vec_from_host(x), gpu.vec_from_host(y0)
+            code = _lib.SB_F64 if dt == np.float64 else _lib.SB_F32
+            _lib.call("sb_spmv_csr_ex", code, rpd.ptr, cbuf.ptr + 4, vbuf.ptr + dt().itemsize,
+                      xv.vec_index.ptr, yv.vec_index.ptr, N, col.size, 1,
+                      __import__("ctypes").byref(A.opts), None)
+            assert rel_err(yv.array(), truth) <= TOL[np.dtype(dt)], (name, "unaligned")
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+def test_gather_dot_is_the_sum_of_the_product(gpu, oracle, dt):
+    import ctypes
+    from sciwasm.sparse_b200 import _lib
+    from sciwasm.sparse_b200.sparse import DeviceArray
+    for name in ("powerlaw", "ragged", "single"):
+        rp, col, val = _mats(dt)[name]
+        N = rp.size - 1
+        x, _ = _x_y(N, dt)
+        truth = float(np.sum(oracle.truth_csr(rp, col, val, x)))
+        out = DeviceArray.from_host(np.zeros(1))
+        c, v, xd = DeviceArray.from_host(col), DeviceArray.from_host(val), \
+            DeviceArray.from_host(x)
+        code = _lib.SB_F64 if dt == np.float64 else _lib.SB_F32
+        _lib.call("sb_gather_dot", code, c.ptr, v.ptr, xd.ptr, col.size, out.ptr, None)
+        got = float(out.to_host()[0])
+        scale = float(np.sum(np.abs(val.astype(np.float64) * x[col])))
+        assert abs(got - truth) <= 10 * TOL[np.dtype(dt)] * max(scale, 1e-300), name
+
+
+def test_spmv_autotune_picks_dia_for_banded_and_keeps_parity(gpu, oracle):
+    """The format autotuner: on a banded matrix (11 diagonals, 2M rows, FP64)
+    DIA moves the fewest bytes and is chosen; the power-law matrix's DIA and
+    ELL forms are refused by the admission test and never timed; the chosen
+    object computes y <- y + A x within tolerance (DIA bit-identical to the
+    oracle's serial loop)."""
+    rp, col, val = synth.banded(2_000_000, half=5, seed=1, dtype=np.float64)
+    N = rp.size - 1
+    A = gpu.csr_from_host(rp, col, val)
+    x, y0 = _x_y(N, np.float64)
+    xv = gpu.vec_from_host(x)
+    M, info = gpu.spmv_autotune(A, xv)
+    assert info["dia_admitted"] and info["ndiags"] == 11 and info["ncols"] == 11
+    assert info["bytes"]["dia"] < info["bytes"]["ell"] < info["bytes"]["csr"]
+    assert info["format"] == "dia", info
+    assert isinstance(M, gpu.sparse_DIA_t) and info["ms"]["dia"] < info["ms"]["csr"]
+    yv = gpu.vec_from_host(y0)
+    gpu.spmv(M, xv, yv)
+    off, dat = synth.csr_to_dia_host(rp, col, val)
+    assert np.array_equal(yv.array().view(np.uint8),
+                          oracle.spmv_dia(off, dat, N, x, y0).view(np.uint8))
+    del A, M
+    rp, col, val = synth.power_law(200_000, seed=2, dtype=np.float64)
+    N = rp.size - 1
+    A = gpu.csr_from_host(rp, col, val)
+    x, y0 = _x_y(N, np.float64)
+    xv = gpu.vec_from_host(x)
+    M, info = gpu.spmv_autotune(A, xv)
+    assert not info["dia_admitted"] and not info["ell_admitted"]
+    assert info["ms"]["dia"] is None and info["ms"]["ell"] is None
+    assert info["format"] in ("csr", "coo") and info["ms"]["csr"] > 0
+    yv = gpu.vec_from_host(y0)
+    gpu.spmv(M, xv, yv)
+    assert rel_err(yv.array(), oracle.truth_csr(rp, col, val, x, y0)) <= 1e-12
+
+
+def _poisson_rows(N, mean, seed):
+    """Poisson(mean) distinct uniform columns per row plus the diagonal."""
+    rng = np.random.default_rng(seed)
+    lens = rng.poisson(mean, N).astype(np.int64)
+    cols = synth._distinct_uniform_cols(rng, lens, np.zeros(N, np.int64), np.full(N, N, np.int64))
+    rows = np.repeat(np.arange(N), lens)
+    allr = np.concatenate([rows, np.arange(N)])
+    allc = np.concatenate([cols, np.arange(N)])
+    key = np.unique(allr * N + allc)
+    r, c = key // N, key % N
+    rp = np.concatenate([[0], np.cumsum(np.bincount(r, minlength=N))]).astype(np.int32)
+    return rp, c.astype(np.int32), rng.uniform(-1, 1, c.size).astype(np.float32)
+
+
+def test_spmv_autotune_statistics_mode(gpu, oracle):
+    """Without timing, the admitted format with the fewest compulsory bytes:
+    DIA for banded and 5-point matrices, CSR (block-stream kernel) for skewed
+    power-law rows, CSR (row blocks) for Poisson row lengths, ELL for rows of
+    one length (no row_ptr to read); the chosen object keeps parity."""
+    cases = {"banded": (synth.banded(50_000, half=5, seed=1, dtype=np.float32), "dia", None),
+             "lap2d": (synth.laplacian_2d(200, dtype=np.float32), "dia", None),
+             "powerlaw": (synth.power_law(60_000, seed=2, dtype=np.float32), "csr", 3),
+             "poisson": (_poisson_rows(60_000, 12.0, seed=3), "csr", 0),
+             "uniform13": (synth.random_lower(60_000, per_row=12, band=60_000, seed=3,
+                                              dtype=np.float32), "ell", None)}
+    for name, ((rp, col, val), fmt, kernel) in cases.items():
+        N = rp.size - 1
+        A = gpu.csr_from_host(rp, col, val)
+        M, info = gpu.spmv_autotune(A, timed=False)
+        assert info["format"] == fmt, (name, info)
+        assert all(v is None for v in info["ms"].values())
+        if kernel is not None:
+            assert info["csr_opts"]["kernel"] == kernel, (name, info)
+        x, y0 = _x_y(N, np.float32)
+        yv = gpu.vec_from_host(y0)
+        gpu.spmv(M, gpu.vec_from_host(x), yv)
+        assert rel_err(yv.array(), oracle.truth_csr(rp, col, val, x, y0)) <= 1e-5, name
