@@ -476,6 +476,25 @@ int sb_sort_rows_by_nnz(int dtype, const int32_t* row_ptr, const int32_t* col, c
  * (a result of the reordered matrix back in the original row order). */
 int sb_unpermute_rows(int dtype, const int32_t* permutation, const void* in, void* out,
                       int32_t N, void* stream);
+/* Replaces reorder_NN (src/parallel/src/sparse32.js:2501-2622, with
+ * reorder_subset :2415-2483, find_next_row :2321-2394 and
+ * assign_w_min_elems :2271-2318): a nearest-neighbour row order.  From the
+ * first non-empty row on, consecutive position ranges sized by the
+ * row-length histogram (at most 1024 rows; with rows sorted by length, as the
+ * reference calls it on sort_rows_by_nnz's output, each range holds rows of
+ * one length) are walked greedily: each visited row joins a window of the
+ * last w (1..32) rows, each window row keeps the w unvisited rows of its
+ * range with the highest Jaccard similarity of 16-column cache lines, and the
+ * next row is the best first candidate over the window.  Bit-exact with the
+ * reference: walk[N] (input row at each new position; positions no walk
+ * reaches keep their index), perm_out[N] = perm_in[walk[i]] (perm_in NULL =
+ * the identity), and the reordered CSR (rows gathered in walk order; the
+ * reference's new row_ptr view is empty, so it writes no row pointers --
+ * here they are written).  Returns after the device work. */
+int sb_reorder_nn(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
+                  int32_t N, int64_t nnz, int32_t w, const int32_t* perm_in, int32_t* walk,
+                  int32_t* perm_out, int32_t* out_row_ptr, int32_t* out_col, void* out_val,
+                  void* stream);
 /* Replaces calculate_csr_locality_index (:2238-2269): the percentage of
  * accesses whose 16-column line was last touched fewer than 16 rows before
  * (NaN for an empty matrix, as the reference's 0/0).  Returns after the

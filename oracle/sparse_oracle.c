@@ -1337,3 +1337,175 @@ void or_spts_csc(int w, const int32_t* cp, const int32_t* row, const void* val, 
   if (w == 4) spts_csc_f32(cp, row, (const float*)val, (const float*)x, (float*)y, N);
   else spts_csc_f64(cp, row, (const double*)val, (const double*)x, (double*)y, N);
 }
+
+/* ======================= nearest-neighbour row reordering ======================= */
+
+/* assign_w_min_elems: src/parallel/src/sparse32.js:2271-2318.  The list
+ * holds float32 values (a Float32Array; -1 = empty) compared as doubles with
+ * the new candidate's double value.  An equal value goes after the existing
+ * ones; a middle insertion into a partly filled list shifts from the last
+ * filled slot, which drops that slot's entry (the list does not grow). */
+static void nn_assign(float* jac, int32_t* nidx, int32_t next, double v, int w) {
+  int i = 0;
+  while (i < w && (double)jac[i] >= 0 && (double)jac[i] >= v) i++;
+  if (i == w) return;
+  if (jac[i] == -1.0f) {
+    jac[i] = (float)v;
+    nidx[i] = next;
+    return;
+  }
+  int j = w - 1;
+  while (jac[j] == -1.0f) j--;
+  while (j != i) {
+    jac[j] = jac[j - 1];
+    nidx[j] = nidx[j - 1];
+    j--;
+  }
+  jac[i] = (float)v;
+  nidx[i] = next;
+}
+
+/* find_next_row: src/parallel/src/sparse32.js:2321-2394.  A row that has
+ * just joined the window (visited 3) gets its list: the w unvisited rows of
+ * [start, end) with the highest Jaccard similarity of 16-column cache lines
+ * (shared line runs / (its runs + their runs - shared runs)).  Returns the
+ * first unvisited row of the row's list (N if none) and its value. */
+static int32_t nn_find_next(int32_t index, int32_t* visited, const int32_t* nlines, float* jac,
+                            int32_t* nidx, int32_t* last_used, const int32_t* row_ptr,
+                            const int32_t* col, int32_t N, int w, int32_t start, int32_t end,
+                            double* maxv) {
+  if (visited[index] == 3) {
+    visited[index] = 1;
+    for (int i = 0; i < w; ++i) {
+      jac[i] = -1.0f;
+      nidx[i] = N;
+    }
+    for (int32_t j = row_ptr[index]; j < row_ptr[index + 1]; ++j) last_used[col[j] / 16] = index;
+    for (int32_t i = start; i < end; ++i) {
+      if (visited[i] != 0) continue;
+      int32_t j = row_ptr[i], alines = 0;
+      while (j < row_ptr[i + 1]) {
+        if (last_used[col[j] / 16] == index) alines++;
+        j++;
+        while (j < row_ptr[i + 1] && col[j - 1] / 16 == col[j] / 16) j++;
+      }
+      const int32_t dissim = nlines[index] + nlines[i] - alines;
+      nn_assign(jac, nidx, i, (double)alines / (double)dissim, w);
+    }
+  }
+  for (int i = 0; i < w; ++i) {
+    if ((double)jac[i] >= 0 && visited[nidx[i]] == 0) {
+      *maxv = (double)jac[i];
+      return nidx[i];
+    }
+  }
+  *maxv = 0.0;
+  return N;
+}
+
+/* reorder_subset: src/parallel/src/sparse32.js:2415-2483.  A greedy walk
+ * from row `start`: each visited row joins a ring window of the last w rows;
+ * the next row is the best first candidate over the window's lists (a later
+ * window slot wins a tie), until no candidate is left. */
+static void nn_subset(const int32_t* row_ptr, const int32_t* col, int32_t N, int32_t start,
+                      int32_t end, const int32_t* nlines, int32_t* visited, int32_t* perm, int w) {
+  int32_t* win = (int32_t*)calloc((size_t)w, sizeof(int32_t));
+  const int32_t nl = N / 16 + 1;
+  int32_t* last_used = (int32_t*)malloc(sizeof(int32_t) * (size_t)nl);
+  for (int32_t i = 0; i < nl; ++i) last_used[i] = -1;
+  float* jac = (float*)calloc((size_t)w * w, sizeof(float));
+  int32_t* nidx = (int32_t*)calloc((size_t)w * w, sizeof(int32_t));
+  int32_t index = start, pos = start;
+  int nnb = 0, count = 0;
+  while (index != N) {
+    visited[index] = 3;
+    win[count++] = index;
+    if (nnb < w) nnb++;
+    if (count == w) count = 0;
+    perm[pos++] = index;
+    int32_t next = N;
+    double mx = 0.0;
+    for (int i = 0; i < nnb; ++i) {
+      double v = 0.0;
+      const int32_t c = nn_find_next(win[i], visited, nlines, jac + (size_t)i * w,
+                                     nidx + (size_t)i * w, last_used, row_ptr, col, N, w, start,
+                                     end, &v);
+      if (mx <= v && c != N) {
+        mx = v;
+        next = c;
+      }
+    }
+    index = next;
+  }
+  free(win);
+  free(last_used);
+  free(jac);
+  free(nidx);
+}
+
+/* reorder_NN: src/parallel/src/sparse32.js:2501-2622.  Empty rows are
+ * skipped (visited 2); each row's number of line runs is counted; from the
+ * first non-empty row on, consecutive position ranges sized by the row-length
+ * histogram (lengths 1, 2, ..., in chunks of at most 1024 rows) are walked
+ * independently.  With rows sorted by length (the reference calls it on the
+ * output of sort_rows_by_nnz) each range holds rows of one length.  Outputs
+ * the walk order `walk` (positions outside every range keep their index),
+ * the new CSR (row i = input row walk[i]) and the permutation composed with
+ * perm_in (new row i = original row perm_in[walk[i]]; perm_in NULL = the
+ * identity).  The reference's new row_ptr view has length nrows + 1 with
+ * nrows undefined, so it writes no row pointers; here they are written. */
+void or_reorder_nn(int w_bytes, const int32_t* row_ptr, const int32_t* col, const void* val,
+                   int32_t N, int w, const int32_t* perm_in, int32_t* walk, int32_t* perm_out,
+                   int32_t* new_row, int32_t* new_col, void* new_val) {
+  int32_t* visited = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
+  int32_t* nlines = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
+  int32_t* freq = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
+  for (int32_t i = 0; i < N; ++i) {
+    walk[i] = i;
+    const int32_t len = row_ptr[i + 1] - row_ptr[i];
+    freq[len]++;
+    if (len == 0) visited[i] = 2;
+  }
+  for (int32_t i = 0; i < N; ++i) {
+    if (visited[i] != 0) continue;
+    int32_t j = row_ptr[i];
+    while (j < row_ptr[i + 1]) {
+      nlines[i]++;
+      j++;
+      while (j < row_ptr[i + 1] && col[j - 1] / 16 == col[j] / 16) j++;
+    }
+  }
+  int32_t start = 0;
+  while (start < N && visited[start] != 0) start++;
+  if (start < N) {
+    const int32_t B = 1024;
+    for (int32_t len = 1; len < N + 1; ++len) {
+      while (freq[len] >= B) {
+        const int32_t end = start + B;
+        freq[len] -= B;
+        nn_subset(row_ptr, col, N, start, end, nlines, visited, walk, w);
+        start = end;
+      }
+      if (freq[len] > 0) {
+        const int32_t end = start + freq[len];
+        freq[len] = 0;
+        nn_subset(row_ptr, col, N, start, end, nlines, visited, walk, w);
+        start = end;
+      }
+    }
+  }
+  int64_t o = 0;
+  new_row[0] = 0;
+  for (int32_t i = 0; i < N; ++i) {
+    const int32_t s = walk[i];
+    for (int32_t k = row_ptr[s]; k < row_ptr[s + 1]; ++k, ++o) {
+      new_col[o] = col[k];
+      copy_elem(new_val, o, val, k, w_bytes);
+    }
+    new_row[i + 1] = (int32_t)o;
+    perm_out[i] = perm_in ? perm_in[s] : s;
+  }
+  free(visited);
+  free(nlines);
+  free(freq);
+}

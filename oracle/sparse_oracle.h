@@ -250,6 +250,14 @@ void or_unpermute_rows(int val_bytes, const int32_t* permutation, const void* in
                        int32_t N);
 /* calculate_csr_locality_index :2238-2269. */
 double or_csr_locality_index(const int32_t* row_ptr, const int32_t* col, int32_t N, int64_t nnz);
+/* reorder_NN (src/parallel/src/sparse32.js:2271-2622): nearest-neighbour row
+ * order by Jaccard similarity of 16-column lines, window w; walk[N] (the
+ * order of input rows), perm_out[N] (composed with perm_in, NULL =
+ * identity), the reordered CSR (row pointers written; the reference's are
+ * not). */
+void or_reorder_nn(int val_bytes, const int32_t* row_ptr, const int32_t* col, const void* val,
+                   int32_t N, int w, const int32_t* perm_in, int32_t* walk, int32_t* perm_out,
+                   int32_t* new_row, int32_t* new_col, void* new_val);
 
 /* ---------------- Matrix Market input ---------------- */
 /* read_MM_header / calculate_actual_nnz / read_matrix_MM_files:

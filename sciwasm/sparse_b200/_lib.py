@@ -143,6 +143,7 @@ SIGNATURES.update({
     "sb_sort_rows_by_nnz": [C.c_int, P, P, P, I32, I64, P, P, P, P, P, C.POINTER(I32), P],
     "sb_unpermute_rows": [C.c_int, P, P, P, I32, P],
     "sb_csr_locality_index": [P, P, I32, I64, C.POINTER(C.c_double), P],
+    "sb_reorder_nn": [C.c_int, P, P, P, I32, I64, I32, P, P, P, P, P, P, P],
     "sb_coo_csc": [C.c_int, P, P, P, I32, I64, P, P, P, P],
     "sb_spts_csc": [C.c_int, P, P, P, I32, I64, P, P, P],
     "sb_mm_read_header": [P, SZ, C.POINTER(MMHeader)],

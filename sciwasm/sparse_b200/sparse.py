@@ -408,6 +408,35 @@ def sort_rows_by_nnz(A_csr, stream=None):
     return B
 
 
+def reorder_NN(A_csr, w=16, stream=None):
+    """reorder_NN (src/parallel/src/sparse32.js:2501-2622): a new CSR whose rows
+    follow a greedy nearest-neighbour walk by the Jaccard similarity of their
+    16-column cache lines (window of w rows; the reference's callers pass 16
+    and the output of sort_rows_by_nnz).  It carries permutation_index (new
+    row -> row of the matrix A_csr came from: A_csr's own permutation_index
+    composed with the walk, or the walk alone), nnz_row_index (its own row
+    lengths; the reference leaves the input order's there) and num_zero_rows ..
+    num_three_rows."""
+    N, nnz = A_csr.N, A_csr.nnz
+    B = allocate_CSR(N, nnz, A_csr.dtype)
+    walk = DeviceArray(N, np.int32)
+    B.permutation_index = DeviceArray(N, np.int32)
+    pin = getattr(A_csr, "permutation_index", None)
+    call("sb_reorder_nn", _dtcode(A_csr.dtype), A_csr.row_index.ptr, A_csr.col_index.ptr,
+         A_csr.val_index.ptr, N, nnz, int(w), pin.ptr if pin is not None else None, walk.ptr,
+         B.permutation_index.ptr, B.row_index.ptr, B.col_index.ptr, B.val_index.ptr,
+         _sp(stream))
+    lens = np.diff(B.row_array()) if N else np.zeros(0, np.int32)
+    B.nnz_row_index = DeviceArray.from_host(lens.astype(np.int32))
+    counts = np.bincount(np.minimum(lens, 4), minlength=5)
+    B.num_zero_rows = int(counts[0])
+    B.num_one_rows = int(counts[:2].sum())
+    B.num_two_rows = int(counts[:3].sum())
+    B.num_three_rows = int(counts[:4].sum())
+    B.walk_index = walk
+    return B
+
+
 def sort_y_rows_by_nnz(y_view, A_csr, stream=None):
     """sort_y_rows_by_nnz (src/parallel/src/sparse32.js:2220-2235): y_view
     (computed with the reordered matrix) back in the original row order; the
