@@ -35,7 +35,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-SECTIONS = ("batched", "laplacian4096_fp32", "spts", "serving", "powerlaw_csr", "serving_sweep")
+SECTIONS = ("batched", "laplacian4096_fp32", "spts", "serving", "powerlaw_csr", "serving_sweep",
+            "gather_ceiling")
 METRIC = "served SpMV/SpTS req/s + p99 vs plain path; SpMV HBM GB/s at \u22641e-5 rel err"
 UNIT = "GB/s"
 
@@ -572,10 +573,20 @@ def run_ours(args, jobs, config, rank, world, local_rank):
     dom = int(np.argmax(tot))
     achieved = objs[dom]["bytes"] / (per_obj_ms[dom] / 1e3) / 1e9
     traffic = profiled_traffic().get(objs[dom]["label"] + ("/small" if args.small else ""))
+    # the gather floor of each matrix: its col/val streams and x gathers with
+    # no row structure (sb_gather_dot), timed the same way
+    floors = {}
+    for o in objs:
+        label = o["job"]["label"]
+        if o["fmt"] == "csr" and label not in floors:
+            floors[label] = gather_floor_ms(stream, o["A"], o["x"])
     detail = {o["label"]: {"ms": round(per_obj_ms[k], 4),
                            "GB_s": round(o["bytes"] / (per_obj_ms[k] / 1e3) / 1e9, 1),
                            "frac": round(o["bytes"] / (per_obj_ms[k] / 1e3) / 1e9 / peak, 3),
                            "rel_err": o["rel_err"],
+                           "gather_floor_ms": round(floors[o["job"]["label"]], 4),
+                           "frac_of_gather_floor": round(floors[o["job"]["label"]] /
+                                                         per_obj_ms[k], 3),
                            **({"tuned": {k2: v for k2, v in o["tuned"].items() if k2 != "ms"}}
                               if "tuned" in o else {})}
               for k, o in enumerate(objs)}
@@ -589,7 +600,10 @@ def run_ours(args, jobs, config, rank, world, local_rank):
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                      "traffic": traffic,
-                     "algorithmic_bytes": objs[dom]["bytes"]},
+                     "algorithmic_bytes": objs[dom]["bytes"],
+                     "gather_floor_ms": round(floors[objs[dom]["job"]["label"]], 4),
+                     "frac_of_gather_floor": round(floors[objs[dom]["job"]["label"]] /
+                                                   per_obj_ms[dom], 3)},
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
                 "path": "sciwasm.sparse_b200.spmv via the C ABI; per call x and y uploaded "
@@ -749,6 +763,64 @@ def _vec(t):
     n = t.numel()
     dt = np.float64 if str(t.dtype) == "torch.float64" else np.float32
     return sb.sparse_vec_t(sb.DeviceArray(n, dt, t.data_ptr()), n)
+
+
+def gather_floor_ms(stream, A, x, reps=20):
+    """Mean device time of sb_gather_dot on A's col/val and x: the column and
+    value streams an SpMV must read and its x gathers, with no row
+    structure -- the floor of any SpMV kernel on this matrix."""
+    import torch
+    from sciwasm.sparse_b200 import _lib
+    from sciwasm.sparse_b200.sparse import DeviceArray
+    out = DeviceArray.from_host(np.zeros(1))
+    code = _lib.SB_F64 if A.dtype == np.float64 else _lib.SB_F32
+    sp = stream.cuda_stream
+
+    def fn():
+        _lib.call("sb_gather_dot", code, A.col_index.ptr, A.val_index.ptr, x.vec_index.ptr,
+                  A.nnz, out.ptr, sp)
+    for _ in range(3):
+        with torch.cuda.stream(stream):
+            fn()
+    return _time_each_ms(stream, fn, reps)
+
+
+def run_gather_ceiling(stream, peak, small=False):
+    """The power-law matrix of the format sweep (2M rows, ~41M nonzeros, FP64;
+    500k rows with small): the gather floor (sb_gather_dot) beside CSR (row
+    blocks with tuned options, block stream) and COO, each as a fraction of
+    the HBM peak and of the floor."""
+    import sciwasm.sparse_b200 as sb
+    from sciwasm.sparse_b200 import _lib, synth
+    n = 500_000 if small else 2_000_000
+    rp, col, val = synth.power_law(n, seed=2, dtype=np.float64)
+    A = sb.csr_from_host(rp, col, val)
+    x = sb.vec_from_host(synth.uniform_vec(n, 0))
+    y = sb.create_vec(n, 0, np.float64)
+    sp = stream.cuda_stream
+    floor = gather_floor_ms(stream, A, x)
+    nnz = col.size
+    out = {"N": n, "nnz": int(nnz), "gather_floor_ms": round(floor, 4),
+           "gather_floor_GB_s": round(nnz * 12 / floor / 1e6, 1)}
+    tuned = sb.csr_autotune(A, x, stream=sp)
+    cands = [("csr_tuned", tuple(tuned[k] for k in ("kernel", "lanes_per_row", "unroll", "grid"))),
+             ("csr_block_stream", (3, 0, 0, 0)), ("csr_row_blocks_8_4_1", (0, 8, 4, 1))]
+    for label, opts in cands:
+        A.opts = _lib.CsrOpts(*opts)
+        for _ in range(3):
+            sb.spmv(A, x, y, stream=sp)
+        ms = _time_each_ms(stream, lambda: sb.spmv(A, x, y, stream=sp), 20)
+        b = algo_bytes("csr", n, nnz, 8)
+        out[label] = {"opts": list(opts), "ms": round(ms, 4), "frac": round(b / ms / 1e6 / peak, 3),
+                      "frac_of_gather_floor": round(floor / ms, 3)}
+    C = sb.coo_from_host(synth.csr_to_coo_rows(rp), col, val, n)
+    for _ in range(3):
+        sb.spmv(C, x, y, stream=sp)
+    ms = _time_each_ms(stream, lambda: sb.spmv(C, x, y, stream=sp), 20)
+    b = algo_bytes("coo", n, nnz, 8)
+    out["coo"] = {"ms": round(ms, 4), "frac": round(b / ms / 1e6 / peak, 3),
+                  "frac_of_gather_floor": round(floor / ms, 3)}
+    return out
 
 
 def run_laplacian_large(stream, peak):
@@ -1255,6 +1327,8 @@ def main():
             out = run_powerlaw_csr(stream, peak, args.csr_opts, args.small)
         elif args.workload == "serving_sweep":
             out = run_serving_sweep(args)
+        elif args.workload == "gather_ceiling":
+            out = run_gather_ceiling(stream, peak, args.small)
         else:
             out = run_serving(args)
         print(json.dumps({"workload": args.workload, "result": out}), flush=True)

@@ -229,7 +229,9 @@ int sb_spmv_ell(int dtype, const int32_t* indices, const void* data, int32_t N, 
 
 /* One matrix of a batch: y <- y + A x for nrhs (1..8) right-hand sides, x
  * and y stored N x nrhs row-major (x[col*nrhs + j]).  flags bit 0 set:
- * y <- A x (y is overwritten, rows without entries get 0).  The y ranges of
+ * y <- A x (y is overwritten, rows without entries get 0).  flags bit 1 set
+ * (CSR, nrhs >= 2, x 16-byte aligned): one row per lane with the nrhs sums
+ * in registers and vector loads of x rows, instead of nrhs lanes per row.  The y ranges of
  * different items must not overlap (x may be shared).
  *   format SB_FMT_CSR (0): row_ptr[N+1], col[nnz], val[nnz]; lanes: lanes
  *     per row (1..32, power of two), 0 = chosen from nnz/N.

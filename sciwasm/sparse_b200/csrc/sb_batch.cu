@@ -269,6 +269,76 @@ __device__ __forceinline__ void batch_block_rhs(const sb_batch_item& it, int r0,
   }
 }
 
+// Several right-hand sides (K = 2..8), one row per lane: the 32 rows of the
+// block are walked together, each lane over its own row in storage order,
+// UNROLL entries per pass (their col/val loads first, then the K-value x
+// rows), with the K sums in registers and no shuffles.  x rows are loaded
+// as float4 / float2 (double2) vectors when K times the value size is a
+// multiple of the vector size, so that every vector load is aligned (x is
+// 16-byte aligned and row c starts at c*K values); otherwise value by value.
+template <typename T, int K>
+__device__ __forceinline__ void load_xrow(const T* __restrict__ xr, T (&v)[K]) {
+  if constexpr (sizeof(T) == 4 && K % 4 == 0) {
+#pragma unroll
+    for (int h = 0; h < K; h += 4) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(xr + h));
+      v[h] = q.x; v[h + 1] = q.y; v[h + 2] = q.z; v[h + 3] = q.w;
+    }
+  } else if constexpr (sizeof(T) == 4 && K % 2 == 0) {
+#pragma unroll
+    for (int h = 0; h < K; h += 2) {
+      const float2 q = __ldg(reinterpret_cast<const float2*>(xr + h));
+      v[h] = q.x; v[h + 1] = q.y;
+    }
+  } else if constexpr (sizeof(T) == 8 && K % 2 == 0) {
+#pragma unroll
+    for (int h = 0; h < K; h += 2) {
+      const double2 q = __ldg(reinterpret_cast<const double2*>(xr + h));
+      v[h] = q.x; v[h + 1] = q.y;
+    }
+  } else {
+#pragma unroll
+    for (int h = 0; h < K; ++h) v[h] = __ldg(xr + h);
+  }
+}
+
+template <typename SV, typename T, int K>
+__device__ __forceinline__ void batch_block_lane_rows(const sb_batch_item& it, int r0, int lane) {
+  constexpr int UNROLL = 4;
+  const int i = r0 + lane;
+  const int N = it.N;
+  const bool overwrite = (it.flags & 1) != 0;
+  if (i >= N) return;
+  const int s = __ldg(it.row_ptr + i), e = __ldg(it.row_ptr + i + 1);
+  const int* __restrict__ col = it.col;
+  const SV* __restrict__ val = (const SV*)it.val;
+  const T* __restrict__ x = (const T*)it.x;
+  T* __restrict__ y = (T*)it.y;
+  T acc[K];
+#pragma unroll
+  for (int h = 0; h < K; ++h) acc[h] = 0;
+  for (int k0 = s; k0 < e; k0 += UNROLL) {
+    int cc[UNROLL];
+    T vv[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      cc[u] = k0 + u < e ? ld_reuse(col + k0 + u) : 0;
+      vv[u] = k0 + u < e ? ldv(val, k0 + u) : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      if (k0 + u < e) {
+        T xv[K];
+        load_xrow<T, K>(x + (long long)cc[u] * K, xv);
+#pragma unroll
+        for (int h = 0; h < K; ++h) acc[h] += vv[u] * xv[h];
+      }
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < K; ++h) put_y(y, (long long)i * K + h, acc[h], overwrite, e > s);
+}
+
 template <typename T> __device__ __forceinline__ T bmul_rn(T a, T b);
 template <> __device__ __forceinline__ float bmul_rn(float a, float b) { return __fmul_rn(a, b); }
 template <> __device__ __forceinline__ double bmul_rn(double a, double b) { return __dmul_rn(a, b); }
@@ -359,6 +429,18 @@ __global__ void __launch_bounds__(kBT, 5)
       }
       if (it.format == SB_FMT_ELL) {
         batch_block_ell<SV, T>(it, r0, lane);
+        continue;
+      }
+      if (it.nrhs > 1 && (it.flags & 2)) {
+        switch (it.nrhs) {
+          case 2: batch_block_lane_rows<SV, T, 2>(it, r0, lane); break;
+          case 3: batch_block_lane_rows<SV, T, 3>(it, r0, lane); break;
+          case 4: batch_block_lane_rows<SV, T, 4>(it, r0, lane); break;
+          case 5: batch_block_lane_rows<SV, T, 5>(it, r0, lane); break;
+          case 6: batch_block_lane_rows<SV, T, 6>(it, r0, lane); break;
+          case 7: batch_block_lane_rows<SV, T, 7>(it, r0, lane); break;
+          default: batch_block_lane_rows<SV, T, 8>(it, r0, lane); break;
+        }
         continue;
       }
       if (it.nrhs > 1) {
@@ -494,6 +576,8 @@ int sb_batch_exec_run(sb_batch_exec* e, const sb_batch_item* items, int32_t n, v
     if (it.format == SB_FMT_CSR) {
       SB_REQUIRE(it.N == 0 || (it.row_ptr && it.x && it.y && (it.nnz == 0 || (it.col && it.val))),
                  "sb_batch_exec_run: item %d: null pointer", i);
+      // the row-per-lane path loads x rows as 16-byte vectors
+      if ((reinterpret_cast<uintptr_t>(it.x) & 15u) != 0) it.flags &= ~2;
       if (it.lanes <= 0) it.lanes = lanes_for(it.nnz, it.N);
       it.lanes = it.lanes > 32 ? 32 : it.lanes;
     } else {

@@ -702,7 +702,7 @@ class BatchExecutor:
         self._items = (_lib.BatchItem * self.capacity)()
         self._keep = []
 
-    def run(self, jobs, stream=None, overwrite=False):
+    def run(self, jobs, stream=None, overwrite=False, lane_rows=False):
         """jobs: iterable of (A, x DeviceArray N*k, y DeviceArray N*k, k) with A
         a CSR, DIA (stride N) or ELL matrix; y += A x, or y = A x with
         overwrite=True."""
@@ -714,7 +714,8 @@ class BatchExecutor:
         for A, x, y, k in jobs:
             it = self._items[n]
             it.x, it.y = x.ptr, y.ptr
-            it.N, it.nrhs, it.lanes, it.flags, it.nnz = A.N, int(k), 0, 1 if overwrite else 0, A.nnz
+            it.N, it.nrhs, it.lanes, it.nnz = A.N, int(k), 0, A.nnz
+            it.flags = (1 if overwrite else 0) | (2 if lane_rows else 0)
             if isinstance(A, sparse_DIA_t):
                 if A.stride != A.N:
                     raise ValueError("batched DIA items need stride == N")

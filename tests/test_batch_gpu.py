@@ -27,9 +27,10 @@ def _batch(seed, count, dt):
     return out
 
 
+@pytest.mark.parametrize("lane_rows", [False, True])
 @pytest.mark.parametrize("storage,dt", [("f32", np.float32), ("f64", np.float64),
                                         ("bf16", np.float32)])
-def test_batch_matches_per_matrix(gpu, oracle, storage, dt):
+def test_batch_matches_per_matrix(gpu, oracle, storage, dt, lane_rows):
     mats = _batch(7, 40, np.float64 if storage == "f64" else np.float32)
     ex = gpu.BatchExecutor(storage, capacity=64)
     jobs, host = [], []
@@ -45,7 +46,7 @@ def test_batch_matches_per_matrix(gpu, oracle, storage, dt):
         jobs.append((A, xd, yd, k))
         host.append((rp, col, val, X, Y0, A))
     for rep in range(2):  # graph replay: second run accumulates again
-        ex.run(jobs)
+        ex.run(jobs, lane_rows=lane_rows)
         gpu.synchronize()
     tol = 1e-4 if storage == "bf16" else TOL[np.dtype(dt)]
     for (A, xd, yd, k), (rp, col, val, X, Y0, Ad) in zip(jobs, host):
