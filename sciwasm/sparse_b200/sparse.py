@@ -1209,6 +1209,18 @@ def fletcher_sum(a) -> int:
     return int(s2 * 256.0 + s1)
 
 
+def clear_vec(y_view, stream=None) -> None:
+    """clear_vec (src/sequential/src/sparse32.js:1319-1322): y = 0, on the
+    device (stream-ordered).  The reference's benchmark clears y this way
+    before every spmv (src/sequential/tests/main32.js:123-124)."""
+    y_view.vec_index.fill_zero(stream)
+
+
+def init_x(x_view) -> None:
+    """init_x (src/sequential/src/sparse32.js:1313-1317): x[i] = i."""
+    x_view.vec_index.upload(np.arange(x_view.vec_nelem, dtype=x_view.dtype))
+
+
 def fletcher_sum_y(y_view) -> int:
     """fletcher_sum_y (src/sequential/src/sparse32.js:1306-1311)."""
     return fletcher_sum(y_view.array())
