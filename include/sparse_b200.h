@@ -211,7 +211,9 @@ int sb_convert_values(int src_dtype, const void* src, int dst_dtype, void* dst, 
 /* Replaces spmv_dia / spmv_dia_wrapper
  * (src/sequential/src/sparse_opt_32.wat:290-425; dispatch
  * src/sequential/src/sparse32.js:1272-1278).  offset[nd] diagonal offsets
- * (device), data[nd*stride] diagonal-major. */
+ * (device), data[nd*stride] diagonal-major.  dtype SB_BF16 (no counterpart in
+ * the reference): BF16 data with f32 x, y and sums in the same per-row
+ * order. */
 int sb_spmv_dia(int dtype, const int32_t* offset, const void* data, int32_t N, int32_t nd,
                 int32_t stride, const void* x, void* y, int32_t inner_max, void* stream);
 

@@ -1004,9 +1004,9 @@ template <> __device__ __forceinline__ double add_rn(double a, double b) { retur
 // separately rounded product (src/sequential/src/sparse_opt_32.wat:290-407).
 // The in-band test is a predicate so that the unrolled loop issues the data
 // and x loads of several diagonals before their dependent additions.
-template <typename T>
+template <typename SV, typename T>
 __global__ void __launch_bounds__(256)
-    dia_row_kernel(const int* __restrict__ offset, const T* __restrict__ data, int N, int nd,
+    dia_row_kernel(const int* __restrict__ offset, const SV* __restrict__ data, int N, int nd,
                    int stride, const T* __restrict__ x, T* __restrict__ y) {
   // smallest and largest offset (whatever their order), for the interior test
   __shared__ int kext[2];
@@ -1029,11 +1029,11 @@ __global__ void __launch_bounds__(256)
   // increments and no predicates
   const int kmin = kext[0], kmax = kext[1];
   if (move == 0 && (long long)i + kmin >= 0 && (long long)i + kmax < N) {
-    const T* dp = data + i;
+    const SV* dp = data + i;
     const T* xp = x + i;
 #pragma unroll 4
     for (int d = 0; d < nd; ++d, dp += stride)
-      t = add_rn(mul_rn(ld_stream(dp), ld_ro(xp + __ldg(offset + d))), t);
+      t = add_rn(mul_rn((T)ld_val(dp), ld_ro(xp + __ldg(offset + d))), t);
     y[i] = t;
     return;
   }
@@ -1042,7 +1042,7 @@ __global__ void __launch_bounds__(256)
     const int k = __ldg(offset + d);
     const bool in = (unsigned)(i + k) < (unsigned)N;
     const long long idx = (long long)d * stride + i - (k < 0 ? move : 0);
-    T a = in ? ld_stream(data + idx) : (T)0;
+    T a = in ? (T)ld_val(data + idx) : (T)0;
     T b = in ? ld_ro(x + i + k) : (T)0;
     T p = mul_rn(a, b);
     t = in ? add_rn(p, t) : t;
@@ -1055,9 +1055,9 @@ __global__ void __launch_bounds__(256)
 // block barrier), and a row's ND data loads and ND x loads are all issued
 // before its additions, which keep the stored order (bit-identical to the
 // runtime-count kernel).
-template <typename T, int ND>
+template <typename SV, typename T, int ND>
 __global__ void __launch_bounds__(256)
-    dia_rows_nd(const int* __restrict__ offset, const T* __restrict__ data, int N, int stride,
+    dia_rows_nd(const int* __restrict__ offset, const SV* __restrict__ data, int N, int stride,
                 const T* __restrict__ x, T* __restrict__ y) {
   int k[ND];
   int kmin = 0x7fffffff, kmax = -0x7fffffff - 1;
@@ -1075,7 +1075,7 @@ __global__ void __launch_bounds__(256)
   if (move == 0 && (long long)i + kmin >= 0 && (long long)i + kmax < N) {
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
-      a[d] = ld_stream(data + (long long)d * stride + i);
+      a[d] = (T)ld_val(data + (long long)d * stride + i);
       b[d] = ld_ro(x + i + k[d]);
     }
 #pragma unroll
@@ -1087,7 +1087,7 @@ __global__ void __launch_bounds__(256)
   for (int d = 0; d < ND; ++d) {
     const bool in = (unsigned)(i + k[d]) < (unsigned)N;
     const long long idx = (long long)d * stride + i - (k[d] < 0 ? move : 0);
-    a[d] = in ? ld_stream(data + idx) : (T)0;
+    a[d] = in ? (T)ld_val(data + idx) : (T)0;
     b[d] = in ? ld_ro(x + i + k[d]) : (T)0;
   }
 #pragma unroll
@@ -1099,19 +1099,19 @@ __global__ void __launch_bounds__(256)
   y[i] = t;
 }
 
-template <typename T>
-static void launch_dia(const int* offset, const T* data, int N, int nd, int stride, const T* x,
+template <typename SV, typename T>
+static void launch_dia(const int* offset, const SV* data, int N, int nd, int stride, const T* x,
                        T* y, cudaStream_t st) {
   const unsigned blocks = (unsigned)((N + 255) / 256);
   switch (nd) {
 #define SB_DIA_ND(n) \
-  case n: dia_rows_nd<T, n><<<blocks, 256, 0, st>>>(offset, data, N, stride, x, y); return;
+  case n: dia_rows_nd<SV, T, n><<<blocks, 256, 0, st>>>(offset, data, N, stride, x, y); return;
     SB_DIA_ND(1) SB_DIA_ND(2) SB_DIA_ND(3) SB_DIA_ND(4) SB_DIA_ND(5) SB_DIA_ND(6) SB_DIA_ND(7)
     SB_DIA_ND(8) SB_DIA_ND(9) SB_DIA_ND(10) SB_DIA_ND(11) SB_DIA_ND(12) SB_DIA_ND(13)
     SB_DIA_ND(14) SB_DIA_ND(15) SB_DIA_ND(16)
 #undef SB_DIA_ND
     default:
-      dia_row_kernel<T><<<blocks, 256, 0, st>>>(offset, data, N, nd, stride, x, y);
+      dia_row_kernel<SV, T><<<blocks, 256, 0, st>>>(offset, data, N, nd, stride, x, y);
   }
 }
 
@@ -1388,7 +1388,7 @@ int sb_spmv_coo_ex(int dtype, const int32_t* row, const int32_t* col, const void
 
 int sb_spmv_dia(int dtype, const int32_t* offset, const void* data, int32_t N, int32_t nd,
                 int32_t stride, const void* x, void* y, int32_t inner_max, void* stream) {
-  int r = check_dtype(dtype, "sb_spmv_dia");
+  int r = dtype == SB_BF16 ? SB_OK : check_dtype(dtype, "sb_spmv_dia");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nd >= 0 && inner_max >= 0, "sb_spmv_dia: negative size");
   SB_REQUIRE(stride >= N, "sb_spmv_dia: stride %d < N %d", stride, N);
@@ -1398,10 +1398,14 @@ int sb_spmv_dia(int dtype, const int32_t* offset, const void* data, int32_t N, i
   cudaStream_t st = as_stream(stream);
   for (int it = 0; it < inner_max; ++it) {
     if (dtype == SB_F32)
-      launch_dia<float>(offset, (const float*)data, N, nd, stride, (const float*)x, (float*)y, st);
+      launch_dia<float, float>(offset, (const float*)data, N, nd, stride, (const float*)x,
+                               (float*)y, st);
+    else if (dtype == SB_BF16)
+      launch_dia<__nv_bfloat16, float>(offset, (const __nv_bfloat16*)data, N, nd, stride,
+                                       (const float*)x, (float*)y, st);
     else
-      launch_dia<double>(offset, (const double*)data, N, nd, stride, (const double*)x, (double*)y,
-                         st);
+      launch_dia<double, double>(offset, (const double*)data, N, nd, stride, (const double*)x,
+                                 (double*)y, st);
     SB_CHECK_LAUNCH("dia_row_kernel");
   }
   return SB_OK;

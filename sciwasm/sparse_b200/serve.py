@@ -663,10 +663,10 @@ class Server:
 
 def _spmv_call(m: ResidentMatrix, storage: str, xp: int, yp: int, stream) -> None:
     """The per-call path's y += A x: the matrix's chosen format where a
-    single-call kernel takes its values (DIA and ELL: f32 and f64), else the
-    CSR."""
+    single-call kernel takes its values (DIA: f32, f64 and BF16; ELL: f32 and
+    f64), else the CSR."""
     M = m.fmt.get(storage, m.csr[storage])
-    if isinstance(M, sparse_DIA_t) and storage != "bf16":
+    if isinstance(M, sparse_DIA_t):
         call("sb_spmv_dia", _dtcode(M.dtype), M.offset_index.ptr, M.data_index.ptr, M.N,
              M.ndiags, M.stride, xp, yp, 1, stream)
     elif isinstance(M, sparse_ELL_t) and storage != "bf16":

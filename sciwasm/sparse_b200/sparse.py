@@ -625,8 +625,8 @@ def spmv(A, x_view, y_view, inner_max=1, stream=None):
         raise ValueError("spmv input : undefined")
     if x_view.dtype != _vec_dtype(A) or y_view.dtype != _vec_dtype(A):
         raise TypeError("x and y must have the matrix's value dtype (f32 for BF16 storage)")
-    if A.dtype == np.uint16 and not isinstance(A, sparse_CSR_t):
-        raise TypeError("BF16 storage is supported for CSR SpMV")
+    if A.dtype == np.uint16 and not isinstance(A, (sparse_CSR_t, sparse_DIA_t)):
+        raise TypeError("BF16 storage is supported for CSR and DIA SpMV")
     if x_view.vec_nelem < A.N or y_view.vec_nelem < A.N:
         raise ValueError("x and y must hold N values")
     dt = _dtcode(A.dtype)

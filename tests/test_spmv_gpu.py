@@ -361,3 +361,25 @@ def test_spmv_autotune_statistics_mode(gpu, oracle):
         yv = gpu.vec_from_host(y0)
         gpu.spmv(M, gpu.vec_from_host(x), yv)
         assert rel_err(yv.array(), oracle.truth_csr(rp, col, val, x, y0)) <= 1e-5, name
+
+
+def test_dia_bf16_storage(gpu, oracle):
+    """DIA with BF16 data (f32 x, y and sums): within tolerance of the FP64
+    product of the stored values, and bit-identical to the batched DIA item
+    on the same data (the same per-row order)."""
+    rp, col, val = synth.laplacian_2d(300, dtype=np.float32)
+    N = rp.size - 1
+    D = gpu.csr_dia(gpu.csr_from_host(rp, col, val))
+    Db = gpu.with_storage(D, "bf16")
+    x, y0 = _x_y(N, np.float32)
+    yv = gpu.vec_from_host(y0)
+    gpu.spmv(Db, gpu.vec_from_host(x), yv)
+    vb = (gpu.csr_with_storage(gpu.csr_from_host(rp, col, val), "bf16").val_array()
+          .astype(np.uint32) << 16).view(np.float32)
+    truth = oracle.truth_csr(rp, col, vb.astype(np.float64), x.astype(np.float64), y0)
+    assert rel_err(yv.array(), truth) <= 1e-5
+    ex = gpu.BatchExecutor("bf16", capacity=2)
+    xd, yd = gpu.DeviceArray.from_host(x), gpu.DeviceArray.from_host(y0)
+    ex.run([(Db, xd, yd, 1)])
+    gpu.synchronize()
+    assert np.array_equal(yd.to_host().view(np.uint32), yv.array().view(np.uint32))
