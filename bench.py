@@ -791,12 +791,12 @@ def gather_floor_ms(stream, A, x, reps=20):
 
 def run_gather_ceiling(stream, peak, small=False):
     """The power-law matrix of the format sweep (2M rows, ~41M nonzeros, FP64;
-    500k rows with small): the gather floor (sb_gather_dot) beside CSR (row
-    blocks with tuned options, block stream) and COO, each as a fraction of
-    the HBM peak and of the floor."""
+    1M rows with small, ~250 MB of col/val, still above L2): the gather floor
+    (sb_gather_dot) beside CSR (row blocks with tuned options, block stream)
+    and COO, each as a fraction of the HBM peak and of the floor."""
     import sciwasm.sparse_b200 as sb
     from sciwasm.sparse_b200 import _lib, synth
-    n = 500_000 if small else 2_000_000
+    n = 1_000_000 if small else 2_000_000
     rp, col, val = synth.power_law(n, seed=2, dtype=np.float64)
     A = sb.csr_from_host(rp, col, val)
     x = sb.vec_from_host(synth.uniform_vec(n, 0))
@@ -868,6 +868,28 @@ def run_laplacian_large(stream, peak):
         out[storage] = {"ms": round(ms, 4), "GB_s": round(gbs, 1), "frac": round(gbs / peak, 3),
                         "algorithmic_bytes": nbytes, "rel_err_vs_fp64": err,
                         "tuned": {k: v for k, v in tuned.items() if k != "ms"}}
+    # the format the statistics choose for a 5-point stencil (DIA, no index
+    # arrays), with FP32 and BF16 data
+    D, info = sb.spmv_autotune(A, timed=False)
+    out["format_choice"] = info["format"]
+    if info["format"] == "dia":
+        for storage in ("f32", "bf16"):
+            Ds = D if storage == "f32" else sb.with_storage(D, "bf16")
+            yt.zero_()
+            with torch.cuda.stream(stream):
+                sb.spmv(Ds, x, y, stream=sp)
+            torch.cuda.synchronize()
+            err = float((yt.double().reshape(n, n) - T).abs().max() / T.abs().max())
+            for _ in range(3):
+                with torch.cuda.stream(stream):
+                    sb.spmv(Ds, x, y, stream=sp)
+            ms = _time_each_ms(stream, lambda: sb.spmv(Ds, x, y, stream=sp), 20)
+            s_v = 2 if storage == "bf16" else 4
+            nbytes = D.ndiags * N * s_v + 4 * D.ndiags + 3 * N * 4
+            gbs = nbytes / (ms / 1e3) / 1e9
+            out[f"dia_{storage}"] = {"ms": round(ms, 4), "GB_s": round(gbs, 1),
+                                     "frac": round(gbs / peak, 3), "algorithmic_bytes": nbytes,
+                                     "rel_err_vs_fp64": err}
     return out
 
 
