@@ -99,10 +99,10 @@ int sb_spmv_coo(int dtype, const int32_t* row, const int32_t* col, const void* v
 /* sb_spmv_coo with flags; no counterpart in the reference.  SB_COO_ROWS_SORTED
  * states that row[] is non-decreasing (as in the reference's COO objects,
  * which create_COO_from_MM leaves sorted by (row, col)): rows that lie wholly
- * inside one 256-entry tile are then added without atomics (taken when the
- * mean row length is at most 16; longer rows keep the atomics, which cost
- * less there).  The flag is the caller's guarantee and is not checked: with
- * unsorted rows the result is wrong.  flags = 0 is sb_spmv_coo. */
+ * inside one 256-entry tile are then stored without atomics, from y values
+ * loaded while the x gathers are in flight.  The flag is the caller's
+ * guarantee and is not checked: with unsorted rows the result is wrong.
+ * flags = 0 is sb_spmv_coo. */
 #define SB_COO_ROWS_SORTED 1
 int sb_spmv_coo_ex(int dtype, const int32_t* row, const int32_t* col, const void* val,
                    const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
@@ -231,9 +231,8 @@ int sb_spmv_ell(int dtype, const int32_t* indices, const void* data, int32_t N, 
 
 /* One matrix of a batch: y <- y + A x for nrhs (1..8) right-hand sides, x
  * and y stored N x nrhs row-major (x[col*nrhs + j]).  flags bit 0 set:
- * y <- A x (y is overwritten, rows without entries get 0).  flags bit 1 set
- * (CSR, nrhs >= 2, x 16-byte aligned): one row per lane with the nrhs sums
- * in registers and vector loads of x rows, instead of nrhs lanes per row.  The y ranges of
+ * y <- A x (y is overwritten, rows without entries get 0).  Other flag bits
+ * must be 0.  The y ranges of
  * different items must not overlap (x may be shared).
  *   format SB_FMT_CSR (0): row_ptr[N+1], col[nnz], val[nnz]; lanes: lanes
  *     per row (1..32, power of two), 0 = chosen from nnz/N.

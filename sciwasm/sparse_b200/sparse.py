@@ -47,6 +47,7 @@ class DeviceArray:
     __slots__ = ("n", "dtype", "nbytes", "ptr", "_owned")
 
     def __init__(self, n: int, dtype, ptr: Optional[int] = None):
+        self.ptr, self._owned = 0, False  # a failed allocation leaves nothing to free
         self.n = int(n)
         self.dtype = np.dtype(dtype)
         self.nbytes = self.n * self.dtype.itemsize
@@ -702,7 +703,7 @@ class BatchExecutor:
         self._items = (_lib.BatchItem * self.capacity)()
         self._keep = []
 
-    def run(self, jobs, stream=None, overwrite=False, lane_rows=False):
+    def run(self, jobs, stream=None, overwrite=False):
         """jobs: iterable of (A, x DeviceArray N*k, y DeviceArray N*k, k) with A
         a CSR, DIA (stride N) or ELL matrix; y += A x, or y = A x with
         overwrite=True."""
@@ -715,7 +716,7 @@ class BatchExecutor:
             it = self._items[n]
             it.x, it.y = x.ptr, y.ptr
             it.N, it.nrhs, it.lanes, it.nnz = A.N, int(k), 0, A.nnz
-            it.flags = (1 if overwrite else 0) | (2 if lane_rows else 0)
+            it.flags = 1 if overwrite else 0
             if isinstance(A, sparse_DIA_t):
                 if A.stride != A.N:
                     raise ValueError("batched DIA items need stride == N")

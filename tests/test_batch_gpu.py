@@ -27,13 +27,15 @@ def _batch(seed, count, dt):
     return out
 
 
-@pytest.mark.parametrize("lane_rows", [False, True])
+@pytest.mark.parametrize("x_aligned", [True, False])
 @pytest.mark.parametrize("storage,dt", [("f32", np.float32), ("f64", np.float64),
                                         ("bf16", np.float32)])
-def test_batch_matches_per_matrix(gpu, oracle, storage, dt, lane_rows):
+def test_batch_matches_per_matrix(gpu, oracle, storage, dt, x_aligned):
+    """x 16-byte aligned: several right-hand sides take one row per lane;
+    x one value off (not 16-byte aligned): nrhs lanes per row."""
     mats = _batch(7, 40, np.float64 if storage == "f64" else np.float32)
     ex = gpu.BatchExecutor(storage, capacity=64)
-    jobs, host = [], []
+    jobs, host, keep = [], [], []
     for idx, (rp, col, val, k) in enumerate(mats):
         N = rp.size - 1
         A = gpu.csr_from_host(rp, col, val)
@@ -42,11 +44,17 @@ def test_batch_matches_per_matrix(gpu, oracle, storage, dt, lane_rows):
         vdt = np.float64 if storage == "f64" else np.float32
         X = synth.uniform_vec(N * k, idx, dtype=vdt).reshape(N, k)
         Y0 = synth.uniform_vec(N * k, 1000 + idx, dtype=vdt).reshape(N, k)
-        xd, yd = gpu.DeviceArray.from_host(X.ravel()), gpu.DeviceArray.from_host(Y0.ravel())
+        if x_aligned:
+            xd = gpu.DeviceArray.from_host(X.ravel())
+        else:
+            base = gpu.DeviceArray.from_host(np.concatenate([[0], X.ravel()]).astype(vdt))
+            xd = gpu.DeviceArray(N * k, vdt, base.ptr + np.dtype(vdt).itemsize)
+            keep.append(base)  # the buffer must outlive the runs
+        yd = gpu.DeviceArray.from_host(Y0.ravel())
         jobs.append((A, xd, yd, k))
         host.append((rp, col, val, X, Y0, A))
     for rep in range(2):  # graph replay: second run accumulates again
-        ex.run(jobs, lane_rows=lane_rows)
+        ex.run(jobs)
         gpu.synchronize()
     tol = 1e-4 if storage == "bf16" else TOL[np.dtype(dt)]
     for (A, xd, yd, k), (rp, col, val, X, Y0, Ad) in zip(jobs, host):
@@ -94,7 +102,7 @@ def test_batch_mixed_formats(gpu, oracle, storage):
     DIA / ELL loop on that column; BF16 items are within tolerance of the FP64
     product of their stored values."""
     vdt = np.float64 if storage == "f64" else np.float32
-    ex = gpu.BatchExecutor(storage, capacity=16)
+    ex = gpu.BatchExecutor(storage, capacity=32)
     cases = []
     for i, (rp, col, val) in enumerate([synth.banded(7_001, half=3, seed=3, dtype=vdt),
                                         synth.laplacian_2d(90, dtype=vdt),

@@ -209,14 +209,16 @@ def test_serving_flags_growth_for_f64_accumulation(gpu):
 def test_pool_admission_evicts_lru_and_refuses_pinned(gpu):
     rp, col, val = synth.banded(50_000, half=5, seed=1)
     one = serve.matrix_bytes(rp.size - 1, col.size, ("f32",))
-    pool = serve.ResidentPool(budget_bytes=2 * one + 100, reserve_bytes=0)
+    # CSR only: these sizes count the CSR bytes (the DIA form a pool adds by
+    # default is charged on top, see test_pool_charges_the_chosen_format)
+    pool = serve.ResidentPool(budget_bytes=2 * one + 100, reserve_bytes=0, spmv_format="csr")
     pool.add("a", rp, col, val)
     pool.add("b", rp, col, val)
     pool.get("a")                       # b is now the least recently used
     pool.add("c", rp, col, val)
     assert set(pool.mats) == {"a", "c"} and pool.admission.used == 2 * one
     pool.close()
-    pool = serve.ResidentPool(budget_bytes=2 * one + 100, reserve_bytes=0)
+    pool = serve.ResidentPool(budget_bytes=2 * one + 100, reserve_bytes=0, spmv_format="csr")
     pool.add("a", rp, col, val, pinned=True)
     pool.add("b", rp, col, val, pinned=True)
     with pytest.raises(serve.AdmissionError):
@@ -260,4 +262,24 @@ def test_serving_cancelled_requests_are_dropped(gpu, oracle):
             else:
                 assert r.status == "done", r.rid
                 assert rel_err(r.y, _truth(oracle, pool, host, r)) <= SERVE_TOL, r.rid
+    pool.close()
+
+
+def test_pool_charges_the_chosen_format(gpu, oracle):
+    """With the default format choice a banded matrix is kept in DIA beside its
+    CSR; the DIA bytes (offsets once, data per storage) are charged to its
+    entry, and when the budget has no room for them the matrix stays CSR."""
+    rp, col, val = synth.banded(50_000, half=5, seed=1)
+    N = rp.size - 1
+    csr_b = serve.matrix_bytes(N, col.size, ("f32", "bf16"))
+    dia_b = 4 * 11 + 11 * N * (4 + 2)
+    pool = serve.ResidentPool(budget_bytes=10 * csr_b, reserve_bytes=0)
+    m = pool.add("band", rp, col, val, spmv_storages=("f32", "bf16"))
+    assert m.format == "dia" and pool.admission.used == csr_b + dia_b
+    assert isinstance(m.fmt["f32"], gpu.sparse_DIA_t) and m.fmt["bf16"].dtype == np.uint16
+    pool.close()
+    pool = serve.ResidentPool(budget_bytes=csr_b + 100, reserve_bytes=0)
+    m = pool.add("band", rp, col, val, spmv_storages=("f32", "bf16"))
+    assert m.format == "csr" and pool.admission.used == csr_b
+    assert m.fmt["f32"] is m.csr["f32"]
     pool.close()

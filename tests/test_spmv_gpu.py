@@ -340,13 +340,13 @@ def _poisson_rows(N, mean, seed):
 
 def test_spmv_autotune_statistics_mode(gpu, oracle):
     """Without timing, the admitted format with the fewest compulsory bytes:
-    DIA for banded and 5-point matrices, CSR (block-stream kernel) for skewed
-    power-law rows, CSR (row blocks) for Poisson row lengths, ELL for rows of
-    one length (no row_ptr to read); the chosen object keeps parity."""
+    DIA for banded and 5-point matrices, CSR row blocks for Poisson row
+    lengths and, one warp per block, for skewed power-law rows, ELL for rows
+    of one length (no row_ptr to read); the chosen object keeps parity."""
     cases = {"banded": (synth.banded(50_000, half=5, seed=1, dtype=np.float32), "dia", None),
              "lap2d": (synth.laplacian_2d(200, dtype=np.float32), "dia", None),
-             "powerlaw": (synth.power_law(60_000, seed=2, dtype=np.float32), "csr", 3),
-             "poisson": (_poisson_rows(60_000, 12.0, seed=3), "csr", 0),
+             "powerlaw": (synth.power_law(60_000, seed=2, dtype=np.float32), "csr", (0, 8, 1)),
+             "poisson": (_poisson_rows(60_000, 12.0, seed=3), "csr", (0, 4, 0)),
              "uniform13": (synth.random_lower(60_000, per_row=12, band=60_000, seed=3,
                                               dtype=np.float32), "ell", None)}
     for name, ((rp, col, val), fmt, kernel) in cases.items():
@@ -356,7 +356,8 @@ def test_spmv_autotune_statistics_mode(gpu, oracle):
         assert info["format"] == fmt, (name, info)
         assert all(v is None for v in info["ms"].values())
         if kernel is not None:
-            assert info["csr_opts"]["kernel"] == kernel, (name, info)
+            o = info["csr_opts"]
+            assert (o["kernel"], o["lanes_per_row"], o["grid"]) == kernel, (name, info)
         x, y0 = _x_y(N, np.float32)
         yv = gpu.vec_from_host(y0)
         gpu.spmv(M, gpu.vec_from_host(x), yv)
@@ -383,3 +384,13 @@ def test_dia_bf16_storage(gpu, oracle):
     ex.run([(Db, xd, yd, 1)])
     gpu.synchronize()
     assert np.array_equal(yd.to_host().view(np.uint32), yv.array().view(np.uint32))
+
+
+def test_clear_vec_and_init_x(gpu):
+    """clear_vec / init_x (src/sequential/src/sparse32.js:1313-1322) on the device."""
+    for dt in DTYPES:
+        v = gpu.vec_from_host(np.full(1000, 3.5, dt))
+        gpu.clear_vec(v)
+        assert np.array_equal(v.array(), np.zeros(1000, dt))
+        gpu.init_x(v)
+        assert np.array_equal(v.array(), np.arange(1000, dtype=dt))

@@ -63,8 +63,9 @@ def test_noalloc_matches_oracle_sync_free_order(gpu, oracle, dt):
     for call in range(2):
         b = synth.uniform_vec(N, 30 + call, dtype=dt)
         y = _dev(np.full(N, np.nan, dt))
+        d_b = _dev(b)  # held: a temporary's device buffer is freed as soon as it is dropped
         st = lib.sb_spts_syncfree_csr_noalloc(code, d_rp.ptr, d_col.ptr, d_val.ptr, N,
-                                              _dev(b).ptr, y.ptr, 0, None)
+                                              d_b.ptr, y.ptr, 0, None)
         assert st == 0, lib.sb_last_error()
         want = oracle.spts_syncfree(rp, col, val, b)
         assert np.array_equal(y.to_host().view(np.uint8), want.view(np.uint8)), call
@@ -86,8 +87,9 @@ def test_noalloc_timeout_then_next_call_is_clean(gpu, oracle):
     grp, gcol, gval = synth.laplacian_3d_lower(8)
     b = synth.uniform_vec(512, 2)
     y = _dev(np.zeros(512))
-    st = lib.sb_spts_syncfree_csr_noalloc(_lib.SB_F64, _dev(grp).ptr, _dev(gcol).ptr,
-                                          _dev(gval).ptr, 512, _dev(b).ptr, y.ptr, 0, None)
+    g = [_dev(a) for a in (grp, gcol, gval, b)]  # held for the duration of the call
+    st = lib.sb_spts_syncfree_csr_noalloc(_lib.SB_F64, g[0].ptr, g[1].ptr, g[2].ptr, 512,
+                                          g[3].ptr, y.ptr, 0, None)
     assert st == 0, lib.sb_last_error()
     want = oracle.spts_syncfree(grp, gcol, gval, b)
     assert np.array_equal(y.to_host().view(np.uint8), want.view(np.uint8))
