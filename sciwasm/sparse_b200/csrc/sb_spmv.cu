@@ -1099,10 +1099,73 @@ __global__ void __launch_bounds__(256)
   y[i] = t;
 }
 
+// dia_rows_nd with R rows per thread (rows base + r*256, so that each load
+// instruction of a warp stays coalesced): the R rows' data, x and y loads
+// are all issued before their additions, which puts R times the bytes in
+// flight per thread -- for 2- and 4-byte values and few diagonals one row
+// per thread leaves too few loads in flight.  Every row is computed as in
+// dia_rows_nd (bit-identical).
+template <typename SV, typename T, int ND, int R>
+__global__ void __launch_bounds__(256)
+    dia_rows_multi(const int* __restrict__ offset, const SV* __restrict__ data, int N, int stride,
+                   const T* __restrict__ x, T* __restrict__ y) {
+  int k[ND];
+  const SV* dp[ND];  // diagonal d's entry of row 0 (rows below the band shift by N - stride)
+  const long long move = (long long)N - stride;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    k[d] = __ldg(offset + d);
+    dp[d] = data + (long long)d * stride - (k[d] < 0 ? move : 0);
+  }
+  const int base = blockIdx.x * (256 * R) + threadIdx.x;
+  T a[R][ND], b[R][ND], t[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int i = base + r * 256;
+    const bool valid = i < N;
+    t[r] = valid ? y[i] : (T)0;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const bool in = valid && (unsigned)(i + k[d]) < (unsigned)N;
+      a[r][d] = in ? (T)ld_val(dp[d] + i) : (T)0;
+      b[r][d] = in ? ld_ro(x + i + k[d]) : (T)0;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int i = base + r * 256;
+    if (i >= N) continue;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const bool in = (unsigned)(i + k[d]) < (unsigned)N;
+      const T p = mul_rn(a[r][d], b[r][d]);
+      t[r] = in ? add_rn(p, t[r]) : t[r];
+    }
+    y[i] = t[r];
+  }
+}
+
 template <typename SV, typename T>
 static void launch_dia(const int* offset, const SV* data, int N, int nd, int stride, const T* x,
                        T* y, cudaStream_t st) {
   const unsigned blocks = (unsigned)((N + 255) / 256);
+  // few diagonals of 2- or 4-byte values: 4 rows per thread (2 for 5..8);
+  // the row index stays 32-bit (N < 2^31 and the grid covers N rows)
+  if constexpr (sizeof(SV) <= 4) {
+    if (nd <= 8 && (long long)N + 256LL * 4 < 0x7fffffffLL) {
+    switch (nd) {
+#define SB_DIA_MR(n, r)                                                                      \
+  case n:                                                                                    \
+    dia_rows_multi<SV, T, n, r><<<(unsigned)((N + 256 * r - 1) / (256 * r)), 256, 0, st>>>( \
+        offset, data, N, stride, x, y);                                                      \
+    return;
+      SB_DIA_MR(1, 4) SB_DIA_MR(2, 4) SB_DIA_MR(3, 4) SB_DIA_MR(4, 4) SB_DIA_MR(5, 2)
+      SB_DIA_MR(6, 2) SB_DIA_MR(7, 2) SB_DIA_MR(8, 2)
+#undef SB_DIA_MR
+      default: break;
+    }
+    }
+  }
   switch (nd) {
 #define SB_DIA_ND(n) \
   case n: dia_rows_nd<SV, T, n><<<blocks, 256, 0, st>>>(offset, data, N, stride, x, y); return;
