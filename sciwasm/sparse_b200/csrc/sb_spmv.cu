@@ -467,7 +467,7 @@ static int launch_csr_rows(const int* row_ptr, const int* col, const SV* val, co
 // reply); rows strictly inside a lane and the rows of the tile's first and
 // last entries, which other tiles may share, keep the atomic.
 template <typename S, typename A, bool VEC, bool SORTED>
-__global__ void __launch_bounds__(kWarpsPerCta * kWarp)
+__global__ void __launch_bounds__(kWarpsPerCta * kWarp, 5)
     coo_tile_kernel(const int* __restrict__ row, const int* __restrict__ col,
                     const S* __restrict__ val, const S* __restrict__ x, S* __restrict__ y,
                     long long nnz, long long ntiles, long long tiles_per_warp) {
@@ -812,7 +812,7 @@ static int launch_csr_tiles(const int* row_ptr, const int* col, const SV* val, c
 // without entries are not written).  The summation order is fixed by the
 // matrix, so results are identical run to run.
 template <typename SV, typename T, bool VEC>
-__global__ void __launch_bounds__(kWarpsPerCta * kWarp)
+__global__ void __launch_bounds__(kWarpsPerCta * kWarp, 5)
     csr_block_stream_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
                             const SV* __restrict__ val, const T* __restrict__ x,
                             T* __restrict__ y, int N, long long nnz) {

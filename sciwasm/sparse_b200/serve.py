@@ -483,6 +483,13 @@ class Server:
         for key, jobs in groups.items():
             if slot.kind == "spmv":
                 slot.executor(key).run(jobs, stream=slot.stream, overwrite=True)
+            elif len(jobs) == 1:
+                # one solve: the single hybrid solve, whose launch suits one
+                # system (the batch kernel gives the same bits)
+                plan, xd, yd = jobs[0]
+                pol = _lib.SB_SPTS_ACC_F64 if key[1] == "f64" else _lib.SB_SPTS_ACC_NATIVE
+                call("sb_spts_solve", plan.ptr, _lib.SB_SPTS_HYBRID, pol, xd.ptr, yd.ptr,
+                     slot.stream)
             else:
                 slot.executor(key).run(jobs, stream=slot.stream)
         d2h = [(r.y.ctypes.data, base + o, _vec_bytes(m, r)) for m, r, o in zip(mats, reqs, yo)]

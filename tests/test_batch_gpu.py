@@ -147,8 +147,10 @@ def test_batch_mixed_formats(gpu, oracle, storage):
             else:
                 want = oracle.spmv_ell(M.indices_array(), M.data_array(), N, M.ncols,
                                        np.ascontiguousarray(X[:, j]), Y0[:, j])
-            assert np.array_equal(Y[:, j].view(np.uint8), want.view(np.uint8)), (fmt, k, j)
+            assert np.array_equal(np.ascontiguousarray(Y[:, j]).view(np.uint8),
+                                  want.view(np.uint8)), (fmt, k, j)
         if k == 1:
             xv, yv = gpu.vec_from_host(X[:, 0]), gpu.vec_from_host(Y0[:, 0])
             gpu.spmv(M, xv, yv)
-            assert np.array_equal(yv.array().view(np.uint8), Y[:, 0].view(np.uint8)), fmt
+            assert np.array_equal(yv.array().view(np.uint8),
+                                  np.ascontiguousarray(Y[:, 0]).view(np.uint8)), fmt
