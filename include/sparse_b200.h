@@ -432,6 +432,12 @@ int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch*
 int sb_spts_batch_destroy(sb_spts_batch* e);
 int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t n,
                       void* stream);
+/* Launch shape of later runs: blocks_per_sm 0 (the default) launches one warp
+ * per 32-row chunk, resident blocks capped by the batch size; > 0 launches at
+ * most that many blocks per SM (and no more than fit), whose warps take
+ * chunks until the batch is done, so that a run leaves SMs to work on other
+ * streams (for instance a second executor's run). */
+int sb_spts_batch_set_grid(sb_spts_batch* e, int32_t blocks_per_sm);
 
 /* ---------------------------------------------------------------------- */
 /* Reductions over a row-sorted COO (rows non-decreasing, as the           */

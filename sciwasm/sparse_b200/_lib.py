@@ -153,6 +153,7 @@ SIGNATURES.update({
     "sb_spts_batch_create": [C.c_int, C.c_int, I32, C.POINTER(P)],
     "sb_spts_batch_destroy": [P],
     "sb_spts_batch_run": [P, C.POINTER(SptsBatchItem), I32, P],
+    "sb_spts_batch_set_grid": [P, I32],
     "sb_batch_exec_create": [C.c_int, I32, C.POINTER(P)],
     "sb_batch_exec_destroy": [P],
     "sb_batch_exec_run": [P, C.POINTER(BatchItem), I32, P],

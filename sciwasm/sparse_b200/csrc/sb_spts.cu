@@ -665,22 +665,21 @@ __global__ void spts_batch_reset(const SptsDesc* __restrict__ items,
   }
 }
 
+// The chunk of warp slot gw of the round layout: its system from the
+// segment table, the chunk itself from the system's ticket (claimed in level
+// order by a running warp), then one row per lane as in spts_hybrid_rows.
 template <typename T, typename A>
-__global__ void __launch_bounds__(kTB)
-    spts_batch_kernel(const SptsDesc* __restrict__ items, const SptsSched* __restrict__ sched,
-                      const int* __restrict__ order, const long long* __restrict__ seg,
-                      int* __restrict__ tickets, long long limit, int* status) {
-  const int lane = threadIdx.x & 31;
-  const int M = sched->M;
-  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (M <= 0 || gw >= sched->warps) return;
+__device__ __forceinline__ void batch_chunk(const SptsDesc* __restrict__ items,
+                                            const int* __restrict__ order,
+                                            const long long* __restrict__ seg,
+                                            int* __restrict__ tickets, int M, long long gw,
+                                            int lane, long long limit, int* status) {
   int lo = 0, hi = M - 1;  // last segment starting at or before gw
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (seg[mid] <= gw) lo = mid; else hi = mid - 1;
   }
   const int sys = order[lo + (int)((gw - seg[lo]) % (M - lo))];
-  // the chunk itself comes from the system's ticket, in the order warps run
   int t = 0;
   if (lane == 0) t = atomicAdd(tickets + sys, 1);
   t = __shfl_sync(0xffffffffu, t, 0);
@@ -701,6 +700,37 @@ __global__ void __launch_bounds__(kTB)
   }
   st_relaxed(yw + i, settled(yi));
   ((T*)d.y)[pi] = yi;
+}
+
+// persistent == 0: one warp per warp slot (the grid covers the layout).
+// persistent != 0: a capped grid whose warps take warp slots from *work
+// until the layout is done, so that the launch leaves SMs to other work (a
+// concurrent batch on another stream).  Either way a chunk is claimed only
+// by a running warp, and a row waits only on rows of its own system claimed
+// earlier, so the launch always makes progress.
+template <typename T, typename A>
+__global__ void __launch_bounds__(kTB)
+    spts_batch_kernel(const SptsDesc* __restrict__ items, const SptsSched* __restrict__ sched,
+                      const int* __restrict__ order, const long long* __restrict__ seg,
+                      int* __restrict__ tickets, long long limit, int* status,
+                      unsigned long long* __restrict__ work, int persistent) {
+  const int lane = threadIdx.x & 31;
+  const int M = sched->M;
+  const long long warps = sched->warps;
+  if (M <= 0) return;
+  if (!persistent) {
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (gw < warps) batch_chunk<T, A>(items, order, seg, tickets, M, gw, lane, limit, status);
+    return;
+  }
+  while (true) {
+    unsigned long long w = 0;
+    if (lane == 0) w = atomicAdd(work, 1ull);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if ((long long)w >= warps) return;
+    batch_chunk<T, A>(items, order, seg, tickets, M, (long long)w, lane, limit, status);
+    __syncwarp();
+  }
 }
 
 // max over rows of sum_{j < diag} |L_ij| / |L_ii| (inf for a zero diagonal),
@@ -1040,11 +1070,13 @@ struct sb_spts_batch {
   int* d_order = nullptr;
   long long* d_seg = nullptr;
   int* d_tickets = nullptr;      // one chunk counter per item
+  unsigned long long* d_work = nullptr;  // warp-slot counter of the capped grid
+  int persistent = 0;            // capped grid: blocks per SM (0 = one warp per slot)
   cudaGraph_t graph_def = nullptr;
   cudaGraphExec_t graph = nullptr;
   cudaGraphNode_t solve_node = nullptr;
   cudaKernelNodeParams solve_params = {};
-  void* solve_args[7] = {};
+  void* solve_args[9] = {};
   long long limit = 0;
   int* status = nullptr;
   cudaStream_t capture_stream = nullptr;
@@ -1064,7 +1096,7 @@ static void spts_batch_release(sb_spts_batch* e) {
   for (void* h : {(void*)e->h_items, (void*)e->h_sched, (void*)e->h_order, (void*)e->h_seg})
     if (h) cudaFreeHost(h);
   for (void* d : {(void*)e->d_items, (void*)e->d_sched, (void*)e->d_order, (void*)e->d_seg,
-                  (void*)e->d_tickets})
+                  (void*)e->d_tickets, (void*)e->d_work})
     if (d) cudaFree(d);
   delete e;
 }
@@ -1137,6 +1169,7 @@ int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch*
   SB_E(cudaMalloc(&e->d_order, sizeof(int) * capacity));
   SB_E(cudaMalloc(&e->d_seg, sizeof(long long) * (capacity + 1)));
   SB_E(cudaMalloc(&e->d_tickets, sizeof(int) * capacity));
+  SB_E(cudaMalloc(&e->d_work, sizeof(unsigned long long)));
   SB_E(cudaStreamCreateWithFlags(&e->capture_stream, cudaStreamNonBlocking));
   SB_E(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming));
   e->h_sched->M = 0;
@@ -1153,6 +1186,7 @@ int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch*
   cudaMemcpyAsync(e->d_seg, e->h_seg, sizeof(long long) * (capacity + 1), cudaMemcpyHostToDevice,
                   cs);
   cudaMemsetAsync(e->d_tickets, 0, sizeof(int) * capacity, cs);
+  cudaMemsetAsync(e->d_work, 0, sizeof(unsigned long long), cs);
   {
     const void* reset = dtype == SB_F64 ? (const void*)spts_batch_reset<double>
                                         : (const void*)spts_batch_reset<float>;
@@ -1166,6 +1200,8 @@ int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch*
   e->solve_args[4] = (void*)&e->d_tickets;
   e->solve_args[5] = (void*)&e->limit;
   e->solve_args[6] = (void*)&e->status;
+  e->solve_args[7] = (void*)&e->d_work;
+  e->solve_args[8] = (void*)&e->persistent;
   const void* kern = spts_batch_kernel_for(dtype, e->policy);
   cudaLaunchKernel(kern, dim3(1), dim3(kTB), e->solve_args, 0, cs);
   SB_E(cudaStreamEndCapture(cs, &e->graph_def));
@@ -1207,6 +1243,14 @@ int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch*
   SB_E(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, e->smem_optin));
 #undef SB_E
   *out = e;
+  return SB_OK;
+}
+
+int sb_spts_batch_set_grid(sb_spts_batch* e, int32_t blocks_per_sm) {
+  SB_REQUIRE(e, "sb_spts_batch_set_grid: null executor");
+  SB_REQUIRE(blocks_per_sm >= 0, "sb_spts_batch_set_grid: negative block count");
+  if (e->pending) SB_CHECK_CUDA(cudaEventSynchronize(e->done));
+  e->persistent = blocks_per_sm;
   return SB_OK;
 }
 
@@ -1274,7 +1318,9 @@ int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t
   e->h_sched->M = n;
   e->h_sched->warps = warps;
   const long long per_block = kTB / 32;
-  const long long blocks = std::max(1LL, (warps + per_block - 1) / per_block);
+  long long blocks = std::max(1LL, (warps + per_block - 1) / per_block);
+  if (e->persistent > 0)
+    blocks = std::min(blocks, (long long)std::min(e->persistent, e->full_per_sm) * sm_count());
   SB_REQUIRE(blocks <= 0x7fffffffLL, "sb_spts_batch_run: batch too large");
   e->solve_params.gridDim = dim3((unsigned)blocks);
   // Resident blocks per SM: one per 8 systems, up to the occupancy limit.
@@ -1287,7 +1333,7 @@ int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t
   // where the occupancy query confirms at least one block still fits.
   unsigned smem = 0;
   const int bps = std::min(e->full_per_sm, std::max(1, (n + 7) / 8));
-  if (bps < e->full_per_sm && e->smem_per_sm > 0) {
+  if (e->persistent == 0 && bps < e->full_per_sm && e->smem_per_sm > 0) {
     long long want = (long long)e->smem_per_sm / bps - e->smem_reserved;
     want = std::min<long long>(want, e->smem_optin) / 1024 * 1024;
     int fit = 0;

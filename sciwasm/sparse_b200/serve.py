@@ -369,8 +369,9 @@ class _Slot:
     """One stream with its device arena and executors; serves batches of one
     kind ("spmv" or "spts")."""
 
-    def __init__(self, index, kind, arena_bytes, max_batch, priority=None):
+    def __init__(self, index, kind, arena_bytes, max_batch, priority=None, spts_grid=0):
         self.index = index
+        self.spts_grid = spts_grid
         self.kind = kind
         self.stream = _stream(priority)
         self.ev_done = _Event()
@@ -390,7 +391,8 @@ class _Slot:
                 self.execs[key] = BatchExecutor(key, capacity=self.max_batch)
             else:
                 dtype, policy = key
-                self.execs[key] = SptsBatch(_STORAGE[dtype], policy, capacity=self.max_batch)
+                self.execs[key] = SptsBatch(_STORAGE[dtype], policy, capacity=self.max_batch,
+                                            blocks_per_sm=self.spts_grid)
         return self.execs[key]
 
     def close(self):
@@ -417,8 +419,10 @@ class Server:
 
     def __init__(self, pool: ResidentPool, max_batch: int = 64, slots: int = 4,
                  arena_bytes: Optional[int] = None, spts_slots: int = 1, spts_batch: int = 256,
-                 priorities: bool = True, spts_arena_bytes: Optional[int] = None):
+                 priorities: bool = True, spts_arena_bytes: Optional[int] = None,
+                 spts_grid: int = 0):
         self.pool = pool
+        self.spts_grid = int(spts_grid)  # SpTS launches: blocks per SM (0 = one warp per chunk)
         self.priorities = bool(priorities)
         self.max_batch = int(max_batch)
         self.nslots = int(slots)
@@ -549,7 +553,7 @@ class Server:
                 all_slots.append(spmv_slots[-1])
             for k in range(self.spts_slots):
                 spts_slots.append(_Slot(self.nslots + k, "spts", self.spts_arena_bytes,
-                                        self.spts_batch, least))
+                                        self.spts_batch, least, self.spts_grid))
                 all_slots.append(spts_slots[-1])
             kinds = {"spmv": (spmv_slots, collections.deque(), self.max_batch),
                      "spts": (spts_slots, collections.deque(), self.spts_batch)}

@@ -1052,7 +1052,9 @@ class SptsBatch:
     persistent launch; every result is bit-identical to
     spts(L, b, y, algo="hybrid", policy=policy)."""
 
-    def __init__(self, dtype=np.float32, policy="native", capacity=256):
+    def __init__(self, dtype=np.float32, policy="native", capacity=256, blocks_per_sm=0):
+        """blocks_per_sm > 0 caps the launch at that many blocks per SM, whose
+        warps take chunks until the batch is done (sb_spts_batch_set_grid)."""
         self.dtype = np.dtype(dtype)
         self.policy = policy
         self.capacity = int(capacity)
@@ -1060,6 +1062,8 @@ class SptsBatch:
         call("sb_spts_batch_create", _dtcode(self.dtype), _SPTS_POLICY[policy], self.capacity,
              C.byref(p))
         self.ptr = p.value
+        if blocks_per_sm:
+            call("sb_spts_batch_set_grid", self.ptr, int(blocks_per_sm))
         self._items = (_lib.SptsBatchItem * self.capacity)()
         self._keep = []
 

@@ -36,9 +36,10 @@ def _bits(a):
     return a.view(np.uint64 if a.dtype == np.float64 else np.uint32)
 
 
+@pytest.mark.parametrize("grid", [0, 1, 3])
 @pytest.mark.parametrize("dt,policy", [(np.float32, "native"), (np.float32, "f64"),
                                        (np.float64, "native")])
-def test_spts_batch_bit_identical_to_hybrid(gpu, oracle, dt, policy):
+def test_spts_batch_bit_identical_to_hybrid(gpu, oracle, dt, policy, grid):
     facs = _factors(dt)
     Ls = [gpu.csr_from_host(rp, col, val) for rp, col, val in facs]
     plans = [gpu.SptsPlan(L) for L in Ls]
@@ -51,7 +52,8 @@ def test_spts_batch_bit_identical_to_hybrid(gpu, oracle, dt, policy):
         yv = gpu.create_vec(L.N, 0, dt)
         gpu.spts(L, bv, yv, algo="hybrid", policy=policy)
         want.append(yv.array())
-    ex = gpu.SptsBatch(dt, policy, capacity=8)
+    # grid 0: one warp per chunk; 1 or 3: a capped grid whose warps loop
+    ex = gpu.SptsBatch(dt, policy, capacity=8, blocks_per_sm=grid)
     pol = _lib.SB_SPTS_ACC_F64 if policy == "f64" else _lib.SB_SPTS_ACC_NATIVE
     for rep in range(3):
         for y in ys:
