@@ -99,10 +99,10 @@ int sb_spmv_coo(int dtype, const int32_t* row, const int32_t* col, const void* v
 /* sb_spmv_coo with flags; no counterpart in the reference.  SB_COO_ROWS_SORTED
  * states that row[] is non-decreasing (as in the reference's COO objects,
  * which create_COO_from_MM leaves sorted by (row, col)): rows that lie wholly
- * inside one 256-entry tile are then stored without atomics, from y values
- * loaded while the x gathers are in flight.  The flag is the caller's
- * guarantee and is not checked: with unsorted rows the result is wrong.
- * flags = 0 is sb_spmv_coo. */
+ * inside one 256-entry tile are then added without atomics (taken when the
+ * mean row length is at most 16; longer rows keep the atomics, which cost
+ * less there).  The flag is the caller's guarantee and is not checked: with
+ * unsorted rows the result is wrong.  flags = 0 is sb_spmv_coo. */
 #define SB_COO_ROWS_SORTED 1
 int sb_spmv_coo_ex(int dtype, const int32_t* row, const int32_t* col, const void* val,
                    const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,

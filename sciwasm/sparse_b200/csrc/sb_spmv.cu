@@ -460,12 +460,8 @@ static int launch_csr_rows(const int* row_ptr, const int* col, const SV* val, co
 
 // SORTED: the caller guarantees non-decreasing rows.  A row that touches
 // neither end of a tile then has all its entries in that tile, so its sum
-// is stored with y[row] = y + sum, where y of the lane's first and last rows
-// was loaded while the x gathers were in flight (a plain read-modify-write
-// at the end waits for its read: power-law 2M rows, 20.5 entries per row,
-// 0.225 -> 0.232 ms against atomics, while the atomics are sent without a
-// reply); rows strictly inside a lane and the rows of the tile's first and
-// last entries, which other tiles may share, keep the atomic.
+// is added with a plain read-modify-write; only the rows of the tile's first
+// and last entries, which other tiles may share, keep the atomic.
 template <typename S, typename A, bool VEC, bool SORTED>
 __global__ void __launch_bounds__(kWarpsPerCta * kWarp)
     coo_tile_kernel(const int* __restrict__ row, const int* __restrict__ col,
@@ -522,20 +518,13 @@ __global__ void __launch_bounds__(kWarpsPerCta * kWarp)
     A acc = 0;
     bool internal = false;
     A first_val = 0;
-    // sorted rows: the y values of the lane's first and last rows, loaded
-    // while the x gathers are in flight, so that a row finished here is
-    // stored without waiting for a read (rows only this tile touches)
-    S y_first = 0, y_last = 0;
-    if (SORTED && cnt > 0) {
-      y_first = y[start_row];
-      y_last = y[r[cnt - 1]];
-    }
 #pragma unroll
     for (int e = 0; e < kItems; ++e) {
       if (e < cnt) {
         if (r[e] != cur) {
           if (!internal) { internal = true; first_val = acc; }
-          else atomicAdd(y + cur, (S)acc);  // strictly inside one lane: a whole row
+          else if (SORTED) y[cur] += (S)acc;  // strictly inside one lane: a whole row
+          else atomicAdd(y + cur, (S)acc);
           cur = r[e];
           acc = 0;
         }
@@ -566,7 +555,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * kWarp)
     A carry = __shfl_up_sync(kFull, S_, 1);
     if (internal) {
       A v = first_val + (cont_prev ? carry : (A)0);
-      if (SORTED && start_row != tile_first) y[start_row] = y_first + (S)v;
+      if (SORTED && start_row != tile_first) y[start_row] += (S)v;
       else atomicAdd(y + start_row, (S)v);
     }
     // tail run: emitted unless the next lane continues it
@@ -574,7 +563,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * kWarp)
     const int next_cnt = __shfl_down_sync(kFull, cnt, 1);
     const bool next_internal_or_diff = (lane == kWarp - 1) || next_cnt == 0 || next_start != end_row;
     if (cnt > 0 && next_internal_or_diff) {
-      if (SORTED && end_row != tile_first && end_row != tile_last) y[end_row] = y_last + (S)S_;
+      if (SORTED && end_row != tile_first && end_row != tile_last) y[end_row] += (S)S_;
       else atomicAdd(y + end_row, (S)S_);
     }
   }
@@ -1436,9 +1425,14 @@ int sb_spmv_coo_ex(int dtype, const int32_t* row, const int32_t* col, const void
   SB_REQUIRE(row && col && val && x && y, "sb_spmv_coo: null pointer");
   if ((r = ensure_device())) return r;
   cudaStream_t st = as_stream(stream);
-  // Sorted rows: rows finished inside a tile are stored without atomics,
-  // from y values loaded while the gathers are in flight.
-  const bool sorted = (flags & SB_COO_ROWS_SORTED) != 0;
+  // A plain add reads y and waits for it; an atomic add is sent without a
+  // reply.  Dropping the atomics pays where rows are short and many (banded,
+  // 11 per row: 0.163 -> 0.130 ms) and costs where they are long and few
+  // (power-law, 20.5 per row: 0.225 -> 0.232 ms), so the sorted-rows kernel
+  // is taken for a mean row length of at most 16.  (Loading y of the lane's
+  // rows while the gathers are in flight, then storing without a wait, was
+  // measured: banded 0.1356 ms, power-law no faster than the atomics.)
+  const bool sorted = (flags & SB_COO_ROWS_SORTED) != 0 && nnz <= 16LL * N;
   for (int it = 0; it < inner_max; ++it) {
     if (dtype == SB_F32)
       r = launch_coo<float, float>(row, col, (const float*)val, (const float*)x, (float*)y, nnz,
