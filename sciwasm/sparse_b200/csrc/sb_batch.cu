@@ -78,6 +78,64 @@ __device__ __forceinline__ void put_y(T* y, long long at, T sum, bool overwrite,
 // compensated f32 sums.
 constexpr int kLong = 128;
 
+// Rows of a block longer than kLong: the whole warp per row, one right-hand
+// side at a time, compensated f32 sums.
+template <typename SV, typename T>
+__device__ __forceinline__ void batch_long_rows(const sb_batch_item& it, int r0, int lane, int s_l,
+                                                int e_l, int len_l) {
+  constexpr int UNROLL = 4;
+  constexpr bool COMP = sizeof(T) == 4;
+  const int* __restrict__ col = it.col;
+  const SV* __restrict__ val = (const SV*)it.val;
+  const T* __restrict__ x = (const T*)it.x;
+  T* __restrict__ y = (T*)it.y;
+  const int K = it.nrhs;
+  const int N = it.N;
+  const bool overwrite = (it.flags & 1) != 0;
+  const int rr = r0 + lane;
+  unsigned longm = __ballot_sync(0xffffffffu, rr < N && len_l > kLong);
+  while (longm) {
+    const int j = __ffs(longm) - 1;
+    longm &= longm - 1;
+    const int s = __shfl_sync(0xffffffffu, s_l, j);
+    const int e = __shfl_sync(0xffffffffu, e_l, j);
+    for (int h = 0; h < K; ++h) {
+      T sum = 0, comp = 0;
+      for (int k0 = s; k0 < e; k0 += 32 * UNROLL) {
+        int cc[UNROLL];
+        T vv[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          const int k = k0 + lane + u * 32;
+          cc[u] = k < e ? ld_reuse(col + k) : 0;
+          vv[u] = k < e ? ldv(val, k) : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          const int k = k0 + lane + u * 32;
+          if (k < e) {
+            const T p = vv[u] * __ldg(x + (long long)cc[u] * K + h);
+            if (COMP) comp_add(sum, comp, p);
+            else sum += p;
+          }
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const T o = __shfl_xor_sync(0xffffffffu, sum, off);
+        if (COMP) {
+          comp += __shfl_xor_sync(0xffffffffu, comp, off);
+          comp_add(sum, comp, o);
+        } else {
+          sum += o;
+        }
+      }
+      if (lane == 0) put_y(y, (long long)(r0 + j) * K + h, COMP ? sum + comp : sum, overwrite, true);
+    }
+  }
+}
+
+
 template <typename SV, typename T, int V>
 __device__ __forceinline__ void batch_block(const sb_batch_item& it, int r0, int lane) {
   constexpr int UNROLL = 4;
@@ -137,47 +195,7 @@ __device__ __forceinline__ void batch_block(const sb_batch_item& it, int r0, int
       }
     }
   }
-  // long rows of the block: the whole warp, one right-hand side at a time
-  unsigned longm = __ballot_sync(0xffffffffu, rr < N && len_l > kLong);
-  while (longm) {
-    const int j = __ffs(longm) - 1;
-    longm &= longm - 1;
-    const int s = __shfl_sync(0xffffffffu, s_l, j);
-    const int e = __shfl_sync(0xffffffffu, e_l, j);
-    for (int h = 0; h < K; ++h) {
-      T sum = 0, comp = 0;
-      for (int k0 = s; k0 < e; k0 += 32 * UNROLL) {
-        int cc[UNROLL];
-        T vv[UNROLL];
-#pragma unroll
-        for (int u = 0; u < UNROLL; ++u) {
-          const int k = k0 + lane + u * 32;
-          cc[u] = k < e ? ld_reuse(col + k) : 0;
-          vv[u] = k < e ? ldv(val, k) : (T)0;
-        }
-#pragma unroll
-        for (int u = 0; u < UNROLL; ++u) {
-          const int k = k0 + lane + u * 32;
-          if (k < e) {
-            const T p = vv[u] * __ldg(x + (long long)cc[u] * K + h);
-            if (COMP) comp_add(sum, comp, p);
-            else sum += p;
-          }
-        }
-      }
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const T o = __shfl_xor_sync(0xffffffffu, sum, off);
-        if (COMP) {
-          comp += __shfl_xor_sync(0xffffffffu, comp, off);
-          comp_add(sum, comp, o);
-        } else {
-          sum += o;
-        }
-      }
-      if (lane == 0) put_y(y, (long long)(r0 + j) * K + h, COMP ? sum + comp : sum, overwrite, true);
-    }
-  }
+  batch_long_rows<SV, T>(it, r0, lane, s_l, e_l, len_l);
 }
 
 // Several right-hand sides (K = 2..8): one 32-row block, the right-hand
@@ -342,6 +360,83 @@ __device__ __forceinline__ void batch_block_lane_rows(const sb_batch_item& it, i
   for (int h = 0; h < K; ++h) put_y(y, (long long)i * K + h, acc[h], overwrite, e > s);
 }
 
+// Several right-hand sides (K = 2..8), V lanes per row (V = the item's lanes,
+// 2..16): the lanes of a row interleave over its entries, so that the col
+// and val loads stay coalesced as in batch_block; each lane keeps K partial
+// sums fed by vector loads of the K-value x rows (x 16-byte aligned), and one
+// shuffle reduction per right-hand side combines the V lanes.  Rows longer
+// than kLong go to the whole warp.
+template <typename SV, typename T, int V, int K>
+__device__ __forceinline__ void batch_block_vk(const sb_batch_item& it, int r0, int lane) {
+  constexpr int UNROLL = K <= 4 ? 4 : 2;
+  constexpr int RPB = 32 / V;
+  const int g = lane / V, q = lane - (lane / V) * V;
+  const int* __restrict__ rp = it.row_ptr;
+  const int* __restrict__ col = it.col;
+  const SV* __restrict__ val = (const SV*)it.val;
+  const T* __restrict__ x = (const T*)it.x;
+  T* __restrict__ y = (T*)it.y;
+  const int N = it.N;
+  const bool overwrite = (it.flags & 1) != 0;
+  const int rr = r0 + lane;
+  const int s_l = rr < N ? __ldg(rp + rr) : 0;
+  const int e_l = rr < N ? __ldg(rp + rr + 1) : 0;
+  const int len_l = e_l - s_l;
+#pragma unroll 1
+  for (int b = 0; b < V; ++b) {
+    const int j = b * RPB + g;
+    const int s = __shfl_sync(0xffffffffu, s_l, j);
+    const int e = __shfl_sync(0xffffffffu, e_l, j);
+    const int len = e - s;
+    T acc[K];
+#pragma unroll
+    for (int h = 0; h < K; ++h) acc[h] = 0;
+    if (len <= kLong) {
+      for (int k0 = s + q; k0 < e; k0 += V * UNROLL) {
+        int cc[UNROLL];
+        T vv[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          const int k = k0 + u * V;
+          cc[u] = k < e ? ld_reuse(col + k) : 0;
+          vv[u] = k < e ? ldv(val, k) : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          if (k0 + u * V < e) {
+            T xv[K];
+            load_xrow<T, K>(x + (long long)cc[u] * K, xv);
+#pragma unroll
+            for (int h = 0; h < K; ++h) acc[h] += vv[u] * xv[h];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < K; ++h) {
+      T a = acc[h];
+#pragma unroll
+      for (int off = V >> 1; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+      if (q == 0 && len <= kLong && r0 + j < N)
+        put_y(y, (long long)(r0 + j) * K + h, a, overwrite, len > 0);
+    }
+  }
+  batch_long_rows<SV, T>(it, r0, lane, s_l, e_l, len_l);
+}
+
+template <typename SV, typename T, int V>
+__device__ __forceinline__ void batch_block_vk_k(const sb_batch_item& it, int r0, int lane) {
+  switch (it.nrhs) {
+    case 2: batch_block_vk<SV, T, V, 2>(it, r0, lane); break;
+    case 3: batch_block_vk<SV, T, V, 3>(it, r0, lane); break;
+    case 4: batch_block_vk<SV, T, V, 4>(it, r0, lane); break;
+    case 5: batch_block_vk<SV, T, V, 5>(it, r0, lane); break;
+    case 6: batch_block_vk<SV, T, V, 6>(it, r0, lane); break;
+    case 7: batch_block_vk<SV, T, V, 7>(it, r0, lane); break;
+    default: batch_block_vk<SV, T, V, 8>(it, r0, lane); break;
+  }
+}
+
 template <typename T> __device__ __forceinline__ T bmul_rn(T a, T b);
 template <> __device__ __forceinline__ float bmul_rn(float a, float b) { return __fmul_rn(a, b); }
 template <> __device__ __forceinline__ double bmul_rn(double a, double b) { return __dmul_rn(a, b); }
@@ -432,6 +527,15 @@ __global__ void __launch_bounds__(kBT, 5)
       }
       if (it.format == SB_FMT_ELL) {
         batch_block_ell<SV, T>(it, r0, lane);
+        continue;
+      }
+      if (it.nrhs > 1 && (it.flags & kLaneRows) && it.lanes >= 2) {
+        switch (it.lanes) {
+          case 2: batch_block_vk_k<SV, T, 2>(it, r0, lane); break;
+          case 4: batch_block_vk_k<SV, T, 4>(it, r0, lane); break;
+          case 8: batch_block_vk_k<SV, T, 8>(it, r0, lane); break;
+          default: batch_block_vk_k<SV, T, 16>(it, r0, lane); break;
+        }
         continue;
       }
       if (it.nrhs > 1 && (it.flags & kLaneRows)) {
@@ -579,9 +683,9 @@ int sb_batch_exec_run(sb_batch_exec* e, const sb_batch_item* items, int32_t n, v
     if (it.format == SB_FMT_CSR) {
       SB_REQUIRE(it.N == 0 || (it.row_ptr && it.x && it.y && (it.nnz == 0 || (it.col && it.val))),
                  "sb_batch_exec_run: item %d: null pointer", i);
-      // several right-hand sides: one row per lane, whose x rows are loaded
-      // as 16-byte vectors, when x is 16-byte aligned (otherwise nrhs lanes
-      // per row); the two give the same bits
+      // several right-hand sides with x 16-byte aligned: x rows loaded as
+      // vectors, by one row per lane (lanes 1) or lanes per row (otherwise
+      // the right-hand sides go across lanes)
       it.flags &= ~kLaneRows;
       if (it.nrhs > 1 && (reinterpret_cast<uintptr_t>(it.x) & 15u) == 0) it.flags |= kLaneRows;
       if (it.lanes <= 0) it.lanes = lanes_for(it.nnz, it.N);

@@ -703,10 +703,11 @@ class BatchExecutor:
         self._items = (_lib.BatchItem * self.capacity)()
         self._keep = []
 
-    def run(self, jobs, stream=None, overwrite=False):
+    def run(self, jobs, stream=None, overwrite=False, lanes=0):
         """jobs: iterable of (A, x DeviceArray N*k, y DeviceArray N*k, k) with A
         a CSR, DIA (stride N) or ELL matrix; y += A x, or y = A x with
-        overwrite=True."""
+        overwrite=True.  lanes: lanes per CSR row for every item (0 = chosen
+        per matrix from its mean row length; see sb_batch_item)."""
         jobs = list(jobs)
         if len(jobs) > self.capacity:
             raise ValueError(f"{len(jobs)} items exceed the executor capacity {self.capacity}")
@@ -715,7 +716,7 @@ class BatchExecutor:
         for A, x, y, k in jobs:
             it = self._items[n]
             it.x, it.y = x.ptr, y.ptr
-            it.N, it.nrhs, it.lanes, it.nnz = A.N, int(k), 0, A.nnz
+            it.N, it.nrhs, it.lanes, it.nnz = A.N, int(k), int(lanes), A.nnz
             it.flags = 1 if overwrite else 0
             if isinstance(A, sparse_DIA_t):
                 if A.stride != A.N:
