@@ -1154,7 +1154,8 @@ def run_serving(args):
     reqs = serving_requests(pool, mv, ts, args.serve_rate, args.serve_seconds, in_ring,
                             out_ring)
     srv = serve.Server(pool, max_batch=args.serve_batch, slots=args.serve_slots,
-                       spts_slots=args.serve_spts_slots, spts_batch=args.serve_spts_batch)
+                       spts_slots=args.serve_spts_slots, spts_batch=args.serve_spts_batch,
+                       spts_grid=args.serve_spts_grid)
     # warm-up: executors, graphs and first-touch costs
     srv.serve([serve.Request(r.rid, 0.0, r.matrix, r.op, r.storage, r.x, r.y)
                for r in reqs[:200]], "batched")
@@ -1193,6 +1194,7 @@ def run_serving(args):
         "max_rel_err_vs_fp64": errs,
         "slots": {"spmv": args.serve_slots, "spts": args.serve_spts_slots},
         "max_batch": {"spmv": args.serve_batch, "spts": args.serve_spts_batch},
+        "spts_blocks_per_sm": args.serve_spts_grid,
         "timing": "host wall clock from each request's arrival to the host seeing its result",
     }
     pool.close()
@@ -1219,7 +1221,8 @@ def run_serving_sweep(args):
     xs *= 2
     xs -= 1
     srv = serve.Server(pool, max_batch=args.serve_batch, slots=args.serve_slots,
-                       spts_slots=args.serve_spts_slots, spts_batch=args.serve_spts_batch)
+                       spts_slots=args.serve_spts_slots, spts_batch=args.serve_spts_batch,
+                       spts_grid=args.serve_spts_grid)
     warm = serving_requests(pool, mv, ts, 2000.0, 0.2, in_ring, out_ring, seed=99)
     for mode in ("batched", "plain"):
         srv.serve([serve.Request(r.rid, 0.0, r.matrix, r.op, r.storage, r.x, r.y)
@@ -1251,6 +1254,9 @@ def run_serving_sweep(args):
            "pool_build_s": round(build_s, 2), "deepest_factor_levels": deepest,
            "formats": dict(collections_counter(pool.mats[n].format for n in mv)),
            "sweep_seconds": args.sweep_seconds, "plain_seconds": args.plain_seconds,
+           "server": {"spmv_slots": args.serve_slots, "spmv_batch": args.serve_batch,
+                      "spts_slots": args.serve_spts_slots, "spts_batch": args.serve_spts_batch,
+                      "spts_blocks_per_sm": args.serve_spts_grid},
            "sweep": sweep,
            "long_trace": {"rate": args.serve_rate, "seconds": args.serve_seconds,
                           "batched": pick(long_b)}}
@@ -1310,8 +1316,10 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=5.0)
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-batch", type=int, default=64)
-    ap.add_argument("--serve-spts-slots", type=int, default=1)
-    ap.add_argument("--serve-spts-batch", type=int, default=256)
+    ap.add_argument("--serve-spts-slots", type=int, default=3)
+    ap.add_argument("--serve-spts-batch", type=int, default=64)
+    ap.add_argument("--serve-spts-grid", type=int, default=1,
+                    help="SpTS launches: persistent blocks per SM (0 = one warp per chunk)")
     ap.add_argument("--serve-rates", default="1000,2000,3000,10000,20000",
                     help="serving_sweep: arrival rates (req/s)")
     ap.add_argument("--sweep-seconds", type=float, default=3.0,

@@ -235,7 +235,8 @@ int sb_spmv_ell(int dtype, const int32_t* indices, const void* data, int32_t N, 
  * must be 0.  The y ranges of
  * different items must not overlap (x may be shared).
  *   format SB_FMT_CSR (0): row_ptr[N+1], col[nnz], val[nnz]; lanes: lanes
- *     per row (1..32, power of two), 0 = chosen from nnz/N.  With nrhs >= 2
+ *     per row (1..32, power of two), 0 = chosen from nnz/N (from nnz/(2N)
+ *     with nrhs >= 2).  With nrhs >= 2
  *     and x 16-byte aligned, lanes 1 = one row per lane with the nrhs sums in
  *     registers, lanes >= 2 = that many lanes interleaved over a row, each
  *     with nrhs partial sums (x rows loaded as vectors in both); with x not

@@ -688,7 +688,10 @@ int sb_batch_exec_run(sb_batch_exec* e, const sb_batch_item* items, int32_t n, v
       // the right-hand sides go across lanes)
       it.flags &= ~kLaneRows;
       if (it.nrhs > 1 && (reinterpret_cast<uintptr_t>(it.x) & 15u) == 0) it.flags |= kLaneRows;
-      if (it.lanes <= 0) it.lanes = lanes_for(it.nnz, it.N);
+      // several right-hand sides: each lane does K multiply-adds per entry,
+      // so half the lanes of one (measured on 512 matrices of mean row
+      // length 12, K = 1..8: 2 lanes 1.77 ms, 4 lanes 1.83, row per lane 1.90)
+      if (it.lanes <= 0) it.lanes = lanes_for(it.nrhs > 1 ? it.nnz / 2 : it.nnz, it.N);
       it.lanes = it.lanes > 32 ? 32 : it.lanes;
     } else {
       SB_REQUIRE(it.width >= 0, "sb_batch_exec_run: item %d: negative width", i);
