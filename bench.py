@@ -995,6 +995,29 @@ def run_batched(stream, peak, n_mats=512, seed=5):
                         "per_call_launches": int(ks.sum()),
                         "max_rel_err_vs_fp64": err, "error_sample_matrices": len(sample)}
         ex.close()
+    # the batch's gather floor: one sb_gather_dot over all matrices' col/val
+    # (FP32 values) with the columns offset into one concatenated x -- the
+    # streams and one x gather per nonzero, no rows, one right-hand side
+    from sciwasm.sparse_b200.sparse import DeviceArray
+    offs = np.concatenate([[0], np.cumsum(Ns)[:-1]])
+    cat_col = torch.cat([A._torch[1] + int(o) for A, o in zip(mats, offs)])
+    cat_val = torch.cat([A._torch[2] for A in mats])
+    cat_x = torch.cat([xc[0] for xc in xcols])
+    dot = DeviceArray.from_host(np.zeros(1))
+
+    def floor_fn():
+        _lib.call("sb_gather_dot", _lib.SB_F32, cat_col.data_ptr(), cat_val.data_ptr(),
+                  cat_x.data_ptr(), nnz_tot, dot.ptr, sp)
+    for _ in range(3):
+        floor_fn()
+    floor = _time_each_ms(stream, floor_fn, 10)
+    out["gather_floor_ms"] = round(floor, 4)
+    out["gather_floor"] = ("sb_gather_dot over the concatenated col/val (FP32) with one "
+                           "x gather per nonzero from the concatenated x: no row structure, "
+                           "no y, one right-hand side -- a lower bound on the batch's time")
+    for storage in ("f32", "bf16"):
+        out[storage]["of_gather_floor"] = round(floor / out[storage]["ms"], 3)
+    del cat_col, cat_val, cat_x
     return out
 
 
@@ -1248,10 +1271,13 @@ def run_serving_sweep(args):
         print(json.dumps({"rate": rate, **sweep[f"{int(rate)}"]}), file=sys.stderr, flush=True)
     reqs = serving_requests(pool, mv, ts, args.serve_rate, args.serve_seconds, in_ring, out_ring)
     long_b = srv.serve(reqs, "batched")
-    deepest = max(pool.mats[n].plans["f32"].nlevels for n in ts)
+    deep = max(ts, key=lambda n: pool.mats[n].plans["f32"].nlevels)
+    deepest = pool.mats[deep].plans["f32"].nlevels
+    single = deepest_single_solve(pool, srv, deep, in_ring, out_ring)
     out = {"pool": f"{args.serve_pool} matrices, rows log-uniform in [1000, "
                    f"{args.serve_max_rows}], 70% SpMV / 30% SpTS requests",
            "pool_build_s": round(build_s, 2), "deepest_factor_levels": deepest,
+           "deepest_single_solve": single,
            "formats": dict(collections_counter(pool.mats[n].format for n in mv)),
            "sweep_seconds": args.sweep_seconds, "plain_seconds": args.plain_seconds,
            "server": {"spmv_slots": args.serve_slots, "spmv_batch": args.serve_batch,
@@ -1264,6 +1290,34 @@ def run_serving_sweep(args):
     in_ring.free()
     out_ring.free()
     return out
+
+
+def deepest_single_solve(pool, srv, name, in_ring, out_ring, reps=10):
+    """The pool's deepest factor solved alone: the device time of one hybrid
+    sb_spts_solve (CUDA events, mean of reps) and the per-call path's latency
+    for one request of it (copies in and out included, median of reps)."""
+    import torch
+    from sciwasm.sparse_b200 import _lib, serve
+    m = pool.get(name)
+    stream = torch.cuda.Stream()
+    x = torch.rand(m.N, device="cuda") * 2 - 1
+    y = torch.empty_like(x)
+    pol = _lib.SB_SPTS_ACC_F64 if m.policy["f32"] == "f64" else _lib.SB_SPTS_ACC_NATIVE
+
+    def fn():
+        _lib.call("sb_spts_solve", m.plans["f32"].ptr, _lib.SB_SPTS_HYBRID, pol, x.data_ptr(),
+                  y.data_ptr(), stream.cuda_stream)
+    for _ in range(3):
+        fn()
+    dev_ms = _time_each_ms(stream, fn, reps)
+    lat = []
+    for k in range(reps):
+        r = serve.Request(k, 0.0, name, "spts", "f32", in_ring.view(0, m.N, np.float32),
+                          out_ring.view(0, m.N, np.float32))
+        lat.append(srv.serve([r], "plain")["p50_ms"])
+    return {"matrix": name, "rows": m.N, "levels": pool.mats[name].plans["f32"].nlevels,
+            "accumulation": m.policy["f32"], "device_ms": round(dev_ms, 3),
+            "plain_request_ms": round(float(np.median(lat)), 3)}
 
 
 def collections_counter(it):

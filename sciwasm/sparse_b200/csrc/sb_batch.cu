@@ -18,6 +18,7 @@
 // in pinned host and device buffers; one run = the graph [copy descriptors,
 // reset the counter, kernel] launched on the caller's stream.
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "sb_common.cuh"
@@ -288,6 +289,69 @@ __device__ __forceinline__ void batch_block_rhs(const sb_batch_item& it, int r0,
   }
 }
 
+// The K-value x row at xr (x 16-byte aligned, xr = x + c*K) when K values are
+// not a whole number of aligned vectors (FP32 K = 3, 5, 6, 7): the aligned
+// 16-byte blocks that cover the row are loaded (one to three random gathers
+// instead of K, or of three float2), and the row is picked out of them by its
+// offset in the first block.  Every block holds bytes of the row, so none
+// starts before x; a row whose last block would run past x's end (the last
+// row or two) is loaded value by value instead, so that no byte outside x
+// is read.
+template <typename T, int K>
+__device__ __forceinline__ void load_xrow_blocks(const T* __restrict__ xr,
+                                                 const T* __restrict__ xend, T (&v)[K]) {
+  constexpr int E = 16 / (int)sizeof(T);        // values per 16-byte block
+  constexpr int NB = (K + 2 * E - 2) / E;       // blocks at the worst offset
+  using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(xr);
+  const int r = (int)((a & 15u) / sizeof(T));   // the row's offset in block 0
+  const T* blk = reinterpret_cast<const T*>(a & ~(uintptr_t)15);
+  const int nb = (r + K + E - 1) / E;
+  if (blk + nb * E > xend) {
+#pragma unroll
+    for (int h = 0; h < K; ++h) v[h] = __ldg(xr + h);
+    return;
+  }
+  T w[NB * E];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    if (b < nb) {
+      const V4 q = __ldg(reinterpret_cast<const V4*>(blk) + b);
+      if constexpr (sizeof(T) == 4) {
+        w[b * 4] = q.x; w[b * 4 + 1] = q.y; w[b * 4 + 2] = q.z; w[b * 4 + 3] = q.w;
+      } else {
+        w[b * 2] = q.x; w[b * 2 + 1] = q.y;
+      }
+    } else {
+#pragma unroll
+      for (int t = 0; t < E; ++t) w[b * E + t] = (T)0;
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < K; ++h) {
+    T t = w[h];
+#pragma unroll
+    for (int rr = 1; rr < E; ++rr)
+      if (r == rr) t = w[h + rr];
+    v[h] = t;
+  }
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void load_xrow(const T* __restrict__ xr, T (&v)[K]);
+
+// x row loader of the several-right-hand-side paths: aligned vectors when K
+// values are whole vectors, the covering blocks otherwise.
+template <typename T, int K>
+__device__ __forceinline__ void load_xrow_any(const T* __restrict__ xr, const T* __restrict__ xend,
+                                              T (&v)[K]) {
+  // FP64 keeps value-by-value loads for odd K: its covering blocks need
+  // more registers than the batch kernel's 48 (ptxas spilled)
+  constexpr bool whole = sizeof(T) == 4 ? (K % 4 == 0 || K <= 2) : true;
+  if constexpr (whole) load_xrow<T, K>(xr, v);
+  else load_xrow_blocks<T, K>(xr, xend, v);
+}
+
 // Several right-hand sides (K = 2..8), one row per lane (the path taken when
 // x is 16-byte aligned; measured on B200 on the 512-matrix batch, FP32 1.99 ->
 // 1.87 ms and BF16 2.15 -> 1.83 ms against K lanes per row, same bits): the 32
@@ -334,6 +398,7 @@ __device__ __forceinline__ void batch_block_lane_rows(const sb_batch_item& it, i
   const int* __restrict__ col = it.col;
   const SV* __restrict__ val = (const SV*)it.val;
   const T* __restrict__ x = (const T*)it.x;
+  const T* __restrict__ xend = x + (long long)it.N * K;
   T* __restrict__ y = (T*)it.y;
   T acc[K];
 #pragma unroll
@@ -350,7 +415,7 @@ __device__ __forceinline__ void batch_block_lane_rows(const sb_batch_item& it, i
     for (int u = 0; u < UNROLL; ++u) {
       if (k0 + u < e) {
         T xv[K];
-        load_xrow<T, K>(x + (long long)cc[u] * K, xv);
+        load_xrow_any<T, K>(x + (long long)cc[u] * K, xend, xv);
 #pragma unroll
         for (int h = 0; h < K; ++h) acc[h] += vv[u] * xv[h];
       }
@@ -375,6 +440,7 @@ __device__ __forceinline__ void batch_block_vk(const sb_batch_item& it, int r0, 
   const int* __restrict__ col = it.col;
   const SV* __restrict__ val = (const SV*)it.val;
   const T* __restrict__ x = (const T*)it.x;
+  const T* __restrict__ xend = x + (long long)it.N * K;
   T* __restrict__ y = (T*)it.y;
   const int N = it.N;
   const bool overwrite = (it.flags & 1) != 0;
@@ -405,7 +471,7 @@ __device__ __forceinline__ void batch_block_vk(const sb_batch_item& it, int r0, 
         for (int u = 0; u < UNROLL; ++u) {
           if (k0 + u * V < e) {
             T xv[K];
-            load_xrow<T, K>(x + (long long)cc[u] * K, xv);
+            load_xrow_any<T, K>(x + (long long)cc[u] * K, xend, xv);
 #pragma unroll
             for (int h = 0; h < K; ++h) acc[h] += vv[u] * xv[h];
           }
@@ -574,6 +640,19 @@ static const void* batch_kernel_for(int dtype) {
   return (const void*)batch_kernel<float, float>;
 }
 
+// Lanes per row of a several-right-hand-side item: each lane does K
+// multiply-adds per entry, so a lane takes about 6-12 entries of a row
+// (measured on 512 matrices of mean row length 13, K = 1..8: 2 lanes 1.77 ms,
+// 4 lanes 1.83, row per lane 1.90).
+static int lanes_for_rhs(long long nnz, int N) {
+  const double avg = N ? (double)nnz / N : 0.0;
+  if (avg <= 3) return 1;
+  if (avg <= 24) return 2;
+  if (avg <= 48) return 4;
+  if (avg <= 96) return 8;
+  return 16;
+}
+
 static int lanes_for(long long nnz, int N) {
   const double avg = N ? (double)nnz / N : 0.0;
   if (avg <= 3) return 1;
@@ -688,10 +767,8 @@ int sb_batch_exec_run(sb_batch_exec* e, const sb_batch_item* items, int32_t n, v
       // the right-hand sides go across lanes)
       it.flags &= ~kLaneRows;
       if (it.nrhs > 1 && (reinterpret_cast<uintptr_t>(it.x) & 15u) == 0) it.flags |= kLaneRows;
-      // several right-hand sides: each lane does K multiply-adds per entry,
-      // so half the lanes of one (measured on 512 matrices of mean row
-      // length 12, K = 1..8: 2 lanes 1.77 ms, 4 lanes 1.83, row per lane 1.90)
-      if (it.lanes <= 0) it.lanes = lanes_for(it.nrhs > 1 ? it.nnz / 2 : it.nnz, it.N);
+      if (it.lanes <= 0)
+        it.lanes = it.nrhs > 1 ? lanes_for_rhs(it.nnz, it.N) : lanes_for(it.nnz, it.N);
       it.lanes = it.lanes > 32 ? 32 : it.lanes;
     } else {
       SB_REQUIRE(it.width >= 0, "sb_batch_exec_run: item %d: negative width", i);
