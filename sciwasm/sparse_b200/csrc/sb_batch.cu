@@ -46,6 +46,7 @@ constexpr int kBT = 256;
 constexpr int kMaxRhs = 8;
 constexpr int kBlocksPerTicket = 4;  // 32-row blocks a warp takes per work-counter update
 constexpr int kLaneRows = 1 << 30;   // internal item flag: one row per lane (set by the run)
+constexpr int kX32 = 1 << 29;        // internal item flag: x 32-byte aligned (set by the run)
 
 __device__ __forceinline__ float ldv(const float* p, long long i) { return ld_reuse(p + i); }
 __device__ __forceinline__ double ldv(const double* p, long long i) { return ld_reuse(p + i); }
@@ -337,18 +338,35 @@ __device__ __forceinline__ void load_xrow_blocks(const T* __restrict__ xr,
   }
 }
 
+// Eight FP32 values from a 32-byte aligned address: one 256-bit load
+// (sm_100), i.e. one gather request where two 16-byte loads took two.
+__device__ __forceinline__ void ld_v8(const float* __restrict__ p, float* w) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(w[0]), "=f"(w[1]), "=f"(w[2]), "=f"(w[3]), "=f"(w[4]), "=f"(w[5]), "=f"(w[6]),
+        "=f"(w[7])
+      : "l"(p));
+}
+
 template <typename T, int K>
 __device__ __forceinline__ void load_xrow(const T* __restrict__ xr, T (&v)[K]);
 
-// x row loader of the several-right-hand-side paths: aligned vectors when K
-// values are whole vectors, the covering blocks otherwise.
-template <typename T, int K>
+// x row loader of the several-right-hand-side paths: with x 32-byte aligned
+// (X32) an FP32 row of 8 values is one 256-bit load; otherwise aligned
+// vectors when K values are whole vectors, the covering 16-byte blocks when
+// not.  Measured on B200 (512-matrix batch, ns per 1000 nonzeros): K = 8
+// 10.2 -> 9.3 with the 256-bit load.  The same 32-byte blocks for K = 3, 5,
+// 6, 7 (1.25-1.75 loads per row instead of 1.5-2.5 16-byte ones) were
+// slower (K = 7: 10.7 -> 11.4): a random gather costs by the bytes it
+// returns, and the second block plus the pick by offset outweighed the
+// fewer requests.
+template <typename T, int K, bool X32>
 __device__ __forceinline__ void load_xrow_any(const T* __restrict__ xr, const T* __restrict__ xend,
                                               T (&v)[K]) {
   // FP64 keeps value-by-value loads for odd K: its covering blocks need
   // more registers than the batch kernel's 48 (ptxas spilled)
   constexpr bool whole = sizeof(T) == 4 ? (K % 4 == 0 || K <= 2) : true;
-  if constexpr (whole) load_xrow<T, K>(xr, v);
+  if constexpr (X32 && sizeof(T) == 4 && K == 8) ld_v8(xr, v);
+  else if constexpr (whole) load_xrow<T, K>(xr, v);
   else load_xrow_blocks<T, K>(xr, xend, v);
 }
 
@@ -387,7 +405,7 @@ __device__ __forceinline__ void load_xrow(const T* __restrict__ xr, T (&v)[K]) {
   }
 }
 
-template <typename SV, typename T, int K>
+template <typename SV, typename T, int K, bool X32>
 __device__ __forceinline__ void batch_block_lane_rows(const sb_batch_item& it, int r0, int lane) {
   constexpr int UNROLL = 4;
   const int i = r0 + lane;
@@ -415,7 +433,7 @@ __device__ __forceinline__ void batch_block_lane_rows(const sb_batch_item& it, i
     for (int u = 0; u < UNROLL; ++u) {
       if (k0 + u < e) {
         T xv[K];
-        load_xrow_any<T, K>(x + (long long)cc[u] * K, xend, xv);
+        load_xrow_any<T, K, X32>(x + (long long)cc[u] * K, xend, xv);
 #pragma unroll
         for (int h = 0; h < K; ++h) acc[h] += vv[u] * xv[h];
       }
@@ -431,7 +449,7 @@ __device__ __forceinline__ void batch_block_lane_rows(const sb_batch_item& it, i
 // sums fed by vector loads of the K-value x rows (x 16-byte aligned), and one
 // shuffle reduction per right-hand side combines the V lanes.  Rows longer
 // than kLong go to the whole warp.
-template <typename SV, typename T, int V, int K>
+template <typename SV, typename T, int V, int K, bool X32>
 __device__ __forceinline__ void batch_block_vk(const sb_batch_item& it, int r0, int lane) {
   constexpr int UNROLL = K <= 4 ? 4 : 2;
   constexpr int RPB = 32 / V;
@@ -471,7 +489,7 @@ __device__ __forceinline__ void batch_block_vk(const sb_batch_item& it, int r0, 
         for (int u = 0; u < UNROLL; ++u) {
           if (k0 + u * V < e) {
             T xv[K];
-            load_xrow_any<T, K>(x + (long long)cc[u] * K, xend, xv);
+            load_xrow_any<T, K, X32>(x + (long long)cc[u] * K, xend, xv);
 #pragma unroll
             for (int h = 0; h < K; ++h) acc[h] += vv[u] * xv[h];
           }
@@ -490,16 +508,36 @@ __device__ __forceinline__ void batch_block_vk(const sb_batch_item& it, int r0, 
   batch_long_rows<SV, T>(it, r0, lane, s_l, e_l, len_l);
 }
 
+// K = 8 with x 32-byte aligned: FP32 x rows as one 256-bit load
 template <typename SV, typename T, int V>
 __device__ __forceinline__ void batch_block_vk_k(const sb_batch_item& it, int r0, int lane) {
   switch (it.nrhs) {
-    case 2: batch_block_vk<SV, T, V, 2>(it, r0, lane); break;
-    case 3: batch_block_vk<SV, T, V, 3>(it, r0, lane); break;
-    case 4: batch_block_vk<SV, T, V, 4>(it, r0, lane); break;
-    case 5: batch_block_vk<SV, T, V, 5>(it, r0, lane); break;
-    case 6: batch_block_vk<SV, T, V, 6>(it, r0, lane); break;
-    case 7: batch_block_vk<SV, T, V, 7>(it, r0, lane); break;
-    default: batch_block_vk<SV, T, V, 8>(it, r0, lane); break;
+    case 2: batch_block_vk<SV, T, V, 2, false>(it, r0, lane); break;
+    case 3: batch_block_vk<SV, T, V, 3, false>(it, r0, lane); break;
+    case 4: batch_block_vk<SV, T, V, 4, false>(it, r0, lane); break;
+    case 5: batch_block_vk<SV, T, V, 5, false>(it, r0, lane); break;
+    case 6: batch_block_vk<SV, T, V, 6, false>(it, r0, lane); break;
+    case 7: batch_block_vk<SV, T, V, 7, false>(it, r0, lane); break;
+    default:
+      if (sizeof(T) == 4 && (it.flags & kX32)) batch_block_vk<SV, T, V, 8, true>(it, r0, lane);
+      else batch_block_vk<SV, T, V, 8, false>(it, r0, lane);
+      break;
+  }
+}
+
+template <typename SV, typename T>
+__device__ __forceinline__ void batch_block_lane_rows_k(const sb_batch_item& it, int r0, int lane) {
+  switch (it.nrhs) {
+    case 2: batch_block_lane_rows<SV, T, 2, false>(it, r0, lane); break;
+    case 3: batch_block_lane_rows<SV, T, 3, false>(it, r0, lane); break;
+    case 4: batch_block_lane_rows<SV, T, 4, false>(it, r0, lane); break;
+    case 5: batch_block_lane_rows<SV, T, 5, false>(it, r0, lane); break;
+    case 6: batch_block_lane_rows<SV, T, 6, false>(it, r0, lane); break;
+    case 7: batch_block_lane_rows<SV, T, 7, false>(it, r0, lane); break;
+    default:
+      if (sizeof(T) == 4 && (it.flags & kX32)) batch_block_lane_rows<SV, T, 8, true>(it, r0, lane);
+      else batch_block_lane_rows<SV, T, 8, false>(it, r0, lane);
+      break;
   }
 }
 
@@ -605,15 +643,7 @@ __global__ void __launch_bounds__(kBT, 5)
         continue;
       }
       if (it.nrhs > 1 && (it.flags & kLaneRows)) {
-        switch (it.nrhs) {
-          case 2: batch_block_lane_rows<SV, T, 2>(it, r0, lane); break;
-          case 3: batch_block_lane_rows<SV, T, 3>(it, r0, lane); break;
-          case 4: batch_block_lane_rows<SV, T, 4>(it, r0, lane); break;
-          case 5: batch_block_lane_rows<SV, T, 5>(it, r0, lane); break;
-          case 6: batch_block_lane_rows<SV, T, 6>(it, r0, lane); break;
-          case 7: batch_block_lane_rows<SV, T, 7>(it, r0, lane); break;
-          default: batch_block_lane_rows<SV, T, 8>(it, r0, lane); break;
-        }
+        batch_block_lane_rows_k<SV, T>(it, r0, lane);
         continue;
       }
       if (it.nrhs > 1) {
@@ -765,8 +795,9 @@ int sb_batch_exec_run(sb_batch_exec* e, const sb_batch_item* items, int32_t n, v
       // several right-hand sides with x 16-byte aligned: x rows loaded as
       // vectors, by one row per lane (lanes 1) or lanes per row (otherwise
       // the right-hand sides go across lanes)
-      it.flags &= ~kLaneRows;
+      it.flags &= ~(kLaneRows | kX32);
       if (it.nrhs > 1 && (reinterpret_cast<uintptr_t>(it.x) & 15u) == 0) it.flags |= kLaneRows;
+      if (it.nrhs == 8 && (reinterpret_cast<uintptr_t>(it.x) & 31u) == 0) it.flags |= kX32;
       if (it.lanes <= 0)
         it.lanes = it.nrhs > 1 ? lanes_for_rhs(it.nnz, it.N) : lanes_for(it.nnz, it.N);
       it.lanes = it.lanes > 32 ? 32 : it.lanes;

@@ -27,12 +27,15 @@ def _batch(seed, count, dt):
     return out
 
 
-@pytest.mark.parametrize("x_aligned", [True, False])
+@pytest.mark.parametrize("x_shift", ["none", "16B", "value"])
 @pytest.mark.parametrize("storage,dt", [("f32", np.float32), ("f64", np.float64),
                                         ("bf16", np.float32)])
-def test_batch_matches_per_matrix(gpu, oracle, storage, dt, x_aligned):
-    """x 16-byte aligned: several right-hand sides take one row per lane;
-    x one value off (not 16-byte aligned): nrhs lanes per row."""
+@pytest.mark.parametrize("lanes", [0, 1, 4])
+def test_batch_matches_per_matrix(gpu, oracle, storage, dt, x_shift, lanes):
+    """x 32-byte aligned: several right-hand sides load FP32 x rows in 32-byte
+    blocks; 16 bytes off: 16-byte vectors or blocks; one value off (not
+    16-byte aligned): nrhs lanes per row.  lanes 0 = the executor's choice,
+    1 = one row per lane, 4 = four lanes interleaved over a row."""
     mats = _batch(7, 40, np.float64 if storage == "f64" else np.float32)
     ex = gpu.BatchExecutor(storage, capacity=64)
     jobs, host, keep = [], [], []
@@ -44,17 +47,19 @@ def test_batch_matches_per_matrix(gpu, oracle, storage, dt, x_aligned):
         vdt = np.float64 if storage == "f64" else np.float32
         X = synth.uniform_vec(N * k, idx, dtype=vdt).reshape(N, k)
         Y0 = synth.uniform_vec(N * k, 1000 + idx, dtype=vdt).reshape(N, k)
-        if x_aligned:
+        if x_shift == "none":
             xd = gpu.DeviceArray.from_host(X.ravel())
+            assert xd.ptr % 32 == 0
         else:
-            base = gpu.DeviceArray.from_host(np.concatenate([[0], X.ravel()]).astype(vdt))
-            xd = gpu.DeviceArray(N * k, vdt, base.ptr + np.dtype(vdt).itemsize)
+            pad = (16 if x_shift == "16B" else np.dtype(vdt).itemsize) // np.dtype(vdt).itemsize
+            base = gpu.DeviceArray.from_host(np.concatenate([np.zeros(pad), X.ravel()]).astype(vdt))
+            xd = gpu.DeviceArray(N * k, vdt, base.ptr + pad * np.dtype(vdt).itemsize)
             keep.append(base)  # the buffer must outlive the runs
         yd = gpu.DeviceArray.from_host(Y0.ravel())
         jobs.append((A, xd, yd, k))
         host.append((rp, col, val, X, Y0, A))
     for rep in range(2):  # graph replay: second run accumulates again
-        ex.run(jobs)
+        ex.run(jobs, lanes=lanes)
         gpu.synchronize()
     tol = 1e-4 if storage == "bf16" else TOL[np.dtype(dt)]
     for (A, xd, yd, k), (rp, col, val, X, Y0, Ad) in zip(jobs, host):
