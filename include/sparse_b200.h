@@ -265,13 +265,16 @@ typedef struct sb_batch_item {
 typedef struct sb_batch_exec sb_batch_exec;
 
 /* An executor for batches of up to `capacity` matrices whose values are
- * stored as dtype (SB_F32, SB_F64 or SB_BF16 with f32 vectors).  It captures
- * one CUDA graph: descriptor upload, work-counter reset and the persistent
- * kernel over all 32-row blocks of the batch. */
+ * stored as dtype (SB_F32, SB_F64 or SB_BF16 with f32 vectors).  It holds two
+ * descriptor sets, each with a captured CUDA graph: descriptor upload,
+ * work-counter reset and the persistent kernel over all 32-row blocks of the
+ * batch.  Runs alternate between the sets. */
 int sb_batch_exec_create(int dtype, int32_t capacity, sb_batch_exec** exec);
 int sb_batch_exec_destroy(sb_batch_exec* exec);
-/* Launch the graph for items[0..n) on `stream` (stream-ordered; the call
- * waits only for the executor's previous run to have read its staging). */
+/* Launch the graph for items[0..n) on `stream` (stream-ordered).  The call
+ * waits only for the run before the previous one (the last user of this
+ * run's descriptor set), so a run can be staged while the previous one
+ * executes. */
 int sb_batch_exec_run(sb_batch_exec* exec, const sb_batch_item* items, int32_t n, void* stream);
 
 /* ---------------------------------------------------------------------- */

@@ -23,21 +23,29 @@
 
 #include "sb_common.cuh"
 
-struct sb_batch_exec {
-  int dtype = 0;
-  int capacity = 0;
-  int device = 0;
-  int grid = 0;
+// One of the executor's two descriptor sets: runs alternate between them, so
+// that a run does not wait for the previous one to finish before staging its
+// descriptors (only for the run before that, which used the same set).
+struct sb_batch_slot {
   sb_batch_item* h_items = nullptr;  // pinned
   long long* h_offsets = nullptr;    // pinned, capacity + 1
   int* h_count = nullptr;            // pinned: [0] = items in the current run
   sb_batch_item* d_items = nullptr;
   long long* d_offsets = nullptr;
-  int* d_count = nullptr;            // [0] items, [1] work counter
-  cudaGraphExec_t graph = nullptr;
-  cudaStream_t capture_stream = nullptr;
+  int* d_count = nullptr;            // [0] items, [2] work counter
+  cudaGraphExec_t graph = nullptr;   // [descriptors, offsets, count up; kernel]
   cudaEvent_t done = nullptr;
   bool pending = false;
+};
+
+struct sb_batch_exec {
+  int dtype = 0;
+  int capacity = 0;
+  int device = 0;
+  int grid = 0;
+  int next = 0;                      // the set the next run uses
+  sb_batch_slot slot[2];
+  cudaStream_t capture_stream = nullptr;
 };
 
 namespace sb {
@@ -694,15 +702,17 @@ static int lanes_for(long long nnz, int N) {
 }
 
 static void exec_release(sb_batch_exec* e) {
-  if (e->graph) cudaGraphExecDestroy(e->graph);
+  for (sb_batch_slot& b : e->slot) {
+    if (b.graph) cudaGraphExecDestroy(b.graph);
+    if (b.done) cudaEventDestroy(b.done);
+    if (b.h_items) cudaFreeHost(b.h_items);
+    if (b.h_offsets) cudaFreeHost(b.h_offsets);
+    if (b.h_count) cudaFreeHost(b.h_count);
+    if (b.d_items) cudaFree(b.d_items);
+    if (b.d_offsets) cudaFree(b.d_offsets);
+    if (b.d_count) cudaFree(b.d_count);
+  }
   if (e->capture_stream) cudaStreamDestroy(e->capture_stream);
-  if (e->done) cudaEventDestroy(e->done);
-  if (e->h_items) cudaFreeHost(e->h_items);
-  if (e->h_offsets) cudaFreeHost(e->h_offsets);
-  if (e->h_count) cudaFreeHost(e->h_count);
-  if (e->d_items) cudaFree(e->d_items);
-  if (e->d_offsets) cudaFree(e->d_offsets);
-  if (e->d_count) cudaFree(e->d_count);
   delete e;
 }
 
@@ -731,37 +741,39 @@ int sb_batch_exec_create(int dtype, int32_t capacity, sb_batch_exec** out) {
     exec_release(e);                              \
     return r;                                     \
   }
-  SB_E(cudaMallocHost(&e->h_items, sizeof(sb_batch_item) * capacity));
-  SB_E(cudaMallocHost(&e->h_offsets, sizeof(long long) * (capacity + 1)));
-  SB_E(cudaMallocHost(&e->h_count, sizeof(int) * 4));
-  SB_E(cudaMalloc(&e->d_items, sizeof(sb_batch_item) * capacity));
-  SB_E(cudaMalloc(&e->d_offsets, sizeof(long long) * (capacity + 1)));
-  SB_E(cudaMalloc(&e->d_count, sizeof(int) * 4));
   SB_E(cudaStreamCreateWithFlags(&e->capture_stream, cudaStreamNonBlocking));
-  SB_E(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming));
   const void* kern = batch_kernel_for(dtype);
   int per = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kBT, 0);
   e->grid = std::max(1, per) * sm_count();
-  // capture: descriptors + offsets + item count (host -> device), reset the
-  // work counter, persistent kernel
-  cudaGraph_t g = nullptr;
-  SB_E(cudaStreamBeginCapture(e->capture_stream, cudaStreamCaptureModeThreadLocal));
-  cudaMemcpyAsync(e->d_items, e->h_items, sizeof(sb_batch_item) * capacity,
-                  cudaMemcpyHostToDevice, e->capture_stream);
-  cudaMemcpyAsync(e->d_offsets, e->h_offsets, sizeof(long long) * (capacity + 1),
-                  cudaMemcpyHostToDevice, e->capture_stream);
-  cudaMemcpyAsync(e->d_count, e->h_count, sizeof(int) * 4, cudaMemcpyHostToDevice,
-                  e->capture_stream);
-  void* args[] = {(void*)&e->d_items, (void*)&e->d_offsets, (void*)&e->d_count};
-  cudaLaunchKernel(kern, dim3(e->grid), dim3(kBT), args, 0, e->capture_stream);
-  SB_E(cudaStreamEndCapture(e->capture_stream, &g));
-  ce = cudaGraphInstantiate(&e->graph, g, 0);
-  cudaGraphDestroy(g);
-  if (ce != cudaSuccess) {
-    r = cuda_status(ce, "cudaGraphInstantiate");
-    exec_release(e);
-    return r;
+  for (sb_batch_slot& b : e->slot) {
+    SB_E(cudaMallocHost(&b.h_items, sizeof(sb_batch_item) * capacity));
+    SB_E(cudaMallocHost(&b.h_offsets, sizeof(long long) * (capacity + 1)));
+    SB_E(cudaMallocHost(&b.h_count, sizeof(int) * 4));
+    SB_E(cudaMalloc(&b.d_items, sizeof(sb_batch_item) * capacity));
+    SB_E(cudaMalloc(&b.d_offsets, sizeof(long long) * (capacity + 1)));
+    SB_E(cudaMalloc(&b.d_count, sizeof(int) * 4));
+    SB_E(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+    // capture: descriptors + offsets + item count (host -> device, the
+    // count's copy also resets the work counter), persistent kernel
+    cudaGraph_t g = nullptr;
+    SB_E(cudaStreamBeginCapture(e->capture_stream, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(b.d_items, b.h_items, sizeof(sb_batch_item) * capacity,
+                    cudaMemcpyHostToDevice, e->capture_stream);
+    cudaMemcpyAsync(b.d_offsets, b.h_offsets, sizeof(long long) * (capacity + 1),
+                    cudaMemcpyHostToDevice, e->capture_stream);
+    cudaMemcpyAsync(b.d_count, b.h_count, sizeof(int) * 4, cudaMemcpyHostToDevice,
+                    e->capture_stream);
+    void* args[] = {(void*)&b.d_items, (void*)&b.d_offsets, (void*)&b.d_count};
+    cudaLaunchKernel(kern, dim3(e->grid), dim3(kBT), args, 0, e->capture_stream);
+    SB_E(cudaStreamEndCapture(e->capture_stream, &g));
+    ce = cudaGraphInstantiate(&b.graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      r = cuda_status(ce, "cudaGraphInstantiate");
+      exec_release(e);
+      return r;
+    }
   }
 #undef SB_E
   *out = e;
@@ -770,7 +782,8 @@ int sb_batch_exec_create(int dtype, int32_t capacity, sb_batch_exec** out) {
 
 int sb_batch_exec_destroy(sb_batch_exec* e) {
   if (!e) return SB_OK;
-  if (e->pending) cudaEventSynchronize(e->done);
+  for (sb_batch_slot& b : e->slot)
+    if (b.pending) cudaEventSynchronize(b.done);
   exec_release(e);
   return SB_OK;
 }
@@ -780,8 +793,11 @@ int sb_batch_exec_run(sb_batch_exec* e, const sb_batch_item* items, int32_t n, v
   SB_REQUIRE(n >= 0 && n <= e->capacity, "sb_batch_exec_run: %d items exceed capacity %d", n,
              e->capacity);
   SB_REQUIRE(n == 0 || items, "sb_batch_exec_run: null items");
-  // the pinned staging buffers are read by the previous run's first node
-  if (e->pending) SB_CHECK_CUDA(cudaEventSynchronize(e->done));
+  // this set's pinned staging buffers were read by the run before the
+  // previous one (its first nodes): wait for that run only
+  sb_batch_slot& b = e->slot[e->next];
+  if (b.pending) SB_CHECK_CUDA(cudaEventSynchronize(b.done));
+  b.pending = false;
   long long acc = 0;
   for (int i = 0; i < n; ++i) {
     sb_batch_item it = items[i];
@@ -809,19 +825,20 @@ int sb_batch_exec_run(sb_batch_exec* e, const sb_batch_item* items, int32_t n, v
                                                                  : it.col != nullptr)),
                  "sb_batch_exec_run: item %d: null pointer", i);
     }
-    e->h_items[i] = it;
-    e->h_offsets[i] = acc;
+    b.h_items[i] = it;
+    b.h_offsets[i] = acc;
     acc += ((long long)it.N + 31) / 32;
   }
-  e->h_offsets[n] = acc;
-  e->h_count[0] = n;
-  e->h_count[1] = 0;
-  e->h_count[2] = 0;
-  e->h_count[3] = 0;
+  b.h_offsets[n] = acc;
+  b.h_count[0] = n;
+  b.h_count[1] = 0;
+  b.h_count[2] = 0;
+  b.h_count[3] = 0;
   cudaStream_t st = as_stream(stream);
-  SB_CHECK_CUDA(cudaGraphLaunch(e->graph, st));
-  SB_CHECK_CUDA(cudaEventRecord(e->done, st));
-  e->pending = true;
+  SB_CHECK_CUDA(cudaGraphLaunch(b.graph, st));
+  SB_CHECK_CUDA(cudaEventRecord(b.done, st));
+  b.pending = true;
+  e->next ^= 1;
   return SB_OK;
 }
 

@@ -708,6 +708,13 @@ class BatchExecutor:
         a CSR, DIA (stride N) or ELL matrix; y += A x, or y = A x with
         overwrite=True.  lanes: lanes per CSR row for every item (0 = chosen
         per matrix from its mean row length; see sb_batch_item)."""
+        self.launch(self.prepare(jobs, overwrite, lanes), stream)
+
+    def prepare(self, jobs, overwrite=False, lanes=0) -> int:
+        """Fill the item descriptors for `jobs` (as run) without launching;
+        returns the item count for launch().  The descriptors stay valid until
+        the next prepare(), so a fixed batch is prepared once and launched
+        many times."""
         jobs = list(jobs)
         if len(jobs) > self.capacity:
             raise ValueError(f"{len(jobs)} items exceed the executor capacity {self.capacity}")
@@ -731,7 +738,11 @@ class BatchExecutor:
                 it.format, it.width = _lib.SB_FMT_CSR, 0
             self._keep.append((A, x, y))
             n += 1
-        call("sb_batch_exec_run", self.ptr, self._items, n, _sp(stream))
+        return n
+
+    def launch(self, n, stream=None):
+        """Run the batch that prepare() described (its first n items)."""
+        call("sb_batch_exec_run", self.ptr, self._items, int(n), _sp(stream))
 
     def close(self):
         if getattr(self, "ptr", None):

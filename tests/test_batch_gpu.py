@@ -99,6 +99,35 @@ def test_batch_same_result_alone_and_in_mix(gpu):
         assert np.array_equal(yd.to_host(), ymix.to_host())
 
 
+def test_batch_back_to_back_runs(gpu):
+    """The executor alternates two descriptor sets: four runs of different
+    batches launched without a synchronisation in between (the third reuses
+    the first one's set) each give the bits of the same batch run alone."""
+    ex = gpu.BatchExecutor("f32", capacity=16)
+    runs = []
+    for r in range(4):
+        jobs = []
+        for i, (rp, col, val, k) in enumerate(_batch(20 + r, 6, np.float32)):
+            N = rp.size - 1
+            A = gpu.csr_from_host(rp, col, val)
+            xd = gpu.DeviceArray.from_host(synth.uniform_vec(N * k, 50 * r + i, dtype=np.float32))
+            yd = gpu.DeviceArray(N * k, np.float32)
+            yd.fill_zero()
+            jobs.append((A, xd, yd, k))
+        runs.append(jobs)
+    for jobs in runs:
+        ex.run(jobs, overwrite=True)
+    gpu.synchronize()
+    together = [[yd.to_host() for _, _, yd, _ in jobs] for jobs in runs]
+    for jobs, want in zip(runs, together):
+        for A, xd, yd, k in jobs:
+            yd.fill_zero()
+        ex.run(jobs, overwrite=True)
+        gpu.synchronize()
+        for (A, xd, yd, k), w in zip(jobs, want):
+            assert np.array_equal(yd.to_host(), w)
+
+
 @pytest.mark.parametrize("storage", ["f32", "f64", "bf16"])
 def test_batch_mixed_formats(gpu, oracle, storage):
     """CSR, DIA and ELL items in one launch.  With one right-hand side a DIA
