@@ -1374,7 +1374,7 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--serve-spts-slots", type=int, default=3)
-    ap.add_argument("--serve-spts-batch", type=int, default=64)
+    ap.add_argument("--serve-spts-batch", type=int, default=32)
     ap.add_argument("--serve-spts-grid", type=int, default=1,
                     help="SpTS launches: persistent blocks per SM (0 = one warp per chunk)")
     ap.add_argument("--serve-rates", default="1000,2000,3000,10000,20000",

@@ -416,13 +416,13 @@ class Server:
     solve.  One launch advances all solves of its batch together.  SpTS
     launches run `spts_grid` persistent blocks per SM (0 = one warp per chunk,
     all resident at once), so a few SpTS slots run side by side without
-    filling the SMs with polling warps (at 20k req/s: 3 slots of 64 solves on
-    1 block per SM gave p99 23 ms, 1 slot of 256 on the full grid 69 ms).
+    filling the SMs with polling warps (at 20k req/s: 3 slots of 32 solves on
+    1 block per SM gave p99 22 ms, 1 slot of 256 on the full grid 69 ms).
     SpMV streams have the higher priority so that their blocks go before
     pending solve blocks."""
 
     def __init__(self, pool: ResidentPool, max_batch: int = 64, slots: int = 4,
-                 arena_bytes: Optional[int] = None, spts_slots: int = 3, spts_batch: int = 64,
+                 arena_bytes: Optional[int] = None, spts_slots: int = 3, spts_batch: int = 32,
                  priorities: bool = True, spts_arena_bytes: Optional[int] = None,
                  spts_grid: int = 1):
         self.pool = pool
