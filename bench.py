@@ -1024,6 +1024,108 @@ def run_batched(stream, peak, n_mats=512, seed=5):
     return out
 
 
+def run_rowshard(args, rank, world, local_rank):
+    """Row-sharded SpMV (strong scaling): the format sweep's CSR matrices
+    (4M-row banded, 2M-row power-law, FP64) split into static_nnz row blocks,
+    one per rank, the whole x on every rank; a step is, per matrix, the
+    rank's block SpMV into its part of y and one in-place all-gather of y
+    (NCCL), so that every rank ends the step with the whole y (the x of an
+    iterative method's next step).  One rank runs the unsplit SpMV with no
+    collective.  Returns rank 0's result (None elsewhere)."""
+    import torch
+    import sciwasm.sparse_b200 as sb
+    from sciwasm.sparse_b200 import _lib
+    from sciwasm.sparse_b200.dist import RowShardedCSR, ShardedY, max_over_ranks
+    sb.load_library()
+    torch.cuda.set_device(local_rank)
+    _lib.call("sb_set_device", local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    jobs = make_workload("format_sweep_fp64", args.small)
+    parts = []
+    for j in jobs:
+        sh = RowShardedCSR(j["rp"], j["col"], j["val"], rank, world)
+        x = torch.from_numpy(j["x"]).to(dev)
+        y = ShardedY(sh.starts, sh.ends, rank, torch.float64, dev)
+        xv = _vec(x)
+        yv = _vec(y.local())
+        tuned = sb.csr_autotune(sh.A, xv, stream=sptr) if sh.A is not None else None
+        parts.append(dict(job=j, sh=sh, x=x, y=y, xv=xv, yv=yv, tuned=tuned,
+                          bytes=algo_bytes("csr", j["N"], int(j["rp"][-1]), 8)))
+    torch.cuda.synchronize()
+    # correctness: one step from y = 0, the gathered y against an FP64 check
+    errs = {}
+    with torch.cuda.stream(stream):
+        for p in parts:
+            p["y"].buf.zero_()
+            if p["sh"].A is not None:
+                sb.spmv(p["sh"].A, p["xv"], p["yv"], stream=sptr)
+            p["y"].allgather()
+    torch.cuda.synchronize()
+    for p in parts:
+        j = p["job"]
+        t = truth_f64(j["rp"], j["col"], j["val"], j["x"])
+        got = p["y"].full().cpu().numpy()
+        errs[j["label"]] = float(np.max(np.abs(got - t)) / max(np.max(np.abs(t)), 1e-300))
+    if max(errs.values()) > 1e-5:
+        raise SystemExit(f"row-shard correctness gate failed: {errs}")
+
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+            torch.cuda.Event(enable_timing=True)) for _ in parts] for _ in range(args.steps)]
+
+    def step(k=None):
+        for i, p in enumerate(parts):
+            if k is not None:
+                ev[k][i][0].record(stream)
+            if p["sh"].A is not None:
+                sb.spmv(p["sh"].A, p["xv"], p["yv"], stream=sptr)
+            if k is not None:
+                ev[k][i][1].record(stream)
+            p["y"].allgather()
+            if k is not None:
+                ev[k][i][2].record(stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        t0.record(stream)
+        for k in range(args.steps):
+            step(k)
+        t1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ms = t0.elapsed_time(t1) / args.steps
+    ms_max = max_over_ranks(ms, device=dev)
+    total = sum(p["bytes"] for p in parts)
+    per = {}
+    for i, p in enumerate(parts):
+        sp = float(np.mean([ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps)]))
+        ag = float(np.mean([ev[k][i][1].elapsed_time(ev[k][i][2]) for k in range(args.steps)]))
+        per[p["job"]["label"]] = {
+            "rows_local": p["sh"].rows, "nnz_local": int(p["sh"].A.nnz) if p["sh"].A else 0,
+            "spmv_ms_max": round(max_over_ranks(sp, device=dev), 4),
+            "allgather_ms_max": round(max_over_ranks(ag, device=dev), 4),
+            "allgather_bytes_in": p["y"].gather_bytes(),
+            "csr_opts": p["tuned"], "max_rel_err": errs[p["job"]["label"]]}
+    if rank != 0:
+        return None
+    return {"world": world, "scaling": "strong",
+            "workload": "format_sweep_fp64 CSR matrices (4M-row banded, 2M-row power-law, FP64) "
+                        "in static_nnz row blocks, x on every rank, y all-gathered each step",
+            "value_GB_s": round(total / (ms_max / 1e3) / 1e9, 1), "unit": UNIT,
+            "ms_per_step": round(ms_max, 4), "algorithmic_bytes": total,
+            "steps": args.steps, "warmup": args.warmup, "per_matrix": per,
+            "timing": "CUDA events on the SpMV stream around the steps, max over ranks; "
+                      "the all-gather runs on NCCL's stream and the SpMV stream waits for it"}
+
+
 def _spts_cpu_baseline(rp, col, val, b, plan_levels, gpu_y, reps=3):
     """CPU-baseline leg of one SpTS case: the oracle's serial analysis and row
     kernel, and its pthread ports of the reference's parallel level-set and
@@ -1350,8 +1452,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="format_sweep_fp64",
-                    help="format_sweep_fp64 (the bench line), laplacian_fp32, or one section "
-                         "alone: " + ", ".join(SECTIONS))
+                    help="format_sweep_fp64 (the bench line), laplacian_fp32, rowshard_fp64 "
+                         "(row-sharded CSR with an all-gather of y, strong scaling), or one "
+                         "section alone: " + ", ".join(SECTIONS))
     ap.add_argument("--csr-fixed", default=None,
                     help="pinned CSR options of the default workload instead of the autotuner, "
                          "e.g. 'banded:0,2,8,0;powerlaw:0,8,4,1' (kernel,lanes,unroll,grid)")
@@ -1397,6 +1500,32 @@ def main():
     if args.workload == "laplacian_fp32":
         config["l2"] = "3.7 MB working set stays L2-resident (reported, not a roofline claim)"
     dtype = config["dtype"]
+
+    if args.workload == "rowshard_fp64":
+        if args.impl == "reference":
+            if rank == 0:
+                jobs = make_workload("format_sweep_fp64", args.small)
+                for j in jobs:
+                    j["formats"] = ["csr"]
+                run_reference(args, jobs, {**config, "dtype": "f64",
+                                           "parallelism": "host threads"})
+            return
+        import datetime
+        import torch
+        if world > 1:
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local_rank))
+        try:
+            out = run_rowshard(args, rank, world, local_rank)
+            if rank == 0:
+                print(json.dumps({"workload": args.workload, "result": out}), flush=True)
+        finally:
+            if world > 1:
+                import torch.distributed as dist
+                dist.destroy_process_group()
+        return
 
     if args.workload in SECTIONS:
         # one configuration alone, one GPU (profiling and focused runs)

@@ -5,9 +5,10 @@ SpMV shards by contiguous row blocks balanced by nonzeros, the partition the
 reference's worker pool uses (static_nnz, src/parallel/src/sparse32.js:2769-2821):
 every rank keeps its block of rows resident and the whole x, computes its own
 y rows with the library's kernels, and the y blocks are disjoint, so the
-data path needs no reduction; `gather_rows` assembles the full y where a
-caller needs it (one all-gather).  `max_over_ranks` is the timing rule of
-multi-GPU measurements: the slowest rank's time.
+data path needs no reduction; `ShardedY` (in place, padded blocks) or
+`gather_rows` assembles the full y where a caller needs it (one
+all-gather).  `max_over_ranks` is the timing rule of multi-GPU
+measurements: the slowest rank's time.
 
 The torch.distributed calls run on whatever backend the process group has
 (NCCL on GPUs, gloo for host-side tests).
@@ -72,6 +73,43 @@ def gather_rows(y_local, starts, ends, group=None):
     parts = [torch.empty_like(buf) for _ in range(world)]
     dist.all_gather(parts, buf, group=group)
     return torch.cat([p[:c] for p, c in zip(parts, counts)])
+
+
+class ShardedY:
+    """y of a row-sharded SpMV as `world` blocks of `maxrows` entries, rank
+    r's rows at r * maxrows: each rank's kernel writes its own block
+    (local()), and one in-place all-gather (NCCL over NVLink on GPUs, gloo
+    on the host) gives every rank the whole y, e.g. as the x of the next
+    iteration.  The padding keeps the blocks equal-sized, which the
+    collective needs; full() drops it."""
+
+    def __init__(self, starts, ends, rank: int, dtype, device):
+        import torch
+        self.counts = [int(e - s) for s, e in zip(starts, ends)]
+        self.world = len(self.counts)
+        self.rank = int(rank)
+        self.maxrows = max(self.counts) if self.counts else 0
+        self.buf = torch.zeros(self.world * self.maxrows, dtype=dtype, device=device)
+
+    def local(self):
+        """This rank's rows (a view into the gathered buffer)."""
+        return self.buf.narrow(0, self.rank * self.maxrows, self.counts[self.rank])
+
+    def allgather(self, group=None) -> None:
+        import torch.distributed as dist
+        if self.world > 1 and self.maxrows > 0:
+            dist.all_gather_into_tensor(
+                self.buf, self.buf.narrow(0, self.rank * self.maxrows, self.maxrows), group=group)
+
+    def full(self):
+        """All N entries in row order (a new tensor)."""
+        import torch
+        return torch.cat([self.buf.narrow(0, r * self.maxrows, c)
+                          for r, c in enumerate(self.counts)])
+
+    def gather_bytes(self) -> int:
+        """Bytes one rank receives per all-gather (the other ranks' blocks)."""
+        return (self.world - 1) * self.maxrows * self.buf.element_size()
 
 
 def max_over_ranks(value: float, device=None, group=None) -> float:

@@ -46,7 +46,12 @@ def _rank_main(rank, world, port, q):
         y_local = orc.spmv_csr(brp, bcol, bval, x, np.zeros(brp.size - 1))
         y = dist.gather_rows(torch.from_numpy(y_local), s, e).numpy()
         t = dist.max_over_ranks(1.5 + rank)
-        q.put((rank, y, t))
+        # the padded in-place layout: this rank's block written in place,
+        # one all-gather, the padding dropped
+        sy = dist.ShardedY(s, e, rank, torch.float64, "cpu")
+        sy.local().copy_(torch.from_numpy(y_local))
+        sy.allgather()
+        q.put((rank, y, t, sy.full().numpy(), sy.gather_bytes(), sy.counts))
     finally:
         tdist.destroy_process_group()
 
@@ -66,6 +71,9 @@ def test_two_gloo_ranks_gather_rows(oracle):
     rp, col, val = synth.power_law(4000, seed=2, cap=200)
     x = synth.uniform_vec(4000, 3)
     full = oracle.spmv_csr(rp, col, val, x, np.zeros(4000))
-    for rank, y, t in out:
+    for rank, y, t, y_padded, nbytes, counts in out:
         assert np.array_equal(y, full)  # each row is computed by one rank
         assert t == 2.5
+        assert np.array_equal(y_padded, full)
+        assert counts[0] != counts[1]  # ragged blocks (balanced by nonzeros)
+        assert nbytes == max(counts) * 8
