@@ -361,17 +361,20 @@ __global__ void spts_level_rows(const int* __restrict__ rrow, const int* __restr
   }
 }
 
-// Grid barrier of a cooperative launch (every block resident).  Thread 0 of
-// each block reads the generation bar[1], then arrives on bar[0] with a
-// release add (ordered after the block's stores, which bar.sync made visible
-// to it); the last to arrive resets bar[0] and advances bar[1] with a release
-// add; the others poll bar[1] with acquire loads and a short sleep, bounded
+// Grid barrier of a cooperative launch (every block resident) on one
+// monotonic arrival counter: at the barrier that closes level l, thread 0 of
+// each block adds 1 with an acquire-release add (ordered after the block's
+// stores, which bar.sync made visible to it) and waits until the counter reaches
+// gridDim.x * (l + 1), polling with acquire loads and a short sleep, bounded
 // by `limit` SM cycles (or by a timeout already recorded in the status
-// word).  Returns false after a timeout, which it records; the caller then
-// returns.
-__device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
+// word).  One atomic per block and level: no reset and no generation word
+// (the earlier form's last arrival reset the counter and advanced a
+// generation, two more dependent atomics per level).  The comparison is
+// wrap-safe: the counter never runs more than gridDim.x ahead of a waiter.
+// Returns false after a timeout, which it records; the caller then returns.
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
   unsigned old;
-  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;"
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;"
                : "=r"(old) : "l"(p), "r"(v) : "memory");
   return old;
 }
@@ -380,19 +383,18 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, long long limit, int* status) {
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned target, long long limit,
+                                             int* status) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
-    const unsigned g = ld_relaxed_u32(bar + 1);
-    if (atom_add_release(bar, 1u) == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      atom_add_release(bar + 1, 1u);
-    } else {
+    // acq_rel: the last block to arrive goes on at once, so its add also
+    // acquires the other blocks' released stores
+    if (atom_add_acq_rel(bar, 1u) + 1u != target) {
       const long long t0 = clock64();
       unsigned ns = SB_SPTS_SLEEP_MIN_NS;
-      while (ld_acquire_u32(bar + 1) == g) {
+      while ((int)(ld_acquire_u32(bar) - target) < 0) {
         if (clock64() - t0 > limit || *(volatile const int*)status) {
           atomicExch(status, SB_DEV_TIMEOUT_DEP);
           ok = 0;
@@ -499,7 +501,7 @@ __global__ void __launch_bounds__(kLevelBlock1)
       nx.i = -1;
       if (q0 + gt < q1) level_row_load(nx, q0 + gt, rrow, rcol, rval, perm, b);
       if (gridDim.x == 1) __syncthreads();  // one block: its barrier orders the L2 accesses
-      else if (!grid_barrier(bar, limit, status)) return;
+      else if (!grid_barrier(bar, gridDim.x * (unsigned)(l + 1), limit, status)) return;
     }
   }
 }
