@@ -420,6 +420,41 @@ struct LevelRow {
   A v[kG];
 };
 
+// A thread's first row of the level after next: where its entries are and
+// where its output goes (the first of the two dependent load rounds of a
+// row, issued one level earlier than the second).
+struct LevelHead {
+  int i = -1, s = 0, end = 0, pi = 0;
+};
+
+__device__ __forceinline__ void level_head_load(LevelHead& h, int i, const int* rrow,
+                                                const int* perm) {
+  h.i = i;
+  h.s = rrow[i];
+  h.end = rrow[i + 1] - 1;
+  h.pi = perm[i];
+}
+
+// The second round: b, the diagonal and up to kG off-diagonal columns and
+// values of the row a head describes.
+template <typename T, typename A>
+__device__ __forceinline__ void level_row_from_head(LevelRow<T, A>& r, const LevelHead& h,
+                                                    const int* rcol, const T* rval, const T* b) {
+  r.i = h.i;
+  if (h.i < 0) return;
+  r.s = h.s;
+  r.end = h.end;
+  r.pi = h.pi;
+  r.bi = (A)b[r.pi];
+  r.diag = (A)rval[r.end];
+#pragma unroll
+  for (int k = 0; k < kG; ++k) {
+    const int j = r.s + k;
+    r.c[k] = j < r.end ? rcol[j] : 0;
+    r.v[k] = j < r.end ? (A)rval[j] : A(0);
+  }
+}
+
 template <typename T, typename A>
 __device__ __forceinline__ void level_row_load(LevelRow<T, A>& r, int i, const int* rrow,
                                                const int* rcol, const T* rval, const int* perm,
@@ -445,13 +480,16 @@ __device__ __forceinline__ void level_row_load(LevelRow<T, A>& r, int i, const i
 // levels are read from L2 (__ldcg), since L1 is not kept coherent with other
 // SMs' stores inside a launch; each row also writes its natural-order
 // output, so no scatter pass follows.  Each thread reads its first row of
-// the next level before waiting at the barrier.  When every level fits in
+// a level in two rounds ahead of time: its row pointers and permutation two
+// levels before, its columns, values, b and diagonal one level before, so
+// that only the y reads after each barrier lie on the level's critical
+// path.  When every level fits in
 // one block of kLevelBlock1 threads, the launch is that one block and the
 // barrier is __syncthreads.
 constexpr int kLevelBlock1 = 512;  // threads of the single-block form
 
 template <typename T, typename A>
-__global__ void __launch_bounds__(kLevelBlock1)
+__global__ void __launch_bounds__(kLevelBlock1, 1)
     spts_level_coop(const int* __restrict__ rrow, const int* __restrict__ rcol,
                     const T* __restrict__ rval, const int* __restrict__ level_ptr, int nlevels,
                     const int* __restrict__ perm, const T* __restrict__ b, T* yw,
@@ -459,9 +497,14 @@ __global__ void __launch_bounds__(kLevelBlock1)
   const int nthreads = gridDim.x * blockDim.x;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   LevelRow<T, A> nx;
+  LevelHead hd;  // the first row of the level after the next one
   {
     const int r0 = __ldg(level_ptr), r1 = __ldg(level_ptr + 1);
     if (r0 + gt < r1) level_row_load(nx, r0 + gt, rrow, rcol, rval, perm, b);
+    if (nlevels > 1) {
+      const int q0 = r1, q1 = __ldg(level_ptr + 2);
+      if (q0 + gt < q1) level_head_load(hd, q0 + gt, rrow, perm);
+    }
   }
   for (int l = 0; l < nlevels; ++l) {
     const int r0 = __ldg(level_ptr + l), r1 = __ldg(level_ptr + l + 1);
@@ -497,9 +540,15 @@ __global__ void __launch_bounds__(kLevelBlock1)
       y[pi] = yi;
     }
     if (l + 1 < nlevels) {
-      const int q0 = r1, q1 = __ldg(level_ptr + l + 2);
-      nx.i = -1;
-      if (q0 + gt < q1) level_row_load(nx, q0 + gt, rrow, rcol, rval, perm, b);
+      // the next level's first row from the head read one level ago, and
+      // the head of the level after it: neither depends on y, so both load
+      // rounds overlap the barrier and the next level's y reads
+      level_row_from_head(nx, hd, rcol, rval, b);
+      hd.i = -1;
+      if (l + 2 < nlevels) {
+        const int q0 = __ldg(level_ptr + l + 2), q1 = __ldg(level_ptr + l + 3);
+        if (q0 + gt < q1) level_head_load(hd, q0 + gt, rrow, perm);
+      }
       if (gridDim.x == 1) __syncthreads();  // one block: its barrier orders the L2 accesses
       else if (!grid_barrier(bar, gridDim.x * (unsigned)(l + 1), limit, status)) return;
     }
