@@ -595,6 +595,29 @@ def run_ours(args, jobs, config, rank, world, local_rank):
     e2e_ms = e0.elapsed_time(e1)
     e2e_ms = max_over_ranks(e2e_ms, device="cuda")
     e2e_value = bytes_step * args.steps * world / (e2e_ms / 1e3) / 1e9
+
+    # the same step's copies alone (same buffers and streams, no kernels):
+    # the host link's floor under the e2e time
+    def copy_step():
+        for o, (xp, yo, nb, xd, yd, sp_k) in zip(objs, host):
+            _lib.call("sb_memcpy_htod", xd.vec_index.ptr, xp, nb, sp_k)
+            _lib.call("sb_memcpy_dtoh", yo, yd.vec_index.ptr, nb, sp_k)
+    copy_step()
+    torch.cuda.synchronize()
+    c0 = torch.cuda.Event(enable_timing=True)
+    c1 = torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    for sd in e2e_streams[1:]:
+        sd.wait_event(c0)
+    for _ in range(args.steps):
+        copy_step()
+    for sd in e2e_streams[1:]:
+        side_done = torch.cuda.Event()
+        side_done.record(sd)
+        stream.wait_event(side_done)
+    c1.record(stream)
+    torch.cuda.synchronize()
+    copy_ms = max_over_ranks(c0.elapsed_time(c1), device="cuda")
     # the read-back results meet the same check as the device results
     for o, (xp, yo, nb, xd, yd, sp_k) in zip(objs, host):
         t = truths[o["job"]["label"]]
@@ -645,6 +668,10 @@ def run_ours(args, jobs, config, rank, world, local_rank):
                                                    per_obj_ms[dom], 3)},
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
+                "ms_per_step": round(e2e_ms / args.steps, 4),
+                "copies_only_ms_per_step": round(copy_ms / args.steps, 4),
+                "frac_of_copy_floor": round(copy_ms / e2e_ms, 3),
+                "host_link_GB_s": round((h2d + d2h) / (copy_ms / args.steps / 1e3) / 1e9, 1),
                 "path": "sciwasm.sparse_b200 via the C ABI, per call the reference "
                         "benchmark's sequence clear_vec(y); spmv(A, x, y) with x uploaded "
                         "from pinned host memory before it and y read back after it "
@@ -1505,7 +1532,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-sections", action="store_true",
                     help="skip the 4096^2 Laplacian, batched and SpTS sections")
-    ap.add_argument("--e2e-streams", type=int, default=2,
+    ap.add_argument("--e2e-streams", type=int, default=3,
                     help="streams the e2e calls rotate over")
     ap.add_argument("--serve-pool", type=int, default=2000)
     ap.add_argument("--serve-max-rows", type=int, default=2_000_000)
