@@ -145,12 +145,10 @@ __device__ __forceinline__ void batch_long_rows(const sb_batch_item& it, int r0,
   }
 }
 
-
 template <typename SV, typename T, int V>
 __device__ __forceinline__ void batch_block(const sb_batch_item& it, int r0, int lane) {
   constexpr int UNROLL = 4;
   constexpr int RPB = 32 / V;
-  constexpr bool COMP = sizeof(T) == 4;
   const int g = lane / V, q = lane - (lane / V) * V;
   const int* __restrict__ rp = it.row_ptr;
   const int* __restrict__ col = it.col;
@@ -723,6 +721,7 @@ using namespace sb;
 extern "C" {
 
 int sb_batch_exec_create(int dtype, int32_t capacity, sb_batch_exec** out) {
+  SB_TRACE("sb_batch_exec_create");
   SB_REQUIRE(out, "sb_batch_exec_create: null output");
   *out = nullptr;
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64 || dtype == SB_BF16,
@@ -781,6 +780,7 @@ int sb_batch_exec_create(int dtype, int32_t capacity, sb_batch_exec** out) {
 }
 
 int sb_batch_exec_destroy(sb_batch_exec* e) {
+  SB_TRACE("sb_batch_exec_destroy");
   if (!e) return SB_OK;
   for (sb_batch_slot& b : e->slot)
     if (b.pending) cudaEventSynchronize(b.done);
@@ -789,6 +789,7 @@ int sb_batch_exec_destroy(sb_batch_exec* e) {
 }
 
 int sb_batch_exec_run(sb_batch_exec* e, const sb_batch_item* items, int32_t n, void* stream) {
+  SB_TRACE("sb_batch_exec_run");
   SB_REQUIRE(e, "sb_batch_exec_run: null executor");
   SB_REQUIRE(n >= 0 && n <= e->capacity, "sb_batch_exec_run: %d items exceed capacity %d", n,
              e->capacity);

@@ -7,6 +7,7 @@
 #include <stdint.h>
 #include <stdio.h>
 #include <stdarg.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "sparse_b200.h"
 
@@ -35,6 +36,19 @@ int ensure_device();  // SB_OK when a CUDA device is usable, else SB_ENODEV
 #define SB_CHECK_LAUNCH(name) SB_CHECK_CUDA(cudaGetLastError())
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---------------------------------------------------------------- tracing
+// An NVTX range over a public entry point (header-only NVTX v3: with no
+// profiler attached a push/pop costs a few instructions), so that a trace
+// (ncu --nvtx, Nsight Systems) attributes each launch to the C-ABI call
+// that made it.
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
+#define SB_TRACE(name) ::sb::TraceRange sb_trace_range__(name)
 
 // Number of SMs of the current device (148 on B200), cached per device.
 int sm_count();

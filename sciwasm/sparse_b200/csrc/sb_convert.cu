@@ -253,6 +253,7 @@ extern "C" {
 int sb_coo_csr(int dtype, const int32_t* row, const int32_t* col, const void* val, int32_t N,
                int64_t nnz, int32_t* csr_row_ptr, int32_t* csr_col, void* csr_val,
                void* stream) {
+  SB_TRACE("sb_coo_csr");
   int r = check_dt(dtype, "sb_coo_csr");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nnz >= 0, "sb_coo_csr: negative size");
@@ -274,6 +275,7 @@ int sb_coo_csr(int dtype, const int32_t* row, const int32_t* col, const void* va
 }
 
 int sb_num_cols(const int32_t* row_ptr, int32_t N, int32_t* nc, void* stream) {
+  SB_TRACE("sb_num_cols");
   SB_REQUIRE(nc && N >= 0, "sb_num_cols: bad argument");
   *nc = 0;
   if (N == 0) return SB_OK;
@@ -299,6 +301,7 @@ int sb_ell_admitted(int64_t ncols, int32_t N, int64_t nnz) {
 
 int sb_csr_ell(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val, int32_t N,
                int64_t nnz, int32_t nc, int32_t* indices, void* data, void* stream) {
+  SB_TRACE("sb_csr_ell");
   int r = check_dt(dtype, "sb_csr_ell");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nnz >= 0 && nc >= 0, "sb_csr_ell: negative size");
@@ -322,6 +325,7 @@ int sb_csr_ell(int dtype, const int32_t* row_ptr, const int32_t* col, const void
 
 int sb_num_diags(const int32_t* row_ptr, const int32_t* col, int32_t N, int32_t* nd,
                  int32_t* stride, void* stream) {
+  SB_TRACE("sb_num_diags");
   SB_REQUIRE(nd && stride && N >= 0, "sb_num_diags: bad argument");
   *nd = 0;
   *stride = N;
@@ -343,6 +347,7 @@ int sb_dia_admitted(int64_t ndiags, int32_t stride, int64_t nnz) {
 int sb_csr_dia(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val, int32_t N,
                int64_t nnz, int32_t nd, int32_t stride, int32_t* offset, void* data,
                void* stream) {
+  SB_TRACE("sb_csr_dia");
   int r = check_dt(dtype, "sb_csr_dia");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nnz >= 0 && nd >= 0, "sb_csr_dia: negative size");
@@ -385,6 +390,7 @@ int sb_csr_dia(int dtype, const int32_t* row_ptr, const int32_t* col, const void
 int sb_coo_csc(int dtype, const int32_t* row, const int32_t* col, const void* val, int32_t N,
                int64_t nnz, int32_t* csc_col_ptr, int32_t* csc_row, void* csc_val,
                void* stream) {
+  SB_TRACE("sb_coo_csc");
   // coo_csc is coo_csr with the roles of rows and columns swapped
   return sb_coo_csr(dtype, col, row, val, N, nnz, csc_col_ptr, csc_row, csc_val, stream);
 }

@@ -137,6 +137,7 @@ extern "C" {
 
 int sb_convert_values(int src_dtype, const void* src, int dst_dtype, void* dst, int64_t n,
                       void* stream) {
+  SB_TRACE("sb_convert_values");
   const bool ok = (src_dtype >= SB_F32 && src_dtype <= SB_BF16) &&
                   (dst_dtype >= SB_F32 && dst_dtype <= SB_BF16);
   SB_REQUIRE(ok, "sb_convert_values: dtypes must be SB_F32, SB_F64 or SB_BF16");
@@ -152,6 +153,7 @@ int sb_convert_values(int src_dtype, const void* src, int dst_dtype, void* dst, 
 }
 
 int sb_map_coo(int dtype, int op, double p, const void* in, void* out, int64_t n, void* stream) {
+  SB_TRACE("sb_map_coo");
   int r = map_check(dtype, op, "sb_map_coo");
   if (r) return r;
   SB_REQUIRE(n >= 0, "sb_map_coo: negative size");
@@ -164,6 +166,7 @@ int sb_map_coo(int dtype, int op, double p, const void* in, void* out, int64_t n
 
 int sb_map_ell(int dtype, int op, double p, const void* in, void* out, int32_t ncols, int32_t N,
                void* stream) {
+  SB_TRACE("sb_map_ell");
   int r = map_check(dtype, op, "sb_map_ell");
   if (r) return r;
   SB_REQUIRE(ncols >= 0 && N >= 0, "sb_map_ell: negative size");
@@ -177,6 +180,7 @@ int sb_map_ell(int dtype, int op, double p, const void* in, void* out, int32_t n
 
 int sb_map_dia(int dtype, int op, double p, const int32_t* offset, const void* in, void* out,
                int32_t ndiags, int32_t stride, int32_t N, void* stream) {
+  SB_TRACE("sb_map_dia");
   int r = map_check(dtype, op, "sb_map_dia");
   if (r) return r;
   SB_REQUIRE(ndiags >= 0 && N >= 0 && stride >= N, "sb_map_dia: bad size");

@@ -268,6 +268,7 @@ using namespace sb;
 extern "C" {
 
 int sb_mm_read_header(const char* text, size_t len, sb_mm_header* h) {
+  SB_TRACE("sb_mm_read_header");
   SB_REQUIRE(text && h, "sb_mm_read_header: null argument");
   memset(h, 0, sizeof(*h));
   const char* p = text;
@@ -325,6 +326,7 @@ int sb_mm_read_header(const char* text, size_t len, sb_mm_header* h) {
 
 int sb_mm_read_entries(const char* text, size_t len, const sb_mm_header* h, int32_t* row,
                        int32_t* col, double* val, int32_t nthreads) {
+  SB_TRACE("sb_mm_read_entries");
   SB_REQUIRE(text && h, "sb_mm_read_entries: null argument");
   SB_REQUIRE(h->nentries == 0 || (row && col), "sb_mm_read_entries: null output");
   const bool pattern = h->field == SB_MM_PATTERN;
@@ -404,6 +406,7 @@ int sb_mm_read_entries(const char* text, size_t len, const sb_mm_header* h, int3
 int sb_mm_coo(int dtype, int lower, const sb_mm_header* h, const int32_t* row,
               const int32_t* col, const double* val, int32_t* out_row, int32_t* out_col,
               void* out_val, int64_t* nnz, void* stream) {
+  SB_TRACE("sb_mm_coo");
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_mm_coo: dtype must be F32 or F64");
   SB_REQUIRE(h && nnz, "sb_mm_coo: null argument");
   SB_REQUIRE(lower == 0 || lower == 1, "sb_mm_coo: lower must be 0 or 1");

@@ -225,6 +225,7 @@ extern "C" {
 
 int sb_diagonal_coo(int dtype, int32_t k, const int32_t* row, const int32_t* col,
                     const void* val, void* diag, int32_t N, int64_t nnz, void* stream) {
+  SB_TRACE("sb_diagonal_coo");
   int r = check(dtype, N, nnz, "sb_diagonal_coo");
   if (r) return r;
   if ((long long)N - std::abs((long long)k) <= 0) {  // the reference returns no vector
@@ -240,6 +241,7 @@ int sb_diagonal_coo(int dtype, int32_t k, const int32_t* row, const int32_t* col
 
 int sb_min_coo(int dtype, int32_t axis, const int32_t* row, const int32_t* col, const void* val,
                void* out, int32_t N, int64_t nnz, void* stream) {
+  SB_TRACE("sb_min_coo");
   int r = check(dtype, N, nnz, "sb_min_coo");
   if (r) return r;
   SB_REQUIRE(out && (nnz == 0 || (row && col && val)), "sb_min_coo: null pointer");
@@ -253,6 +255,7 @@ int sb_min_coo(int dtype, int32_t axis, const int32_t* row, const int32_t* col, 
 
 int sb_sum_coo(int dtype, int32_t axis, const int32_t* row, const int32_t* col, const void* val,
                void* out, int32_t N, int64_t nnz, void* stream) {
+  SB_TRACE("sb_sum_coo");
   int r = check(dtype, N, nnz, "sb_sum_coo");
   if (r) return r;
   SB_REQUIRE(out && (nnz == 0 || (row && col && val)), "sb_sum_coo: null pointer");

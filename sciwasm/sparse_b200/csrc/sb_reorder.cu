@@ -530,6 +530,7 @@ int sb_sort_rows_by_nnz(int dtype, const int32_t* row_ptr, const int32_t* col, c
                         int32_t N, int64_t nnz, int32_t* out_row_ptr, int32_t* out_col,
                         void* out_val, int32_t* nnz_per_row, int32_t* permutation,
                         int32_t* small_rows, void* stream) {
+  SB_TRACE("sb_sort_rows_by_nnz");
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_sort_rows_by_nnz: dtype must be F32 or F64");
   SB_REQUIRE(N >= 0 && nnz >= 0 && nnz <= 0x7fffffffLL, "sb_sort_rows_by_nnz: bad size");
   SB_REQUIRE(N == 0 || (row_ptr && out_row_ptr && nnz_per_row && permutation),
@@ -552,6 +553,7 @@ int sb_sort_rows_by_nnz(int dtype, const int32_t* row_ptr, const int32_t* col, c
 
 int sb_unpermute_rows(int dtype, const int32_t* permutation, const void* in, void* out,
                       int32_t N, void* stream) {
+  SB_TRACE("sb_unpermute_rows");
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_unpermute_rows: dtype must be F32 or F64");
   SB_REQUIRE(N >= 0, "sb_unpermute_rows: bad size");
   if (N == 0) return SB_OK;
@@ -572,6 +574,7 @@ int sb_reorder_nn(int dtype, const int32_t* row_ptr, const int32_t* col, const v
                   int32_t N, int64_t nnz, int32_t w, const int32_t* perm_in, int32_t* walk,
                   int32_t* perm_out, int32_t* out_row_ptr, int32_t* out_col, void* out_val,
                   void* stream) {
+  SB_TRACE("sb_reorder_nn");
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_reorder_nn: dtype must be F32 or F64");
   SB_REQUIRE(N >= 0 && nnz >= 0 && nnz <= 0x7fffffffLL, "sb_reorder_nn: bad size");
   SB_REQUIRE(w >= 1 && w <= kNNMaxW, "sb_reorder_nn: window %d outside 1..%d", w, kNNMaxW);
@@ -594,6 +597,7 @@ int sb_reorder_nn(int dtype, const int32_t* row_ptr, const int32_t* col, const v
 
 int sb_csr_locality_index(const int32_t* row_ptr, const int32_t* col, int32_t N, int64_t nnz,
                           double* index, void* stream) {
+  SB_TRACE("sb_csr_locality_index");
   SB_REQUIRE(index, "sb_csr_locality_index: null output");
   SB_REQUIRE(N >= 0 && nnz >= 0 && nnz <= 0x7fffffffLL, "sb_csr_locality_index: bad size");
   *index = 0.0;

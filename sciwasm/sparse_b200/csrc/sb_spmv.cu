@@ -1276,6 +1276,7 @@ extern "C" {
 int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                    const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
                    const sb_csr_opts* opts, void* stream) {
+  SB_TRACE("sb_spmv_csr_ex");
   int r = dtype == SB_BF16 ? SB_OK : check_dtype(dtype, "sb_spmv_csr");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nnz >= 0 && inner_max >= 0, "sb_spmv_csr: negative size");
@@ -1320,12 +1321,14 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
 int sb_spmv_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                 const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
                 void* stream) {
+  SB_TRACE("sb_spmv_csr");
   return sb_spmv_csr_ex(dtype, row_ptr, col, val, x, y, N, nnz, inner_max, nullptr, stream);
 }
 
 int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                     const void* x, int32_t N, int64_t nnz, int32_t reps, sb_csr_opts* best,
                     float* best_ms, void* stream) {
+  SB_TRACE("sb_csr_autotune");
   int r = dtype == SB_BF16 ? SB_OK : check_dtype(dtype, "sb_csr_autotune");
   if (r) return r;
   SB_REQUIRE(best && N >= 0 && nnz >= 0, "sb_csr_autotune: bad argument");
@@ -1387,6 +1390,7 @@ int sb_csr_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const
 
 int sb_gather_dot(int dtype, const int32_t* col, const void* val, const void* x, int64_t nnz,
                   double* out, void* stream) {
+  SB_TRACE("sb_gather_dot");
   int r = check_dtype(dtype, "sb_gather_dot");
   if (r) return r;
   SB_REQUIRE(nnz >= 0, "sb_gather_dot: negative size");
@@ -1412,12 +1416,14 @@ int sb_gather_dot(int dtype, const int32_t* col, const void* val, const void* x,
 int sb_spmv_coo(int dtype, const int32_t* row, const int32_t* col, const void* val,
                 const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
                 void* stream) {
+  SB_TRACE("sb_spmv_coo");
   return sb_spmv_coo_ex(dtype, row, col, val, x, y, N, nnz, inner_max, 0, stream);
 }
 
 int sb_spmv_coo_ex(int dtype, const int32_t* row, const int32_t* col, const void* val,
                    const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
                    int32_t flags, void* stream) {
+  SB_TRACE("sb_spmv_coo_ex");
   int r = check_dtype(dtype, "sb_spmv_coo");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nnz >= 0 && inner_max >= 0, "sb_spmv_coo: negative size");
@@ -1447,6 +1453,7 @@ int sb_spmv_coo_ex(int dtype, const int32_t* row, const int32_t* col, const void
 
 int sb_spmv_dia(int dtype, const int32_t* offset, const void* data, int32_t N, int32_t nd,
                 int32_t stride, const void* x, void* y, int32_t inner_max, void* stream) {
+  SB_TRACE("sb_spmv_dia");
   int r = dtype == SB_BF16 ? SB_OK : check_dtype(dtype, "sb_spmv_dia");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nd >= 0 && inner_max >= 0, "sb_spmv_dia: negative size");
@@ -1472,6 +1479,7 @@ int sb_spmv_dia(int dtype, const int32_t* offset, const void* data, int32_t N, i
 
 int sb_spmv_ell(int dtype, const int32_t* indices, const void* data, int32_t N, int32_t nc,
                 const void* x, void* y, int32_t inner_max, void* stream) {
+  SB_TRACE("sb_spmv_ell");
   int r = check_dtype(dtype, "sb_spmv_ell");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nc >= 0 && inner_max >= 0, "sb_spmv_ell: negative size");

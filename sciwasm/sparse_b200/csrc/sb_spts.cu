@@ -1161,6 +1161,7 @@ static const void* spts_batch_kernel_for(int dtype, int policy) {
 extern "C" {
 
 int sb_spts_plan_growth(const sb_spts_plan* plan, double* growth, void* stream) {
+  SB_TRACE("sb_spts_plan_growth");
   SB_REQUIRE(plan && growth, "sb_spts_plan_growth: null argument");
   *growth = 0.0;
   if (plan->N == 0) return SB_OK;
@@ -1186,6 +1187,7 @@ int sb_spts_plan_growth(const sb_spts_plan* plan, double* growth, void* stream) 
 }
 
 int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch** out) {
+  SB_TRACE("sb_spts_batch_create");
   SB_REQUIRE(out, "sb_spts_batch_create: null output");
   *out = nullptr;
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_spts_batch_create: dtype must be F32 or F64");
@@ -1298,6 +1300,7 @@ int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch*
 }
 
 int sb_spts_batch_set_grid(sb_spts_batch* e, int32_t blocks_per_sm) {
+  SB_TRACE("sb_spts_batch_set_grid");
   SB_REQUIRE(e, "sb_spts_batch_set_grid: null executor");
   SB_REQUIRE(blocks_per_sm >= 0, "sb_spts_batch_set_grid: negative block count");
   if (e->pending) SB_CHECK_CUDA(cudaEventSynchronize(e->done));
@@ -1306,6 +1309,7 @@ int sb_spts_batch_set_grid(sb_spts_batch* e, int32_t blocks_per_sm) {
 }
 
 int sb_spts_batch_destroy(sb_spts_batch* e) {
+  SB_TRACE("sb_spts_batch_destroy");
   if (!e) return SB_OK;
   if (e->pending) cudaEventSynchronize(e->done);
   spts_batch_release(e);
@@ -1314,6 +1318,7 @@ int sb_spts_batch_destroy(sb_spts_batch* e) {
 
 int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t n,
                       void* stream) {
+  SB_TRACE("sb_spts_batch_run");
   SB_REQUIRE(e, "sb_spts_batch_run: null executor");
   SB_REQUIRE(n >= 0 && n <= e->capacity, "sb_spts_batch_run: %d items exceed capacity %d", n,
              e->capacity);
@@ -1405,6 +1410,7 @@ int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t
 int sb_spts_syncfree_csr_noalloc(int dtype, const int32_t* row_ptr, const int32_t* col,
                                  const void* val, int32_t N, const void* b, void* y,
                                  int64_t spin_limit_cycles, void* stream) {
+  SB_TRACE("sb_spts_syncfree_csr_noalloc");
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_spts_syncfree_csr_noalloc: bad dtype");
   SB_REQUIRE(N >= 0, "sb_spts_syncfree_csr_noalloc: negative size");
   if (N > kNoAllocMaxRows) {
@@ -1450,6 +1456,7 @@ int sb_spts_syncfree_csr_noalloc(int dtype, const int32_t* row_ptr, const int32_
 
 int sb_spts_analyze(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                     int32_t N, int64_t nnz, void* stream, sb_spts_plan** plan) {
+  SB_TRACE("sb_spts_analyze");
   SB_REQUIRE(plan, "sb_spts_analyze: null plan output");
   *plan = nullptr;
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_spts_analyze: dtype must be F32 or F64");
@@ -1482,6 +1489,7 @@ int sb_spts_analyze(int dtype, const int32_t* row_ptr, const int32_t* col, const
 }
 
 int sb_spts_plan_destroy(sb_spts_plan* plan) {
+  SB_TRACE("sb_spts_plan_destroy");
   if (!plan) return SB_OK;
   cudaDeviceSynchronize();
   plan_release(plan);
@@ -1490,6 +1498,7 @@ int sb_spts_plan_destroy(sb_spts_plan* plan) {
 }
 
 int sb_spts_plan_info(const sb_spts_plan* plan, int32_t* nlevels, int32_t* solvable) {
+  SB_TRACE("sb_spts_plan_info");
   SB_REQUIRE(plan && nlevels && solvable, "sb_spts_plan_info: null argument");
   *nlevels = plan->nlevels;
   *solvable = plan->solvable;
@@ -1497,6 +1506,7 @@ int sb_spts_plan_info(const sb_spts_plan* plan, int32_t* nlevels, int32_t* solva
 }
 
 int sb_spts_plan_analysis_ms(const sb_spts_plan* plan, float* ms) {
+  SB_TRACE("sb_spts_plan_analysis_ms");
   SB_REQUIRE(plan && ms, "sb_spts_plan_analysis_ms: null argument");
   *ms = plan->analysis_ms;
   return SB_OK;
@@ -1504,6 +1514,7 @@ int sb_spts_plan_analysis_ms(const sb_spts_plan* plan, float* ms) {
 
 int sb_spts_plan_levels(const sb_spts_plan* plan, int32_t* level, int32_t* level_ptr,
                         int32_t* permutation, int32_t* order, void* stream) {
+  SB_TRACE("sb_spts_plan_levels");
   SB_REQUIRE(plan, "sb_spts_plan_levels: null plan");
   const size_t n = sizeof(int) * (size_t)plan->N;
   cudaStream_t st = as_stream(stream);
@@ -1521,6 +1532,7 @@ int sb_spts_plan_levels(const sb_spts_plan* plan, int32_t* level, int32_t* level
 
 int sb_spts_plan_reordered(const sb_spts_plan* plan, int32_t* row_ptr, int32_t* col, void* val,
                            void* stream) {
+  SB_TRACE("sb_spts_plan_reordered");
   SB_REQUIRE(plan, "sb_spts_plan_reordered: null plan");
   cudaStream_t st = as_stream(stream);
   if (plan->N == 0) return SB_OK;
@@ -1538,6 +1550,7 @@ int sb_spts_plan_reordered(const sb_spts_plan* plan, int32_t* row_ptr, int32_t* 
 
 int sb_spts_solve(const sb_spts_plan* plan, int algo, int policy, const void* b, void* y,
                   void* stream) {
+  SB_TRACE("sb_spts_solve");
   SB_REQUIRE(plan, "sb_spts_solve: null plan");
   SB_REQUIRE(algo == SB_SPTS_LEVEL || algo == SB_SPTS_SYNCFREE || algo == SB_SPTS_HYBRID,
              "sb_spts_solve: unknown algorithm %d", algo);
@@ -1558,6 +1571,7 @@ int sb_spts_solve(const sb_spts_plan* plan, int algo, int policy, const void* b,
 int sb_spts_syncfree_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                          int32_t N, const void* b, void* y, int64_t spin_limit_cycles,
                          void* stream) {
+  SB_TRACE("sb_spts_syncfree_csr");
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_spts_syncfree_csr: bad dtype");
   SB_REQUIRE(N >= 0, "sb_spts_syncfree_csr: negative size");
   if (N == 0) return SB_OK;
@@ -1598,6 +1612,7 @@ int sb_spts_syncfree_csr(int dtype, const int32_t* row_ptr, const int32_t* col, 
 
 int sb_spts_csc(int dtype, const int32_t* col_ptr, const int32_t* row, const void* val,
                 int32_t N, int64_t nnz, const void* x, void* y, void* stream) {
+  SB_TRACE("sb_spts_csc");
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64, "sb_spts_csc: dtype must be F32 or F64");
   SB_REQUIRE(N >= 0 && nnz >= 0 && nnz <= 0x7fffffffLL, "sb_spts_csc: bad size");
   if (N == 0) return SB_OK;

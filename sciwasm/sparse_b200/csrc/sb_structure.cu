@@ -414,6 +414,7 @@ using namespace sb;
 extern "C" {
 
 int sb_count_nonzeros(int dtype, const void* val, int64_t n, int64_t* count, void* stream) {
+  SB_TRACE("sb_count_nonzeros");
   int r = dt_ok(dtype, "sb_count_nonzeros");
   if (r) return r;
   SB_REQUIRE(count && n >= 0, "sb_count_nonzeros: bad argument");
@@ -431,6 +432,7 @@ int sb_count_nonzeros(int dtype, const void* val, int64_t n, int64_t* count, voi
 
 int sb_copy_nonzeros_coo(int dtype, const int32_t* row, const int32_t* col, const void* val,
                          int64_t nnz, int32_t* orow, int32_t* ocol, void* oval, void* stream) {
+  SB_TRACE("sb_copy_nonzeros_coo");
   int r = dt_ok(dtype, "sb_copy_nonzeros_coo");
   if (r) return r;
   SB_REQUIRE(nnz >= 0 && nnz < 0x7fffffffLL, "sb_copy_nonzeros_coo: bad size");
@@ -448,6 +450,7 @@ int sb_copy_nonzeros_coo(int dtype, const int32_t* row, const int32_t* col, cons
 int sb_copy_nonzeros_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                          int32_t N, int64_t nnz, int32_t* orow_ptr, int32_t* ocol, void* oval,
                          void* stream) {
+  SB_TRACE("sb_copy_nonzeros_csr");
   int r = dt_ok(dtype, "sb_copy_nonzeros_csr");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nnz >= 0 && nnz < 0x7fffffffLL, "sb_copy_nonzeros_csr: bad size");
@@ -465,6 +468,7 @@ int sb_copy_nonzeros_csr(int dtype, const int32_t* row_ptr, const int32_t* col, 
 int sb_count_nonzeros_dia(int dtype, const int32_t* offset, const void* data, int32_t nd,
                           int32_t stride, int32_t N, int32_t* count_diags, int64_t* count,
                           void* stream) {
+  SB_TRACE("sb_count_nonzeros_dia");
   int r = dt_ok(dtype, "sb_count_nonzeros_dia");
   if (r) return r;
   SB_REQUIRE(count_diags && count && nd >= 0 && N >= 0 && stride >= N,
@@ -487,6 +491,7 @@ int sb_count_nonzeros_dia(int dtype, const int32_t* offset, const void* data, in
 
 int sb_copy_nonzeros_dia(int dtype, const int32_t* offset, const void* data, int32_t nd,
                          int32_t stride, int32_t N, int32_t* ooffset, void* odata, void* stream) {
+  SB_TRACE("sb_copy_nonzeros_dia");
   int r = dt_ok(dtype, "sb_copy_nonzeros_dia");
   if (r) return r;
   SB_REQUIRE(nd >= 0 && N >= 0 && stride >= N, "sb_copy_nonzeros_dia: bad size");
@@ -503,6 +508,7 @@ int sb_copy_nonzeros_dia(int dtype, const int32_t* offset, const void* data, int
 
 int sb_count_nonzeros_ell(int dtype, const void* data, int32_t nc, int32_t N, int32_t* count_cols,
                           int64_t* count, void* stream) {
+  SB_TRACE("sb_count_nonzeros_ell");
   int r = dt_ok(dtype, "sb_count_nonzeros_ell");
   if (r) return r;
   SB_REQUIRE(count_cols && count && nc >= 0 && N >= 0, "sb_count_nonzeros_ell: bad argument");
@@ -537,6 +543,7 @@ int sb_count_nonzeros_ell(int dtype, const void* data, int32_t nc, int32_t N, in
 
 int sb_copy_nonzeros_ell(int dtype, const void* data, const int32_t* indices, int32_t nc,
                          int32_t N, int32_t out_nc, void* odata, int32_t* oindices, void* stream) {
+  SB_TRACE("sb_copy_nonzeros_ell");
   int r = dt_ok(dtype, "sb_copy_nonzeros_ell");
   if (r) return r;
   SB_REQUIRE(nc >= 0 && N >= 0 && out_nc >= 0, "sb_copy_nonzeros_ell: bad size");
@@ -556,6 +563,7 @@ int sb_copy_nonzeros_ell(int dtype, const void* data, const int32_t* indices, in
 
 int sb_transpose_coo(int dtype, const int32_t* row, const int32_t* col, const void* val,
                      int64_t nnz, int32_t* orow, int32_t* ocol, void* oval, void* stream) {
+  SB_TRACE("sb_transpose_coo");
   int r = dt_ok(dtype, "sb_transpose_coo");
   if (r) return r;
   SB_REQUIRE(nnz >= 0, "sb_transpose_coo: bad size");
@@ -572,6 +580,7 @@ int sb_transpose_coo(int dtype, const int32_t* row, const int32_t* col, const vo
 int sb_transpose_csr(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                      int32_t N, int64_t nnz, int32_t* orow_ptr, int32_t* ocol, void* oval,
                      void* stream) {
+  SB_TRACE("sb_transpose_csr");
   int r = dt_ok(dtype, "sb_transpose_csr");
   if (r) return r;
   SB_REQUIRE(N >= 0 && nnz >= 0 && nnz < 0x7fffffffLL, "sb_transpose_csr: bad size");
@@ -588,6 +597,7 @@ int sb_transpose_csr(int dtype, const int32_t* row_ptr, const int32_t* col, cons
 
 int sb_transpose_dia(int dtype, const int32_t* offset, const void* data, int32_t nd,
                      int32_t stride, int32_t N, int32_t* ooffset, void* odata, void* stream) {
+  SB_TRACE("sb_transpose_dia");
   int r = dt_ok(dtype, "sb_transpose_dia");
   if (r) return r;
   SB_REQUIRE(nd >= 0 && N >= 0 && stride >= N, "sb_transpose_dia: bad size");
@@ -609,6 +619,7 @@ int sb_transpose_dia(int dtype, const int32_t* offset, const void* data, int32_t
 
 int sb_count_transpose_cols_ell(int dtype, const void* data, const int32_t* indices, int32_t nc,
                                 int32_t N, int32_t* count_cols, void* stream) {
+  SB_TRACE("sb_count_transpose_cols_ell");
   int r = dt_ok(dtype, "sb_count_transpose_cols_ell");
   if (r) return r;
   SB_REQUIRE(count_cols && nc >= 0 && N >= 0, "sb_count_transpose_cols_ell: bad argument");
@@ -636,6 +647,7 @@ int sb_count_transpose_cols_ell(int dtype, const void* data, const int32_t* indi
 
 int sb_transpose_ell(int dtype, const void* data, const int32_t* indices, int32_t nc, int32_t N,
                      int32_t out_nc, void* odata, int32_t* oindices, void* stream) {
+  SB_TRACE("sb_transpose_ell");
   int r = dt_ok(dtype, "sb_transpose_ell");
   if (r) return r;
   SB_REQUIRE(nc >= 0 && N >= 0 && out_nc >= 0, "sb_transpose_ell: bad size");

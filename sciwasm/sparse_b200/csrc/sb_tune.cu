@@ -96,6 +96,7 @@ extern "C" {
 int sb_spmv_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                      const void* x, int32_t N, int64_t nnz, int32_t mode, int32_t reps,
                      sb_spmv_choice* out, void* stream) {
+  SB_TRACE("sb_spmv_autotune");
   SB_REQUIRE(out, "sb_spmv_autotune: null output");
   *out = sb_spmv_choice{};
   for (int k = 0; k < 4; ++k) out->ms[k] = -1.f;
@@ -199,6 +200,7 @@ int sb_spmv_autotune(int dtype, const int32_t* row_ptr, const int32_t* col, cons
 
 int sb_csr_coo(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val, int32_t N,
                int64_t nnz, int32_t* coo_row, int32_t* coo_col, void* coo_val, void* stream) {
+  SB_TRACE("sb_csr_coo");
   SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64 || dtype == SB_BF16, "sb_csr_coo: bad dtype");
   SB_REQUIRE(N >= 0 && nnz >= 0, "sb_csr_coo: negative size");
   if (N == 0 || nnz == 0) return SB_OK;
