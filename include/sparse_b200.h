@@ -426,15 +426,21 @@ int sb_spts_plan_growth(const sb_spts_plan* plan, double* growth, void* stream);
  * solved with the arithmetic of SB_SPTS_HYBRID, so each result is
  * bit-identical to sb_spts_solve(plan, SB_SPTS_HYBRID, policy, b, y).  An
  * executor serves one value dtype (SB_F32 or SB_F64) and one accumulation
- * policy; a plan may appear once per run, and the solves of one plan must be
- * ordered (one stream, or events) because they share its work vector and
- * ready flags.  Stream-ordered; a dependency wait that runs out is reported
- * by sb_device_status (code 2). */
+ * policy.  A solve keeps its rows' values, published with a pending
+ * sentinel, in a work vector of N values of the plan's dtype: the plan's own
+ * (work = NULL), or one the caller gives (work != NULL, aligned to the value
+ * size, not shared with any solve in flight; no counterpart in the
+ * reference).  Solves on the plan's own vector must be ordered (one stream,
+ * or events) and a plan may appear once per run with it; solves with their
+ * own work vectors may repeat a plan in one run and run concurrently with
+ * other runs on the same plan.  Stream-ordered; a dependency wait that runs
+ * out is reported by sb_device_status (code 2). */
 typedef struct sb_spts_batch sb_spts_batch;
 typedef struct sb_spts_batch_item {
   sb_spts_plan* plan;
   const void* b; /* right-hand side, natural row order */
   void* y;       /* solution, natural row order        */
+  void* work;    /* N values of the plan's dtype, or NULL (the plan's own) */
 } sb_spts_batch_item;
 int sb_spts_batch_create(int dtype, int policy, int32_t capacity, sb_spts_batch** out);
 int sb_spts_batch_destroy(sb_spts_batch* e);

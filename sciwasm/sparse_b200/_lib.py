@@ -133,7 +133,7 @@ SB_MM_REAL, SB_MM_INTEGER, SB_MM_PATTERN, SB_MM_COMPLEX = 0, 1, 2, 3
 
 
 class SptsBatchItem(C.Structure):
-    _fields_ = [("plan", P), ("b", P), ("y", P)]
+    _fields_ = [("plan", P), ("b", P), ("y", P), ("work", P)]
 
 
 SIGNATURES.update({

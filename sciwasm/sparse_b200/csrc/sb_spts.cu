@@ -1335,13 +1335,19 @@ int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t
                 "stored last", i);
       return SB_EINVAL;
     }
+    const size_t vs = p->dtype == SB_F64 ? 8 : 4;
+    SB_REQUIRE(reinterpret_cast<uintptr_t>(items[i].work) % vs == 0,
+               "sb_spts_batch_run: item %d: work vector not aligned to the value size", i);
   }
   {
-    std::vector<const sb_spts_plan*> ps(n);
-    for (int i = 0; i < n; ++i) ps[i] = items[i].plan;
+    // a plan's own work vector serves one solve per run
+    std::vector<const sb_spts_plan*> ps;
+    for (int i = 0; i < n; ++i)
+      if (!items[i].work) ps.push_back(items[i].plan);
     std::sort(ps.begin(), ps.end());
-    for (int i = 1; i < n; ++i)
-      SB_REQUIRE(ps[i] != ps[i - 1], "sb_spts_batch_run: a plan appears twice in one batch");
+    for (size_t i = 1; i < ps.size(); ++i)
+      SB_REQUIRE(ps[i] != ps[i - 1],
+                 "sb_spts_batch_run: a plan appears twice in one batch with its own work vector");
   }
   // the pinned staging buffers are read by the previous run's first nodes
   if (e->pending) SB_CHECK_CUDA(cudaEventSynchronize(e->done));
@@ -1354,7 +1360,7 @@ int sb_spts_batch_run(sb_spts_batch* e, const sb_spts_batch_item* items, int32_t
     d.rcol = p->rcol;
     d.rval = p->rval;
     d.perm = p->perm;
-    d.yw = p->ywork;
+    d.yw = items[i].work ? items[i].work : p->ywork;
     d.b = items[i].b;
     d.y = items[i].y;
     d.N = p->N;

@@ -16,8 +16,9 @@ The pieces:
   live in host memory (pinned, so that copies overlap with device work).
   - "batched": continuous batching.  Requests are released as their arrival
     times pass into one queue per kind.  Whenever a slot of that kind is
-    free, the oldest pending requests that fit its device arena (and, for
-    solves, whose factor has no solve in flight) are packed into one batch:
+    free, the oldest pending requests that fit its device arena (x, y and,
+    for a solve, its own work vector, so that solves of one factor can share
+    a batch and overlap each other across slots) are packed into one batch:
     their inputs go up with one copy per contiguous host range, all SpMVs of
     a value storage run as one graph-replayed persistent launch (all solves
     of a dtype and accumulation policy as one graph-replayed launch), and
@@ -432,9 +433,11 @@ class Server:
         self.nslots = int(slots)
         self.spts_slots = int(spts_slots)
         self.spts_batch = int(spts_batch)
-        need = 2 * 8 * max(pool.max_rows, 1) + 2 * _ALIGN  # the largest single request
+        # the largest single request: x and y (and a solve's work vector)
+        need = 2 * 8 * max(pool.max_rows, 1) + 2 * _ALIGN
+        need_spts = 3 * 8 * max(pool.max_rows, 1) + 3 * _ALIGN
         self.arena_bytes = _al(max(int(arena_bytes or (256 << 20)), need))
-        self.spts_arena_bytes = _al(max(int(spts_arena_bytes or (1 << 30)), need))
+        self.spts_arena_bytes = _al(max(int(spts_arena_bytes or (1 << 30)), need_spts))
         self._cancel_lock = threading.Lock()
         self._cancelled: set = set()
 
@@ -466,74 +469,77 @@ class Server:
             raise ValueError(f"request {r.rid}: x and y must be contiguous")
 
     # ------------------------------------------------------------ batched
-    def _launch(self, slot: _Slot, reqs: list) -> None:
+    def _launch(self, slot: _Slot, reqs: list, busy_plans: frozenset = frozenset()) -> None:
         mats = [self.pool.get(r.matrix) for r in reqs]
         base = slot.arena.ptr
         off = 0
-        xo, yo = [], []
+        xo, yo, wo = [], [], []
         for m, r in zip(mats, reqs):
             xo.append(off)
             off += _al(_vec_bytes(m, r))
         for m, r in zip(mats, reqs):
             yo.append(off)
             off += _al(_vec_bytes(m, r))
+        for m, r in zip(mats, reqs):  # a solve's own work vector (N values)
+            wo.append(off if r.op == "spts" else -1)
+            off += _al(_vec_bytes(m, r)) if r.op == "spts" else 0
         h2d = [(base + o, r.x.ctypes.data, _vec_bytes(m, r)) for m, r, o in zip(mats, reqs, xo)]
         slot.copies = _copies(h2d, "h2d", slot.stream)
         groups = collections.defaultdict(list)
-        for m, r, a, b in zip(mats, reqs, xo, yo):
+        for m, r, a, b, w in zip(mats, reqs, xo, yo, wo):
             vt = _VEC[r.storage]
             xd = DeviceArray(m.N, vt, base + a)
             yd = DeviceArray(m.N, vt, base + b)
             if r.op == "spmv":
                 groups[r.storage].append((m.fmt.get(r.storage, m.csr[r.storage]), xd, yd, 1))
             else:
-                groups[(r.storage, m.policy[r.storage])].append((m.plans[r.storage], xd, yd))
+                groups[(r.storage, m.policy[r.storage])].append(
+                    (m.plans[r.storage], xd, yd, DeviceArray(m.N, vt, base + w),
+                     (r.matrix, r.storage)))
+        slot.plans = []
         for key, jobs in groups.items():
             if slot.kind == "spmv":
                 slot.executor(key).run(jobs, stream=slot.stream, overwrite=True)
-            elif len(jobs) == 1:
-                # one solve: the single hybrid solve, whose launch suits one
+            elif len(jobs) == 1 and jobs[0][4] not in busy_plans:
+                # one solve whose plan is idle: the single hybrid solve on the
+                # plan's own work vector and tickets, whose launch suits one
                 # system (the batch kernel gives the same bits)
-                plan, xd, yd = jobs[0]
+                plan, xd, yd, _, pk = jobs[0]
                 pol = _lib.SB_SPTS_ACC_F64 if key[1] == "f64" else _lib.SB_SPTS_ACC_NATIVE
                 call("sb_spts_solve", plan.ptr, _lib.SB_SPTS_HYBRID, pol, xd.ptr, yd.ptr,
                      slot.stream)
+                slot.plans.append(pk)
             else:
-                slot.executor(key).run(jobs, stream=slot.stream)
+                # every solve on its own work vector: a plan may repeat in the
+                # batch and run beside other slots' solves of it
+                slot.executor(key).run([j[:4] for j in jobs], stream=slot.stream)
         d2h = [(r.y.ctypes.data, base + o, _vec_bytes(m, r)) for m, r, o in zip(mats, reqs, yo)]
         slot.copies += _copies(d2h, "d2h", slot.stream)
         slot.ev_done.record(slot.stream)
         slot.launches = len(groups)
         slot.busy = True
         slot.reqs = reqs
-        slot.plans = [(r.matrix, r.storage) for r in reqs if r.op == "spts"]
         self.pool.busy.update(r.matrix for r in reqs)
 
-    def _take(self, pending: collections.deque, busy_plans: set, arena: int,
+    def _take(self, pending: collections.deque, arena: int,
               max_batch: Optional[int] = None) -> list:
         """Pending requests for one batch, oldest first: at most max_batch,
-        within the arena, at most one solve per plan and none on a plan with
-        a solve in flight (those wait in order for a later batch)."""
+        within the arena (x and y, and a work vector for a solve, which
+        then needs nothing of its plan's own: solves of a plan may share a
+        batch and overlap the plan's solves in other slots)."""
         max_batch = self.max_batch if max_batch is None else max_batch
         take, keep = [], []
         used = 0
-        seen = set()
         while pending and len(take) < max_batch:
             r = pending.popleft()
             if self._is_cancelled(r):
                 r.status = "cancelled"
                 continue
             m = self.pool.mats[r.matrix]
-            need = 2 * _al(_vec_bytes(m, r))
-            key = (r.matrix, r.storage)
-            if r.op == "spts" and (key in busy_plans or key in seen):
-                keep.append(r)
-                continue
+            need = (3 if r.op == "spts" else 2) * _al(_vec_bytes(m, r))
             if used + need > arena:
                 keep.append(r)
                 break
-            if r.op == "spts":
-                seen.add(key)
             used += need
             take.append(r)
         pending.extendleft(reversed(keep))
@@ -587,12 +593,12 @@ class Server:
                         if free is None:
                             break
                         before = len(pending)
-                        take = self._take(pending, busy_plans, free.arena_bytes, mb)
+                        take = self._take(pending, free.arena_bytes, mb)
                         # cancelled requests left the queue without a batch
                         done += before - len(pending) - len(take)
                         if not take:
                             break
-                        self._launch(free, take)
+                        self._launch(free, take, frozenset(busy_plans))
                         for r in take:
                             r.slot = free.index
                         busy_plans.update(free.plans)

@@ -1080,16 +1080,22 @@ class SptsBatch:
         self._keep = []
 
     def run(self, jobs, stream=None):
-        """jobs: iterable of (SptsPlan, b DeviceArray, y DeviceArray), natural order."""
+        """jobs: iterable of (SptsPlan, b DeviceArray, y DeviceArray[, work
+        DeviceArray]), natural order.  With a work vector (N values of the
+        plan's dtype) a solve does not use its plan's own, so a plan may
+        repeat in one run and run beside other solves of it."""
         jobs = list(jobs)
         if len(jobs) > self.capacity:
             raise ValueError(f"{len(jobs)} solves exceed the executor capacity {self.capacity}")
         n = 0
         self._keep = []
-        for plan, b, y in jobs:
+        for job in jobs:
+            plan, b, y = job[:3]
+            work = job[3] if len(job) > 3 else None
             it = self._items[n]
             it.plan, it.b, it.y = plan.ptr, b.ptr, y.ptr
-            self._keep.append((plan, b, y))
+            it.work = work.ptr if work is not None else None
+            self._keep.append(job)
             n += 1
         call("sb_spts_batch_run", self.ptr, self._items, n, _sp(stream))
 

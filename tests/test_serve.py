@@ -74,30 +74,32 @@ def _req(rid, mat, op="spmv", storage="f32"):
     return serve.Request(rid, 0.0, mat, op, storage, None, None)
 
 
-def test_take_respects_batch_arena_and_plans():
+def test_take_respects_batch_arena():
     pool = _FakePool({"A": 1000, "L": 2000, "B": 100_000})
     srv = serve.Server(pool, max_batch=4, slots=2, arena_bytes=1 << 20)
     pend = collections.deque([_req(0, "A"), _req(1, "L", "spts"), _req(2, "L", "spts"),
                               _req(3, "A", "spmv", "bf16"), _req(4, "A"), _req(5, "A")])
-    take = srv._take(pend, set(), srv.arena_bytes)
-    # the second solve on L waits (one solve per plan in a batch)
-    assert [r.rid for r in take] == [0, 1, 3, 4]
-    assert [r.rid for r in pend] == [2, 5]
-    # with L's plan in flight, its solve waits but later requests go
-    take = srv._take(pend, {("L", "f32")}, srv.arena_bytes)
-    assert [r.rid for r in take] == [5] and [r.rid for r in pend] == [2]
+    take = srv._take(pend, srv.arena_bytes)
+    # solves carry their own work vectors: two solves of L share a batch
+    assert [r.rid for r in take] == [0, 1, 2, 3]
+    assert [r.rid for r in pend] == [4, 5]
     # arena: sized for the largest request (two B); a third B waits and so
     # does everything behind it
     assert srv.arena_bytes == 2 * 2 * 400_128
     pend = collections.deque([_req(10, "B"), _req(11, "B"), _req(12, "B"), _req(13, "A")])
-    take = srv._take(pend, set(), srv.arena_bytes)
+    take = srv._take(pend, srv.arena_bytes)
     assert [r.rid for r in take] == [10, 11] and [r.rid for r in pend] == [12, 13]
+    # a solve takes x, y and its work vector in the arena
+    pend = collections.deque([_req(20, "B", "spts"), _req(21, "B", "spts")])
+    take = srv._take(pend, 5 * 400_128)
+    assert [r.rid for r in take] == [20] and [r.rid for r in pend] == [21]
 
 
 def test_server_arena_holds_largest_request():
     pool = _FakePool({"big": 30_000_000})
     srv = serve.Server(pool, arena_bytes=1 << 20)
     assert srv.arena_bytes >= 2 * 8 * 30_000_000
+    assert srv.spts_arena_bytes >= 3 * 8 * 30_000_000
 
 
 def test_poisson_arrivals():
@@ -114,7 +116,7 @@ def test_take_drops_cancelled_requests():
     srv.cancel(1)
     srv.cancel(3)
     pend = collections.deque(reqs)
-    take = srv._take(pend, set(), srv.arena_bytes)
+    take = srv._take(pend, srv.arena_bytes)
     assert [r.rid for r in take] == [0, 2] and not pend
     assert [r.status for r in reqs] == ["pending", "cancelled", "pending", "cancelled"]
 

@@ -74,6 +74,45 @@ def test_spts_batch_bit_identical_to_hybrid(gpu, oracle, dt, policy, grid):
     assert rel_err(want[1], truth) <= (1e-5 if dt == np.float32 else 1e-12)
 
 
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_spts_batch_own_work_vectors(gpu, dt):
+    """Solves with their own work vectors: one plan three times in a run (with
+    different right-hand sides) while a second executor, on another stream,
+    solves the same plan on its work vector and a third solve uses the plan's
+    own; every result equals the single hybrid solve's bits."""
+    rp, col, val = synth.random_lower(20_000, per_row=7, band=500, seed=5, dtype=dt)
+    L = gpu.csr_from_host(rp, col, val)
+    plan = gpu.SptsPlan(L)
+    bs = [gpu.DeviceArray.from_host(synth.uniform_vec(L.N, 70 + i, dtype=dt)) for i in range(5)]
+    want = []
+    for b in bs:
+        yv = gpu.create_vec(L.N, 0, dt)
+        gpu.spts(L, gpu.sparse_vec_t(b, L.N), yv, algo="hybrid")
+        want.append(yv.array())
+    ys = [gpu.DeviceArray(L.N, dt) for _ in bs]
+    ws = [gpu.DeviceArray(L.N, dt) for _ in bs]
+    s1, s2 = C.c_void_p(), C.c_void_p()
+    _lib.call("sb_stream_create", C.byref(s1))
+    _lib.call("sb_stream_create", C.byref(s2))
+    ex1 = gpu.SptsBatch(dt, "native", capacity=4, blocks_per_sm=1)
+    ex2 = gpu.SptsBatch(dt, "native", capacity=4, blocks_per_sm=1)
+    for rep in range(2):
+        for y in ys:
+            y.fill_zero()
+        gpu.synchronize()
+        ex1.run([(plan, bs[0], ys[0], ws[0]), (plan, bs[1], ys[1], ws[1]),
+                 (plan, bs[2], ys[2]), (plan, bs[3], ys[3], ws[3])], stream=s1.value)
+        ex2.run([(plan, bs[4], ys[4], ws[4])], stream=s2.value)
+        gpu.synchronize()
+        for i, (y, w) in enumerate(zip(ys, want)):
+            assert np.array_equal(_bits(y.to_host()), _bits(w)), (rep, i)
+    code = C.c_int(0)
+    _lib.call("sb_device_status", C.byref(code))
+    assert code.value == 0
+    _lib.call("sb_stream_destroy", s1)
+    _lib.call("sb_stream_destroy", s2)
+
+
 def test_spts_batch_rejects_bad_items(gpu):
     L32 = gpu.csr_from_host(*synth.laplacian_3d_lower(6, dtype=np.float32))
     L64 = gpu.csr_from_host(*synth.laplacian_3d_lower(6, dtype=np.float64))
@@ -84,7 +123,10 @@ def test_spts_batch_rejects_bad_items(gpu):
     with pytest.raises(_lib.SparseError):
         ex.run([(p64, b, y)])                       # plan dtype differs
     with pytest.raises(_lib.SparseError):
-        ex.run([(p32, b, y), (p32, b, y)])          # one plan twice
+        ex.run([(p32, b, y), (p32, b, y)])          # one plan twice on its own vector
+    w_odd = gpu.DeviceArray(L32.N + 1, np.float32)
+    with pytest.raises(_lib.SparseError):           # work vector not 4-byte aligned
+        ex.run([(p32, b, y, gpu.DeviceArray(L32.N, np.float32, w_odd.ptr + 2))])
     with pytest.raises(ValueError):
         ex.run([(p32, b, y)] * 5)                   # above capacity
     upper = gpu.csr_from_host(np.array([0, 2, 3], np.int32), np.array([0, 1, 1], np.int32),
