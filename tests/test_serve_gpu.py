@@ -103,7 +103,9 @@ def test_spts_batch_own_work_vectors(gpu, dt):
         ex1.run([(plan, bs[0], ys[0], ws[0]), (plan, bs[1], ys[1], ws[1]),
                  (plan, bs[2], ys[2]), (plan, bs[3], ys[3], ws[3])], stream=s1.value)
         ex2.run([(plan, bs[4], ys[4], ws[4])], stream=s2.value)
-        gpu.synchronize()
+        # non-blocking streams: the legacy stream's synchronize does not cover them
+        gpu.synchronize(s1.value)
+        gpu.synchronize(s2.value)
         for i, (y, w) in enumerate(zip(ys, want)):
             assert np.array_equal(_bits(y.to_host()), _bits(w)), (rep, i)
     code = C.c_int(0)
