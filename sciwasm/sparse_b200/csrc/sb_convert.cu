@@ -10,6 +10,8 @@
 // payload is the original position, so equal keys keep their COO order.
 #include <algorithm>
 
+#include <climits>
+
 #include "sb_common.cuh"
 #include "sb_prims.cuh"
 
@@ -106,7 +108,11 @@ __global__ void mark_diagonals(const int* __restrict__ row_ptr, const int* __res
   if (i >= N) return;
   for (int j = row_ptr[i]; j < row_ptr[i + 1]; ++j) {
     const int c = col[j];
-    if (c >= 0 && c < N) ind[(long long)N + c - i - 1] = 1;
+    if (c < 0 || c >= N) continue;
+    // every row of a band marks the same few flags: store only while the
+    // flag reads 0 (a stale 0 costs one more idempotent store)
+    int* f = ind + ((long long)N + c - i - 1);
+    if (*f == 0) *f = 1;
   }
 }
 
@@ -117,6 +123,57 @@ __global__ void compact_diagonals(const int* __restrict__ present, const int* __
   const long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= nd_all) return;
   if (present[d]) offset[rank[d]] = (int)(d - (N - 1));
+}
+
+// csr_dia fill for at most kDiaGather diagonals: thread per row; slot k of
+// row i receives the row's LAST entry in column i + offset[k] (the
+// reference's row-major loop, :1559-1571, lets a later duplicate overwrite
+// an earlier one), else +0, so every slot is written exactly once with
+// writes coalesced across rows, and no zero fill or scatter is needed.  Rows
+// of up to kDiaRowRegs entries are held in registers.
+constexpr int kDiaGather = 64;
+constexpr int kDiaRowRegs = 16;
+
+template <typename T>
+__global__ void csr_to_dia_rows(const int* __restrict__ row_ptr, const int* __restrict__ col,
+                                const T* __restrict__ val, int N, int nd,
+                                const int* __restrict__ offset, T* __restrict__ data) {
+  __shared__ int off_s[kDiaGather];
+  for (int k = threadIdx.x; k < nd; k += blockDim.x) off_s[k] = offset[k];
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int s = row_ptr[i], e = row_ptr[i + 1];
+  if (e - s <= kDiaRowRegs) {
+    int rel[kDiaRowRegs];
+    T v[kDiaRowRegs];
+#pragma unroll
+    for (int u = 0; u < kDiaRowRegs; ++u) {
+      const bool in = s + u < e;
+      const int c = in ? col[s + u] : -1;
+      // out-of-range columns are not stored (the reference skips them)
+      rel[u] = (in && c >= 0 && c < N) ? c - i : INT_MIN;
+      v[u] = in ? val[s + u] : T(0);
+    }
+    for (int k = 0; k < nd; ++k) {
+      const int want = off_s[k];
+      T out = T(0);
+#pragma unroll
+      for (int u = 0; u < kDiaRowRegs; ++u)
+        if (rel[u] == want) out = v[u];
+      data[(long long)k * N + i] = out;
+    }
+    return;
+  }
+  for (int k = 0; k < nd; ++k) {
+    const int want = off_s[k];
+    T out = T(0);
+    for (int j = s; j < e; ++j) {
+      const int c = col[j];
+      if (c >= 0 && c < N && c - i == want) out = val[j];
+    }
+    data[(long long)k * N + i] = out;
+  }
 }
 
 // csr_dia fill: thread per row, entries in storage order so a later
@@ -371,16 +428,26 @@ int sb_csr_dia(int dtype, const int32_t* row_ptr, const int32_t* col, const void
   const long long nall = 2LL * N - 1;
   compact_diagonals<<<grid_for(nall), kThreads, 0, st>>>(present, rank, nall, N, offset);
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess)
-    e = cudaMemsetAsync(data, 0, dtype_size(dtype) * (size_t)nd * (size_t)stride, st);
-  if (e == cudaSuccess) {
+  if (e == cudaSuccess && nd <= kDiaGather) {
+    // gather: every slot written once (stride == N)
     if (dtype == SB_F32)
-      csr_to_dia<float><<<grid_for(N), kThreads, 0, st>>>(row_ptr, col, (const float*)val, N,
-                                                          stride, rank, (float*)data);
+      csr_to_dia_rows<float><<<grid_for(N), kThreads, 0, st>>>(
+          row_ptr, col, (const float*)val, N, nd, offset, (float*)data);
     else
-      csr_to_dia<double><<<grid_for(N), kThreads, 0, st>>>(row_ptr, col, (const double*)val, N,
-                                                           stride, rank, (double*)data);
+      csr_to_dia_rows<double><<<grid_for(N), kThreads, 0, st>>>(
+          row_ptr, col, (const double*)val, N, nd, offset, (double*)data);
     e = cudaGetLastError();
+  } else if (e == cudaSuccess) {
+    e = cudaMemsetAsync(data, 0, dtype_size(dtype) * (size_t)nd * (size_t)stride, st);
+    if (e == cudaSuccess) {
+      if (dtype == SB_F32)
+        csr_to_dia<float><<<grid_for(N), kThreads, 0, st>>>(row_ptr, col, (const float*)val, N,
+                                                            stride, rank, (float*)data);
+      else
+        csr_to_dia<double><<<grid_for(N), kThreads, 0, st>>>(row_ptr, col, (const double*)val, N,
+                                                             stride, rank, (double*)data);
+      e = cudaGetLastError();
+    }
   }
   scratch_free(present, st);
   if (e != cudaSuccess) return cuda_status(e, "sb_csr_dia");
