@@ -104,15 +104,24 @@ __global__ void csr_to_ell(const int* __restrict__ row_ptr, const int* __restric
 // reference (:1498); stores of 1 from several threads are benign.
 __global__ void mark_diagonals(const int* __restrict__ row_ptr, const int* __restrict__ col, int N,
                                int* __restrict__ ind) {
+  // every row of a band marks the same few flags: a block keeps the flags
+  // it set in a small direct-mapped cache and stores only on a miss (a race
+  // on a slot costs at most one more idempotent store); random columns miss
+  // and store as before, with no load of the flag in front of the store
+  __shared__ long long seen[64];
+  for (int t = threadIdx.x; t < 64; t += blockDim.x) seen[t] = -1;
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   for (int j = row_ptr[i]; j < row_ptr[i + 1]; ++j) {
     const int c = col[j];
     if (c < 0 || c >= N) continue;
-    // every row of a band marks the same few flags: store only while the
-    // flag reads 0 (a stale 0 costs one more idempotent store)
-    int* f = ind + ((long long)N + c - i - 1);
-    if (*f == 0) *f = 1;
+    const long long d = (long long)N + c - i - 1;
+    long long* slot = seen + (d & 63);
+    if (*(volatile long long*)slot != d) {
+      ind[d] = 1;
+      *(volatile long long*)slot = d;
+    }
   }
 }
 
