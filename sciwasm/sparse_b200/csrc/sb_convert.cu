@@ -101,26 +101,41 @@ __global__ void csr_to_ell(const int* __restrict__ row_ptr, const int* __restric
 }
 
 // Presence of diagonal c - i, stored at index N + c - i - 1 as in the
-// reference (:1498); stores of 1 from several threads are benign.
-__global__ void mark_diagonals(const int* __restrict__ row_ptr, const int* __restrict__ col, int N,
-                               int* __restrict__ ind) {
-  // every row of a band marks the same few flags: a block keeps the flags
-  // it set in a small direct-mapped cache and stores only on a miss (a race
-  // on a slot costs at most one more idempotent store); random columns miss
-  // and store as before, with no load of the flag in front of the store
-  __shared__ long long seen[64];
-  for (int t = threadIdx.x; t < 64; t += blockDim.x) seen[t] = -1;
-  __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+// reference (:1498); stores of 1 from several threads are benign.  Rows
+// [r0, r1).  CHECK: a flag is stored only while it reads 0 (a stale 0 costs
+// one more idempotent store).  Every row of a band marks the same few
+// flags, and those repeated stores to a handful of addresses dominated a
+// 4M-row band's conversion (csr_dia 1.17 -> 0.56 ms with the check); with
+// random columns the check is a load round trip in front of every store
+// (a 2M-row power-law num_diags 0.39 -> 0.90 ms), so it is used only where
+// a prefix of the rows spans few diagonals.  SPAN: the prefix pass, which
+// also reduces the smallest and largest N + c - i it marks into span[0]
+// (min) and span[1] (max): one reduction per warp, no returning atomics.
+template <bool CHECK, bool SPAN>
+__global__ void mark_diagonals(const int* __restrict__ row_ptr, const int* __restrict__ col,
+                               int N, int r0, int r1, int* __restrict__ ind,
+                               unsigned* __restrict__ span) {
+  const int i = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r1) return;
+  unsigned lo = 0xffffffffu, hi = 0;
   for (int j = row_ptr[i]; j < row_ptr[i + 1]; ++j) {
     const int c = col[j];
     if (c < 0 || c >= N) continue;
     const long long d = (long long)N + c - i - 1;
-    long long* slot = seen + (d & 63);
-    if (*(volatile long long*)slot != d) {
-      ind[d] = 1;
-      *(volatile long long*)slot = d;
+    int* f = ind + d;
+    if (!CHECK || *f == 0) *f = 1;
+    if (SPAN) {
+      lo = min(lo, (unsigned)d);
+      hi = max(hi, (unsigned)d);
+    }
+  }
+  if (SPAN) {
+    const unsigned m = __activemask();
+    lo = __reduce_min_sync(m, lo);
+    hi = __reduce_max_sync(m, hi);
+    if ((threadIdx.x & 31) == __ffs(m) - 1) {
+      atomicMin(span, lo);
+      atomicMax(span + 1, hi);
     }
   }
 }
@@ -283,16 +298,40 @@ static int coo_csr_impl(const int* row, const int* col, const T* val, int N, lon
   return r;
 }
 
+constexpr int kDiaPrefixRows = 4096;   // rows of the counting prefix pass
+constexpr int kDiaFewDiagonals = 64;   // prefix span below this many diagonals: check before storing
+
 static int num_diags_impl(const int* row_ptr, const int* col, int N, int** present_out,
                           int** rank_out, int* nd, cudaStream_t st) {
   const long long nall = 2LL * N - 1;
   int* present = nullptr;
-  int r = scratch_alloc((void**)&present, sizeof(int) * (size_t)(2 * nall + 1), st);
+  int r = scratch_alloc((void**)&present, sizeof(int) * (size_t)(2 * nall + 2), st);
   if (r) return r;
   int* rank = present + nall;
+  unsigned* span = reinterpret_cast<unsigned*>(rank + nall);  // the allocation's last 2 ints
   SB_CHECK_CUDA(cudaMemsetAsync(present, 0, sizeof(int) * (size_t)nall, st));
-  mark_diagonals<<<grid_for(N), kThreads, 0, st>>>(row_ptr, col, N, present);
+  SB_CHECK_CUDA(cudaMemsetAsync(span, 0xff, sizeof(unsigned), st));
+  SB_CHECK_CUDA(cudaMemsetAsync(span + 1, 0, sizeof(unsigned), st));
+  // a prefix of the rows, measuring the span of the diagonals it marks: a
+  // narrow span (a band) makes the rest check before storing, a wide one
+  // store plainly
+  const int pre = std::min(N, kDiaPrefixRows);
+  mark_diagonals<false, true><<<grid_for(pre), kThreads, 0, st>>>(row_ptr, col, N, 0, pre,
+                                                                  present, span);
   SB_CHECK_LAUNCH("mark_diagonals");
+  unsigned hs[2] = {0xffffffffu, 0};
+  SB_CHECK_CUDA(cudaMemcpyAsync(hs, span, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  SB_CHECK_CUDA(cudaStreamSynchronize(st));
+  if (N > pre) {
+    const bool narrow = hs[1] >= hs[0] && hs[1] - hs[0] < (unsigned)kDiaFewDiagonals;
+    if (narrow)
+      mark_diagonals<true, false><<<grid_for(N - pre), kThreads, 0, st>>>(row_ptr, col, N, pre, N,
+                                                                        present, span);
+    else
+      mark_diagonals<false, false><<<grid_for(N - pre), kThreads, 0, st>>>(row_ptr, col, N, pre,
+                                                                         N, present, span);
+    SB_CHECK_LAUNCH("mark_diagonals");
+  }
   r = prim::exclusive_scan(present, rank, nall, st);
   if (r) {
     scratch_free(present, st);
