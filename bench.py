@@ -1085,6 +1085,35 @@ def run_batched(stream, peak, n_mats=512, seed=5):
     for storage in ("f32", "bf16"):
         out[storage]["of_gather_floor"] = round(floor / out[storage]["ms"], 3)
     del cat_col, cat_val, cat_x
+    # the floor with each matrix's right-hand sides: per K, one
+    # sb_gather_dot_rows over the matrices with K right-hand sides, which
+    # gathers a K-value x row per nonzero with the batch kernel's loads
+    rows_floor, by_k = 0.0, {}
+    for K in sorted(set(int(k) for k in ks)):
+        idx = [i for i in range(n_mats) if int(ks[i]) == K]
+        offs_k = np.concatenate([[0], np.cumsum([int(Ns[i]) for i in idx])[:-1]])
+        cc = torch.cat([mats[i]._torch[1] + int(o) for i, o in zip(idx, offs_k)])
+        vv = torch.cat([mats[i]._torch[2] for i in idx])
+        xx = torch.cat([xs[i] for i in idx])
+        nnz_k = int(cc.numel())
+        rows_k = int(sum(int(Ns[i]) for i in idx))
+
+        def rows_fn():
+            _lib.call("sb_gather_dot_rows", _lib.SB_F32, cc.data_ptr(), vv.data_ptr(),
+                      xx.data_ptr(), rows_k, K, nnz_k, dot.ptr, sp)
+        for _ in range(3):
+            rows_fn()
+        t = _time_each_ms(stream, rows_fn, 10)
+        by_k[str(K)] = round(t, 4)
+        rows_floor += t
+        del cc, vv, xx
+    out["gather_floor_rows_ms"] = round(rows_floor, 4)
+    out["gather_floor_rows_by_k_ms"] = by_k
+    out["gather_floor_rows"] = ("per number of right-hand sides K, sb_gather_dot_rows over those "
+                                "matrices' col/val (FP32) gathering one K-value x row per nonzero "
+                                "with the batch kernel's loads; no rows, no y; the sum over K")
+    for storage in ("f32", "bf16"):
+        out[storage]["of_gather_floor_rows"] = round(rows_floor / out[storage]["ms"], 3)
     return out
 
 

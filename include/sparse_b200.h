@@ -200,6 +200,16 @@ int sb_csr_coo(int dtype, const int32_t* row_ptr, const int32_t* col, const void
 int sb_gather_dot(int dtype, const int32_t* col, const void* val, const void* x, int64_t nnz,
                   double* out, void* stream);
 
+/* The gather floor of several right-hand sides (no counterpart in the
+ * reference): *out = sum over k of val[k] * (sum over h < nrhs of
+ * x[col[k]*nrhs + h]), x holding x_rows rows of nrhs values (row-major, as
+ * sb_batch_item's x).  It streams col and val and gathers each entry's x row
+ * with the loads the batched SpMV uses, nothing else: the floor of a batched
+ * SpMV over the same entries.  dtype SB_F32, SB_F64, or SB_BF16 (bf16 values,
+ * f32 x).  out is a device double. */
+int sb_gather_dot_rows(int dtype, const int32_t* col, const void* val, const void* x,
+                       int64_t x_rows, int32_t nrhs, int64_t nnz, double* out, void* stream);
+
 /* Reduced-precision storage (no counterpart in the reference, which keeps
  * f32 or f64 values): sb_spmv_csr / sb_spmv_csr_ex accept dtype SB_BF16 for
  * BF16-stored values with f32 x, y and f32 accumulation (long rows use

@@ -160,6 +160,7 @@ SIGNATURES.update({
     "sb_convert_values": [C.c_int, P, C.c_int, P, I64, P],
     "sb_spmv_csr_ex": [C.c_int, P, P, P, P, P, I32, I64, I32, C.POINTER(CsrOpts), P],
     "sb_gather_dot": [C.c_int, P, P, P, I64, P, P],
+    "sb_gather_dot_rows": [C.c_int, P, P, P, I64, I32, I64, P, P],
     "sb_spmv_autotune": [C.c_int, P, P, P, P, I32, I64, I32, I32, C.POINTER(SpmvChoice), P],
     "sb_csr_coo": [C.c_int, P, P, P, I32, I64, P, P, P, P],
     "sb_csr_autotune": [C.c_int, P, P, P, P, I32, I64, I32, C.POINTER(CsrOpts),

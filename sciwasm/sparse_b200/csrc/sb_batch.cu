@@ -714,6 +714,87 @@ static void exec_release(sb_batch_exec* e) {
   delete e;
 }
 
+// The gather floor of several right-hand sides: sum over entries of
+// val[k] * (sum over h of x[col[k]*K + h]), streaming col and val (8
+// entries per thread, coalesced) and gathering each entry's K-value x row
+// with the loaders of the batch kernel (aligned vectors, covering 16-byte
+// blocks, or one 256-bit load for 8 FP32 values with x 32-byte aligned);
+// no row structure and no y.  The floor a batched SpMV over the same
+// entries and right-hand sides is measured against.
+template <typename SV, typename T, int K, bool VEC, bool X32>
+__global__ void __launch_bounds__(256)
+    gather_rows_kernel(const int* __restrict__ col, const SV* __restrict__ val,
+                       const T* __restrict__ x, long long x_rows, long long nnz,
+                       double* __restrict__ out) {
+  constexpr int kItems = 8;
+  const long long nthreads = (long long)gridDim.x * blockDim.x;
+  const T* __restrict__ xend = x + x_rows * K;
+  T acc = 0;
+  for (long long k0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * kItems; k0 < nnz;
+       k0 += nthreads * kItems) {
+    int c[kItems];
+    T v[kItems];
+#pragma unroll
+    for (int e = 0; e < kItems; ++e) {
+      c[e] = k0 + e < nnz ? ld_reuse(col + k0 + e) : 0;
+      v[e] = k0 + e < nnz ? (T)ldv(val, k0 + e) : (T)0;
+    }
+#pragma unroll
+    for (int e = 0; e < kItems; ++e) {
+      if (k0 + e < nnz) {
+        T xv[K];
+        if constexpr (VEC) {
+          load_xrow_any<T, K, X32>(x + (long long)c[e] * K, xend, xv);
+        } else {
+#pragma unroll
+          for (int h = 0; h < K; ++h) xv[h] = __ldg(x + (long long)c[e] * K + h);
+        }
+        T t = 0;
+#pragma unroll
+        for (int h = 0; h < K; ++h) t += xv[h];
+        acc += v[e] * t;
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, (double)acc);
+}
+
+template <typename SV, typename T, int K>
+static void launch_gather_rows(const int* col, const void* val, const void* x, long long x_rows,
+                               long long nnz, double* out, cudaStream_t st) {
+  const uintptr_t xa = reinterpret_cast<uintptr_t>(x);
+  const bool vec = (xa & 15u) == 0, x32 = (xa & 31u) == 0;
+  const long long steps = (nnz + 7) / 8;
+  const unsigned ctas = (unsigned)std::max(
+      1LL, std::min((steps + 255) / 256, (long long)sm_count() * 8));
+  if (vec && x32 && K == 8 && sizeof(T) == 4)
+    gather_rows_kernel<SV, T, K, true, true><<<ctas, 256, 0, st>>>(
+        col, (const SV*)val, (const T*)x, x_rows, nnz, out);
+  else if (vec)
+    gather_rows_kernel<SV, T, K, true, false><<<ctas, 256, 0, st>>>(
+        col, (const SV*)val, (const T*)x, x_rows, nnz, out);
+  else
+    gather_rows_kernel<SV, T, K, false, false><<<ctas, 256, 0, st>>>(
+        col, (const SV*)val, (const T*)x, x_rows, nnz, out);
+}
+
+template <typename SV, typename T>
+static void gather_rows_k(int K, const int* col, const void* val, const void* x,
+                          long long x_rows, long long nnz, double* out, cudaStream_t st) {
+  switch (K) {
+    case 1: launch_gather_rows<SV, T, 1>(col, val, x, x_rows, nnz, out, st); break;
+    case 2: launch_gather_rows<SV, T, 2>(col, val, x, x_rows, nnz, out, st); break;
+    case 3: launch_gather_rows<SV, T, 3>(col, val, x, x_rows, nnz, out, st); break;
+    case 4: launch_gather_rows<SV, T, 4>(col, val, x, x_rows, nnz, out, st); break;
+    case 5: launch_gather_rows<SV, T, 5>(col, val, x, x_rows, nnz, out, st); break;
+    case 6: launch_gather_rows<SV, T, 6>(col, val, x, x_rows, nnz, out, st); break;
+    case 7: launch_gather_rows<SV, T, 7>(col, val, x, x_rows, nnz, out, st); break;
+    default: launch_gather_rows<SV, T, 8>(col, val, x, x_rows, nnz, out, st); break;
+  }
+}
+
 }  // namespace sb
 
 using namespace sb;
@@ -840,6 +921,30 @@ int sb_batch_exec_run(sb_batch_exec* e, const sb_batch_item* items, int32_t n, v
   SB_CHECK_CUDA(cudaEventRecord(b.done, st));
   b.pending = true;
   e->next ^= 1;
+  return SB_OK;
+}
+
+int sb_gather_dot_rows(int dtype, const int32_t* col, const void* val, const void* x,
+                       int64_t x_rows, int32_t nrhs, int64_t nnz, double* out, void* stream) {
+  SB_TRACE("sb_gather_dot_rows");
+  SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64 || dtype == SB_BF16,
+             "sb_gather_dot_rows: bad dtype");
+  SB_REQUIRE(nrhs >= 1 && nrhs <= kMaxRhs && nnz >= 0 && x_rows >= 0,
+             "sb_gather_dot_rows: 1 <= nrhs <= 8 and non-negative sizes required");
+  SB_REQUIRE(out, "sb_gather_dot_rows: null output");
+  int r = ensure_device();
+  if (r) return r;
+  cudaStream_t st = as_stream(stream);
+  SB_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(double), st));
+  if (nnz == 0) return SB_OK;
+  SB_REQUIRE(col && val && x, "sb_gather_dot_rows: null pointer");
+  if (dtype == SB_F64)
+    gather_rows_k<double, double>(nrhs, col, val, x, x_rows, nnz, out, st);
+  else if (dtype == SB_BF16)
+    gather_rows_k<__nv_bfloat16, float>(nrhs, col, val, x, x_rows, nnz, out, st);
+  else
+    gather_rows_k<float, float>(nrhs, col, val, x, x_rows, nnz, out, st);
+  SB_CHECK_LAUNCH("gather_rows_kernel");
   return SB_OK;
 }
 

@@ -188,3 +188,30 @@ def test_batch_mixed_formats(gpu, oracle, storage):
             gpu.spmv(M, xv, yv)
             assert np.array_equal(yv.array().view(np.uint8),
                                   np.ascontiguousarray(Y[:, 0]).view(np.uint8)), fmt
+
+
+@pytest.mark.parametrize("x_shift", ["none", "16B", "value"])
+def test_gather_dot_rows_floor(gpu, x_shift):
+    """sb_gather_dot_rows sums val[k] * (x row of col[k]) for 1..8 values per
+    row with the batch kernel's loads (32-byte, 16-byte and unaligned x)."""
+    import ctypes as C
+    from sciwasm.sparse_b200 import _lib
+    rng = np.random.default_rng(9)
+    rows, nnz = 3001, 20_011
+    col = rng.integers(0, rows, nnz).astype(np.int32)
+    col[-1] = rows - 1  # the last x row, whose covering blocks would pass x's end
+    val = rng.uniform(-1, 1, nnz).astype(np.float32)
+    cd, vd = gpu.DeviceArray.from_host(col), gpu.DeviceArray.from_host(val)
+    out = gpu.DeviceArray(1, np.float64)
+    for K in range(1, 9):
+        X = rng.uniform(-1, 1, rows * K).astype(np.float32)
+        pad = {"none": 0, "16B": 4, "value": 1}[x_shift]
+        base = gpu.DeviceArray.from_host(np.concatenate([np.zeros(pad, np.float32), X]))
+        xptr = base.ptr + 4 * pad
+        _lib.call("sb_gather_dot_rows", _lib.SB_F32, cd.ptr, vd.ptr, xptr, rows, K, nnz,
+                  out.ptr, None)
+        gpu.synchronize()
+        got = float(out.to_host()[0])
+        want = float(np.dot(val.astype(np.float64),
+                            X.astype(np.float64).reshape(rows, K).sum(axis=1)[col]))
+        assert abs(got - want) <= 1e-4 * max(1.0, np.sum(np.abs(val))), (K, got, want)
