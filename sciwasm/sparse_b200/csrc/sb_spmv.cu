@@ -1134,6 +1134,75 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// BF16 data, up to 16 diagonals: two adjacent rows per thread (rows 2j and
+// 2j+1), so that one 4-byte load brings both rows' values of a diagonal
+// (with stride == N and N even the pair is 4-byte aligned in every
+// diagonal), y moves as a float2 and x as a float2 where i + k is even.
+// One row per thread with 2-byte loads left too few bytes in flight (ncu,
+// 5-point Laplacian 4096^2: DRAM 43% of peak, long-scoreboard stalls 17.8
+// per issue at 85% warps active).  A pair with a row outside the band's
+// full range takes dia_rows_nd's per-row form.  Every row is computed as in
+// dia_rows_nd (bit-identical: a bf16 value widens to f32 by a 16-bit shift).
+template <int ND>
+__global__ void __launch_bounds__(256)
+    dia_rows_pair_bf16(const int* __restrict__ offset, const __nv_bfloat16* __restrict__ data,
+                       int N, const float* __restrict__ x, float* __restrict__ y) {
+  int k[ND];
+  int kmin = 0x7fffffff, kmax = -0x7fffffff - 1;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    k[d] = __ldg(offset + d);
+    kmin = min(kmin, k[d]);
+    kmax = max(kmax, k[d]);
+  }
+  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= N) return;
+  if ((long long)i + kmin >= 0 && (long long)i + 1 + kmax < N) {
+    float2 t = *reinterpret_cast<const float2*>(y + i);
+    float a0[ND], a1[ND], b0[ND], b1[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const unsigned w = (unsigned)ld_stream(
+          reinterpret_cast<const int*>(data + (long long)d * N + i));
+      a0[d] = __uint_as_float(w << 16);
+      a1[d] = __uint_as_float(w & 0xffff0000u);
+      if ((k[d] & 1) == 0) {
+        const float2 xv = __ldg(reinterpret_cast<const float2*>(x + i + k[d]));
+        b0[d] = xv.x;
+        b1[d] = xv.y;
+      } else {
+        b0[d] = ld_ro(x + i + k[d]);
+        b1[d] = ld_ro(x + i + 1 + k[d]);
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      t.x = add_rn(mul_rn(a0[d], b0[d]), t.x);
+      t.y = add_rn(mul_rn(a1[d], b1[d]), t.y);
+    }
+    *reinterpret_cast<float2*>(y + i) = t;
+    return;
+  }
+#pragma unroll 1
+  for (int r = i; r < i + 2 && r < N; ++r) {
+    float t = y[r];
+    float a[ND], b[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const bool in = (unsigned)(r + k[d]) < (unsigned)N;
+      a[d] = in ? ld_val(data + (long long)d * N + r) : 0.f;
+      b[d] = in ? ld_ro(x + r + k[d]) : 0.f;
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const bool in = (unsigned)(r + k[d]) < (unsigned)N;
+      const float p = mul_rn(a[d], b[d]);
+      t = in ? add_rn(p, t) : t;
+    }
+    y[r] = t;
+  }
+}
+
 template <typename SV, typename T>
 static void launch_dia(const int* offset, const SV* data, int N, int nd, int stride, const T* x,
                        T* y, cudaStream_t st) {
@@ -1155,6 +1224,28 @@ static void launch_dia(const int* offset, const SV* data, int N, int nd, int str
 #undef SB_DIA_MR
       default: break;
     }
+    }
+  }
+  if constexpr (sizeof(SV) == 2) {
+    // BF16: two rows per thread where the pair loads are aligned
+    const bool pair_ok = nd >= 1 && nd <= 16 && stride == N && (N % 2) == 0 &&
+                         (reinterpret_cast<uintptr_t>(data) & 3u) == 0 &&
+                         (reinterpret_cast<uintptr_t>(x) & 7u) == 0 &&
+                         (reinterpret_cast<uintptr_t>(y) & 7u) == 0;
+    if (pair_ok) {
+      const unsigned pblocks = (unsigned)((N / 2 + 255) / 256);
+      switch (nd) {
+#define SB_DIA_PAIR(n)                                                                   \
+  case n:                                                                                \
+    dia_rows_pair_bf16<n><<<pblocks, 256, 0, st>>>(offset, data, N, x, y);             \
+    return;
+        SB_DIA_PAIR(1) SB_DIA_PAIR(2) SB_DIA_PAIR(3) SB_DIA_PAIR(4) SB_DIA_PAIR(5)
+        SB_DIA_PAIR(6) SB_DIA_PAIR(7) SB_DIA_PAIR(8) SB_DIA_PAIR(9) SB_DIA_PAIR(10)
+        SB_DIA_PAIR(11) SB_DIA_PAIR(12) SB_DIA_PAIR(13) SB_DIA_PAIR(14) SB_DIA_PAIR(15)
+        SB_DIA_PAIR(16)
+#undef SB_DIA_PAIR
+        default: break;
+      }
     }
   }
   switch (nd) {
