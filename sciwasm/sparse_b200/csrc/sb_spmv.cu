@@ -1134,19 +1134,31 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// BF16 data, up to 16 diagonals: two adjacent rows per thread (rows 2j and
-// 2j+1), so that one 4-byte load brings both rows' values of a diagonal
-// (with stride == N and N even the pair is 4-byte aligned in every
-// diagonal), y moves as a float2 and x as a float2 where i + k is even.
+// BF16 or FP32 data with f32 vectors, up to 16 diagonals: two adjacent rows
+// per thread (rows 2j and 2j+1), so that one 4- or 8-byte load brings both
+// rows' values of a diagonal (with stride == N and N even the pair is
+// aligned in every diagonal), y moves as a float2 and x as a float2 where
+// i + k is even.
 // One row per thread with 2-byte loads left too few bytes in flight (ncu,
 // 5-point Laplacian 4096^2: DRAM 43% of peak, long-scoreboard stalls 17.8
 // per issue at 85% warps active).  A pair with a row outside the band's
 // full range takes dia_rows_nd's per-row form.  Every row is computed as in
 // dia_rows_nd (bit-identical: a bf16 value widens to f32 by a 16-bit shift).
-template <int ND>
+__device__ __forceinline__ void ld_pair(const __nv_bfloat16* p, float& a0, float& a1) {
+  const unsigned w = (unsigned)ld_stream(reinterpret_cast<const int*>(p));
+  a0 = __uint_as_float(w << 16);
+  a1 = __uint_as_float(w & 0xffff0000u);
+}
+__device__ __forceinline__ void ld_pair(const float* p, float& a0, float& a1) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+  a0 = v.x;
+  a1 = v.y;
+}
+
+template <typename SV, int ND>
 __global__ void __launch_bounds__(256)
-    dia_rows_pair_bf16(const int* __restrict__ offset, const __nv_bfloat16* __restrict__ data,
-                       int N, const float* __restrict__ x, float* __restrict__ y) {
+    dia_rows_pair(const int* __restrict__ offset, const SV* __restrict__ data,
+                  int N, const float* __restrict__ x, float* __restrict__ y) {
   int k[ND];
   int kmin = 0x7fffffff, kmax = -0x7fffffff - 1;
 #pragma unroll
@@ -1162,10 +1174,7 @@ __global__ void __launch_bounds__(256)
     float a0[ND], a1[ND], b0[ND], b1[ND];
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
-      const unsigned w = (unsigned)ld_stream(
-          reinterpret_cast<const int*>(data + (long long)d * N + i));
-      a0[d] = __uint_as_float(w << 16);
-      a1[d] = __uint_as_float(w & 0xffff0000u);
+      ld_pair(data + (long long)d * N + i, a0[d], a1[d]);
       if ((k[d] & 1) == 0) {
         const float2 xv = __ldg(reinterpret_cast<const float2*>(x + i + k[d]));
         b0[d] = xv.x;
@@ -1190,7 +1199,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
       const bool in = (unsigned)(r + k[d]) < (unsigned)N;
-      a[d] = in ? ld_val(data + (long long)d * N + r) : 0.f;
+      a[d] = in ? (float)ld_val(data + (long long)d * N + r) : 0.f;
       b[d] = in ? ld_ro(x + r + k[d]) : 0.f;
     }
 #pragma unroll
@@ -1207,10 +1216,34 @@ template <typename SV, typename T>
 static void launch_dia(const int* offset, const SV* data, int N, int nd, int stride, const T* x,
                        T* y, cudaStream_t st) {
   const unsigned blocks = (unsigned)((N + 255) / 256);
-  // few diagonals of 4-byte values: 4 rows per thread (2 for 5..8); the row
-  // index stays 32-bit (N < 2^31 and the grid covers N rows).  Measured on
-  // B200, 5-point Laplacian 4096^2: FP32 0.1068 -> 0.1006 ms; BF16 data
-  // 0.1016 -> 0.3035 ms, so 2-byte values keep one row per thread.
+  if constexpr (sizeof(T) == 4) {
+    // BF16 / FP32 data: two rows per thread where the pair loads are aligned
+    const bool pair_ok = nd >= 1 && nd <= 16 && stride == N && (N % 2) == 0 &&
+                         (reinterpret_cast<uintptr_t>(data) & (2 * sizeof(SV) - 1)) == 0 &&
+                         (reinterpret_cast<uintptr_t>(x) & 7u) == 0 &&
+                         (reinterpret_cast<uintptr_t>(y) & 7u) == 0;
+    if (pair_ok) {
+      const unsigned pblocks = (unsigned)((N / 2 + 255) / 256);
+      switch (nd) {
+#define SB_DIA_PAIR(n)                                                                   \
+  case n:                                                                                \
+    dia_rows_pair<SV, n><<<pblocks, 256, 0, st>>>(offset, data, N, x, y);              \
+    return;
+        SB_DIA_PAIR(1) SB_DIA_PAIR(2) SB_DIA_PAIR(3) SB_DIA_PAIR(4) SB_DIA_PAIR(5)
+        SB_DIA_PAIR(6) SB_DIA_PAIR(7) SB_DIA_PAIR(8) SB_DIA_PAIR(9) SB_DIA_PAIR(10)
+        SB_DIA_PAIR(11) SB_DIA_PAIR(12) SB_DIA_PAIR(13) SB_DIA_PAIR(14) SB_DIA_PAIR(15)
+        SB_DIA_PAIR(16)
+#undef SB_DIA_PAIR
+        default: break;
+      }
+    }
+  }
+  // few diagonals of 4-byte values where the pair form does not apply: 4
+  // rows per thread (2 for 5..8), strided by 256; the row index stays
+  // 32-bit (N < 2^31 and the grid covers N rows).  Measured on B200,
+  // 5-point Laplacian 4096^2: FP32 0.1068 (one row per thread) -> 0.1006
+  // (this form) -> 0.0823 ms (the pair form); BF16 data 0.1016 -> 0.3035 ms
+  // in this form, 0.0802 ms in the pair form.
   if constexpr (sizeof(SV) == 4) {
     if (nd <= 8 && (long long)N + 256LL * 4 < 0x7fffffffLL) {
     switch (nd) {
@@ -1224,28 +1257,6 @@ static void launch_dia(const int* offset, const SV* data, int N, int nd, int str
 #undef SB_DIA_MR
       default: break;
     }
-    }
-  }
-  if constexpr (sizeof(SV) == 2) {
-    // BF16: two rows per thread where the pair loads are aligned
-    const bool pair_ok = nd >= 1 && nd <= 16 && stride == N && (N % 2) == 0 &&
-                         (reinterpret_cast<uintptr_t>(data) & 3u) == 0 &&
-                         (reinterpret_cast<uintptr_t>(x) & 7u) == 0 &&
-                         (reinterpret_cast<uintptr_t>(y) & 7u) == 0;
-    if (pair_ok) {
-      const unsigned pblocks = (unsigned)((N / 2 + 255) / 256);
-      switch (nd) {
-#define SB_DIA_PAIR(n)                                                                   \
-  case n:                                                                                \
-    dia_rows_pair_bf16<n><<<pblocks, 256, 0, st>>>(offset, data, N, x, y);             \
-    return;
-        SB_DIA_PAIR(1) SB_DIA_PAIR(2) SB_DIA_PAIR(3) SB_DIA_PAIR(4) SB_DIA_PAIR(5)
-        SB_DIA_PAIR(6) SB_DIA_PAIR(7) SB_DIA_PAIR(8) SB_DIA_PAIR(9) SB_DIA_PAIR(10)
-        SB_DIA_PAIR(11) SB_DIA_PAIR(12) SB_DIA_PAIR(13) SB_DIA_PAIR(14) SB_DIA_PAIR(15)
-        SB_DIA_PAIR(16)
-#undef SB_DIA_PAIR
-        default: break;
-      }
     }
   }
   switch (nd) {
