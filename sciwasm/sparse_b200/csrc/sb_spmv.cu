@@ -1212,6 +1212,79 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// BF16 data, up to 16 diagonals, N a multiple of 4: four adjacent rows per
+// thread, one 8-byte load of a diagonal's four values, x as a float4 where
+// i + k is a multiple of 4 (two float2 where it is even, else four
+// values), y as a float4.  A quad with a row outside the band's full range
+// takes the per-row form.  Every row is computed as in dia_rows_nd.
+template <int ND>
+__global__ void __launch_bounds__(256)
+    dia_rows_quad_bf16(const int* __restrict__ offset, const __nv_bfloat16* __restrict__ data,
+                       int N, const float* __restrict__ x, float* __restrict__ y) {
+  int k[ND];
+  int kmin = 0x7fffffff, kmax = -0x7fffffff - 1;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    k[d] = __ldg(offset + d);
+    kmin = min(kmin, k[d]);
+    kmax = max(kmax, k[d]);
+  }
+  const int i = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= N) return;
+  if ((long long)i + kmin >= 0 && (long long)i + 3 + kmax < N) {
+    float4 t = *reinterpret_cast<const float4*>(y + i);
+    float a[ND][4], b[ND][4];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const uint2 w = ld_stream_v4(reinterpret_cast<const unsigned short*>(data) +
+                                   (long long)d * N + i);
+      a[d][0] = __uint_as_float(w.x << 16);
+      a[d][1] = __uint_as_float(w.x & 0xffff0000u);
+      a[d][2] = __uint_as_float(w.y << 16);
+      a[d][3] = __uint_as_float(w.y & 0xffff0000u);
+      const float* xp = x + i + k[d];
+      if ((k[d] & 3) == 0) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(xp));
+        b[d][0] = v.x; b[d][1] = v.y; b[d][2] = v.z; b[d][3] = v.w;
+      } else if ((k[d] & 1) == 0) {
+        const float2 v0 = __ldg(reinterpret_cast<const float2*>(xp));
+        const float2 v1 = __ldg(reinterpret_cast<const float2*>(xp + 2));
+        b[d][0] = v0.x; b[d][1] = v0.y; b[d][2] = v1.x; b[d][3] = v1.y;
+      } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) b[d][u] = ld_ro(xp + u);
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      t.x = add_rn(mul_rn(a[d][0], b[d][0]), t.x);
+      t.y = add_rn(mul_rn(a[d][1], b[d][1]), t.y);
+      t.z = add_rn(mul_rn(a[d][2], b[d][2]), t.z);
+      t.w = add_rn(mul_rn(a[d][3], b[d][3]), t.w);
+    }
+    *reinterpret_cast<float4*>(y + i) = t;
+    return;
+  }
+#pragma unroll 1
+  for (int r = i; r < i + 4 && r < N; ++r) {
+    float t = y[r];
+    float av[ND], bv[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const bool in = (unsigned)(r + k[d]) < (unsigned)N;
+      av[d] = in ? ld_val(data + (long long)d * N + r) : 0.f;
+      bv[d] = in ? ld_ro(x + r + k[d]) : 0.f;
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const bool in = (unsigned)(r + k[d]) < (unsigned)N;
+      const float p = mul_rn(av[d], bv[d]);
+      t = in ? add_rn(p, t) : t;
+    }
+    y[r] = t;
+  }
+}
+
 template <typename SV, typename T>
 static void launch_dia(const int* offset, const SV* data, int N, int nd, int stride, const T* x,
                        T* y, cudaStream_t st) {
@@ -1222,6 +1295,25 @@ static void launch_dia(const int* offset, const SV* data, int N, int nd, int str
                          (reinterpret_cast<uintptr_t>(data) & (2 * sizeof(SV) - 1)) == 0 &&
                          (reinterpret_cast<uintptr_t>(x) & 7u) == 0 &&
                          (reinterpret_cast<uintptr_t>(y) & 7u) == 0;
+    if constexpr (sizeof(SV) == 2) {
+      const bool quad_ok = pair_ok && (N % 4) == 0 &&
+                           (reinterpret_cast<uintptr_t>(data) & 7u) == 0 &&
+                           (reinterpret_cast<uintptr_t>(x) & 15u) == 0 &&
+                           (reinterpret_cast<uintptr_t>(y) & 15u) == 0;
+      if (quad_ok) {
+        const unsigned qblocks = (unsigned)((N / 4 + 255) / 256);
+        switch (nd) {
+#define SB_DIA_QUAD(n)                                                                   \
+  case n:                                                                                \
+    dia_rows_quad_bf16<n><<<qblocks, 256, 0, st>>>(offset, data, N, x, y);             \
+    return;
+          SB_DIA_QUAD(1) SB_DIA_QUAD(2) SB_DIA_QUAD(3) SB_DIA_QUAD(4) SB_DIA_QUAD(5)
+          SB_DIA_QUAD(6) SB_DIA_QUAD(7) SB_DIA_QUAD(8)
+#undef SB_DIA_QUAD
+          default: break;
+        }
+      }
+    }
     if (pair_ok) {
       const unsigned pblocks = (unsigned)((N / 2 + 255) / 256);
       switch (nd) {

@@ -364,19 +364,22 @@ def test_spmv_autotune_statistics_mode(gpu, oracle):
         assert rel_err(yv.array(), oracle.truth_csr(rp, col, val, x, y0)) <= 1e-5, name
 
 
-@pytest.mark.parametrize("shape", ["laplacian_even", "laplacian_odd", "band_even"])
+@pytest.mark.parametrize("shape", ["laplacian_even", "laplacian_odd", "band_even", "band_2mod4"])
 def test_dia_bf16_storage(gpu, oracle, shape):
     """DIA with BF16 data (f32 x, y and sums): within tolerance of the FP64
     product of the stored values, and bit-identical to the batched DIA item
     on the same data (the same per-row order).  Even N takes two rows per
-    thread (offsets odd and even: scalar and paired x loads; edge pairs per
-    row), odd N one row per thread."""
+    thread, N a multiple of 4 four (offsets odd, even and multiples of 4:
+    scalar, paired and quadruple x loads; edge groups per row), odd N one
+    row per thread."""
     if shape == "laplacian_even":
         rp, col, val = synth.laplacian_2d(300, dtype=np.float32)
     elif shape == "laplacian_odd":
         rp, col, val = synth.laplacian_2d(301, dtype=np.float32)
-    else:
+    elif shape == "band_even":
         rp, col, val = synth.banded(20_000, half=5, seed=4, dtype=np.float32)
+    else:
+        rp, col, val = synth.banded(20_002, half=5, seed=4, dtype=np.float32)
     N = rp.size - 1
     D = gpu.csr_dia(gpu.csr_from_host(rp, col, val))
     Db = gpu.with_storage(D, "bf16")
