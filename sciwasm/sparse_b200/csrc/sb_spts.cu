@@ -488,7 +488,7 @@ __device__ __forceinline__ void level_row_load(LevelRow<T, A>& r, int i, const i
 // barrier is __syncthreads.
 constexpr int kLevelBlock1 = 512;  // threads of the single-block form
 
-template <typename T, typename A>
+template <typename T, typename A, bool TWO>
 __global__ void __launch_bounds__(kLevelBlock1, 1)
     spts_level_coop(const int* __restrict__ rrow, const int* __restrict__ rcol,
                     const T* __restrict__ rval, const int* __restrict__ level_ptr, int nlevels,
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(kLevelBlock1, 1)
   {
     const int r0 = __ldg(level_ptr), r1 = __ldg(level_ptr + 1);
     if (r0 + gt < r1) level_row_load(nx, r0 + gt, rrow, rcol, rval, perm, b);
-    if (nlevels > 1) {
+    if (TWO && nlevels > 1) {
       const int q0 = r1, q1 = __ldg(level_ptr + 2);
       if (q0 + gt < q1) level_head_load(hd, q0 + gt, rrow, perm);
     }
@@ -540,14 +540,21 @@ __global__ void __launch_bounds__(kLevelBlock1, 1)
       y[pi] = yi;
     }
     if (l + 1 < nlevels) {
-      // the next level's first row from the head read one level ago, and
-      // the head of the level after it: neither depends on y, so both load
-      // rounds overlap the barrier and the next level's y reads
-      level_row_from_head(nx, hd, rcol, rval, b);
-      hd.i = -1;
-      if (l + 2 < nlevels) {
-        const int q0 = __ldg(level_ptr + l + 2), q1 = __ldg(level_ptr + l + 3);
-        if (q0 + gt < q1) level_head_load(hd, q0 + gt, rrow, perm);
+      if constexpr (TWO) {
+        // the next level's first row from the head read one level ago, and
+        // the head of the level after it: neither depends on y, so both load
+        // rounds overlap the barrier and the next level's y reads
+        level_row_from_head(nx, hd, rcol, rval, b);
+        hd.i = -1;
+        if (l + 2 < nlevels) {
+          const int q0 = __ldg(level_ptr + l + 2), q1 = __ldg(level_ptr + l + 3);
+          if (q0 + gt < q1) level_head_load(hd, q0 + gt, rrow, perm);
+        }
+      } else {
+        // both rounds of the next level's first row, before the barrier
+        const int q0 = r1, q1 = __ldg(level_ptr + l + 2);
+        nx.i = -1;
+        if (q0 + gt < q1) level_row_load(nx, q0 + gt, rrow, rcol, rval, perm, b);
       }
       if (gridDim.x == 1) __syncthreads();  // one block: its barrier orders the L2 accesses
       else if (!grid_barrier(bar, gridDim.x * (unsigned)(l + 1), limit, status)) return;
@@ -1027,11 +1034,16 @@ static int solve_impl(const sb_spts_plan* p, int algo, const T* b, T* y, long lo
     // every level fits in it (no grid barrier), else blocks of kT threads for
     // the widest level, at most one per SM (fewer blocks make each barrier
     // cheaper), all of them resident
-    auto k = spts_level_coop<T, A>;
     int widest = 0;
     for (int l = 0; l < p->nlevels; ++l)
       widest = std::max(widest, p->h_level_ptr[l + 1] - p->h_level_ptr[l]);
     const int threads = widest <= kLevelBlock1 ? kLevelBlock1 : kT;
+    // the two-round prefetch except for the one-block FP32 form, where the
+    // one-round form measured faster (1M-row random factor, 3470 levels:
+    // 6.54 against 7.27 ms; FP64 10.2 -> 9.40 ms and every grid form
+    // faster with two rounds)
+    const bool two = !(threads == kLevelBlock1 && sizeof(T) == 4 && sizeof(A) == 4);
+    auto k = two ? spts_level_coop<T, A, true> : spts_level_coop<T, A, false>;
     int per = 0, coop = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, threads, 0);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, p->device);
