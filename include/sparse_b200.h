@@ -141,6 +141,26 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
                    const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
                    const sb_csr_opts* opts, void* stream);
 
+/* Row-sharded CSR SpMV with its all-gather fused into the stores (no
+ * counterpart in the reference; the parallel reference shares one y in a
+ * worker pool's memory).  The caller's rank holds rows [row_offset,
+ * row_offset + rows) of the global matrix as a CSR of `rows` rows whose
+ * columns keep their global numbers (x holds all columns).  For each of
+ * those rows t = y_in[i] + sum_j A_ij x_j is computed by the row-block kernel
+ * with `opts` (kernel 0; lanes, unroll, grid as in sb_spmv_csr_ex, so the
+ * bits equal sb_spmv_csr_ex's with the same options) and stored to
+ * dst[d][row_offset + i] for every d < ndst (1..8); rows without entries
+ * store y_in[i] unchanged.  dst (a host array) holds device pointers of
+ * full-length y buffers: this GPU's own, or other GPUs' buffers mapped for
+ * peer access (stores over NVLink; no multicast).  When every rank has run
+ * its block into every rank's buffer and the ranks have synchronised, each
+ * buffer holds the whole y.  dtype SB_F32, SB_F64, or SB_BF16 (bf16 values,
+ * f32 vectors). */
+int sb_spmv_csr_allgather(int dtype, const int32_t* row_ptr, const int32_t* col,
+                          const void* val, const void* x, const void* y_in, int32_t rows,
+                          int64_t nnz, int64_t row_offset, void* const* dst, int32_t ndst,
+                          const sb_csr_opts* opts, void* stream);
+
 /* Times the candidate kernel options around this matrix's row-length
  * statistics (reps calls each, on a scratch y) and returns the fastest in
  * *best (and its time per call in *best_ms).  Returns after timing. */

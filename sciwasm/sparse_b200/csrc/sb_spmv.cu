@@ -316,11 +316,38 @@ __device__ __forceinline__ void comp_add(T& s, T& c, T v) {
 // val is read by several consecutive load instructions: those loads
 // allocate in L1 (ld_reuse).  SV is the stored value type (f32, f64 or
 // BF16); x, y and the sums are T.
-template <typename SV, typename T, int V, int UNROLL>
+// Where the row kernel's sums go.  YOut: y itself (rows without entries
+// keep their y, as in the reference).  YScatter: the value of every row,
+// also of rows without entries (whose y is passed on unchanged), to up to 8
+// destination vectors at the row's global index -- this GPU's own buffers
+// or other GPUs' buffers mapped over NVLink (plain stores, no multicast), so
+// that a row-sharded SpMV leaves the whole y in every rank's buffer without
+// a separate all-gather.
+template <typename T>
+struct YOut {
+  static constexpr bool kAll = false;
+  T* y;
+  __device__ __forceinline__ void put(long long i, T v) const { y[i] = v; }
+};
+constexpr int kMaxScatter = 8;
+template <typename T>
+struct YScatter {
+  static constexpr bool kAll = true;
+  T* d[kMaxScatter];
+  int n;
+  long long r0;
+  __device__ __forceinline__ void put(long long i, T v) const {
+#pragma unroll
+    for (int k = 0; k < kMaxScatter; ++k)
+      if (k < n) d[k][r0 + i] = v;
+  }
+};
+
+template <typename SV, typename T, int V, int UNROLL, class Out>
 __global__ void __launch_bounds__(256)
     csr_rows_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
-                    const SV* __restrict__ val, const T* __restrict__ x, T* __restrict__ y,
-                    int N) {
+                    const SV* __restrict__ val, const T* __restrict__ x, const T* y_in,
+                    Out out, int N) {
   constexpr int RPB = kWarp / V;           // rows per batch
   constexpr int SHORT = V * UNROLL;        // a short row needs one unrolled pass
   constexpr bool COMP = sizeof(T) == 4;    // compensate long f32 sums
@@ -335,7 +362,7 @@ __global__ void __launch_bounds__(256)
     const int s_l = rr < N ? __ldg(row_ptr + rr) : 0;
     const int e_l = rr < N ? __ldg(row_ptr + rr + 1) : 0;
     const int len_l = e_l - s_l;
-    const T y_l = (rr < N && len_l > 0) ? y[rr] : (T)0;
+    const T y_l = (rr < N && (len_l > 0 || Out::kAll)) ? y_in[rr] : (T)0;
 #pragma unroll
     for (int b = 0; b < V; ++b) {
       const int j = b * RPB + g;  // row of this group within the block
@@ -361,7 +388,8 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int off = V >> 1; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
       const T yj = __shfl_sync(kFull, y_l, j);
-      if (q == 0 && len > 0 && len <= SHORT && r0 + j < N) y[r0 + j] = yj + sum;
+      if (q == 0 && len > 0 && len <= SHORT && r0 + j < N) out.put(r0 + j, yj + sum);
+      else if (Out::kAll && q == 0 && len == 0 && r0 + j < N) out.put(r0 + j, yj);
     }
     // long rows of the block: whole warp each
     unsigned longm = __ballot_sync(kFull, rr < N && len_l > SHORT);
@@ -400,7 +428,7 @@ __global__ void __launch_bounds__(256)
         }
       }
       const T yj = __shfl_sync(kFull, y_l, j);
-      if (lane == 0) y[r0 + j] = COMP ? yj + (sum + comp) : yj + sum;
+      if (lane == 0) out.put(r0 + j, COMP ? yj + (sum + comp) : yj + sum);
     }
   }
 }
@@ -409,26 +437,29 @@ __global__ void __launch_bounds__(256)
 // regular rows); grid 1: one warp per block, the hardware handing blocks to
 // SMs as they free up, so blocks holding long rows do not hold back a fixed
 // share of the others (best for skewed row lengths).
-template <typename SV, typename T, int V, int UNROLL>
-static int launch_csr_rows_v(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
-                             int N, int grid, cudaStream_t st) {
-  auto kern = csr_rows_kernel<SV, T, V, UNROLL>;
+template <typename SV, typename T, int V, int UNROLL, class Out>
+static int launch_csr_rows_v(const int* row_ptr, const int* col, const SV* val, const T* x,
+                             const T* y_in, Out out, int N, int grid, cudaStream_t st) {
+  auto kern = csr_rows_kernel<SV, T, V, UNROLL, Out>;
   const long long warps_needed = ((long long)N + kWarp - 1) / kWarp;
   const long long warps =
       grid == 1 ? warps_needed
                 : std::min(warps_needed, (long long)resident_ctas(kern, 256) * 8);
   const unsigned ctas = (unsigned)((warps + 7) / 8);
-  kern<<<ctas, 256, 0, st>>>(row_ptr, col, val, x, y, N);
+  kern<<<ctas, 256, 0, st>>>(row_ptr, col, val, x, y_in, out, N);
   SB_CHECK_LAUNCH("csr_rows_kernel");
   return SB_OK;
 }
 
-template <typename SV, typename T, int V>
-static int launch_csr_rows_u(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
-                             int N, int unroll, int grid, cudaStream_t st) {
-  if (unroll <= 2) return launch_csr_rows_v<SV, T, V, 2>(row_ptr, col, val, x, y, N, grid, st);
-  if (unroll >= 8) return launch_csr_rows_v<SV, T, V, 8>(row_ptr, col, val, x, y, N, grid, st);
-  return launch_csr_rows_v<SV, T, V, 4>(row_ptr, col, val, x, y, N, grid, st);
+template <typename SV, typename T, int V, class Out>
+static int launch_csr_rows_u(const int* row_ptr, const int* col, const SV* val, const T* x,
+                             const T* y_in, Out out, int N, int unroll, int grid,
+                             cudaStream_t st) {
+  if (unroll <= 2)
+    return launch_csr_rows_v<SV, T, V, 2>(row_ptr, col, val, x, y_in, out, N, grid, st);
+  if (unroll >= 8)
+    return launch_csr_rows_v<SV, T, V, 8>(row_ptr, col, val, x, y_in, out, N, grid, st);
+  return launch_csr_rows_v<SV, T, V, 4>(row_ptr, col, val, x, y_in, out, N, grid, st);
 }
 
 // Default lanes per row from the mean row length (about three items per lane).
@@ -440,20 +471,31 @@ static int default_lanes(int N, long long nnz) {
   return 16;
 }
 
+template <typename SV, typename T, class Out>
+static int launch_csr_rows_out(const int* row_ptr, const int* col, const SV* val, const T* x,
+                               const T* y_in, Out out, int N, long long nnz, int lanes,
+                               int unroll, int grid, cudaStream_t st) {
+  if (lanes <= 0) lanes = default_lanes(N, nnz);
+  if (unroll <= 0) unroll = 4;
+#define SB_CSR_L(v) \
+  return launch_csr_rows_u<SV, T, v>(row_ptr, col, val, x, y_in, out, N, unroll, grid, st)
+  switch (lanes) {
+    case 1: SB_CSR_L(1);
+    case 2: SB_CSR_L(2);
+    case 4: SB_CSR_L(4);
+    case 8: SB_CSR_L(8);
+    case 16: SB_CSR_L(16);
+    default: SB_CSR_L(32);
+  }
+#undef SB_CSR_L
+}
+
 template <typename SV, typename T>
 static int launch_csr_rows(const int* row_ptr, const int* col, const SV* val, const T* x, T* y,
                            int N, long long nnz, int lanes, int unroll, int grid,
                            cudaStream_t st) {
-  if (lanes <= 0) lanes = default_lanes(N, nnz);
-  if (unroll <= 0) unroll = 4;
-  switch (lanes) {
-    case 1: return launch_csr_rows_u<SV, T, 1>(row_ptr, col, val, x, y, N, unroll, grid, st);
-    case 2: return launch_csr_rows_u<SV, T, 2>(row_ptr, col, val, x, y, N, unroll, grid, st);
-    case 4: return launch_csr_rows_u<SV, T, 4>(row_ptr, col, val, x, y, N, unroll, grid, st);
-    case 8: return launch_csr_rows_u<SV, T, 8>(row_ptr, col, val, x, y, N, unroll, grid, st);
-    case 16: return launch_csr_rows_u<SV, T, 16>(row_ptr, col, val, x, y, N, unroll, grid, st);
-    default: return launch_csr_rows_u<SV, T, 32>(row_ptr, col, val, x, y, N, unroll, grid, st);
-  }
+  return launch_csr_rows_out<SV, T>(row_ptr, col, val, x, y, YOut<T>{y}, N, nnz, lanes, unroll,
+                                    grid, st);
 }
 
 // ------------------------------------------------------------ COO
@@ -1466,6 +1508,54 @@ static int check_dtype(int dtype, const char* fn) {
 using namespace sb;
 
 extern "C" {
+
+int sb_spmv_csr_allgather(int dtype, const int32_t* row_ptr, const int32_t* col,
+                          const void* val, const void* x, const void* y_in, int32_t rows,
+                          int64_t nnz, int64_t row_offset, void* const* dst, int32_t ndst,
+                          const sb_csr_opts* opts, void* stream) {
+  SB_TRACE("sb_spmv_csr_allgather");
+  SB_REQUIRE(dtype == SB_F32 || dtype == SB_F64 || dtype == SB_BF16,
+             "sb_spmv_csr_allgather: bad dtype");
+  SB_REQUIRE(rows >= 0 && nnz >= 0 && row_offset >= 0, "sb_spmv_csr_allgather: negative size");
+  SB_REQUIRE(nnz <= 0x7fffffffLL, "sb_spmv_csr_allgather: nnz exceeds int32 row_ptr range");
+  SB_REQUIRE(ndst >= 1 && ndst <= kMaxScatter && dst,
+             "sb_spmv_csr_allgather: 1 <= ndst <= 8 destinations required");
+  for (int k = 0; k < ndst; ++k) SB_REQUIRE(dst[k], "sb_spmv_csr_allgather: null destination %d", k);
+  if (opts) {
+    const int l = opts->lanes_per_row;
+    SB_REQUIRE(l == 0 || l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32,
+               "sb_spmv_csr_allgather: lanes_per_row must be 0 or a power of two <= 32");
+    SB_REQUIRE(opts->grid == 0 || opts->grid == 1, "sb_spmv_csr_allgather: grid must be 0 or 1");
+  }
+  if (rows == 0) return SB_OK;
+  SB_REQUIRE(row_ptr && y_in && (nnz == 0 || (col && val && x)),
+             "sb_spmv_csr_allgather: null pointer");
+  int r = ensure_device();
+  if (r) return r;
+  cudaStream_t st = as_stream(stream);
+  const int lanes = opts ? opts->lanes_per_row : 0, unroll = opts ? opts->unroll : 0;
+  const int grid = opts ? opts->grid : 0;
+  if (dtype == SB_F64) {
+    YScatter<double> out{};
+    for (int k = 0; k < ndst; ++k) out.d[k] = (double*)dst[k];
+    out.n = ndst;
+    out.r0 = row_offset;
+    return launch_csr_rows_out<double, double>(row_ptr, col, (const double*)val,
+                                               (const double*)x, (const double*)y_in, out, rows,
+                                               nnz, lanes, unroll, grid, st);
+  }
+  YScatter<float> out{};
+  for (int k = 0; k < ndst; ++k) out.d[k] = (float*)dst[k];
+  out.n = ndst;
+  out.r0 = row_offset;
+  if (dtype == SB_BF16)
+    return launch_csr_rows_out<__nv_bfloat16, float>(row_ptr, col, (const __nv_bfloat16*)val,
+                                                     (const float*)x, (const float*)y_in, out,
+                                                     rows, nnz, lanes, unroll, grid, st);
+  return launch_csr_rows_out<float, float>(row_ptr, col, (const float*)val, (const float*)x,
+                                           (const float*)y_in, out, rows, nnz, lanes, unroll,
+                                           grid, st);
+}
 
 int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const void* val,
                    const void* x, void* y, int32_t N, int64_t nnz, int32_t inner_max,
