@@ -1128,7 +1128,8 @@ def run_rowshard(args, rank, world, local_rank):
     import torch
     import sciwasm.sparse_b200 as sb
     from sciwasm.sparse_b200 import _lib
-    from sciwasm.sparse_b200.dist import RowShardedCSR, ShardedY, max_over_ranks
+    from sciwasm.sparse_b200.dist import PeerY, RowShardedCSR, ShardedY, max_over_ranks
+    peer = args.exchange == "peer"
     sb.load_library()
     torch.cuda.set_device(local_rank)
     _lib.call("sb_set_device", local_rank)
@@ -1140,26 +1141,44 @@ def run_rowshard(args, rank, world, local_rank):
     for j in jobs:
         sh = RowShardedCSR(j["rp"], j["col"], j["val"], rank, world)
         x = torch.from_numpy(j["x"]).to(dev)
-        y = ShardedY(sh.starts, sh.ends, rank, torch.float64, dev)
+        y = PeerY(j["N"], torch.float64, dev) if peer else \
+            ShardedY(sh.starts, sh.ends, rank, torch.float64, dev)
         xv = _vec(x)
-        yv = _vec(y.local())
+        yv = None if peer else _vec(y.local())
         tuned = sb.csr_autotune(sh.A, xv, stream=sptr) if sh.A is not None else None
         parts.append(dict(job=j, sh=sh, x=x, y=y, xv=xv, yv=yv, tuned=tuned,
                           bytes=algo_bytes("csr", j["N"], int(j["rp"][-1]), 8)))
+
+    def exchange_step(p):
+        """This rank's block SpMV and the exchange that completes y."""
+        if peer:
+            # the rows go straight into every rank's buffer, then a barrier
+            p["sh"].spmv_allgather(p["x"].data_ptr(), p["y"].rows_ptr(p["sh"].r0), p["y"].ptrs,
+                                   stream=sptr)
+            return
+        if p["sh"].A is not None:
+            sb.spmv(p["sh"].A, p["xv"], p["yv"], stream=sptr)
+
+    def exchange_finish(p):
+        if peer:
+            p["y"].barrier()
+        else:
+            p["y"].allgather()
     torch.cuda.synchronize()
     # correctness: one step from y = 0, the gathered y against an FP64 check
     errs = {}
     with torch.cuda.stream(stream):
         for p in parts:
             p["y"].buf.zero_()
-            if p["sh"].A is not None:
-                sb.spmv(p["sh"].A, p["xv"], p["yv"], stream=sptr)
-            p["y"].allgather()
+            if peer:
+                p["y"].barrier()  # every buffer zeroed before any rank stores
+            exchange_step(p)
+            exchange_finish(p)
     torch.cuda.synchronize()
     for p in parts:
         j = p["job"]
         t = truth_f64(j["rp"], j["col"], j["val"], j["x"])
-        got = p["y"].full().cpu().numpy()
+        got = (p["y"].buf if peer else p["y"].full()).cpu().numpy()
         errs[j["label"]] = float(np.max(np.abs(got - t)) / max(np.max(np.abs(t)), 1e-300))
     if max(errs.values()) > 1e-5:
         raise SystemExit(f"row-shard correctness gate failed: {errs}")
@@ -1171,11 +1190,10 @@ def run_rowshard(args, rank, world, local_rank):
         for i, p in enumerate(parts):
             if k is not None:
                 ev[k][i][0].record(stream)
-            if p["sh"].A is not None:
-                sb.spmv(p["sh"].A, p["xv"], p["yv"], stream=sptr)
+            exchange_step(p)
             if k is not None:
                 ev[k][i][1].record(stream)
-            p["y"].allgather()
+            exchange_finish(p)
             if k is not None:
                 ev[k][i][2].record(stream)
 
@@ -1204,19 +1222,23 @@ def run_rowshard(args, rank, world, local_rank):
         per[p["job"]["label"]] = {
             "rows_local": p["sh"].rows, "nnz_local": int(p["sh"].A.nnz) if p["sh"].A else 0,
             "spmv_ms_max": round(max_over_ranks(sp, device=dev), 4),
-            "allgather_ms_max": round(max_over_ranks(ag, device=dev), 4),
-            "allgather_bytes_in": p["y"].gather_bytes(),
+            "exchange_ms_max": round(max_over_ranks(ag, device=dev), 4),
+            "exchange_bytes_in": (p["sh"].N - p["sh"].rows) * 8 if peer else p["y"].gather_bytes(),
             "csr_opts": p["tuned"], "max_rel_err": errs[p["job"]["label"]]}
     if rank != 0:
         return None
     return {"world": world, "scaling": "strong",
             "workload": "format_sweep_fp64 CSR matrices (4M-row banded, 2M-row power-law, FP64) "
                         "in static_nnz row blocks, x on every rank, y all-gathered each step",
+            "exchange": ("peer: each rank's SpMV stores its rows into every rank's y buffer "
+                         "(sb_spmv_csr_allgather; symmetric memory when world > 1), then a "
+                         "barrier" if peer else "allgather: NCCL in-place all-gather of y"),
             "value_GB_s": round(total / (ms_max / 1e3) / 1e9, 1), "unit": UNIT,
             "ms_per_step": round(ms_max, 4), "algorithmic_bytes": total,
             "steps": args.steps, "warmup": args.warmup, "per_matrix": per,
             "timing": "CUDA events on the SpMV stream around the steps, max over ranks; "
-                      "the all-gather runs on NCCL's stream and the SpMV stream waits for it"}
+                      "the exchange is stream-ordered after the SpMV (NCCL's stream is waited "
+                      "for; the peer barrier runs on the SpMV stream)"}
 
 
 def _spts_cpu_baseline(rp, col, val, b, plan_levels, gpu_y, reps=3):
@@ -1561,6 +1583,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-sections", action="store_true",
                     help="skip the 4096^2 Laplacian, batched and SpTS sections")
+    ap.add_argument("--exchange", default="allgather", choices=["allgather", "peer"],
+                    help="rowshard_fp64: how y is completed on every rank")
     ap.add_argument("--e2e-streams", type=int, default=3,
                     help="streams the e2e calls rotate over")
     ap.add_argument("--serve-pool", type=int, default=2000)

@@ -132,6 +132,42 @@ class ShardedY:
         return (self.world - 1) * self.maxrows * self.buf.element_size()
 
 
+class PeerY:
+    """y of a row-sharded SpMV exchanged by the SpMV's own stores
+    (RowShardedCSR.spmv_allgather): every rank holds a full-length y buffer,
+    and each rank's kernel stores its rows into all ranks' buffers -- peers'
+    buffers mapped through a torch symmetric-memory rendezvous when the
+    world has more than one rank (stores over NVLink, no multicast), this
+    GPU's own buffer alone otherwise -- followed by the rendezvous' barrier.
+    Every run of this build has one GPU, so the world > 1 branch has not run
+    on GPUs."""
+
+    def __init__(self, N: int, dtype, device, group=None):
+        import torch
+        import torch.distributed as dist
+        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        self.hdl = None
+        if self.world > 1:
+            if self.world > 8:
+                raise ValueError("the fused exchange stores to at most 8 buffers")
+            import torch.distributed._symmetric_memory as symm
+            self.buf = symm.empty(N, dtype=dtype, device=device)
+            self.hdl = symm.rendezvous(self.buf, group or dist.group.WORLD)
+            self.ptrs = [int(q) for q in self.hdl.buffer_ptrs]
+        else:
+            self.buf = torch.zeros(N, dtype=dtype, device=device)
+            self.ptrs = [self.buf.data_ptr()]
+
+    def rows_ptr(self, r0: int) -> int:
+        """Device address of row r0 of this rank's buffer."""
+        return self.buf.data_ptr() + int(r0) * self.buf.element_size()
+
+    def barrier(self) -> None:
+        """After every rank's stores: all buffers complete (stream-ordered)."""
+        if self.hdl is not None:
+            self.hdl.barrier(channel=0)
+
+
 def max_over_ranks(value: float, device=None, group=None) -> float:
     """The largest `value` over all ranks (the time of the slowest rank)."""
     import torch

@@ -77,3 +77,13 @@ def test_two_gloo_ranks_gather_rows(oracle):
         assert np.array_equal(y_padded, full)
         assert counts[0] != counts[1]  # ragged blocks (balanced by nonzeros)
         assert nbytes == max(counts) * 8
+
+
+def test_peer_y_single_rank_layout():
+    """PeerY with one rank: its own full-length buffer is the only
+    destination, row r starts r values in, and the barrier is a no-op."""
+    import torch
+    py = dist.PeerY(1000, torch.float64, "cpu")
+    assert py.world == 1 and py.ptrs == [py.buf.data_ptr()]
+    assert py.rows_ptr(5) == py.buf.data_ptr() + 40
+    py.barrier()
