@@ -1153,8 +1153,8 @@ def run_rowshard(args, rank, world, local_rank):
         """This rank's block SpMV and the exchange that completes y."""
         if peer:
             # the rows go straight into every rank's buffer, then a barrier
-            p["sh"].spmv_allgather(p["x"].data_ptr(), p["y"].rows_ptr(p["sh"].r0), p["y"].ptrs,
-                                   stream=sptr)
+            p["sh"].spmv_allgather(p["x"].data_ptr(), p["y"].rows_ptr(p["sh"].r0),
+                                   p["y"].ptrs_dev.data_ptr(), len(p["y"].ptrs), stream=sptr)
             return
         if p["sh"].A is not None:
             sb.spmv(p["sh"].A, p["xv"], p["yv"], stream=sptr)

@@ -150,9 +150,10 @@ int sb_spmv_csr_ex(int dtype, const int32_t* row_ptr, const int32_t* col, const 
  * with `opts` (kernel 0; lanes, unroll, grid as in sb_spmv_csr_ex, so the
  * bits equal sb_spmv_csr_ex's with the same options) and stored to
  * dst[d][row_offset + i] for every d < ndst (1..8); rows without entries
- * store y_in[i] unchanged.  dst (a host array) holds device pointers of
- * full-length y buffers: this GPU's own, or other GPUs' buffers mapped for
- * peer access (stores over NVLink; no multicast).  When every rank has run
+ * store y_in[i] unchanged.  dst is a DEVICE array (8-byte aligned) of ndst
+ * device pointers of full-length y buffers: this GPU's own, or other GPUs'
+ * buffers mapped for peer access (stores over NVLink; no multicast); a
+ * caller keeps it for the life of its exchange.  When every rank has run
  * its block into every rank's buffer and the ranks have synchronised, each
  * buffer holds the whole y.  dtype SB_F32, SB_F64, or SB_BF16 (bf16 values,
  * f32 vectors). */

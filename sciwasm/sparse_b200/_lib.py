@@ -159,7 +159,7 @@ SIGNATURES.update({
     "sb_batch_exec_run": [P, C.POINTER(BatchItem), I32, P],
     "sb_convert_values": [C.c_int, P, C.c_int, P, I64, P],
     "sb_spmv_csr_ex": [C.c_int, P, P, P, P, P, I32, I64, I32, C.POINTER(CsrOpts), P],
-    "sb_spmv_csr_allgather": [C.c_int, P, P, P, P, P, I32, I64, I64, C.POINTER(P), I32,
+    "sb_spmv_csr_allgather": [C.c_int, P, P, P, P, P, I32, I64, I64, P, I32,
                               C.POINTER(CsrOpts), P],
     "sb_gather_dot": [C.c_int, P, P, P, I64, P, P],
     "sb_gather_dot_rows": [C.c_int, P, P, P, I64, I32, I64, P, P],

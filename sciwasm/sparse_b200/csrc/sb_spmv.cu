@@ -326,6 +326,7 @@ __device__ __forceinline__ void comp_add(T& s, T& c, T v) {
 template <typename T>
 struct YOut {
   static constexpr bool kAll = false;
+  static constexpr int kMinBlocks = 1;
   T* y;
   __device__ __forceinline__ void put(long long i, T v) const { y[i] = v; }
 };
@@ -333,18 +334,24 @@ constexpr int kMaxScatter = 8;
 template <typename T>
 struct YScatter {
   static constexpr bool kAll = true;
-  T* d[kMaxScatter];
+  static constexpr int kMinBlocks = 8;  // the plain kernel's 32 registers
+  const unsigned long long* d;  // device array of n destination addresses
   int n;
   long long r0;
   __device__ __forceinline__ void put(long long i, T v) const {
-#pragma unroll
-    for (int k = 0; k < kMaxScatter; ++k)
-      if (k < n) d[k][r0 + i] = v;
+    for (int k = 0; k < n; ++k) {
+      // read at each store (an L1 hit): held in registers, the 8
+      // addresses took the kernel from 32 to 48 registers and cut its
+      // resident warps from 64 to 40 per SM
+      unsigned long long a;
+      asm volatile("ld.global.nc.u64 %0, [%1];" : "=l"(a) : "l"(d + k));
+      reinterpret_cast<T*>(a)[r0 + i] = v;
+    }
   }
 };
 
 template <typename SV, typename T, int V, int UNROLL, class Out>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, Out::kMinBlocks)
     csr_rows_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
                     const SV* __restrict__ val, const T* __restrict__ x, const T* y_in,
                     Out out, int N) {
@@ -1520,7 +1527,8 @@ int sb_spmv_csr_allgather(int dtype, const int32_t* row_ptr, const int32_t* col,
   SB_REQUIRE(nnz <= 0x7fffffffLL, "sb_spmv_csr_allgather: nnz exceeds int32 row_ptr range");
   SB_REQUIRE(ndst >= 1 && ndst <= kMaxScatter && dst,
              "sb_spmv_csr_allgather: 1 <= ndst <= 8 destinations required");
-  for (int k = 0; k < ndst; ++k) SB_REQUIRE(dst[k], "sb_spmv_csr_allgather: null destination %d", k);
+  SB_REQUIRE((reinterpret_cast<uintptr_t>(dst) & 7u) == 0,
+             "sb_spmv_csr_allgather: destination array not 8-byte aligned");
   if (opts) {
     const int l = opts->lanes_per_row;
     SB_REQUIRE(l == 0 || l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32,
@@ -1535,9 +1543,10 @@ int sb_spmv_csr_allgather(int dtype, const int32_t* row_ptr, const int32_t* col,
   cudaStream_t st = as_stream(stream);
   const int lanes = opts ? opts->lanes_per_row : 0, unroll = opts ? opts->unroll : 0;
   const int grid = opts ? opts->grid : 0;
+  const unsigned long long* dd = reinterpret_cast<const unsigned long long*>(dst);
   if (dtype == SB_F64) {
     YScatter<double> out{};
-    for (int k = 0; k < ndst; ++k) out.d[k] = (double*)dst[k];
+    out.d = dd;
     out.n = ndst;
     out.r0 = row_offset;
     return launch_csr_rows_out<double, double>(row_ptr, col, (const double*)val,
@@ -1545,7 +1554,7 @@ int sb_spmv_csr_allgather(int dtype, const int32_t* row_ptr, const int32_t* col,
                                                nnz, lanes, unroll, grid, st);
   }
   YScatter<float> out{};
-  for (int k = 0; k < ndst; ++k) out.d[k] = (float*)dst[k];
+  out.d = dd;
   out.n = ndst;
   out.r0 = row_offset;
   if (dtype == SB_BF16)

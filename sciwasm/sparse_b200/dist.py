@@ -59,24 +59,25 @@ class RowShardedCSR:
         if self.A is not None:
             spmv(self.A, x_view, y_view, inner_max, stream)
 
-    def spmv_allgather(self, x_ptr: int, y_in_ptr: int, dst_ptrs, opts=None, stream=None):
+    def spmv_allgather(self, x_ptr: int, y_in_ptr: int, dst_dev_ptr: int, ndst: int,
+                       opts=None, stream=None):
         """The all-gather fused into the SpMV (sb_spmv_csr_allgather): this
         rank's rows t = y_in + A[r0:r1, :] x are stored at rows r0.. of every
-        buffer in dst_ptrs (device pointers of full-length y buffers: this
-        GPU's own, or peers' buffers mapped for peer access, e.g. the
-        buffer_ptrs of a torch symmetric-memory rendezvous).  Once every
-        rank has run and the ranks have synchronised, each buffer holds the
-        whole y.  y_in_ptr points at this rank's `rows` values."""
+        one of ndst full-length y buffers, whose device pointers are in the
+        device array at dst_dev_ptr (this GPU's own buffers, or peers'
+        buffers mapped for peer access, e.g. the buffer_ptrs of a torch
+        symmetric-memory rendezvous; see PeerY).  Once every rank has run and
+        the ranks have synchronised, each buffer holds the whole y.  y_in_ptr
+        points at this rank's `rows` values."""
         import ctypes as C
         from . import _lib
         from .sparse import _dtcode, _sp
         if self.A is None:
             return
-        ptrs = (C.c_void_p * len(dst_ptrs))(*[int(p) for p in dst_ptrs])
         o = opts if opts is not None else getattr(self.A, "opts", None)
         _lib.call("sb_spmv_csr_allgather", _dtcode(self.A.dtype), self.A.row_index.ptr,
                   self.A.col_index.ptr, self.A.val_index.ptr, int(x_ptr), int(y_in_ptr),
-                  self.rows, self.A.nnz, self.r0, ptrs, len(dst_ptrs),
+                  self.rows, self.A.nnz, self.r0, C.c_void_p(int(dst_dev_ptr)), int(ndst),
                   C.byref(o) if o is not None else None, _sp(stream))
 
 
@@ -157,6 +158,8 @@ class PeerY:
         else:
             self.buf = torch.zeros(N, dtype=dtype, device=device)
             self.ptrs = [self.buf.data_ptr()]
+        # the destination addresses in device memory, as the kernel reads them
+        self.ptrs_dev = torch.tensor(self.ptrs, dtype=torch.int64, device=device)
 
     def rows_ptr(self, r0: int) -> int:
         """Device address of row r0 of this rank's buffer."""

@@ -86,4 +86,5 @@ def test_peer_y_single_rank_layout():
     py = dist.PeerY(1000, torch.float64, "cpu")
     assert py.world == 1 and py.ptrs == [py.buf.data_ptr()]
     assert py.rows_ptr(5) == py.buf.data_ptr() + 40
+    assert py.ptrs_dev.tolist() == py.ptrs
     py.barrier()

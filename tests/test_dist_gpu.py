@@ -62,12 +62,13 @@ def test_allgather_fused_emulated_ranks(gpu, dt):
     bits = np.uint64 if dt == np.float64 else np.uint32
     for world in (3, 1):
         bufs = [gpu.DeviceArray.from_host(np.full(N, np.nan, dt)) for _ in range(world)]
+        dsts = gpu.DeviceArray.from_host(np.array([b.ptr for b in bufs], np.uint64))
         keep = []
         for rank in range(world):
             sh = dist.RowShardedCSR(rp, col, val, rank, world)
             yin = gpu.DeviceArray.from_host(np.ascontiguousarray(y0[sh.r0:sh.r1]))
             keep.append((sh, yin))
-            sh.spmv_allgather(xv.ptr, yin.ptr, [b.ptr for b in bufs], opts=opts)
+            sh.spmv_allgather(xv.ptr, yin.ptr, dsts.ptr, world, opts=opts)
         gpu.synchronize()
         for b in bufs:
             assert np.array_equal(b.to_host().view(bits), want.view(bits)), world
