@@ -326,7 +326,12 @@ __device__ __forceinline__ void comp_add(T& s, T& c, T v) {
 template <typename T>
 struct YOut {
   static constexpr bool kAll = false;
-  static constexpr int kMinBlocks = 1;
+  // 6 blocks of 256 per SM (at most 42 registers): the unbounded kernel held
+  // 58-72 registers and 4 blocks per SM (ncu, banded 2 lanes x unroll 8:
+  // 47% warps active, long-scoreboard 23 per issue).  Measured in the format
+  // sweep: banded CSR 0.1345 -> 0.1155 ms, power-law CSR 0.253 -> 0.243 ms
+  // (8 blocks: 0.121 / 0.256 ms).
+  static constexpr int kMinBlocks = 6;
   T* y;
   __device__ __forceinline__ void put(long long i, T v) const { y[i] = v; }
 };
