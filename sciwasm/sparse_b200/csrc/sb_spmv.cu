@@ -326,12 +326,15 @@ __device__ __forceinline__ void comp_add(T& s, T& c, T v) {
 template <typename T>
 struct YOut {
   static constexpr bool kAll = false;
-  // 6 blocks of 256 per SM (at most 42 registers): the unbounded kernel held
-  // 58-72 registers and 4 blocks per SM (ncu, banded 2 lanes x unroll 8:
-  // 47% warps active, long-scoreboard 23 per issue).  Measured in the format
-  // sweep: banded CSR 0.1345 -> 0.1155 ms, power-law CSR 0.253 -> 0.243 ms
-  // (8 blocks: 0.121 / 0.256 ms).
-  static constexpr int kMinBlocks = 6;
+  // FP64: 6 blocks of 256 per SM (at most 42 registers); the unbounded
+  // kernel held 58-72 registers and 4 blocks per SM (ncu, banded 2 lanes x
+  // unroll 8: 47% warps active, long-scoreboard 23 per issue).  Measured in
+  // the format sweep: banded CSR 0.1345 -> 0.1155 ms, power-law CSR 0.253 ->
+  // 0.243 ms (8 blocks: 0.121 / 0.256 ms).  FP32 and BF16 stay unbounded:
+  // the same bound slowed the 4096^2 Laplacian's 1-lane, unroll-8 kernel
+  // (FP32 0.176 -> 0.185 ms, BF16 0.158 -> 0.190 ms).
+  template <typename V>
+  static constexpr int min_blocks() { return sizeof(V) == 8 ? 6 : 1; }
   T* y;
   __device__ __forceinline__ void put(long long i, T v) const { y[i] = v; }
 };
@@ -339,7 +342,8 @@ constexpr int kMaxScatter = 8;
 template <typename T>
 struct YScatter {
   static constexpr bool kAll = true;
-  static constexpr int kMinBlocks = 8;  // the plain kernel's 32 registers
+  template <typename V>
+  static constexpr int min_blocks() { return 8; }  // 32 registers
   const unsigned long long* d;  // device array of n destination addresses
   int n;
   long long r0;
@@ -356,7 +360,7 @@ struct YScatter {
 };
 
 template <typename SV, typename T, int V, int UNROLL, class Out>
-__global__ void __launch_bounds__(256, Out::kMinBlocks)
+__global__ void __launch_bounds__(256, Out::template min_blocks<T>())
     csr_rows_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
                     const SV* __restrict__ val, const T* __restrict__ x, const T* y_in,
                     Out out, int N) {
