@@ -326,15 +326,13 @@ __device__ __forceinline__ void comp_add(T& s, T& c, T v) {
 template <typename T>
 struct YOut {
   static constexpr bool kAll = false;
-  // FP64: 6 blocks of 256 per SM (at most 42 registers); the unbounded
-  // kernel held 58-72 registers and 4 blocks per SM (ncu, banded 2 lanes x
-  // unroll 8: 47% warps active, long-scoreboard 23 per issue).  Measured in
-  // the format sweep: banded CSR 0.1345 -> 0.1155 ms, power-law CSR 0.253 ->
-  // 0.243 ms (8 blocks: 0.121 / 0.256 ms).  FP32 and BF16 stay unbounded:
-  // the same bound slowed the 4096^2 Laplacian's 1-lane, unroll-8 kernel
-  // (FP32 0.176 -> 0.185 ms, BF16 0.158 -> 0.190 ms).
+  // 0: no minimum (the compiler's own choice, 32 registers for the kernels
+  // the tuner picks).  An explicit minimum of 1 let ptxas take 48-62
+  // registers, 4 blocks per SM (format sweep: banded CSR 0.114 -> 0.1345 ms,
+  // 4096^2 Laplacian FP32 0.176 -> 0.215 ms); 6 blocks (at most 42) only
+  // recovered part of it.
   template <typename V>
-  static constexpr int min_blocks() { return sizeof(V) == 8 ? 6 : 1; }
+  static constexpr int min_blocks() { return 0; }
   T* y;
   __device__ __forceinline__ void put(long long i, T v) const { y[i] = v; }
 };
