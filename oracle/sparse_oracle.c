@@ -2,9 +2,10 @@
  * sparse_oracle.c -- CPU restatement of SciWasm.Sparse's sparse kernels.
  *
  * TEST INFRASTRUCTURE ONLY (correctness oracle + timed CPU baseline); the
- * product never links it.  Parity status: UNPINNED by reference artefacts
- * (the reference ships no golden vectors or fixtures for this path and cannot
- * run here).  Each function cites the reference lines it restates; paths are
+ * product never links it.  Parity status: the restatements of the reference's
+ * WebAssembly kernels are pinned bit for bit to outputs of those kernels run
+ * from their .wat text (tests/golden/wat_vectors.npz); the restatements of its
+ * JavaScript functions by hand-derived known answers only.  Each function cites the reference lines it restates; paths are
  * relative to the SciWasm.Sparse project root.  Build with
  * -O2 -ffp-contract=off -fno-fast-math so that separate mul and add are kept
  * (wasm has no fused multiply-add).

@@ -6,11 +6,16 @@
  * cpu_baseline / --impl reference leg may load it; the product path
  * (libsparse_b200.so and the sciwasm.sparse_b200 package) never does.
  *
- * Parity status: UNPINNED by reference artefacts.  The reference ships no
- * golden vectors, fixtures or known-answer tests for this path, its JS/wasm
- * code cannot run in this environment (no JS or wasm runtime), and the only
- * published pins are Fletcher checksums of real-world matrices whose files
- * are not distributed with it.  Every function below restates one reference
+ * Parity status: the functions that restate the reference's WebAssembly
+ * kernels (SpMV in four formats, eliminate_zeros, transposes, diagonal/min
+ * reductions, the exact element-wise maps, the CSC, sync-free and level-set
+ * triangular solves) are PINNED bit for bit to outputs of those kernels,
+ * executed from the reference's .wat text by tests/golden/wat_machine.py
+ * (vectors in tests/golden/wat_vectors.npz, checked by
+ * tests/test_wat_vectors.py).  The restatements of its JavaScript functions
+ * (conversions, level sets, static_nnz, Matrix Market input, reorderings) are
+ * pinned by hand-derived known answers only: the reference ships no golden
+ * vectors and no JS engine is available.  Every function below restates one reference
  * function line by line (cited as file:line, paths relative to the
  * SciWasm.Sparse project root) and is compiled with -ffp-contract=off so that
  * wasm's separate mul/add (wasm has no FMA) is reproduced bit for bit.

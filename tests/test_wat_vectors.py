@@ -1,0 +1,153 @@
+"""The oracle against outputs of the reference's own WebAssembly kernels.
+
+tests/golden/wat_vectors.npz holds inputs and outputs of SciWasm.Sparse's
+hand-written .wat kernels, executed by tests/golden/wat_machine.py (see
+make_wat_vectors.py for how they were made).  Every comparison here is bit
+for bit: the oracle restates those kernels and must give the same bits, which
+pins it to the reference as it ships.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+from make_wat_vectors import load_case  # noqa: E402
+
+OPS = {"sign": 7, "abs": 8, "neg": 9, "sqrt": 10, "ceil": 11, "floor": 12, "trunc": 13,
+       "nearest": 14, "deg2rad": 5, "rad2deg": 6}
+TAGS = ["f32", "f64"]
+
+
+@pytest.fixture(scope="module")
+def vec():
+    return np.load(os.path.join(HERE, "golden", "wat_vectors.npz"))
+
+
+def same(a, b):
+    """Bit-identical, except that any NaN equals any NaN: WebAssembly leaves
+    the sign and payload of a NaN result nondeterministic."""
+    a, b = np.asarray(a), np.asarray(b)
+    if a.shape != b.shape or a.dtype != b.dtype:
+        return False
+    if a.dtype.kind == "f":
+        na, nb = np.isnan(a), np.isnan(b)
+        if not np.array_equal(na, nb):
+            return False
+        a, b = a[~na], b[~nb]
+    return np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_spmv(vec, oracle, tag):
+    c = load_case(vec, f"spmv_csr_{tag}")
+    assert same(oracle.spmv_csr(c["row_ptr"], c["col"], c["val"], c["x"], c["y0"]), c["y"])
+    c = load_case(vec, f"spmv_csr3_{tag}")
+    y = c["y0"]
+    for _ in range(3):
+        y = oracle.spmv_csr(c["row_ptr"], c["col"], c["val"], c["x"], y)
+    assert same(y, c["y"])
+    c = load_case(vec, f"spmv_coo_{tag}")
+    assert same(oracle.spmv_coo(c["row"], c["col"], c["val"], c["x"], c["y0"]), c["y"])
+    c = load_case(vec, f"spmv_dia_{tag}")
+    assert same(oracle.spmv_dia(c["offset"], c["data"], int(c["N"]), c["x"], c["y0"],
+                                int(c["stride"])), c["y"])
+    c = load_case(vec, f"spmv_ell_{tag}")
+    assert same(oracle.spmv_ell(c["indices"], c["data"], int(c["N"]), int(c["nc"]), c["x"], c["y0"]),
+                c["y"])
+
+
+def test_eliminate_zeros(vec, oracle):
+    c = load_case(vec, "nz_coo_f32")
+    orow, ocol, oval = oracle.copy_nonzeros_coo(c["row"], c["col"], c["val"])
+    assert orow.size == int(c["count"])
+    assert same(orow, c["orow"]) and same(ocol, c["ocol"]) and same(oval, c["oval"])
+    c = load_case(vec, "nz_csr_f32")
+    orp, ocol, oval = oracle.copy_nonzeros_csr(c["row_ptr"], c["col"], c["val"])
+    assert same(orp, c["orow_ptr"]) and same(ocol, c["ocol"]) and same(oval, c["oval"])
+    c = load_case(vec, "nz_dia_f32")
+    cd, cnt, ooff, odat = oracle.nonzeros_dia(c["offset"], c["data"], int(c["N"]), int(c["stride"]))
+    assert (cd, cnt) == (int(c["count_diags"]), int(c["count"]))
+    assert same(ooff, c["ooffset"]) and same(odat, c["odata"])
+    c = load_case(vec, "nz_ell_f32")
+    onc, cnt, od, oi = oracle.nonzeros_ell(c["data"], c["indices"], int(c["nc"]), int(c["N"]))
+    assert (onc, cnt) == (int(c["count_cols"]), int(c["count"]))
+    assert same(od, c["odata"]) and same(oi, c["oindices"])
+
+
+def test_transpose(vec, oracle):
+    c = load_case(vec, "tr_csr_f32")
+    orp, ocol, oval = oracle.transpose_csr(c["row_ptr"], c["col"], c["val"])
+    assert same(orp, c["orow_ptr"]) and same(ocol, c["ocol"]) and same(oval, c["oval"])
+    c = load_case(vec, "tr_dia_f32")
+    ooff, odat = oracle.transpose_dia(c["offset"], c["data"], int(c["N"]), int(c["stride"]))
+    assert same(ooff, c["ooffset"]) and same(odat, c["odata"])
+    c = load_case(vec, "tr_ell_f32")
+    onc, od, oi = oracle.transpose_ell(c["data"], c["indices"], int(c["nc"]), int(c["N"]))
+    assert onc == int(c["ncols"])
+    assert same(od, c["odata"]) and same(oi, c["oindices"])
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_reductions(vec, oracle, tag):
+    for k in (0, 3, -4):
+        c = load_case(vec, f"diag{k}_{tag}")
+        assert same(oracle.diagonal_coo(k, c["row"], c["col"], c["val"], int(c["N"])), c["diag"]), k
+    c = load_case(vec, f"min_{tag}")
+    assert same(oracle.min_coo(1, c["row"], c["val"], int(c["N"])), c["out"])
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_spts_csc(vec, oracle, tag):
+    """Columns whose entries below the diagonal come in fours run only the
+    kernel's 4-wide SIMD body: bit-identical in both precisions.  With a
+    remainder, the FP64 module's scalar loop addresses y as row*4 bytes (a
+    4-byte scale on 8-byte values, sparse_opt_64.wat spts_csc $inner_loop),
+    so its output is not a triangular solve; the oracle keeps the FP32
+    module's per-entry rule (row*4 on 4-byte values), which the FP64 SIMD body
+    also follows, and matches the FP32 module bit for bit on every column."""
+    c = load_case(vec, f"spts_csc4_{tag}")
+    assert same(oracle.spts_csc(c["col_ptr"], c["row"], c["val"], c["x"]), c["y"])
+    c = load_case(vec, f"spts_csc_{tag}")
+    got = oracle.spts_csc(c["col_ptr"], c["row"], c["val"], c["x"])
+    if tag == "f32":
+        assert same(got, c["y"])
+    else:
+        assert not same(got, c["y"])
+
+
+@pytest.mark.parametrize("tag", TAGS)
+@pytest.mark.parametrize("op", sorted(OPS))
+def test_exact_maps(vec, oracle, tag, op):
+    pi = np.float32(np.pi) if tag == "f32" else np.pi
+    p = float(pi) if op in ("deg2rad", "rad2deg") else 0.0
+    c = load_case(vec, f"map_{op}_coo_{tag}")
+    want = oracle.map_values(c["val"], 0, OPS[op], p)
+    if "out" in c:
+        assert same(want, c["out"])
+    assert same(want, c["self_out"])
+    c = load_case(vec, f"map_{op}_ell_{tag}")
+    assert same(oracle.map_values(c["val"], 1, OPS[op], p), c["out"])
+    c = load_case(vec, f"map_{op}_dia_{tag}")
+    got = oracle.map_dia(c["offset"], c["data"], int(c["N"]), OPS[op], p,
+                         out=None if tag == "f32" else c["data"], stride=int(c["stride"]))
+    assert same(got, c["out"])
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_multiply_scalar(vec, oracle, tag):
+    c = load_case(vec, f"map_multiply_coo_{tag}")
+    assert same(oracle.map_values(c["val"], 0, 15, float(c["p"])), c["self_out"])
+
+
+@pytest.mark.parametrize("name", ["lower", "lower_narrow"])
+def test_spts(vec, oracle, name):
+    c = load_case(vec, f"spts_syncfree_{name}")
+    assert same(oracle.spts_syncfree(c["row_ptr"], c["col"], c["val"], c["b"]), c["y"])
+    c = load_case(vec, f"spts_level_{name}")
+    assert same(oracle.spts_csr(c["lrow_ptr"], c["lcol"], c["lval"], c["b"]), c["y"])
+    L = oracle.level_sets(c["row_ptr"], c["col"], c["val"])
+    assert same(L["row_ptr"], c["lrow_ptr"]) and same(L["col"], c["lcol"])
