@@ -86,6 +86,38 @@ def test_coo_csr_powerlaw_shuffled(gpu, oracle):
     assert _same(C.val_array(), want[2])
 
 
+def _rows_of_lengths(lens, seed, dt, N=None):
+    """A shuffled COO whose rows hold the given numbers of entries, with
+    repeated columns (equal (row, col) keys), NaN and signed zeros."""
+    rng = np.random.default_rng(seed)
+    N = N or max(len(lens), max(lens) // 2 + 1)
+    row = np.repeat(np.arange(len(lens), dtype=np.int32), lens)
+    col = np.concatenate([rng.integers(0, max(1, l // 2 + 1), l) for l in lens]).astype(np.int32)
+    col = np.minimum(col, N - 1)
+    val = rng.standard_normal(row.size).astype(dt)
+    val[rng.random(row.size) < 0.02] = np.nan
+    val[rng.random(row.size) < 0.02] = -0.0
+    perm = rng.permutation(row.size)
+    return row[perm], col[perm], val[perm], N
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("longest", [2048, 5000])
+def test_coo_csr_row_length_tiers(gpu, oracle, dt, longest):
+    """Row lengths on both sides of every tier edge of the row-bucket sort
+    (one thread up to 16, one warp up to 256, one block up to 2048); a row
+    longer than 2048 sends the whole matrix through the radix sort.  Half the
+    columns of a row repeat, so the tie order of equal keys is checked."""
+    lens = [0, 1, 2, 3, 7, 8, 9, 15, 16, 17, 31, 32, 33, 255, 256, 257, 511, 512, 513, 1000,
+            2047, longest, 0, 5]
+    row, col, val, N = _rows_of_lengths(lens, longest, dt)
+    want = oracle.coo_csr(row, col, val, N)
+    C = gpu.coo_csr(gpu.coo_from_host(row, col, val, N))
+    assert _same(C.row_array(), want[0])
+    assert _same(C.col_array(), want[1])
+    assert _same(C.val_array(), want[2])
+
+
 def test_coo_csr_empty(gpu):
     A = gpu.coo_from_host(np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32), 4)
     C = gpu.coo_csr(A)
