@@ -308,8 +308,8 @@ def _timed_call(stream, fn, reps=3):
 def device_conversions(jobs, stream):
     """Objects of the format sweep built on the device.  For each matrix: a
     COO sorted by (row, col) is uploaded (the "coo" object), coo_csr runs on
-    it (the copy-speed path) and on a shuffled copy (the stable radix-sort
-    path, whose output becomes the "csr" object), then csr_dia and csr_ell
+    it (the copy-speed path) and on a shuffled copy (the row-bucket sort,
+    whose output becomes the "csr" object), then csr_dia and csr_ell
     run on the CSR (refused for the power-law matrix, as in the reference).
     Returns (objects, timings, host copies of inputs and outputs for the
     bit-exact check)."""

@@ -245,9 +245,11 @@ DEF_PAR_CSR(double, f64)
 DEF_PAR_COO(float, f32)
 DEF_PAR_COO(double, f64)
 
-/* Row-split DIA (src/parallel/tests/main32.js:749-790, row-major kernel
- * src/parallel/src/sparse_opt_32.wat:8213-8269): each worker applies every
- * diagonal to its own row range, so the per-row order equals the serial one. */
+/* Row-split column-layout DIA: the "dia_col_basic" worker kernel
+ * (src/parallel/tests/main32.js:749-790, src/parallel/src/sparse_opt_32.wat
+ * spmv_dia_col_basic, :8991): each worker applies every diagonal to its own
+ * row range, so the per-row order equals the serial one (and equals the
+ * row-layout "dia_row" kernel's, :8213-8269). */
 #define DEF_PAR_DIA(T, SFX)                                                         \
   static void par_dia_##SFX(par_job* j, int id) {                                   \
     int nt = j->nt;                                                                 \
@@ -285,7 +287,8 @@ DEF_PAR_COO(double, f64)
 DEF_PAR_DIA(float, f32)
 DEF_PAR_DIA(double, f64)
 
-/* Row-split column-major ELL (src/parallel/src/sparse_opt_32.wat:11055-11106). */
+/* Row-split column-layout ELL: the "ell_col" worker kernel
+ * (src/parallel/tests/main32.js:1048-1080, src/parallel/src/sparse_opt_32.wat:11055-11106). */
 #define DEF_PAR_ELL(T, SFX)                                                         \
   static void par_ell_##SFX(par_job* j, int id) {                                   \
     int nt = j->nt;                                                                 \

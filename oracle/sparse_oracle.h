@@ -79,7 +79,8 @@ void or_par_spmv_coo_f32(int nthreads, const int32_t* row, const int32_t* col,
 void or_par_spmv_coo_f64(int nthreads, const int32_t* row, const int32_t* col,
                          const double* val, const double* x, double* y, int32_t N,
                          int64_t nnz, double* wy);
-/* Parallel DIA / ELL: even row split (src/parallel/tests/main32.js:749-790,
+/* Parallel DIA / ELL: even row split over the column-layout data, the
+ * "dia_col_basic" and "ell_col" worker kernels (src/parallel/tests/main32.js:749-790,
  * :1048-1080). */
 void or_par_spmv_dia_f64(int nthreads, const int32_t* offset, const double* data,
                          int32_t N, int32_t nd, int32_t stride, const double* x, double* y);

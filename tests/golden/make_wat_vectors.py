@@ -18,7 +18,10 @@ Kernels run, by file of the reference (paths relative to its project root):
       count_transpose_cols_ell, diagonal_coo, min_coo, spts_csc and the exact
       element-wise maps (abs, neg, sqrt, ceil, floor, trunc, nearest, sign,
       multiply_scalar, deg2rad, rad2deg; COO/CSR, DIA and ELL forms)
-  src/parallel/src/sparse_opt_32.wat: spts_level_csr (one worker)
+  src/parallel/src/sparse_opt_32.wat: spts_level_csr (one worker) and the
+      worker SpMV kernels spmv_csr/coo/dia/ell_wrapper, sum,
+      spmv_dia_col_basic_wrapper and spmv_ell_col_wrapper (three workers run
+      in turn)
   src/parallel/src/spts_opt_32.wat:   spts_csr_sync_free_wrapper (one worker)
 The transcendental maps call imported JavaScript Math functions, which are
 not part of the reference, so they are not pinned here.
@@ -365,6 +368,80 @@ def main(ref):
         rec(f"spts_level_{name}", row_ptr=lrp, col=lcol, val=lval, level_ptr=L["level_ptr"],
             lrow_ptr=L["row_ptr"], lcol=L["col"], lval=L["val"], permutation=L["permutation"],
             b=bp, y=M.get(a[4], dt, Nl))
+
+    # ---- the parallel build's worker kernels, three workers run in turn --
+    # (src/parallel/src/worker32.js "csr", "spmv_coo"/"sum", "dia_row",
+    # "ell_row"; the CPU baseline restates this partitioning).  Workers write
+    # disjoint rows of y (CSR, DIA, ELL) or their own private y (COO), so
+    # running them one after another gives the threaded result.
+    nw = 3
+    N = 300
+    rp, col, val = ragged_csr(N, 21, dt)
+    r3 = np.random.default_rng(22)
+    x = r3.standard_normal(N).astype(dt)
+    y0 = r3.standard_normal(N).astype(dt)
+    rs, re = ob.static_nnz(rp, nw)
+    M = Mem(par)
+    a = [M.put(rp), M.put(col), M.put(val), M.put(x), M.put(y0)]
+    for w in range(nw):
+        par.call("spmv_csr_wrapper", w, a[0] + 4 * int(rs[w]), a[1], a[2], a[3],
+                 a[4] + 4 * int(rs[w]), int(re[w] - rs[w]), 1)
+    rec("par_csr", row_ptr=rp, col=col, val=val, x=x, y0=y0, nw=nw, y=M.get(a[4], dt, N))
+
+    row, ccol, cval = coo_of(rp, col, val)
+    p = r3.permutation(row.size)
+    row, ccol, cval = row[p], ccol[p], cval[p]
+    nnz = row.size
+    per, rem = nnz // nw, nnz - (nnz // nw) * nw
+    nper, nrem = N // nw, N - (N // nw) * nw
+    M = Mem(par)
+    a = [M.put(row), M.put(ccol), M.put(cval), M.put(x), M.put(y0)]
+    wy = [M.zeros(N, dt) for _ in range(nw)]
+    for w in range(nw):
+        s, e = w * per, (w + 1) * per + (rem if w == nw - 1 else 0)
+        par.call("spmv_coo_wrapper", w, a[0] + 4 * s, a[1] + 4 * s, a[2] + 4 * s, a[3], wy[w],
+                 e - s, 1)
+    for d in range(nw):
+        for w in range(nw):
+            s, e = w * nper, (w + 1) * nper + (nrem if w == nw - 1 else 0)
+            par.call("sum", a[4], wy[d], s, e)
+    rec("par_coo", row=row, col=ccol, val=cval, N=N, x=x, y0=y0, nw=nw, y=M.get(a[4], dt, N))
+
+    brp, bcol, bval = banded_csr(N, (-7, -2, 0, 1, 5), 23, dt)
+    off, dat, nd, stride = ob.csr_dia(brp, bcol, bval)
+    # the parallel build stores DIA and ELL data row by row (data[i*nd + k],
+    # src/parallel/src/sparse32.js csr_dia / csr_ell), the sequential build
+    # and the oracle column by column: the vectors keep the column layout
+    dat_rows = dat.reshape(nd, stride)[:, :N].T.copy()
+    M = Mem(par)
+    po, pd, px, py = M.put(off), M.put(dat_rows), M.put(x), M.put(y0)
+    for w in range(nw):
+        s, e = w * nper, (w + 1) * nper + (nrem if w == nw - 1 else 0)
+        par.call("spmv_dia_wrapper", w, po, pd, s, e, nd, N, px, py, 1)
+    rec("par_dia", offset=off, data=dat, N=N, x=x, y0=y0, nw=nw, y=M.get(py, dt, N))
+    # the column-layout worker kernel (tests/main32.js "dia_col_basic": end row inclusive)
+    M = Mem(par)
+    po, pd, px, py = M.put(off), M.put(dat), M.put(x), M.put(y0)
+    for w in range(nw):
+        s, e = w * nper, (w + 1) * nper - 1 + (nrem if w == nw - 1 else 0)
+        par.call("spmv_dia_col_basic_wrapper", w, po, pd, s, e, nd, N, stride, px, py, 1)
+    rec("par_dia_col", offset=off, data=dat, N=N, x=x, y0=y0, nw=nw, y=M.get(py, dt, N))
+
+    ind, edat, nc = ob.csr_ell(rp, col, val)
+    M = Mem(par)
+    pi_, pd = M.put(ind.reshape(nc, N).T.copy()), M.put(edat.reshape(nc, N).T.copy())
+    px, py = M.put(x), M.put(y0)
+    for w in range(nw):
+        s, e = w * nper, (w + 1) * nper + (nrem if w == nw - 1 else 0)
+        par.call("spmv_ell_wrapper", w, pi_, pd, s, e, nc, N, px, py, 1)
+    rec("par_ell", indices=ind, data=edat, N=N, nc=nc, x=x, y0=y0, nw=nw, y=M.get(py, dt, N))
+    # the column-layout worker kernel (tests/main32.js "ell_col")
+    M = Mem(par)
+    pi_, pd, px, py = M.put(ind), M.put(edat), M.put(x), M.put(y0)
+    for w in range(nw):
+        s, e = w * nper, (w + 1) * nper + (nrem if w == nw - 1 else 0)
+        par.call("spmv_ell_col_wrapper", w, pi_, pd, s, e, nc, N, px, py, 1)
+    rec("par_ell_col", indices=ind, data=edat, N=N, nc=nc, x=x, y0=y0, nw=nw, y=M.get(py, dt, N))
 
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT}: {len(out)} arrays, {os.path.getsize(OUT)} bytes")

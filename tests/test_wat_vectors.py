@@ -151,3 +151,33 @@ def test_spts(vec, oracle, name):
     assert same(oracle.spts_csr(c["lrow_ptr"], c["lcol"], c["lval"], c["b"]), c["y"])
     L = oracle.level_sets(c["row_ptr"], c["col"], c["val"])
     assert same(L["row_ptr"], c["lrow_ptr"]) and same(L["col"], c["lcol"])
+
+
+def test_parallel_worker_kernels(vec, oracle):
+    """The threaded CPU baseline (the oracle's port of the parallel build's
+    worker partitioning) against the parallel build's own worker kernels run
+    in turn: static_nnz row ranges for CSR, nnz ranges into private y copies
+    summed in worker order for COO, even row ranges for DIA and ELL."""
+    c = load_case(vec, "par_csr")
+    nw = int(c["nw"])
+    y = c["y0"].copy()
+    oracle.par_spmv_csr(nw, c["row_ptr"], c["col"], c["val"], c["x"], y)
+    assert same(y, c["y"])
+    c = load_case(vec, "par_coo")
+    y = c["y0"].copy()
+    wy = np.zeros(nw * int(c["N"]), c["val"].dtype)
+    oracle.par_spmv_coo(nw, c["row"], c["col"], c["val"], c["x"], y, int(c["N"]), wy)
+    assert same(y, c["y"])
+    # DIA and ELL: the column-layout worker kernels the port restates
+    # (dia_col_basic, ell_col), and the row-layout ones (dia_row, ell_row),
+    # whose per-row arithmetic is the same
+    for case in ("par_dia_col", "par_dia"):
+        c = load_case(vec, case)
+        y = c["y0"].copy()
+        oracle.par_spmv_dia(nw, c["offset"], c["data"], int(c["N"]), c["x"], y)
+        assert same(y, c["y"]), case
+    for case in ("par_ell_col", "par_ell"):
+        c = load_case(vec, case)
+        y = c["y0"].copy()
+        oracle.par_spmv_ell(nw, c["indices"], c["data"], int(c["N"]), int(c["nc"]), c["x"], y)
+        assert same(y, c["y"]), case
