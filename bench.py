@@ -36,7 +36,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SECTIONS = ("batched", "laplacian4096_fp32", "spts", "serving", "powerlaw_csr", "serving_sweep",
-            "gather_ceiling")
+            "gather_ceiling", "conversions")
 METRIC = "served SpMV/SpTS req/s + p99 vs plain path; SpMV HBM GB/s at \u22641e-5 rel err"
 UNIT = "GB/s"
 
@@ -401,6 +401,16 @@ def device_conversions(jobs, stream):
         conv[j["label"]] = c
         check[j["label"]] = chk
     return objs, conv, check
+
+
+def run_conversions(stream, small):
+    """The format sweep's device conversions alone (coo_csr on sorted and
+    shuffled input, csr_dia, csr_ell), timed as in the bench line; for
+    profiling the conversion kernels.  The oracle check is left to the full
+    run."""
+    jobs = make_workload("format_sweep_fp64", small)
+    _, conv, _ = device_conversions(jobs, stream)
+    return conv
 
 
 def conversions_cpu_check(conv, check):
@@ -1666,6 +1676,8 @@ def main():
             out = run_serving_sweep(args)
         elif args.workload == "gather_ceiling":
             out = run_gather_ceiling(stream, peak, args.small)
+        elif args.workload == "conversions":
+            out = run_conversions(stream, args.small)
         else:
             out = run_serving(args)
         print(json.dumps({"workload": args.workload, "result": out}), flush=True)
