@@ -18,7 +18,8 @@ Kernels run, by file of the reference (paths relative to its project root):
       count_transpose_cols_ell, diagonal_coo, min_coo, spts_csc and the exact
       element-wise maps (abs, neg, sqrt, ceil, floor, trunc, nearest, sign,
       multiply_scalar, deg2rad, rad2deg; COO/CSR, DIA and ELL forms)
-  src/parallel/src/sparse_opt_32.wat: spts_level_csr (one worker) and the
+  src/parallel/src/sparse_opt_32.wat: spts_level_csr and the hybrid
+      metadata + spts_csr_opt_level_sync_free_wrapper (one worker), and the
       worker SpMV kernels spmv_csr/coo/dia/ell_wrapper, sum,
       spmv_dia_col_basic_wrapper and spmv_ell_col_wrapper (three workers run
       in turn)
@@ -368,6 +369,26 @@ def main(ref):
         rec(f"spts_level_{name}", row_ptr=lrp, col=lcol, val=lval, level_ptr=L["level_ptr"],
             lrow_ptr=L["row_ptr"], lcol=L["col"], lval=L["val"], permutation=L["permutation"],
             b=bp, y=M.get(a[4], dt, Nl))
+        # the hybrid level/sync-free solve (tests/main32.js "spts_metadata" then
+        # "spts_csr_opt_level_sync_free", one worker): y starts at 1.0 as
+        # spts_init_y leaves it, the level flag at -1, the worker level at -1
+        nl = L["nlevels"]
+        M = Mem(par)
+        lp = M.put(L["level_ptr"].astype(np.int32))
+        a = [M.put(L["row_ptr"]), M.put(L["col"]), M.put(L["val"]), M.put(bp),
+             M.put(np.ones(Nl, dt))]
+        perm = M.put(L["permutation"])
+        bar, gfl = M.zeros(1, np.int32), M.zeros(1, np.int32)
+        glevel, grows = M.put(np.array([-1], np.int32)), M.zeros(1, np.int32)
+        alevel = M.zeros(nl + 1, np.int32)
+        rli, rwi = M.zeros(Nl, np.int32), M.zeros(Nl, np.int32)
+        wlev = M.put(np.array([-1], np.int32))
+        par.call("metadata", 0, lp, nl, 1, Nl, rli, rwi)
+        par.call("spts_csr_opt_level_sync_free_wrapper", 0, lp, *a, perm, nl, bar, gfl, glevel,
+                 grows, alevel, rli, rwi, wlev, 1, Nl, 1)
+        rec(f"spts_hybrid_{name}", lrow_ptr=L["row_ptr"], lcol=L["col"], lval=L["val"],
+            permutation=L["permutation"], row_ptr=lrp, col=lcol, val=lval, b=bp,
+            y=M.get(a[4], dt, Nl))
 
     # ---- the parallel build's worker kernels, three workers run in turn --
     # (src/parallel/src/worker32.js "csr", "spmv_coo"/"sum", "dia_row",

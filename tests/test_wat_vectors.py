@@ -151,6 +151,10 @@ def test_spts(vec, oracle, name):
     assert same(oracle.spts_csr(c["lrow_ptr"], c["lcol"], c["lval"], c["b"]), c["y"])
     L = oracle.level_sets(c["row_ptr"], c["col"], c["val"])
     assert same(L["row_ptr"], c["lrow_ptr"]) and same(L["col"], c["lcol"])
+    # the reference's hybrid (level-ordered rows with sync-free waits) computes
+    # each row as the level-set row kernel does
+    c = load_case(vec, f"spts_hybrid_{name}")
+    assert same(oracle.spts_csr(c["lrow_ptr"], c["lcol"], c["lval"], c["b"]), c["y"])
 
 
 def test_parallel_worker_kernels(vec, oracle):
