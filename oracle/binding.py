@@ -3,8 +3,8 @@
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
 bench.py's CPU-baseline leg, as the checker and the timed CPU baseline.  The
 product package never imports this module.  Parity status of the oracle:
-pinned to the reference's WebAssembly kernels by executed vectors, its
-JavaScript functions by known answers (see sparse_oracle.h).
+pinned to the reference's WebAssembly kernels and JavaScript functions by
+vectors executed from their source (see sparse_oracle.h).
 """
 from __future__ import annotations
 

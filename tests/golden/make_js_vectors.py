@@ -1,0 +1,202 @@
+"""Make tests/golden/js_vectors.npz: outputs of the reference's JavaScript functions.
+
+Runs SciWasm.Sparse's host-side functions -- the format conversions, the
+level-set analysis and the static_nnz partitioner -- through js_machine.py (a
+JavaScript interpreter in Python) on small seeded inputs and stores every
+input and output array.  tests/test_js_vectors.py checks the oracle against
+them bit for bit, so the restatements of these functions are pinned to the
+reference's code as it ships.
+
+Usage (where the reference sources are available; the vectors are committed
+and nothing reads the reference at test time):
+
+    python tests/golden/make_js_vectors.py /path/to/SciWasm.Sparse
+
+Functions run (paths relative to the reference's project root):
+  src/sequential/src/sparse32.js (Float32Array values) and sparse64.js
+  (Float64Array values): coo_csr with its per-row sort, num_cols, csr_ell,
+  num_diags, csr_dia (admitted and refused), coo_csc, quick_sort_COO
+  src/parallel/src/sparse32.js: static_nnz, CSR_create_level_sets_with_reorder
+The host objects these functions touch (linear memory, _malloc, the
+allocate_* helpers and matrix constructors, console.log) are supplied here.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+from js_machine import UNDEF, JSMachine, JSObject  # noqa: E402
+from make_wat_vectors import banded_csr, coo_of, lower_csr, ragged_csr  # noqa: E402
+
+OUT = os.path.join(HERE, "js_vectors.npz")
+
+
+def machine(src, names, val_kind):
+    m = JSMachine(mem_bytes=16 << 20)
+    vb = 4 if val_kind == "Float32Array" else 8
+    I4 = 4.0
+
+    def obj(**kw):
+        return JSObject({k: (float(v) if isinstance(v, (int, np.integer)) else v)
+                         for k, v in kw.items()})
+
+    def allocate_CSR(nrows, nnz):
+        return obj(row_index=m.malloc(I4 * (nrows + 1)), nnz_row_index=m.malloc(I4 * nrows),
+                   col_index=m.malloc(I4 * nnz), val_index=m.malloc(vb * nnz), N=nrows, nnz=nnz)
+
+    def allocate_DIA(N, nnz, ndiags, stride):
+        return obj(offset_index=m.malloc(I4 * ndiags), data_index=m.malloc(vb * ndiags * stride),
+                   ndiags=ndiags, stride=stride, N=N, nnz=nnz)
+
+    def allocate_ELL(N, nnz, ncols):
+        return obj(indices_index=m.malloc(I4 * ncols * N), data_index=m.malloc(vb * ncols * N),
+                   ncols=ncols, N=N, nnz=nnz)
+
+    class Ctor:
+        def construct(self, row_index, col_index, val_index, nnz_row_index, N, nnz):
+            return obj(row_index=row_index, col_index=col_index, val_index=val_index,
+                       nnz_row_index=nnz_row_index, nrows=N, nnz=nnz)
+
+    m.define("allocate_CSR", allocate_CSR)
+    m.define("allocate_DIA", allocate_DIA)
+    m.define("allocate_ELL", allocate_ELL)
+    m.define("sswasm_CSR_t", Ctor())
+    m.define("num_workers", 4.0)   # read by the level-set function's statistics only
+    m.load(src, names)
+    return m, obj
+
+
+def put(m, arr):
+    a = m.malloc(arr.nbytes)
+    m.mem[int(a):int(a) + arr.nbytes] = np.ascontiguousarray(arr).tobytes()
+    return a
+
+
+def get(m, addr, dtype, n):
+    n = int(n)
+    dt = np.dtype(dtype)
+    return np.frombuffer(bytes(m.mem[int(addr):int(addr) + dt.itemsize * n]), dt).copy()
+
+
+def shuffled_coo(N, seed, dt, dup=0.1):
+    rng = np.random.default_rng(seed)
+    rp, col, val = ragged_csr(N, seed, dt)
+    row, col, val = coo_of(rp, col, val)
+    nd = int(row.size * dup)
+    src, dst = rng.integers(0, row.size, nd), rng.integers(0, row.size, nd)
+    row[dst], col[dst] = row[src], col[src]          # repeated (row, col) keys
+    p = rng.permutation(row.size)
+    return row[p].copy(), col[p].copy(), val[p].copy()
+
+
+def main(ref):
+    out = {}
+
+    def rec(case, **arrs):
+        for k, v in arrs.items():
+            out[f"{case}/{k}"] = np.asarray(v)
+
+    conv = ["coo_csr", "sort", "num_cols", "csr_ell", "num_diags", "csr_dia", "coo_csc",
+            "quick_sort_COO"]
+    for tag, fname, dt, kind in (("f32", "sparse32.js", np.float32, "Float32Array"),
+                                 ("f64", "sparse64.js", np.float64, "Float64Array")):
+        src = open(os.path.join(ref, "src/sequential/src", fname)).read()
+        N = 150
+        # coo_csr on a shuffled COO with repeated keys
+        m, obj = machine(src, conv, kind)
+        row, col, val = shuffled_coo(N, 31, dt)
+        A = obj(row_index=put(m, row), col_index=put(m, col), val_index=put(m, val), N=N,
+                nnz=row.size)
+        C = m.call("coo_csr", A)
+        crp = get(m, C.get("row_index"), np.int32, N + 1)
+        ccol = get(m, C.get("col_index"), np.int32, row.size)
+        cval = get(m, C.get("val_index"), dt, row.size)
+        rec(f"coo_csr_{tag}", row=row, col=col, val=val, N=N, row_ptr=crp, ccol=ccol, cval=cval)
+        # coo_csc on the same COO
+        m, obj = machine(src, conv, kind)
+        A = obj(row_index=put(m, row), col_index=put(m, col), val_index=put(m, val), N=N,
+                nnz=row.size)
+        S = obj(col_index=m.malloc(4 * (N + 1)), row_index=m.malloc(4 * row.size),
+                val_index=m.malloc(dt().itemsize * row.size), ncols=N, nnz=row.size)
+        m.call("coo_csc", A, S)
+        rec(f"coo_csc_{tag}", row=row, col=col, val=val, N=N,
+            col_ptr=get(m, S.get("col_index"), np.int32, N + 1),
+            srow=get(m, S.get("row_index"), np.int32, row.size),
+            sval=get(m, S.get("val_index"), dt, row.size))
+        # quick_sort_COO (unstable; repeated keys included)
+        m, obj = machine(src, conv, kind)
+        A = obj(row_index=put(m, row), col_index=put(m, col), val_index=put(m, val), N=N,
+                nnz=row.size)
+        m.call("quick_sort_COO", A, 0.0, float(row.size - 1))
+        rec(f"qsort_{tag}", row=row, col=col, val=val,
+            srow=get(m, A.get("row_index"), np.int32, row.size),
+            scol=get(m, A.get("col_index"), np.int32, row.size),
+            sval=get(m, A.get("val_index"), dt, row.size))
+
+        # csr_ell / csr_dia on a band with a repeated entry, and refused forms
+        cases = {"band": banded_csr(N, (-4, -1, 0, 2, 6), 32, dt),
+                 "ragged": ragged_csr(N, 33, dt)}
+        brp, bcol, bval = cases["band"]
+        # a repeated (row, col) entry: csr_dia keeps the later one
+        bcol = bcol.copy()
+        bcol[brp[10] + 1] = bcol[brp[10]]
+        cases["band"] = (brp, bcol, bval)
+        for cname, (rp, ccol_, cval_) in cases.items():
+            m, obj = machine(src, conv, kind)
+            nnz = ccol_.size
+            A = obj(row_index=put(m, rp), col_index=put(m, ccol_), val_index=put(m, cval_), N=N,
+                    nnz=nnz)
+            nc = m.call("num_cols", A)
+            E = m.call("csr_ell", A)
+            nd = m.call("num_diags", A)
+            D = m.call("csr_dia", A)
+            arrs = dict(row_ptr=rp, col=ccol_, val=cval_, nc=nc, nd=nd.get(0.0),
+                        stride=nd.get(1.0), ell=E is not UNDEF, dia=D is not UNDEF)
+            if E is not UNDEF:
+                w = int(E.get("ncols"))
+                arrs["indices"] = get(m, E.get("indices_index"), np.int32, w * N)
+                arrs["edata"] = get(m, E.get("data_index"), dt, w * N)
+            if D is not UNDEF:
+                w, st = int(D.get("ndiags")), int(D.get("stride"))
+                arrs["offset"] = get(m, D.get("offset_index"), np.int32, w)
+                arrs["ddata"] = get(m, D.get("data_index"), dt, w * st)
+            rec(f"fmt_{cname}_{tag}", **arrs)
+
+    # ---- the parallel build's partitioner and level sets (Float32Array) ----
+    src = open(os.path.join(ref, "src/parallel/src/sparse32.js")).read()
+    dt = np.float32
+    tiny = np.array([0, 3, 3, 8, 9, 11, 15], np.int32)   # 6 rows for 8 workers
+    for nw, (rp, col, val) in ((3, ragged_csr(200, 34, dt)), (5, ragged_csr(97, 35, dt)),
+                               (8, (tiny, np.zeros(15, np.int32), np.ones(15, dt)))):
+        m, obj = machine(src, ["static_nnz"], "Float32Array")
+        N = rp.size - 1
+        A = obj(row_index=put(m, rp), nnz_row_index=m.malloc(4 * N), N=N, nnz=col.size)
+        # the callers pass fresh Int32Array(num_workers) (tests/main32.js:176-187)
+        rs = m.builtins["Int32Array"].construct(float(nw))
+        re_ = m.builtins["Int32Array"].construct(float(nw))
+        m.call("static_nnz", A, float(nw), rs, re_)
+        rec(f"static_nnz_{N}_{nw}", row_ptr=rp, nw=nw, row_start=rs.a.copy(), row_end=re_.a.copy())
+    for name, (rp, col, val) in (("lower", lower_csr(300, 37, dt)),
+                                 ("narrow", lower_csr(200, 38, dt, band=3))):
+        m, obj = machine(src, ["CSR_create_level_sets_with_reorder"], "Float32Array")
+        N, nnz = rp.size - 1, col.size
+        A = obj(row_index=put(m, rp), col_index=put(m, col), val_index=put(m, val), nrows=N,
+                nnz=nnz)
+        L = m.call("CSR_create_level_sets_with_reorder", A)
+        nl = int(L.get("nlevels"))
+        rec(f"levels_{name}", row_ptr=rp, col=col, val=val, nlevels=nl,
+            level_ptr=get(m, L.get("level_index"), np.int32, nl + 1),
+            permutation=get(m, L.get("permutation_index"), np.int32, N),
+            nrow_ptr=get(m, L.get("row_index"), np.int32, N + 1),
+            ncol=get(m, L.get("col_index"), np.int32, nnz),
+            nval=get(m, L.get("val_index"), dt, nnz))
+
+    np.savez_compressed(OUT, **out)
+    print(f"wrote {OUT}: {len(out)} arrays, {os.path.getsize(OUT)} bytes")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SCIWASM_SPARSE_SRC", "."))

@@ -1,0 +1,98 @@
+"""The oracle against outputs of the reference's own JavaScript functions.
+
+tests/golden/js_vectors.npz holds inputs and outputs of SciWasm.Sparse's
+host-side JavaScript (coo_csr, coo_csc, quick_sort_COO, num_cols/csr_ell,
+num_diags/csr_dia, static_nnz, CSR_create_level_sets_with_reorder), executed
+by tests/golden/js_machine.py (see make_js_vectors.py).  Every comparison is
+bit for bit.  The device conversions and level sets are checked bit for bit
+against the same oracle functions by the -m gpu tests, at small and at full
+size.
+"""
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TAGS = ["f32", "f64"]
+
+
+@pytest.fixture(scope="module")
+def vec():
+    return np.load(os.path.join(HERE, "golden", "js_vectors.npz"))
+
+
+def case(z, name):
+    pre = name + "/"
+    return {k[len(pre):]: z[k] for k in z.files if k.startswith(pre)}
+
+
+def same(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return a.shape == b.shape and a.dtype == b.dtype and np.array_equal(
+        a.view(np.uint8), b.view(np.uint8))
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_coo_csr(vec, oracle, tag):
+    """Stable order of repeated (row, col) keys: the per-row bubble sort."""
+    c = case(vec, f"coo_csr_{tag}")
+    rp, col, val = oracle.coo_csr(c["row"], c["col"], c["val"], int(c["N"]))
+    assert same(rp, c["row_ptr"]) and same(col, c["ccol"]) and same(val, c["cval"])
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_coo_csc(vec, oracle, tag):
+    c = case(vec, f"coo_csc_{tag}")
+    cp, row, val = oracle.coo_csc(c["row"], c["col"], c["val"], int(c["N"]))
+    assert same(cp, c["col_ptr"]) and same(row, c["srow"]) and same(val, c["sval"])
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_quick_sort_coo(vec, oracle, tag):
+    """The unstable quicksort, repeated keys included: the same pivots and
+    swaps leave equal keys in the same order."""
+    c = case(vec, f"qsort_{tag}")
+    row, col, val = oracle.quick_sort_coo(c["row"], c["col"], c["val"])
+    assert same(row, c["srow"]) and same(col, c["scol"]) and same(val, c["sval"])
+
+
+@pytest.mark.parametrize("tag", TAGS)
+@pytest.mark.parametrize("name", ["band", "ragged"])
+def test_csr_ell_and_csr_dia(vec, oracle, tag, name):
+    c = case(vec, f"fmt_{name}_{tag}")
+    rp, col, val = c["row_ptr"], c["col"], c["val"]
+    assert oracle.num_cols(rp) == int(c["nc"])
+    nd, stride = oracle.num_diags(rp, col)
+    assert (nd, stride) == (int(c["nd"]), int(c["stride"]))
+    ell = oracle.csr_ell(rp, col, val)
+    assert (ell is not None) == bool(c["ell"])
+    if ell is not None:
+        assert same(ell[0], c["indices"]) and same(ell[1], c["edata"])
+    dia = oracle.csr_dia(rp, col, val)
+    assert (dia is not None) == bool(c["dia"])
+    if dia is not None:
+        assert same(dia[0], c["offset"]) and same(dia[1], c["ddata"])
+
+
+def test_admission_outcomes_cover_both_branches(vec):
+    assert bool(case(vec, "fmt_band_f32")["dia"]) and bool(case(vec, "fmt_band_f32")["ell"])
+    assert not bool(case(vec, "fmt_ragged_f32")["dia"])
+
+
+@pytest.mark.parametrize("name", ["static_nnz_200_3", "static_nnz_97_5", "static_nnz_6_8"])
+def test_static_nnz(vec, oracle, name):
+    c = case(vec, name)
+    rs, re = oracle.static_nnz(c["row_ptr"], int(c["nw"]))
+    assert same(rs, c["row_start"]) and same(re, c["row_end"])
+
+
+@pytest.mark.parametrize("name", ["lower", "narrow"])
+def test_level_sets(vec, oracle, name):
+    c = case(vec, f"levels_{name}")
+    L = oracle.level_sets(c["row_ptr"], c["col"], c["val"])
+    assert L["nlevels"] == int(c["nlevels"])
+    assert same(L["level_ptr"], c["level_ptr"])
+    assert same(L["permutation"], c["permutation"])
+    assert same(L["row_ptr"], c["nrow_ptr"]) and same(L["col"], c["ncol"])
+    assert same(L["val"], c["nval"])
