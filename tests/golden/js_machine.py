@@ -158,10 +158,16 @@ def to_number(v):
     if v is None:
         return 0.0
     if isinstance(v, str):
-        try:
-            return float(v.strip() or 0)
-        except ValueError:
-            return math.nan
+        t = v.strip(" \t\n\r\v\f")
+        if t == "":
+            return 0.0
+        if re.fullmatch(r"[+-]?(\d+\.?\d*|\.\d+)([eE][+-]?\d+)?", t):
+            return float(t)
+        if re.fullmatch(r"0[xX][0-9a-fA-F]+", t):
+            return float(int(t, 16))
+        if t in ("Infinity", "+Infinity", "-Infinity"):
+            return -math.inf if t[0] == "-" else math.inf
+        return math.nan
     raise JSError(f"ToNumber of {v!r}")
 
 
@@ -359,6 +365,11 @@ class Parser:
                 self.eat()
                 self.semi()
                 return (v,)
+            if v == "throw":
+                self.eat()
+                e = self.expression()
+                self.semi()
+                return ("throw", e)
             if v == "function":
                 return self.function()
             if v == "try":
@@ -647,7 +658,10 @@ class JSMachine:
         console = JSObject({"log": lambda *a: UNDEF})
         malloc = JSObject({"exports": JSObject({"_malloc": self.malloc,
                                                 "_free": lambda *a: UNDEF})})
+        error = JSObject()
+        error.construct = lambda *a: JSObject({"message": a[0] if a else ""})
         b = {"Math": math_obj, "console": console, "parseInt": js_parseint,
+             "Number": lambda *a: to_number(a[0]) if a else 0.0, "Error": error,
              "memory": JSObject({"buffer": self.buffer}), "malloc_instance": malloc}
         for k in TypedArray.KINDS:
             b[k] = self._typed_ctor(k)
@@ -722,6 +736,9 @@ class JSMachine:
             raise _Continue()
         elif k == "empty":
             pass
+        elif k == "throw":
+            v = self.ev(s[1], fr)
+            raise JSError(v.get("message") if isinstance(v, JSObject) else v)
         elif k == "func":
             fr[0][s[1]] = JSFunction(self, s)
         elif k == "try":
@@ -759,8 +776,14 @@ class JSMachine:
             if isinstance(key, float) and isinstance(obj, JSObject):
                 key = number_to_string(key)
             return obj.get(key)
-        if isinstance(obj, str) and key == "length":
-            return float(len(obj))
+        if isinstance(obj, str):
+            if key == "length":
+                return float(len(obj))
+            if key == "split":
+                return lambda sep=UNDEF, *r: JSArray([obj] if sep is UNDEF else obj.split(sep))
+            i = _as_index(key)
+            if i is not None:
+                return obj[i] if 0 <= i < len(obj) else UNDEF
         raise JSError(f"TypeError: cannot read {key!r} of {obj!r}")
 
     def put_prop(self, obj, key, v):
@@ -887,6 +910,8 @@ class JSMachine:
             elif isinstance(a, (JSObject, JSArray, TypedArray)) or isinstance(
                     b, (JSObject, JSArray, TypedArray)):
                 same = a is b
+            elif isinstance(a, str) and isinstance(b, str):
+                same = a == b
             else:
                 same = to_number(a) == to_number(b)
             return same if op == "==" else not same

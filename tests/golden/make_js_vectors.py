@@ -15,7 +15,10 @@ and nothing reads the reference at test time):
 Functions run (paths relative to the reference's project root):
   src/sequential/src/sparse32.js (Float32Array values) and sparse64.js
   (Float64Array values): coo_csr with its per-row sort, num_cols, csr_ell,
-  num_diags, csr_dia (admitted and refused), coo_csc, quick_sort_COO
+  num_diags, csr_dia (admitted and refused), coo_csc, quick_sort_COO;
+  sparse32.js: read_matrix_MM_files (with read_MM_header and
+  calculate_actual_nnz) on the lines load_file produces, then
+  create_COO_from_MM or create_LCOO_from_MM
   src/parallel/src/sparse32.js: static_nnz, CSR_create_level_sets_with_reorder
 The host objects these functions touch (linear memory, _malloc, the
 allocate_* helpers and matrix constructors, console.log) are supplied here.
@@ -28,7 +31,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
-from js_machine import UNDEF, JSMachine, JSObject  # noqa: E402
+from js_machine import UNDEF, JSArray, JSMachine, JSObject  # noqa: E402
 from make_wat_vectors import banded_csr, coo_of, lower_csr, ragged_csr  # noqa: E402
 
 OUT = os.path.join(HERE, "js_vectors.npz")
@@ -90,6 +93,29 @@ def shuffled_coo(N, seed, dt, dup=0.1):
     row[dst], col[dst] = row[src], col[src]          # repeated (row, col) keys
     p = rng.permutation(row.size)
     return row[p].copy(), col[p].copy(), val[p].copy()
+
+
+def mm_texts():
+    """The Matrix Market known-answer files, and two seeded ones (general real
+    with explicit zeros and repeated coordinates; symmetric real)."""
+    out = []
+    for f in sorted(os.listdir(os.path.join(HERE, "mm"))):
+        with open(os.path.join(HERE, "mm", f)) as fh:
+            out.append((f.split(".")[0], fh.read()))
+    rng = np.random.default_rng(40)
+    n, ne = 60, 400
+    r, c = rng.integers(1, n + 1, ne), rng.integers(1, n + 1, ne)
+    r[-20:], c[-20:] = r[:20], c[:20]
+    v = np.round(rng.standard_normal(ne), 6)
+    v[rng.random(ne) < 0.05] = 0.0
+    lines = ["%%MatrixMarket matrix coordinate real general", "% seeded", f"{n} {n} {ne}"]
+    lines += [f"{a} {b} {float(x)!r}" for a, b, x in zip(r, c, v)]
+    out.append(("gen_real_seeded", "\n".join(lines) + "\n"))
+    keep = r >= c
+    lines = ["%%MatrixMarket matrix coordinate real symmetric", f"{n} {n} {int(keep.sum())}"]
+    lines += [f"{a} {b} {float(x)!r}" for a, b, x in zip(r[keep], c[keep], v[keep])]
+    out.append(("sym_real_seeded", "\n".join(lines) + "\n"))
+    return out
 
 
 def main(ref):
@@ -164,6 +190,39 @@ def main(ref):
                 arrs["offset"] = get(m, D.get("offset_index"), np.int32, w)
                 arrs["ddata"] = get(m, D.get("data_index"), dt, w * st)
             rec(f"fmt_{cname}_{tag}", **arrs)
+
+    # ---- Matrix Market input: read_matrix_MM_files on the lines load_file
+    # hands over (text up to its last newline, split at newlines), then
+    # create_COO_from_MM or create_LCOO_from_MM, each ending in quick_sort_COO
+    src = open(os.path.join(ref, "src/sequential/src/sparse32.js")).read()
+    mm_names = ["read_MM_header", "calculate_actual_nnz", "read_matrix_MM_files",
+                "create_COO_from_MM", "create_LCOO_from_MM", "quick_sort_COO"]
+    for fname, text in mm_texts():
+        for lower in (False, True):
+            m, obj = machine(src, mm_names, "Float32Array")
+
+            def allocate_COO_from_MM(info, m=m, obj=obj):
+                nnz = int(info.get("nnz"))
+                return obj(row_index=m.malloc(4 * nnz), col_index=m.malloc(4 * nnz),
+                           val_index=m.malloc(4 * nnz), N=info.get("nrows"), nnz=nnz)
+
+            m.define("allocate_COO_from_MM", allocate_COO_from_MM)
+            portion = text[:text.rfind("\n")]
+            files = JSArray([JSArray(portion.split("\n"))])
+            info = obj(field="", symmetry="", nrows=0, ncols=0, nentries=0, nnz=0)
+            m.call("read_matrix_MM_files", files, 1.0, info)
+            nnz_read = int(info.get("nnz"))
+            if lower:
+                A = m.call("create_LCOO_from_MM", info)
+            else:
+                A = allocate_COO_from_MM(info)
+                m.call("create_COO_from_MM", info, A)
+            nnz = int(A.get("nnz"))
+            rec(f"mm_{fname}_{'lower' if lower else 'full'}",
+                text=np.frombuffer(text.encode(), np.uint8), nnz=nnz_read,
+                row=get(m, A.get("row_index"), np.int32, nnz),
+                col=get(m, A.get("col_index"), np.int32, nnz),
+                val=get(m, A.get("val_index"), np.float32, nnz))
 
     # ---- the parallel build's partitioner and level sets (Float32Array) ----
     src = open(os.path.join(ref, "src/parallel/src/sparse32.js")).read()

@@ -35,6 +35,10 @@ function counts(x) {
   return [n, ind[1]];
 }
 function parse(a) { return [parseInt(a / 2), -(parseInt((2*a-1)/2)), 7 / 2, 7 % 3, 1 / 0] }
+function strings(line) {
+  var f = line.split(" ");
+  return [f[0][0] == "%", f[1] == "7", Number(f[1]) == 7, f.length, line[99]];
+}
 function views(addr) {
   var v = new Int32Array(memory.buffer, addr, 2);
   v[1] = v[0] + 40;
@@ -75,6 +79,13 @@ def test_postfix_in_condition():
 def test_numbers():
     _, r = run("parse", 7.0)
     assert r.items[:4] == [3.0, -6.0, 3.5, 1.0] and r.items[4] == math.inf
+
+
+def test_strings():
+    m = JSMachine(mem_bytes=1 << 16)
+    m.load(SRC, ["strings"])
+    r = m.call("strings", "%a 7 x").items
+    assert r[:4] == [True, True, True, 3.0] and r[4] is UNDEF
 
 
 def test_memory_views():

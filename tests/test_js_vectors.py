@@ -96,3 +96,20 @@ def test_level_sets(vec, oracle, name):
     assert same(L["permutation"], c["permutation"])
     assert same(L["row_ptr"], c["nrow_ptr"]) and same(L["col"], c["ncol"])
     assert same(L["val"], c["nval"])
+
+
+MM_CASES = ["gen_integer", "gen_pattern", "sym_pattern", "sym_real", "gen_real_seeded",
+            "sym_real_seeded"]
+
+
+@pytest.mark.parametrize("name", MM_CASES)
+@pytest.mark.parametrize("lower", [False, True])
+def test_matrix_market(vec, oracle, name, lower):
+    """read_matrix_MM_files on load_file's lines, then create_COO_from_MM or
+    create_LCOO_from_MM and quick_sort_COO: the oracle's reader and COO
+    builder give the same nnz and the same (row, col, value) order."""
+    c = case(vec, f"mm_{name}_{'lower' if lower else 'full'}")
+    info = oracle.mm_read(c["text"].tobytes())
+    assert info["nnz"] == int(c["nnz"])
+    row, col, val = oracle.mm_coo(info, np.float32, lower=lower)
+    assert same(row, c["row"]) and same(col, c["col"]) and same(val, c["val"])
