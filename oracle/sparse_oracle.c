@@ -4,9 +4,9 @@
  * TEST INFRASTRUCTURE ONLY (correctness oracle + timed CPU baseline); the
  * product never links it.  Parity status: the restatements of the reference's
  * WebAssembly kernels and of its JavaScript conversions, partitioner, level
- * sets and Matrix Market input are pinned bit for bit to outputs of those
- * functions run from their source text (tests/golden/wat_vectors.npz,
- * tests/golden/js_vectors.npz); reorder_NN by hand-derived known answers.  Each function cites the reference lines it restates; paths are
+ * sets, Matrix Market input and row reorderings are pinned bit for bit to
+ * outputs of those functions run from their source text
+ * (tests/golden/wat_vectors.npz, tests/golden/js_vectors.npz).  Each function cites the reference lines it restates; paths are
  * relative to the SciWasm.Sparse project root.  Build with
  * -O2 -ffp-contract=off -fno-fast-math so that separate mul and add are kept
  * (wasm has no fused multiply-add).

@@ -14,10 +14,10 @@
  * (vectors in tests/golden/wat_vectors.npz, checked by
  * tests/test_wat_vectors.py).  The restatements of its JavaScript functions
  * (coo_csr, coo_csc, quick_sort_COO, csr_ell, csr_dia, static_nnz, the level
- * sets, Matrix Market input) are PINNED the same way to those functions
- * executed from their source by tests/golden/js_machine.py
- * (tests/golden/js_vectors.npz, tests/test_js_vectors.py); reorder_NN by
- * hand-derived known answers and an independent restatement.  Every function below restates one reference
+ * sets, Matrix Market input, row reorderings including reorder_NN) are PINNED
+ * the same way to those functions executed from their source by
+ * tests/golden/js_machine.py (tests/golden/js_vectors.npz,
+ * tests/test_js_vectors.py).  Every function below restates one reference
  * function line by line (cited as file:line, paths relative to the
  * SciWasm.Sparse project root) and is compiled with -ffp-contract=off so that
  * wasm's separate mul/add (wasm has no FMA) is reproduced bit for bit.

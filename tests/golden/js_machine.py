@@ -636,6 +636,8 @@ class JSMachine:
         def make(*args):
             if len(args) >= 2 and args[0] is self.buffer:
                 n = args[2] if len(args) > 2 else (len(self.mem) - int(args[1])) // 4
+                n = to_number(n)
+                n = 0 if n != n else n     # ToIndex: a NaN length is 0
                 return TypedArray(kind, self.view(kind, args[1], n))
             if isinstance(args[0], (int, float)):
                 return TypedArray(kind, np.zeros(int(args[0]), TypedArray.KINDS[kind]))
@@ -658,10 +660,12 @@ class JSMachine:
         console = JSObject({"log": lambda *a: UNDEF})
         malloc = JSObject({"exports": JSObject({"_malloc": self.malloc,
                                                 "_free": lambda *a: UNDEF})})
+        array = JSObject()
+        array.construct = lambda n=0.0, *r: JSArray([UNDEF] * int(to_number(n)))
         error = JSObject()
         error.construct = lambda *a: JSObject({"message": a[0] if a else ""})
         b = {"Math": math_obj, "console": console, "parseInt": js_parseint,
-             "Number": lambda *a: to_number(a[0]) if a else 0.0, "Error": error,
+             "Number": lambda *a: to_number(a[0]) if a else 0.0, "Error": error, "Array": array,
              "memory": JSObject({"buffer": self.buffer}), "malloc_instance": malloc}
         for k in TypedArray.KINDS:
             b[k] = self._typed_ctor(k)

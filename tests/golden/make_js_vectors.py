@@ -20,6 +20,11 @@ Functions run (paths relative to the reference's project root):
   calculate_actual_nnz) on the lines load_file produces, then
   create_COO_from_MM or create_LCOO_from_MM
   src/parallel/src/sparse32.js: static_nnz, CSR_create_level_sets_with_reorder
+  (its sswasm_CSR_t constructor is not defined in the shipped sources; it is
+  supplied here storing its arguments as row_index, col_index, val_index,
+  nnz_row_index, nrows, nnz -- the fields the function reads),
+  sort_rows_by_nnz, sort_y_rows_by_nnz, calculate_csr_locality_index,
+  reorder_NN
 The host objects these functions touch (linear memory, _malloc, the
 allocate_* helpers and matrix constructors, console.log) are supplied here.
 """
@@ -252,6 +257,61 @@ def main(ref):
             nrow_ptr=get(m, L.get("row_index"), np.int32, N + 1),
             ncol=get(m, L.get("col_index"), np.int32, nnz),
             nval=get(m, L.get("val_index"), dt, nnz))
+
+    # ---- row reordering (src/parallel/src/sparse32.js): sort_rows_by_nnz,
+    # sort_y_rows_by_nnz, calculate_csr_locality_index, and reorder_NN on the
+    # row-sorted matrix with w = 16 as tests/main32.js:339 calls it.  The new
+    # matrices come from the file's sparse_CSR_t, which stores N and nnz but
+    # no `nrows`; both functions size their new row-pointer view by
+    # `A_csr_new.nrows + 1`, so that view is empty and the reference writes no
+    # row pointers (recorded here as what the memory held: zeros).
+    reo = ["sort_rows_by_nnz", "sort_y_rows_by_nnz", "calculate_csr_locality_index",
+           "reorder_subset", "find_next_row", "assign_w_min_elems", "reorder_NN"]
+    for name, (rp, col, val) in (("ragged", ragged_csr(300, 41, dt)),
+                                 ("band", banded_csr(200, (-9, -3, 0, 1, 17), 42, dt))):
+        m, obj = machine(src, reo, "Float32Array")
+
+        class CSRCtor:
+            def construct(self, row_index, col_index, val_index, nnz_row_index, N, nnz, obj=obj):
+                return obj(row_index=row_index, col_index=col_index, val_index=val_index,
+                           nnz_row_index=nnz_row_index, N=N, nnz=nnz, num_zero_rows=0,
+                           num_one_rows=0, num_two_rows=0, num_three_rows=0)
+
+        m.define("sparse_CSR_t", CSRCtor())
+        m.define("pretty_print_CSR_permutation", lambda *a: UNDEF)
+        m.define("free_memory_y", lambda *a: UNDEF)
+        N, nnz = rp.size - 1, col.size
+        A = obj(row_index=put(m, rp), col_index=put(m, col), val_index=put(m, val), N=N, nnz=nnz)
+        loc = m.call("calculate_csr_locality_index", A)
+        S = m.call("sort_rows_by_nnz", A)
+        y = np.random.default_rng(43).standard_normal(N).astype(dt)
+        yv = obj(y_index=put(m, y), y_nelem=N)
+        m.call("sort_y_rows_by_nnz", yv, S)
+        rec(f"sortrows_{name}", row_ptr=rp, col=col, val=val, locality=loc,
+            permutation=get(m, S.get("permutation_index"), np.int32, N),
+            nnz_per_row=get(m, S.get("nnz_row_index"), np.int32, N),
+            nrow_ptr=get(m, S.get("row_index"), np.int32, N + 1),
+            ncol=get(m, S.get("col_index"), np.int32, nnz),
+            nval=get(m, S.get("val_index"), dt, nnz),
+            small_rows=np.array([S.get(k) for k in ("num_zero_rows", "num_one_rows",
+                                                     "num_two_rows", "num_three_rows")], np.int32),
+            y=y, y_new=get(m, yv.get("y_index"), dt, N))
+        # reorder_NN on the sorted matrix; its row pointers are the sorted
+        # matrix's own (a correct CSR, written here since the reference's
+        # view of them was empty)
+        # (the reference's nnz_per_row holds the original order's lengths)
+        lens = get(m, S.get("nnz_row_index"), np.int32, N)[get(m, S.get("permutation_index"),
+                                                               np.int32, N)]
+        srp = np.concatenate([[0], np.cumsum(lens)])
+        m.mem[int(S.get("row_index")):int(S.get("row_index")) + 4 * (N + 1)] = \
+            srp.astype(np.int32).tobytes()
+        R = m.call("reorder_NN", S, 16.0)
+        rec(f"reorder_nn_{name}", srow_ptr=srp.astype(np.int32),
+            scol=get(m, S.get("col_index"), np.int32, nnz), sval=get(m, S.get("val_index"), dt, nnz),
+            sperm=get(m, S.get("permutation_index"), np.int32, N),
+            permutation=get(m, R.get("permutation_index"), np.int32, N),
+            ncol=get(m, R.get("col_index"), np.int32, nnz),
+            nval=get(m, R.get("val_index"), dt, nnz))
 
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT}: {len(out)} arrays, {os.path.getsize(OUT)} bytes")

@@ -113,3 +113,36 @@ def test_matrix_market(vec, oracle, name, lower):
     assert info["nnz"] == int(c["nnz"])
     row, col, val = oracle.mm_coo(info, np.float32, lower=lower)
     assert same(row, c["row"]) and same(col, c["col"]) and same(val, c["val"])
+
+
+@pytest.mark.parametrize("name", ["ragged", "band"])
+def test_row_reordering(vec, oracle, name):
+    """sort_rows_by_nnz, sort_y_rows_by_nnz and calculate_csr_locality_index
+    as the parallel build ships them.  Its new matrix comes from a
+    sparse_CSR_t without `nrows`, so the view it writes row pointers through
+    is empty: the reference leaves them unwritten, the oracle (and the device)
+    write the prefix sums of the row lengths."""
+    c = case(vec, f"sortrows_{name}")
+    assert oracle.csr_locality_index(c["row_ptr"], c["col"]) == float(c["locality"])
+    S = oracle.sort_rows_by_nnz(c["row_ptr"], c["col"], c["val"])
+    assert same(S["permutation"], c["permutation"])
+    # the reference stores the original order's row lengths in the new
+    # matrix's nnz_per_row; the oracle stores the new matrix's own
+    assert same(c["nnz_per_row"], np.diff(c["row_ptr"]).astype(np.int32))
+    assert same(S["nnz_per_row"], c["nnz_per_row"][c["permutation"]])
+    assert same(S["col"], c["ncol"]) and same(S["val"], c["nval"])
+    assert same(S["small_rows"], c["small_rows"])
+    assert not np.any(c["nrow_ptr"])
+    assert same(S["row_ptr"][1:], np.cumsum(S["nnz_per_row"]).astype(np.int32))
+    assert same(oracle.unpermute_rows(c["permutation"], c["y"]), c["y_new"])
+
+
+@pytest.mark.parametrize("name", ["ragged", "band"])
+def test_reorder_nn(vec, oracle, name):
+    """reorder_NN (w = 16) on the row-sorted matrix: the nearest-neighbour
+    walk composed with the sort's permutation, and the reordered columns and
+    values."""
+    c = case(vec, f"reorder_nn_{name}")
+    R = oracle.reorder_nn(c["srow_ptr"], c["scol"], c["sval"], w=16, perm_in=c["sperm"])
+    assert same(R["permutation"], c["permutation"])
+    assert same(R["col"], c["ncol"]) and same(R["val"], c["nval"])
