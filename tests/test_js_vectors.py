@@ -146,3 +146,13 @@ def test_reorder_nn(vec, oracle, name):
     R = oracle.reorder_nn(c["srow_ptr"], c["scol"], c["sval"], w=16, perm_in=c["sperm"])
     assert same(R["permutation"], c["permutation"])
     assert same(R["col"], c["ncol"]) and same(R["val"], c["nval"])
+
+
+@pytest.mark.parametrize("name", ["static_nnz_200_3", "static_nnz_97_5", "static_nnz_6_8"])
+def test_static_nnz_host_partitioner(vec, name):
+    """The library's own host partitioner (row shards across GPUs) gives the
+    reference's ranges, including the row_end it leaves at 0."""
+    from sciwasm.sparse_b200.sparse import static_nnz
+    c = case(vec, name)
+    rs, re = static_nnz(c["row_ptr"], int(c["nw"]))
+    assert same(rs, c["row_start"]) and same(re, c["row_end"])
