@@ -19,7 +19,8 @@ Functions run (paths relative to the reference's project root):
   sparse32.js: read_matrix_MM_files (with read_MM_header and
   calculate_actual_nnz) on the lines load_file produces, then
   create_COO_from_MM or create_LCOO_from_MM
-  src/parallel/src/sparse32.js: static_nnz, CSR_create_level_sets_with_reorder
+  src/parallel/src/sparse32.js: static_nnz, CSR_create_level_sets,
+  CSR_create_level_sets_with_reorder
   (its sswasm_CSR_t constructor is not defined in the shipped sources; it is
   supplied here storing its arguments as row_index, col_index, val_index,
   nnz_row_index, nrows, nnz -- the fields the function reads),
@@ -243,8 +244,28 @@ def main(ref):
         re_ = m.builtins["Int32Array"].construct(float(nw))
         m.call("static_nnz", A, float(nw), rs, re_)
         rec(f"static_nnz_{N}_{nw}", row_ptr=rp, nw=nw, row_start=rs.a.copy(), row_end=re_.a.copy())
+    # a lower factor whose rows 5 and 40 are empty (the level rule puts an
+    # empty row on level 1, since only a row of exactly one entry is level 0)
+    erp, ecol, evl = lower_csr(120, 39, dt)
+    keep = np.ones(ecol.size, bool)
+    for r in (5, 40):
+        keep[erp[r]:erp[r + 1]] = False
+    elens = np.diff(erp)
+    elens[[5, 40]] = 0
+    erp = np.concatenate([[0], np.cumsum(elens)]).astype(np.int32)
+    ecol, evl = ecol[keep], evl[keep]
     for name, (rp, col, val) in (("lower", lower_csr(300, 37, dt)),
-                                 ("narrow", lower_csr(200, 38, dt, band=3))):
+                                 ("narrow", lower_csr(200, 38, dt, band=3)),
+                                 ("empty_rows", (erp, ecol, evl))):
+        m, obj = machine(src, ["CSR_create_level_sets"], "Float32Array")
+        N, nnz = rp.size - 1, col.size
+        A = obj(row_index=put(m, rp), col_index=put(m, col), val_index=put(m, val), nrows=N,
+                nnz=nnz)
+        m.call("CSR_create_level_sets", A)
+        nl = int(A.get("nlevels"))
+        rec(f"levels_plain_{name}", row_ptr=rp, col=col, val=val, nlevels=nl,
+            level_ptr=get(m, A.get("level_index"), np.int32, nl + 1),
+            permutation=get(m, A.get("permutation_index"), np.int32, N))
         m, obj = machine(src, ["CSR_create_level_sets_with_reorder"], "Float32Array")
         N, nnz = rp.size - 1, col.size
         A = obj(row_index=put(m, rp), col_index=put(m, col), val_index=put(m, val), nrows=N,

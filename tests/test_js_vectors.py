@@ -87,8 +87,12 @@ def test_static_nnz(vec, oracle, name):
     assert same(rs, c["row_start"]) and same(re, c["row_end"])
 
 
-@pytest.mark.parametrize("name", ["lower", "narrow"])
+@pytest.mark.parametrize("name", ["lower", "narrow", "empty_rows"])
 def test_level_sets(vec, oracle, name):
+    c = case(vec, f"levels_plain_{name}")
+    L = oracle.level_sets(c["row_ptr"], c["col"], c["val"])
+    assert L["nlevels"] == int(c["nlevels"])
+    assert same(L["level_ptr"], c["level_ptr"]) and same(L["permutation"], c["permutation"])
     c = case(vec, f"levels_{name}")
     L = oracle.level_sets(c["row_ptr"], c["col"], c["val"])
     assert L["nlevels"] == int(c["nlevels"])
