@@ -16,7 +16,7 @@ Functions run (paths relative to the reference's project root):
   src/sequential/src/sparse32.js (Float32Array values) and sparse64.js
   (Float64Array values): coo_csr with its per-row sort, num_cols, csr_ell,
   num_diags, csr_dia (admitted and refused), coo_csc, quick_sort_COO;
-  sparse32.js: read_matrix_MM_files (with read_MM_header and
+  sparse32.js: fletcher_sum_y; read_matrix_MM_files (with read_MM_header and
   calculate_actual_nnz) on the lines load_file produces, then
   create_COO_from_MM or create_LCOO_from_MM
   src/parallel/src/sparse32.js: static_nnz, CSR_create_level_sets,
@@ -196,6 +196,16 @@ def main(ref):
                 arrs["offset"] = get(m, D.get("offset_index"), np.int32, w)
                 arrs["ddata"] = get(m, D.get("data_index"), dt, w * st)
             rec(f"fmt_{cname}_{tag}", **arrs)
+
+    # ---- fletcher_sum_y, the reference benchmark's checksum of y (FP32) ----
+    src = open(os.path.join(ref, "src/sequential/src/sparse32.js")).read()
+    rng = np.random.default_rng(44)
+    for i, y in enumerate((rng.standard_normal(1000).astype(np.float32),
+                           (rng.standard_normal(777) * 1e4).astype(np.float32),
+                           np.array([0.0, -0.0, 254.99, 255.0, -1.5, 3e7], np.float32))):
+        m, obj = machine(src, ["matlab_modulo", "fletcher_sum", "fletcher_sum_y"], "Float32Array")
+        yv = obj(vec_index=put(m, y), vec_nelem=y.size)
+        rec(f"fletcher_{i}", y=y, sum=m.call("fletcher_sum_y", yv))
 
     # ---- Matrix Market input: read_matrix_MM_files on the lines load_file
     # hands over (text up to its last newline, split at newlines), then

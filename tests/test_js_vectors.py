@@ -160,3 +160,13 @@ def test_static_nnz_host_partitioner(vec, name):
     c = case(vec, name)
     rs, re = static_nnz(c["row_ptr"], int(c["nw"]))
     assert same(rs, c["row_start"]) and same(re, c["row_end"])
+
+
+@pytest.mark.parametrize("i", [0, 1, 2])
+def test_fletcher_sum(vec, oracle, i):
+    """fletcher_sum_y, the checksum the reference benchmark prints for y:
+    the oracle's and the library's host restatement give the same integer."""
+    from sciwasm.sparse_b200.sparse import fletcher_sum
+    c = case(vec, f"fletcher_{i}")
+    assert oracle.fletcher(c["y"]) == int(c["sum"])
+    assert fletcher_sum(c["y"]) == int(c["sum"])
