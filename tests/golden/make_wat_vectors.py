@@ -13,7 +13,8 @@ and nothing reads the reference at test time):
 
 Kernels run, by file of the reference (paths relative to its project root):
   src/sequential/src/sparse_opt_32.wat, sparse_opt_64.wat:
-      spmv_coo, spmv_csr, spmv_csr_wrapper (inner_max), spmv_dia, spmv_ell,
+      spmv_coo, spmv_csr, spmv_dia, spmv_ell and their _wrapper forms
+      (inner_max), sum_coo (as shipped),
       count/copy_nonzeros_{coo,csr,dia,ell}, transpose_{csr,dia,ell},
       count_transpose_cols_ell, diagonal_coo, min_coo, spts_csc and the exact
       element-wise maps (abs, neg, sqrt, ceil, floor, trunc, nearest, sign,
@@ -201,6 +202,28 @@ def main(ref):
         pi_, pd, px, py = M.put(ind), M.put(edat), M.put(x), M.put(y0)
         mod.call("spmv_ell", pi_, pd, N, nc, px, py)
         rec(f"spmv_ell_{tag}", indices=ind, data=edat, N=N, nc=nc, x=x, y0=y0, y=M.get(py, dt, N))
+
+        # the inner_max wrappers of the other formats (y += A x, three times)
+        M = Mem(mod)
+        a = [M.put(row), M.put(ccol), M.put(cval), M.put(x), M.put(y0)]
+        mod.call("spmv_coo_wrapper", *a, row.size, 3)
+        rec(f"spmv_coo3_{tag}", row=row, col=ccol, val=cval, N=N, x=x, y0=y0, y=M.get(a[4], dt, N))
+        M = Mem(mod)
+        po, pd, px, py = M.put(off), M.put(dat), M.put(x), M.put(y0)
+        mod.call("spmv_dia_wrapper", po, pd, N, nd, stride, px, py, 3)
+        rec(f"spmv_dia3_{tag}", offset=off, data=dat, N=N, stride=stride, x=x, y0=y0,
+            y=M.get(py, dt, N))
+        M = Mem(mod)
+        pi_, pd, px, py = M.put(ind), M.put(edat), M.put(x), M.put(y0)
+        mod.call("spmv_ell_wrapper", pi_, pd, N, nc, px, py, 3)
+        rec(f"spmv_ell3_{tag}", indices=ind, data=edat, N=N, nc=nc, x=x, y0=y0, y=M.get(py, dt, N))
+
+        # sum_coo (axis 1) as shipped: its row counter also advances per entry
+        srow, scol, sval = coo_of(rp, col, val)
+        M = Mem(mod)
+        a = [M.put(srow), M.put(scol), M.put(sval), M.zeros(N, dt)]
+        mod.call("sum_coo", 1, *a, N, srow.size)
+        rec(f"sum_coo_{tag}", row=srow, col=scol, val=sval, N=N, out=M.get(a[3], dt, N))
 
         # ---- eliminate_zeros and transpose (the FP32 module exports them) --
         if "count_nonzeros_coo" in mod.exports:

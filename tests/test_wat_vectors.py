@@ -60,6 +60,37 @@ def test_spmv(vec, oracle, tag):
                 c["y"])
 
 
+@pytest.mark.parametrize("tag", TAGS)
+def test_spmv_wrappers_inner_max(vec, oracle, tag):
+    """The _wrapper exports repeat y += A x inner_max times."""
+    c = load_case(vec, f"spmv_coo3_{tag}")
+    y = c["y0"]
+    for _ in range(3):
+        y = oracle.spmv_coo(c["row"], c["col"], c["val"], c["x"], y)
+    assert same(y, c["y"])
+    c = load_case(vec, f"spmv_dia3_{tag}")
+    y = c["y0"]
+    for _ in range(3):
+        y = oracle.spmv_dia(c["offset"], c["data"], int(c["N"]), c["x"], y, int(c["stride"]))
+    assert same(y, c["y"])
+    c = load_case(vec, f"spmv_ell3_{tag}")
+    y = c["y0"]
+    for _ in range(3):
+        y = oracle.spmv_ell(c["indices"], c["data"], int(c["N"]), int(c["nc"]), c["x"], y)
+    assert same(y, c["y"])
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_sum_coo_as_shipped_is_not_a_row_sum(vec, oracle, tag):
+    """The shipped sum_coo export advances its row counter for every entry it
+    adds, so its output is not the row sums (no JS method calls it).  The
+    library gives row sums (a deliberate difference); this records what the
+    export does."""
+    c = load_case(vec, f"sum_coo_{tag}")
+    rows = oracle.sum_coo_rows(1, c["row"], c["val"], int(c["N"]))
+    assert not same(rows, c["out"])
+
+
 def test_eliminate_zeros(vec, oracle):
     c = load_case(vec, "nz_coo_f32")
     orow, ocol, oval = oracle.copy_nonzeros_coo(c["row"], c["col"], c["val"])
