@@ -82,6 +82,8 @@ _SIG = {
     "or_unpermute_rows": ([C.c_int, _P, _P, _P, _I32], None),
     "or_csr_locality_index": ([_P, _P, _I32, _I64], C.c_double),
     "or_reorder_nn": ([C.c_int, _P, _P, _P, _I32, C.c_int, _P, _P, _P, _P, _P, _P], None),
+    "or_reorder_nn_ex": ([C.c_int, C.c_int, _P, _P, _P, _I32, C.c_int, _P, _P, _P, _P, _P, _P],
+                         None),
     "or_mm_read": ([_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P], C.c_int),
     "or_mm_coo": ([C.c_int, C.c_int, _I32, _I32, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P],
                   _I64),
@@ -523,16 +525,18 @@ def unpermute_rows(permutation, y):
     return out
 
 
-def reorder_nn(row_ptr, col, val, w=16, perm_in=None):
-    """dict(walk, permutation, row_ptr, col, val) of reorder_NN."""
+def reorder_nn(row_ptr, col, val, w=16, perm_in=None, list_bytes=4):
+    """dict(walk, permutation, row_ptr, col, val) of reorder_NN.  list_bytes:
+    4 = the FP32 build's float32 similarity list (the device's rule), 8 = the
+    FP64 build's double list."""
     row_ptr, col, val = _i32(row_ptr), _i32(col), np.ascontiguousarray(val)
     N = row_ptr.size - 1
     pin = None if perm_in is None else _i32(perm_in)
     walk, perm = np.zeros(N, np.int32), np.zeros(N, np.int32)
     nrp = np.zeros(N + 1, np.int32)
     ncol, nval = np.zeros(col.size, np.int32), np.zeros(col.size, val.dtype)
-    lib().or_reorder_nn(val.dtype.itemsize, _p(row_ptr), _p(col), _p(val), N, int(w), _p(pin),
-                        _p(walk), _p(perm), _p(nrp), _p(ncol), _p(nval))
+    lib().or_reorder_nn_ex(val.dtype.itemsize, int(list_bytes), _p(row_ptr), _p(col), _p(val), N,
+                           int(w), _p(pin), _p(walk), _p(perm), _p(nrp), _p(ncol), _p(nval))
     return dict(walk=walk, permutation=perm, row_ptr=nrp, col=ncol, val=nval)
 
 

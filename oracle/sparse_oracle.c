@@ -1346,27 +1346,32 @@ void or_spts_csc(int w, const int32_t* cp, const int32_t* row, const void* val, 
 /* ======================= nearest-neighbour row reordering ======================= */
 
 /* assign_w_min_elems: src/parallel/src/sparse32.js:2271-2318.  The list
- * holds float32 values (a Float32Array; -1 = empty) compared as doubles with
- * the new candidate's double value.  An equal value goes after the existing
- * ones; a middle insertion into a partly filled list shifts from the last
- * filled slot, which drops that slot's entry (the list does not grow). */
-static void nn_assign(float* jac, int32_t* nidx, int32_t next, double v, int w) {
+ * holds float32 values in the FP32 build (a Float32Array, :2444) and doubles
+ * in the FP64 build (a Float64Array, src/parallel/src/sparse64.js:1593);
+ * jac is kept in doubles here and `r32` rounds each stored value to float32
+ * for the FP32 build.  -1 = empty; values compare as doubles with the new
+ * candidate's double value.  An equal value goes after the existing ones; a
+ * middle insertion into a partly filled list shifts from the last filled
+ * slot, which drops that slot's entry (the list does not grow). */
+static double nn_store(double v, int r32) { return r32 ? (double)(float)v : v; }
+
+static void nn_assign(double* jac, int32_t* nidx, int32_t next, double v, int w, int r32) {
   int i = 0;
-  while (i < w && (double)jac[i] >= 0 && (double)jac[i] >= v) i++;
+  while (i < w && jac[i] >= 0 && jac[i] >= v) i++;
   if (i == w) return;
-  if (jac[i] == -1.0f) {
-    jac[i] = (float)v;
+  if (jac[i] == -1.0) {
+    jac[i] = nn_store(v, r32);
     nidx[i] = next;
     return;
   }
   int j = w - 1;
-  while (jac[j] == -1.0f) j--;
+  while (jac[j] == -1.0) j--;
   while (j != i) {
     jac[j] = jac[j - 1];
     nidx[j] = nidx[j - 1];
     j--;
   }
-  jac[i] = (float)v;
+  jac[i] = nn_store(v, r32);
   nidx[i] = next;
 }
 
@@ -1375,14 +1380,14 @@ static void nn_assign(float* jac, int32_t* nidx, int32_t next, double v, int w) 
  * [start, end) with the highest Jaccard similarity of 16-column cache lines
  * (shared line runs / (its runs + their runs - shared runs)).  Returns the
  * first unvisited row of the row's list (N if none) and its value. */
-static int32_t nn_find_next(int32_t index, int32_t* visited, const int32_t* nlines, float* jac,
+static int32_t nn_find_next(int32_t index, int32_t* visited, const int32_t* nlines, double* jac,
                             int32_t* nidx, int32_t* last_used, const int32_t* row_ptr,
                             const int32_t* col, int32_t N, int w, int32_t start, int32_t end,
-                            double* maxv) {
+                            double* maxv, int r32) {
   if (visited[index] == 3) {
     visited[index] = 1;
     for (int i = 0; i < w; ++i) {
-      jac[i] = -1.0f;
+      jac[i] = -1.0;
       nidx[i] = N;
     }
     for (int32_t j = row_ptr[index]; j < row_ptr[index + 1]; ++j) last_used[col[j] / 16] = index;
@@ -1395,12 +1400,12 @@ static int32_t nn_find_next(int32_t index, int32_t* visited, const int32_t* nlin
         while (j < row_ptr[i + 1] && col[j - 1] / 16 == col[j] / 16) j++;
       }
       const int32_t dissim = nlines[index] + nlines[i] - alines;
-      nn_assign(jac, nidx, i, (double)alines / (double)dissim, w);
+      nn_assign(jac, nidx, i, (double)alines / (double)dissim, w, r32);
     }
   }
   for (int i = 0; i < w; ++i) {
-    if ((double)jac[i] >= 0 && visited[nidx[i]] == 0) {
-      *maxv = (double)jac[i];
+    if (jac[i] >= 0 && visited[nidx[i]] == 0) {
+      *maxv = jac[i];
       return nidx[i];
     }
   }
@@ -1413,12 +1418,13 @@ static int32_t nn_find_next(int32_t index, int32_t* visited, const int32_t* nlin
  * the next row is the best first candidate over the window's lists (a later
  * window slot wins a tie), until no candidate is left. */
 static void nn_subset(const int32_t* row_ptr, const int32_t* col, int32_t N, int32_t start,
-                      int32_t end, const int32_t* nlines, int32_t* visited, int32_t* perm, int w) {
+                      int32_t end, const int32_t* nlines, int32_t* visited, int32_t* perm, int w,
+                      int r32) {
   int32_t* win = (int32_t*)calloc((size_t)w, sizeof(int32_t));
   const int32_t nl = N / 16 + 1;
   int32_t* last_used = (int32_t*)malloc(sizeof(int32_t) * (size_t)nl);
   for (int32_t i = 0; i < nl; ++i) last_used[i] = -1;
-  float* jac = (float*)calloc((size_t)w * w, sizeof(float));
+  double* jac = (double*)calloc((size_t)w * w, sizeof(double));
   int32_t* nidx = (int32_t*)calloc((size_t)w * w, sizeof(int32_t));
   int32_t index = start, pos = start;
   int nnb = 0, count = 0;
@@ -1434,7 +1440,7 @@ static void nn_subset(const int32_t* row_ptr, const int32_t* col, int32_t N, int
       double v = 0.0;
       const int32_t c = nn_find_next(win[i], visited, nlines, jac + (size_t)i * w,
                                      nidx + (size_t)i * w, last_used, row_ptr, col, N, w, start,
-                                     end, &v);
+                                     end, &v, r32);
       if (mx <= v && c != N) {
         mx = v;
         next = c;
@@ -1459,9 +1465,10 @@ static void nn_subset(const int32_t* row_ptr, const int32_t* col, int32_t N, int
  * perm_in (new row i = original row perm_in[walk[i]]; perm_in NULL = the
  * identity).  The reference's new row_ptr view has length nrows + 1 with
  * nrows undefined, so it writes no row pointers; here they are written. */
-void or_reorder_nn(int w_bytes, const int32_t* row_ptr, const int32_t* col, const void* val,
-                   int32_t N, int w, const int32_t* perm_in, int32_t* walk, int32_t* perm_out,
-                   int32_t* new_row, int32_t* new_col, void* new_val) {
+void or_reorder_nn_ex(int w_bytes, int list_bytes, const int32_t* row_ptr, const int32_t* col,
+                      const void* val, int32_t N, int w, const int32_t* perm_in, int32_t* walk,
+                      int32_t* perm_out, int32_t* new_row, int32_t* new_col, void* new_val) {
+  const int r32 = list_bytes == 4;
   int32_t* visited = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
   int32_t* nlines = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
   int32_t* freq = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
@@ -1488,13 +1495,13 @@ void or_reorder_nn(int w_bytes, const int32_t* row_ptr, const int32_t* col, cons
       while (freq[len] >= B) {
         const int32_t end = start + B;
         freq[len] -= B;
-        nn_subset(row_ptr, col, N, start, end, nlines, visited, walk, w);
+        nn_subset(row_ptr, col, N, start, end, nlines, visited, walk, w, r32);
         start = end;
       }
       if (freq[len] > 0) {
         const int32_t end = start + freq[len];
         freq[len] = 0;
-        nn_subset(row_ptr, col, N, start, end, nlines, visited, walk, w);
+        nn_subset(row_ptr, col, N, start, end, nlines, visited, walk, w, r32);
         start = end;
       }
     }
@@ -1513,4 +1520,13 @@ void or_reorder_nn(int w_bytes, const int32_t* row_ptr, const int32_t* col, cons
   free(visited);
   free(nlines);
   free(freq);
+}
+
+/* The FP32 build's list (float32 values) whatever the value width: the rule
+ * the device follows for both precisions. */
+void or_reorder_nn(int w_bytes, const int32_t* row_ptr, const int32_t* col, const void* val,
+                   int32_t N, int w, const int32_t* perm_in, int32_t* walk, int32_t* perm_out,
+                   int32_t* new_row, int32_t* new_col, void* new_val) {
+  or_reorder_nn_ex(w_bytes, 4, row_ptr, col, val, N, w, perm_in, walk, perm_out, new_row, new_col,
+                   new_val);
 }

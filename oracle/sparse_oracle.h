@@ -266,6 +266,13 @@ double or_csr_locality_index(const int32_t* row_ptr, const int32_t* col, int32_t
 void or_reorder_nn(int val_bytes, const int32_t* row_ptr, const int32_t* col, const void* val,
                    int32_t N, int w, const int32_t* perm_in, int32_t* walk, int32_t* perm_out,
                    int32_t* new_row, int32_t* new_col, void* new_val);
+/* The same with the similarity list's element width chosen: list_bytes 4 is
+ * the FP32 build's Float32Array (src/parallel/src/sparse32.js:2444, what
+ * or_reorder_nn and the device use), 8 the FP64 build's Float64Array
+ * (src/parallel/src/sparse64.js:1593). */
+void or_reorder_nn_ex(int val_bytes, int list_bytes, const int32_t* row_ptr, const int32_t* col,
+                      const void* val, int32_t N, int w, const int32_t* perm_in, int32_t* walk,
+                      int32_t* perm_out, int32_t* new_row, int32_t* new_col, void* new_val);
 
 /* ---------------- Matrix Market input ---------------- */
 /* read_MM_header / calculate_actual_nnz / read_matrix_MM_files:

@@ -298,9 +298,15 @@ def main(ref):
     # row pointers (recorded here as what the memory held: zeros).
     reo = ["sort_rows_by_nnz", "sort_y_rows_by_nnz", "calculate_csr_locality_index",
            "reorder_subset", "find_next_row", "assign_w_min_elems", "reorder_NN"]
-    for name, (rp, col, val) in (("ragged", ragged_csr(300, 41, dt)),
-                                 ("band", banded_csr(200, (-9, -3, 0, 1, 17), 42, dt))):
-        m, obj = machine(src, reo, "Float32Array")
+    reo_jobs = []
+    for tag, fname, dtr, kind in (("", "sparse32.js", np.float32, "Float32Array"),
+                                  ("_f64", "sparse64.js", np.float64, "Float64Array")):
+        srcr = open(os.path.join(ref, "src/parallel/src", fname)).read()
+        reo_jobs += [(f"ragged{tag}", srcr, kind, ragged_csr(300, 41, dtr)),
+                     (f"band{tag}", srcr, kind, banded_csr(200, (-9, -3, 0, 1, 17), 42, dtr))]
+    for name, src_r, kind, (rp, col, val) in reo_jobs:
+        dt = val.dtype.type
+        m, obj = machine(src_r, reo, kind)
 
         class CSRCtor:
             def construct(self, row_index, col_index, val_index, nnz_row_index, N, nnz, obj=obj):

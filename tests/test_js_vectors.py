@@ -119,7 +119,7 @@ def test_matrix_market(vec, oracle, name, lower):
     assert same(row, c["row"]) and same(col, c["col"]) and same(val, c["val"])
 
 
-@pytest.mark.parametrize("name", ["ragged", "band"])
+@pytest.mark.parametrize("name", ["ragged", "band", "ragged_f64", "band_f64"])
 def test_row_reordering(vec, oracle, name):
     """sort_rows_by_nnz, sort_y_rows_by_nnz and calculate_csr_locality_index
     as the parallel build ships them.  Its new matrix comes from a
@@ -141,15 +141,28 @@ def test_row_reordering(vec, oracle, name):
     assert same(oracle.unpermute_rows(c["permutation"], c["y"]), c["y_new"])
 
 
-@pytest.mark.parametrize("name", ["ragged", "band"])
+@pytest.mark.parametrize("name", ["ragged", "band", "ragged_f64", "band_f64"])
 def test_reorder_nn(vec, oracle, name):
     """reorder_NN (w = 16) on the row-sorted matrix: the nearest-neighbour
     walk composed with the sort's permutation, and the reordered columns and
     values."""
     c = case(vec, f"reorder_nn_{name}")
-    R = oracle.reorder_nn(c["srow_ptr"], c["scol"], c["sval"], w=16, perm_in=c["sperm"])
+    # the FP32 build keeps the similarity list in a Float32Array, the FP64
+    # build (sparse64.js) in a Float64Array
+    lb = 8 if name.endswith("_f64") else 4
+    R = oracle.reorder_nn(c["srow_ptr"], c["scol"], c["sval"], w=16, perm_in=c["sperm"],
+                          list_bytes=lb)
     assert same(R["permutation"], c["permutation"])
     assert same(R["col"], c["ncol"]) and same(R["val"], c["nval"])
+
+
+def test_reorder_nn_list_precision_matters(vec, oracle):
+    """On this matrix the FP64 build's double list walks differently from the
+    float32 list that the FP32 build, the oracle's default and the device use
+    for both precisions (a known difference for FP64 matrices)."""
+    c = case(vec, "reorder_nn_ragged_f64")
+    R = oracle.reorder_nn(c["srow_ptr"], c["scol"], c["sval"], w=16, perm_in=c["sperm"])
+    assert not same(R["permutation"], c["permutation"])
 
 
 @pytest.mark.parametrize("name", ["static_nnz_200_3", "static_nnz_97_5", "static_nnz_6_8"])
