@@ -20,7 +20,7 @@ Functions run (paths relative to the reference's project root):
   calculate_actual_nnz) on the lines load_file produces, then
   create_COO_from_MM or create_LCOO_from_MM
   src/parallel/src/sparse32.js: static_nnz, CSR_create_level_sets,
-  CSR_create_level_sets_with_reorder
+  CSR_create_level_sets_with_reorder (and its copy in spts32.js)
   (its sswasm_CSR_t constructor is not defined in the shipped sources; it is
   supplied here storing its arguments as row_index, col_index, val_index,
   nnz_row_index, nrows, nnz -- the fields the function reads),
@@ -254,6 +254,7 @@ def main(ref):
         re_ = m.builtins["Int32Array"].construct(float(nw))
         m.call("static_nnz", A, float(nw), rs, re_)
         rec(f"static_nnz_{N}_{nw}", row_ptr=rp, nw=nw, row_start=rs.a.copy(), row_end=re_.a.copy())
+    spts_src = open(os.path.join(ref, "src/parallel/src/spts32.js")).read()
     # a lower factor whose rows 5 and 40 are empty (the level rule puts an
     # empty row on level 1, since only a row of exactly one entry is level 0)
     erp, ecol, evl = lower_csr(120, 39, dt)
@@ -276,6 +277,20 @@ def main(ref):
         rec(f"levels_plain_{name}", row_ptr=rp, col=col, val=val, nlevels=nl,
             level_ptr=get(m, A.get("level_index"), np.int32, nl + 1),
             permutation=get(m, A.get("permutation_index"), np.int32, N))
+        # the same function as the SpTS module (src/parallel/src/spts32.js)
+        # ships it, which the SpTS benchmark calls
+        m, obj = machine(spts_src, ["CSR_create_level_sets_with_reorder"], "Float32Array")
+        N, nnz = rp.size - 1, col.size
+        A = obj(row_index=put(m, rp), col_index=put(m, col), val_index=put(m, val), nrows=N,
+                nnz=nnz)
+        L = m.call("CSR_create_level_sets_with_reorder", A)
+        nl = int(L.get("nlevels"))
+        rec(f"levels_spts_{name}", row_ptr=rp, col=col, val=val, nlevels=nl,
+            level_ptr=get(m, L.get("level_index"), np.int32, nl + 1),
+            permutation=get(m, L.get("permutation_index"), np.int32, N),
+            nrow_ptr=get(m, L.get("row_index"), np.int32, N + 1),
+            ncol=get(m, L.get("col_index"), np.int32, nnz),
+            nval=get(m, L.get("val_index"), dt, nnz))
         m, obj = machine(src, ["CSR_create_level_sets_with_reorder"], "Float32Array")
         N, nnz = rp.size - 1, col.size
         A = obj(row_index=put(m, rp), col_index=put(m, col), val_index=put(m, val), nrows=N,

@@ -93,6 +93,14 @@ def test_level_sets(vec, oracle, name):
     L = oracle.level_sets(c["row_ptr"], c["col"], c["val"])
     assert L["nlevels"] == int(c["nlevels"])
     assert same(L["level_ptr"], c["level_ptr"]) and same(L["permutation"], c["permutation"])
+    for kind in ("levels", "levels_spts"):     # sparse32.js's and spts32.js's copies
+        c = case(vec, f"{kind}_{name}")
+        L = oracle.level_sets(c["row_ptr"], c["col"], c["val"])
+        assert L["nlevels"] == int(c["nlevels"])
+        assert same(L["level_ptr"], c["level_ptr"])
+        assert same(L["permutation"], c["permutation"])
+        assert same(L["row_ptr"], c["nrow_ptr"]) and same(L["col"], c["ncol"])
+        assert same(L["val"], c["nval"])
     c = case(vec, f"levels_{name}")
     L = oracle.level_sets(c["row_ptr"], c["col"], c["val"])
     assert L["nlevels"] == int(c["nlevels"])
