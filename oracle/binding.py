@@ -41,6 +41,10 @@ _SIG = {
     "or_par_spmv_dia_f64": ([C.c_int, _P, _P, _I32, _I32, _I32, _P, _P], None),
     "or_par_spmv_ell_f32": ([C.c_int, _P, _P, _I32, _I32, _P, _P], None),
     "or_par_spmv_ell_f64": ([C.c_int, _P, _P, _I32, _I32, _P, _P], None),
+    "or_par_spmv_dia_rows_f32": ([C.c_int, _P, _P, _I32, _I32, _P, _P], None),
+    "or_par_spmv_dia_rows_f64": ([C.c_int, _P, _P, _I32, _I32, _P, _P], None),
+    "or_par_spmv_ell_rows_f32": ([C.c_int, _P, _P, _I32, _I32, _P, _P], None),
+    "or_par_spmv_ell_rows_f64": ([C.c_int, _P, _P, _I32, _I32, _P, _P], None),
     "or_coo_csr": ([C.c_int, _P, _P, _P, _I32, _I64, _P, _P, _P], None),
     "or_coo_csc": ([C.c_int, _P, _P, _P, _I32, _I64, _P, _P, _P], None),
     "or_num_cols": ([_P, _I32], _I32),
@@ -202,6 +206,19 @@ def par_spmv_dia(nthreads, offset, data, N, x, y):
 def par_spmv_ell(nthreads, indices, data, N, nc, x, y):
     getattr(lib(), "or_par_spmv_ell_" + _sfx(data.dtype))(
         nthreads, _p(indices), _p(data), N, nc, _p(x), _p(y))
+
+
+def par_spmv_dia_rows(nthreads, offset, data_rows, N, x, y):
+    """Parallel CPU baseline over row-by-row DIA data (data_rows[i*nd + d]);
+    updates y in place."""
+    getattr(lib(), "or_par_spmv_dia_rows_" + _sfx(data_rows.dtype))(
+        nthreads, _p(offset), _p(data_rows), N, offset.size, _p(x), _p(y))
+
+
+def par_spmv_ell_rows(nthreads, ind_rows, data_rows, N, nc, x, y):
+    """Parallel CPU baseline over row-by-row ELL slots; updates y in place."""
+    getattr(lib(), "or_par_spmv_ell_rows_" + _sfx(data_rows.dtype))(
+        nthreads, _p(ind_rows), _p(data_rows), N, nc, _p(x), _p(y))
 
 
 # ------------------------------------------------------------------ conversions

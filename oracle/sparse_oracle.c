@@ -320,6 +320,79 @@ DEF_PAR_DIA(double, f64)
 DEF_PAR_ELL(float, f32)
 DEF_PAR_ELL(double, f64)
 
+/* Row-split row-layout DIA and ELL: the "dia_row" and "ell_row" worker
+ * kernels (src/parallel/tests/main32.js:688-694 and the ELL dispatch beside
+ * it; src/parallel/src/sparse_opt_32.wat:8213-8269 spmv_dia and :8292-8347
+ * spmv_ell), over the parallel build's row-by-row data (data[i*nd + d],
+ * src/parallel/src/sparse32.js csr_dia / csr_ell).  Per row: t = y_i; for
+ * each slot in order, t = v*x + t (DIA: only while the column is in range;
+ * ELL: until a negative index); y_i = t.  The same per-row order as the
+ * column-layout kernels above. */
+#define DEF_PAR_ROWS(T, SFX)                                                        \
+  static void par_dia_rows_##SFX(par_job* j, int id) {                              \
+    int nt = j->nt;                                                                 \
+    const int32_t* offset = (const int32_t*)j->a[0];                                \
+    const T* data = (const T*)j->a[1];                                              \
+    const T* x = (const T*)j->a[3];                                                 \
+    T* y = (T*)j->m[0];                                                             \
+    int32_t N = (int32_t)j->n[0], nd = (int32_t)j->n[1];                            \
+    int32_t npw = N / nt, remN = N - npw * nt;                                      \
+    int32_t s = id * npw, e = (id + 1) * npw + (id == nt - 1 ? remN : 0);           \
+    for (int32_t i = s; i < e; ++i) {                                               \
+      const T* row = data + (int64_t)i * nd;                                        \
+      T t = y[i];                                                                   \
+      for (int32_t d = 0; d < nd; ++d) {                                            \
+        const int32_t c = i + offset[d];                                            \
+        if (c >= 0 && c < N) {                                                      \
+          T p = row[d] * x[c];                                                      \
+          t = p + t;                                                                \
+        }                                                                           \
+      }                                                                             \
+      y[i] = t;                                                                     \
+    }                                                                               \
+  }                                                                                 \
+  void or_par_spmv_dia_rows_##SFX(int nthreads, const int32_t* offset, const T* data, \
+                                  int32_t N, int32_t nd, const T* x, T* y) {        \
+    par_job job;                                                                    \
+    job.nt = clamp_threads(nthreads);                                               \
+    job.fn = par_dia_rows_##SFX;                                                    \
+    job.a[0] = offset; job.a[1] = data; job.a[3] = x; job.m[0] = y;                 \
+    job.n[0] = N; job.n[1] = nd;                                                    \
+    par_run(&job);                                                                  \
+  }                                                                                 \
+  static void par_ell_rows_##SFX(par_job* j, int id) {                              \
+    int nt = j->nt;                                                                 \
+    const int32_t* indices = (const int32_t*)j->a[0];                               \
+    const T* data = (const T*)j->a[1];                                              \
+    const T* x = (const T*)j->a[3];                                                 \
+    T* y = (T*)j->m[0];                                                             \
+    int32_t N = (int32_t)j->n[0], nc = (int32_t)j->n[1];                            \
+    int32_t npw = N / nt, remN = N - npw * nt;                                      \
+    int32_t s = id * npw, e = (id + 1) * npw + (id == nt - 1 ? remN : 0);           \
+    for (int32_t i = s; i < e; ++i) {                                               \
+      const int64_t base = (int64_t)i * nc;                                         \
+      T t = y[i];                                                                   \
+      for (int32_t k = 0; k < nc; ++k) {                                            \
+        const int32_t c = indices[base + k];                                        \
+        if (c < 0) break;                                                           \
+        T p = data[base + k] * x[c];                                                \
+        t = p + t;                                                                  \
+      }                                                                             \
+      y[i] = t;                                                                     \
+    }                                                                               \
+  }                                                                                 \
+  void or_par_spmv_ell_rows_##SFX(int nthreads, const int32_t* indices, const T* data, \
+                                  int32_t N, int32_t nc, const T* x, T* y) {        \
+    par_job job;                                                                    \
+    job.nt = clamp_threads(nthreads);                                               \
+    job.fn = par_ell_rows_##SFX;                                                    \
+    job.a[0] = indices; job.a[1] = data; job.a[3] = x; job.m[0] = y;                \
+    job.n[0] = N; job.n[1] = nc;                                                    \
+    par_run(&job);                                                                  \
+  }
+DEF_PAR_ROWS(float, f32)
+DEF_PAR_ROWS(double, f64)
+
 /* ======================= conversions ======================= */
 
 static void swap_bytes(void* a, int64_t i, int64_t j, int w) {

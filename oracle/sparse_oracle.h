@@ -92,6 +92,17 @@ void or_par_spmv_ell_f64(int nthreads, const int32_t* indices, const double* dat
                          int32_t N, int32_t nc, const double* x, double* y);
 void or_par_spmv_ell_f32(int nthreads, const int32_t* indices, const float* data,
                          int32_t N, int32_t nc, const float* x, float* y);
+/* The same over the parallel build's row-by-row layout (data[i*nd + d],
+ * indices[i*nc + k]): the "dia_row" / "ell_row" worker kernels
+ * (src/parallel/src/sparse_opt_32.wat:8213-8269, :8292-8347). */
+void or_par_spmv_dia_rows_f32(int nthreads, const int32_t* offset, const float* data, int32_t N,
+                              int32_t nd, const float* x, float* y);
+void or_par_spmv_dia_rows_f64(int nthreads, const int32_t* offset, const double* data, int32_t N,
+                              int32_t nd, const double* x, double* y);
+void or_par_spmv_ell_rows_f32(int nthreads, const int32_t* indices, const float* data, int32_t N,
+                              int32_t nc, const float* x, float* y);
+void or_par_spmv_ell_rows_f64(int nthreads, const int32_t* indices, const double* data, int32_t N,
+                              int32_t nc, const double* x, double* y);
 
 /* ---------------- conversions ---------------- */
 /* coo_csr: src/sequential/src/sparse32.js:1674-1720 with the per-row stable

@@ -216,3 +216,16 @@ def test_parallel_worker_kernels(vec, oracle):
         y = c["y0"].copy()
         oracle.par_spmv_ell(nw, c["indices"], c["data"], int(c["N"]), int(c["nc"]), c["x"], y)
         assert same(y, c["y"]), case
+    # the row-layout kernels restated over row-by-row data (the vectors keep
+    # the column layout; the reference's row kernels ran on its transpose)
+    c = load_case(vec, "par_dia")
+    N, nd = int(c["N"]), c["offset"].size
+    y = c["y0"].copy()
+    oracle.par_spmv_dia_rows(nw, c["offset"], c["data"].reshape(nd, N).T.copy(), N, c["x"], y)
+    assert same(y, c["y"])
+    c = load_case(vec, "par_ell")
+    N, nc = int(c["N"]), int(c["nc"])
+    y = c["y0"].copy()
+    oracle.par_spmv_ell_rows(nw, c["indices"].reshape(nc, N).T.copy(),
+                             c["data"].reshape(nc, N).T.copy(), N, nc, c["x"], y)
+    assert same(y, c["y"])
