@@ -24,7 +24,8 @@ Kernels run, by file of the reference (paths relative to its project root):
       worker SpMV kernels spmv_csr/coo/dia/ell_wrapper, sum,
       spmv_dia_col_basic_wrapper and spmv_ell_col_wrapper (three workers run
       in turn)
-  src/parallel/src/spts_opt_32.wat:   spts_csr_sync_free_wrapper (one worker)
+  src/parallel/src/spts_opt_32.wat:   spts_csr_sync_free_wrapper and
+      spts_csr_level_sync_free_wrapper (one worker)
 The transcendental maps call imported JavaScript Math functions, which are
 not part of the reference, so they are not pinned here.
 """
@@ -409,6 +410,19 @@ def main(ref):
         par.call("metadata", 0, lp, nl, 1, Nl, rli, rwi)
         par.call("spts_csr_opt_level_sync_free_wrapper", 0, lp, *a, perm, nl, bar, gfl, glevel,
                  grows, alevel, rli, rwi, wlev, 1, Nl, 1)
+        # the SpTS module's own level/sync-free hybrid (spts_opt_32.wat
+        # spts_csr_level_sync_free_wrapper, one worker): the sync-free row
+        # arithmetic on the level-ordered matrix
+        M2 = Mem(spts)
+        lp2 = M2.put(L["level_ptr"].astype(np.int32))
+        a2 = [M2.put(L["row_ptr"]), M2.put(L["col"]), M2.put(L["val"]), M2.put(bp),
+              M2.zeros(Nl, dt)]
+        perm2 = M2.put(L["permutation"])
+        bar2, gfl2, fl2 = M2.zeros(1, np.int32), M2.zeros(1, np.int32), M2.zeros(Nl, np.int32)
+        spts.call("spts_csr_level_sync_free_wrapper", 0, lp2, *a2, perm2, nl, bar2, gfl2, fl2, 1,
+                  Nl, 1)
+        rec(f"spts_lsf_{name}", lrow_ptr=L["row_ptr"], lcol=L["col"], lval=L["val"], b=bp,
+            y=M2.get(a2[4], dt, Nl))
         rec(f"spts_hybrid_{name}", lrow_ptr=L["row_ptr"], lcol=L["col"], lval=L["val"],
             permutation=L["permutation"], row_ptr=lrp, col=lcol, val=lval, b=bp,
             y=M.get(a[4], dt, Nl))

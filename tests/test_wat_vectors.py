@@ -186,6 +186,12 @@ def test_spts(vec, oracle, name):
     # each row as the level-set row kernel does
     c = load_case(vec, f"spts_hybrid_{name}")
     assert same(oracle.spts_csr(c["lrow_ptr"], c["lcol"], c["lval"], c["b"]), c["y"])
+    # the SpTS module's own hybrid uses the sync-free row arithmetic instead
+    # (subtract as you go): the reference ships both; the device's "hybrid"
+    # is the first, its "syncfree" computes the second's values
+    c = load_case(vec, f"spts_lsf_{name}")
+    assert same(oracle.spts_syncfree(c["lrow_ptr"], c["lcol"], c["lval"], c["b"]), c["y"])
+    assert not same(oracle.spts_csr(c["lrow_ptr"], c["lcol"], c["lval"], c["b"]), c["y"])
 
 
 def test_parallel_worker_kernels(vec, oracle):
