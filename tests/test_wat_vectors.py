@@ -192,6 +192,13 @@ def test_spts(vec, oracle, name):
     c = load_case(vec, f"spts_lsf_{name}")
     assert same(oracle.spts_syncfree(c["lrow_ptr"], c["lcol"], c["lval"], c["b"]), c["y"])
     assert not same(oracle.spts_csr(c["lrow_ptr"], c["lcol"], c["lval"], c["b"]), c["y"])
+    # ... and the natural-order sync-free solve, permuted, gives the same bits
+    lv = load_case(vec, f"spts_level_{name}")
+    perm = lv["permutation"]
+    b = np.empty_like(c["b"])
+    b[perm] = c["b"]
+    y = oracle.spts_syncfree(lv["row_ptr"], lv["col"], lv["val"], b)
+    assert same(y[perm], c["y"])
 
 
 def test_parallel_worker_kernels(vec, oracle):
