@@ -58,6 +58,26 @@ MOD = r"""
     (f64.load (local.get $p)))
   (func (export "spin") (param $p i32)
     (loop $w (br_if $w (i32.eqz (i32.load (local.get $p))))))
+  (func (export "two") (result i32 i32)
+    (i32.const 4) (i32.const 9))
+  (func (export "sum2") (result i32)
+    (call $two_internal) (i32.add))
+  (func $two_internal (result i32 i32) (i32.const 40) (i32.const 2))
+  (func (export "divrem") (param $a i32) (param $b i32) (result i32 i32)
+    (i32.div_s (local.get $a) (local.get $b)) (i32.rem_s (local.get $a) (local.get $b)))
+  (func (export "nearest") (param $a f64) (result f64) (f64.nearest (local.get $a)))
+  (func (export "nearest32") (param $a f32) (result f32) (f32.nearest (local.get $a)))
+  (func (export "pick") (param $c i32) (result i32)
+    (select (i32.const 11) (i32.const 22) (local.get $c)))
+  (func (export "copy") (param $d i32) (param $s i32) (param $n i32)
+    (memory.copy (local.get $d) (local.get $s) (local.get $n)))
+  (func (export "early") (param $a i32) (result i32)
+    (block $out (result i32)
+      (loop $l
+        (br_if $out (i32.const 5) (i32.gt_s (local.get $a) (i32.const 3)))
+        (local.set $a (i32.add (local.get $a) (i32.const 1)))
+        (br $l))
+      (i32.const 0)))
 )
 """
 
@@ -97,3 +117,27 @@ def test_wait_that_cannot_end_is_an_error(m):
     m.write(256, np.zeros(1, np.int32))
     with pytest.raises(RuntimeError, match="instruction limit"):
         m.call("spin", 256)
+
+
+def test_multi_value_and_calls(m):
+    assert m.call("two") == [4, 9]
+    assert m.call("sum2") == [42]
+
+
+def test_signed_division_truncates(m):
+    q, r = m.call("divrem", -7, 2)
+    assert (q, r) == ((-3) & 0xFFFFFFFF, (-1) & 0xFFFFFFFF)
+
+
+def test_nearest_ties_to_even(m):
+    assert [m.call("nearest", v)[0] for v in (0.5, 1.5, 2.5, -0.5, -2.5)] == [0.0, 2.0, 2.0, -0.0, -2.0]
+    assert np.signbit(m.call("nearest", -0.5)[0])
+    assert [float(m.call("nearest32", v)[0]) for v in (0.5, 1.5, 2.5)] == [0.0, 2.0, 2.0]
+
+
+def test_select_copy_and_branch_values(m):
+    assert m.call("pick", 1) == [11] and m.call("pick", 0) == [22]
+    m.write(512, np.arange(8, dtype=np.uint8))
+    m.call("copy", 600, 512, 8)
+    assert bytes(m.mem[600:608]) == bytes(range(8))
+    assert m.call("early", 0) == [5]
